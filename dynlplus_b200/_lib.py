@@ -1,0 +1,79 @@
+"""ctypes binding of libdlp.so (the C ABI declared in include/dlp.h).
+
+The library is the only compute path: if it is missing, every call raises. There is no CPU
+fallback. `python -m dynlplus_b200.build` (or `__graft_entry__.build()`) creates it in-tree.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdlp.so")
+
+DLP_F32, DLP_F64, DLP_BF16 = 0, 1, 2
+STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported precision combination", 3: "CUDA runtime error",
+          4: "iteration cap reached", 5: "cancelled", 6: "workspace too small", 7: "row capacity exceeded",
+          8: "device-side check failed"}
+
+_P, _I, _Q, _D, _Z = ct.c_void_p, ct.c_int32, ct.c_int64, ct.c_double, ct.c_size_t
+_CODES = {"p": _P, "i": _I, "q": _Q, "d": _D, "z": _Z}
+
+# name -> (argument codes, return type). Kept in the order of include/dlp.h.
+SIGNATURES: dict[str, tuple[str, object]] = {
+    "dlp_version": ("", ct.c_int),
+    "dlp_status_string": ("i", ct.c_char_p),
+    "dlp_last_cuda_error": ("", ct.c_int),
+    "dlp_sm_count": ("", ct.c_int),
+    "dlp_spmm": ("ppppiipipqipddpqdpqiiidp", ct.c_int),
+    "dlp_frontier_jacobi": ("ppppipiipqpqpdpqipppidp", ct.c_int),
+    "dlp_push_scatter": ("ppppipiipqpqipidp", ct.c_int),
+    "dlp_mark_neighbors": ("ppppipp", ct.c_int),
+    "dlp_push_take": ("piipqpqppqipp", ct.c_int),
+    "dlp_violating": ("piipqpipppp", ct.c_int),
+    "dlp_compact_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_compact": ("ppipppzp", ct.c_int),
+    "dlp_colreduce_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_colreduce": ("iiipqpqpipppzp", ct.c_int),
+    "dlp_cc_edges": ("ippqppp", ct.c_int),
+    "dlp_cc_graph": ("ippppippppp", ct.c_int),
+    "dlp_cc_relabel": ("ippppzp", ct.c_int),
+}
+
+_lib = None
+
+
+class DLPError(RuntimeError):
+    """A libdlp entry point returned a non-zero status."""
+
+    def __init__(self, name: str, status: int, cuda: int = 0):
+        msg = f"{name} failed: {STATUS.get(status, status)} (status {status}"
+        msg += f", cudaError {cuda})" if status == 3 else ")"
+        super().__init__(msg)
+        self.status = status
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libdlp.so is missing at {LIB_PATH}: build it with `python -m dynlplus_b200.build`")
+        L = ct.CDLL(LIB_PATH)
+        for name, (codes, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = [_CODES[c] for c in codes]
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def call(name: str, *args) -> None:
+    """Call an int-returning entry point and raise DLPError on a non-zero status."""
+    st = getattr(lib(), name)(*args)
+    if st != 0:
+        raise DLPError(name, st, lib().dlp_last_cuda_error() if st == 3 else 0)
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)

@@ -1,0 +1,61 @@
+"""Connected components on the device (dynlp/cc.py:8-23).
+
+`connected_components(n, rows, cols)` returns (int32 labels in [0, n_comp), n_comp) with the
+reference's canonical numbering: components ranked by their smallest vertex id (the reference's
+`unique(..., return_inverse=True)` relabel, cc.py:22). The kernel is a lock-free union-find
+(hook larger root under smaller, path halving) rather than the reference's host-synchronised
+hook/jump rounds; the labels are identical bit for bit.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+from .backend import code, ptr, stream, workspace
+
+
+def min_vertex_roots(n, rows, cols) -> torch.Tensor:
+    """parent[v] = smallest vertex id in v's component (int32, device)."""
+    rows = rows.to(torch.int32).contiguous()
+    cols = cols.to(torch.int32).contiguous()
+    dev = rows.device
+    parent = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call("dlp_cc_edges", int(n), ptr(rows), ptr(cols), int(rows.numel()), ptr(parent), ptr(err), stream())
+    if int(err.item()):
+        raise ValueError("connected_components: edge endpoint outside [0, n)")
+    return parent[:n]
+
+
+def relabel(parent: torch.Tensor, sync: bool = True):
+    """Rank of each root among the roots (unique + inverse); returns (labels, n_comp)."""
+    n = int(parent.numel())
+    label = torch.empty(max(n, 1), dtype=torch.int32, device=parent.device)
+    nc = torch.empty(1, dtype=torch.int32, device=parent.device)
+    ws = workspace("compact").get(_lib.lib().dlp_compact_workspace_bytes(n))
+    _lib.call("dlp_cc_relabel", n, ptr(parent), ptr(label), ptr(nc), ptr(ws), ws.numel(), stream())
+    return (label[:n], int(nc.item())) if sync else (label[:n], nc)
+
+
+def connected_components(n, rows, cols):
+    """(labels in [0, n_comp), n_comp) for an undirected edge list (dynlp/cc.py:8-23)."""
+    if n == 0:
+        dev = rows.device if torch.is_tensor(rows) else None
+        return torch.zeros(0, dtype=torch.int32, device=dev), 0
+    return relabel(min_vertex_roots(n, rows, cols))
+
+
+def graph_components(G, vmask=None, sink=None, w=None):
+    """Min-vertex-id roots over the stored entries of a row-range graph with a sink vertex n.
+
+    Entry (u, v) joins u and v when vmask[u] and vmask[v] (and w != 0 when w is given); it joins
+    u and the sink when vmask[u] and sink[v]. Returns parent of length n + 1 (device int32).
+    This is the grounding check of dynlp/stream.py:150-159 and :275-280 in one launch.
+    """
+    n = G.shape[0]
+    dev = G.indices.device
+    parent = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call("dlp_cc_graph", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(w),
+              code(w) if w is not None else 0, ptr(vmask), ptr(sink), ptr(parent), ptr(err), stream())
+    return parent, err

@@ -1,0 +1,187 @@
+// Connected components (dynlp/cc.py:8-23) as a lock-free union-find: every edge hooks the larger
+// of its two roots under the smaller one with atomicCAS, finds use path halving, and a final pass
+// compresses every vertex to its root. Because a root is only ever hooked under a smaller id, the
+// root of each component is its minimum vertex id, whatever the schedule: the result is the
+// reference's canonical labelling before its rank relabel (cc.py:22), bit-exact.
+#include "common.cuh"
+
+namespace dlp {
+
+int compact_roots(const int32_t *parent, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
+                  cudaStream_t s);
+size_t compact_ws_bytes(int32_t n);
+
+constexpr int kCcThreads = 256;
+constexpr int kMaxSteps = 1 << 26;  // bound on any chase / retry loop (far above any path length)
+
+__global__ void k_cc_init(int32_t *parent, int32_t n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) parent[i] = (int32_t)i;
+}
+
+// Root of x with path halving. parent[] only ever decreases, so stale reads are safe.
+__device__ __forceinline__ int32_t find_root(volatile int32_t *parent, int32_t x, int32_t *err) {
+  int32_t cur = parent[x];
+  if (cur == x) return x;
+  int32_t prev = x;
+  int steps = 0;
+  int32_t next;
+  while (cur > (next = parent[cur])) {
+    parent[prev] = next;
+    prev = cur;
+    cur = next;
+    if (++steps > kMaxSteps) {
+      if (err) atomicExch(err, DLP_ERR_DEVICE);
+      break;
+    }
+  }
+  return cur;
+}
+
+__device__ __forceinline__ void unite(int32_t *parent_, int32_t a, int32_t b, int32_t *err) {
+  volatile int32_t *parent = parent_;
+  int32_t ra = find_root(parent, a, err), rb = find_root(parent, b, err);
+  int steps = 0;
+  while (ra != rb) {
+    if (ra < rb) {
+      const int32_t t = ra;
+      ra = rb;
+      rb = t;
+    }
+    // hook ra (larger) under rb (smaller)
+    const int32_t ret = atomicCAS(parent_ + ra, ra, rb);
+    if (ret == ra) break;
+    ra = ret;  // ra was hooked meanwhile: climb from its new parent
+    if (++steps > kMaxSteps) {
+      if (err) atomicExch(err, DLP_ERR_DEVICE);
+      break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kCcThreads)
+    k_cc_edges(int32_t n, const int32_t *__restrict__ rows, const int32_t *__restrict__ cols, int64_t m,
+               int32_t *parent, int32_t *err) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int32_t a = rows[i], b = cols[i];
+    if ((unsigned)a >= (unsigned)n || (unsigned)b >= (unsigned)n) {
+      if (err) atomicExch(err, DLP_ERR_DEVICE);
+      continue;
+    }
+    if (a != b) unite(parent, a, b, err);
+  }
+}
+
+// 8 lanes per row over the row ranges; sink vertex id = n.
+template <typename TW>
+__global__ void __launch_bounds__(kCcThreads)
+    k_cc_graph(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+               const int32_t *__restrict__ col, const TW *__restrict__ w, const uint8_t *__restrict__ vmask,
+               const uint8_t *__restrict__ sink, int32_t *parent, int32_t *err) {
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = t0; t < (long long)n * 8; t += stride) {
+    const int32_t u = (int32_t)(t >> 3);
+    const int l = (int)(t & 7);
+    if (vmask && !vmask[u]) continue;
+    const int beg = rbeg[u], end = rend[u];
+    for (int j = beg + l; j < end; j += 8) {
+      if (w && cvt<float>(w[j]) == 0.0f) continue;
+      const int32_t v = col[j];
+      if ((unsigned)v >= (unsigned)n) {
+        if (err) atomicExch(err, DLP_ERR_DEVICE);
+        continue;
+      }
+      if (!vmask || vmask[v]) {
+        if (u != v) unite(parent, u, v, err);
+      } else if (sink && sink[v]) {
+        unite(parent, u, n, err);
+      }
+    }
+  }
+}
+
+__global__ void k_cc_compress(int32_t *parent_, int32_t n, int32_t *err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  volatile int32_t *parent = parent_;
+  int32_t x = parent[i];
+  int steps = 0;
+  while (true) {
+    const int32_t p = parent[x];
+    if (p == x) break;
+    x = p;
+    if (++steps > kMaxSteps) {
+      if (err) atomicExch(err, DLP_ERR_DEVICE);
+      break;
+    }
+  }
+  parent[i] = x;
+}
+
+__global__ void k_cc_gather_rank(const int32_t *__restrict__ parent, int32_t n, int32_t *label) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t p = parent[i];
+  if (p != (int32_t)i) label[i] = label[p];
+}
+
+static int grid_persist(long long work) {
+  long long blocks = (work + kCcThreads - 1) / kCcThreads;
+  const long long cap = (long long)sm_count() * 8;
+  if (blocks > cap) blocks = cap;
+  return (int)(blocks < 1 ? 1 : blocks);
+}
+
+}  // namespace dlp
+
+using namespace dlp;
+
+extern "C" {
+
+int dlp_cc_edges(int32_t n, const int32_t *rows, const int32_t *cols, int64_t m, int32_t *parent, int32_t *err,
+                 dlp_stream_t stream) {
+  if (n < 0 || m < 0 || (n > 0 && !parent) || (m > 0 && (!rows || !cols))) return DLP_ERR_INVALID;
+  if (n == 0) return DLP_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  k_cc_init<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n);
+  if (m > 0) k_cc_edges<<<grid_persist(m), kCcThreads, 0, s>>>(n, rows, cols, m, parent, err);
+  k_cc_compress<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n, err);
+  return check_launch();
+}
+
+int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                 int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err,
+                 dlp_stream_t stream) {
+  if (n < 0 || !parent) return DLP_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  k_cc_init<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1);
+  if (n > 0) {
+    if (!rbeg || !rend || !col) return DLP_ERR_INVALID;
+    const int grid = grid_persist((long long)n * 8);
+    if (!w || w_dtype == DLP_F32)
+      k_cc_graph<float><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const float *)w, vmask, sink, parent, err);
+    else if (w_dtype == DLP_F64)
+      k_cc_graph<double><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const double *)w, vmask, sink, parent,
+                                                     err);
+    else if (w_dtype == DLP_BF16)
+      k_cc_graph<bf16><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const bf16 *)w, vmask, sink, parent, err);
+    else
+      return DLP_ERR_DTYPE;
+  }
+  k_cc_compress<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1, err);
+  return check_launch();
+}
+
+int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,
+                   dlp_stream_t stream) {
+  if (n < 0 || (n > 0 && (!parent || !label)) || !n_comp) return DLP_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  // label[root] = rank of the root among roots; then every vertex copies its root's rank.
+  DLP_TRY(compact_roots(parent, n, label, n_comp, ws, ws_bytes, s));
+  if (n > 0) k_cc_gather_rank<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n, label);
+  return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// Shared device helpers for libdlp (sm_100a only).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dlp.h"
+
+namespace dlp {
+
+using bf16 = __nv_bfloat16;
+
+// ---- status plumbing --------------------------------------------------------------------------
+void set_cuda_error(cudaError_t e);
+int check_launch();  // cudaGetLastError -> status
+int sm_count();
+
+#define DLP_TRY(expr)                 \
+  do {                                \
+    int _st = (expr);                 \
+    if (_st != DLP_OK) return _st;    \
+  } while (0)
+
+#define DLP_CUDA(expr)                         \
+  do {                                         \
+    cudaError_t _e = (expr);                   \
+    if (_e != cudaSuccess) {                   \
+      ::dlp::set_cuda_error(_e);               \
+      return DLP_ERR_CUDA;                     \
+    }                                          \
+  } while (0)
+
+inline size_t dtype_size(int dt) { return dt == DLP_F64 ? 8 : dt == DLP_F32 ? 4 : dt == DLP_BF16 ? 2 : 0; }
+
+// ---- conversions ------------------------------------------------------------------------------
+template <typename TA, typename T>
+__device__ __forceinline__ TA cvt(T x) { return static_cast<TA>(x); }
+template <>
+__device__ __forceinline__ float cvt<float, bf16>(bf16 x) { return __bfloat162float(x); }
+template <>
+__device__ __forceinline__ double cvt<double, bf16>(bf16 x) { return (double)__bfloat162float(x); }
+template <>
+__device__ __forceinline__ bf16 cvt<bf16, float>(float x) { return __float2bfloat16_rn(x); }
+template <>
+__device__ __forceinline__ bf16 cvt<bf16, double>(double x) { return __double2bfloat16(x); }
+
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T *p) { return __ldcs(p); }
+template <>
+__device__ __forceinline__ bf16 ld_stream<bf16>(const bf16 *p) {
+  unsigned short u = __ldcs(reinterpret_cast<const unsigned short *>(p));
+  return __ushort_as_bfloat16(u);
+}
+
+// Load VW consecutive elements of T (16-byte vector when VW*sizeof(T) == 16), converted to TA.
+template <typename T, int VW, typename TA>
+__device__ __forceinline__ void load_vec(const T *__restrict__ p, TA (&out)[VW]) {
+  if constexpr (VW * sizeof(T) == 16) {
+    const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(p));
+    const T *e = reinterpret_cast<const T *>(&raw);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[i] = cvt<TA>(e[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[i] = cvt<TA>(p[i]);
+  }
+}
+
+// Same, through the coherent path (data written earlier in the same kernel or by atomics).
+template <typename T, int VW, typename TA>
+__device__ __forceinline__ void load_vec_coherent(const T *p, TA (&out)[VW]) {
+  if constexpr (VW * sizeof(T) == 16) {
+    const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(p));
+    const T *e = reinterpret_cast<const T *>(&raw);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[i] = cvt<TA>(e[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[i] = cvt<TA>(__ldcg(p + i));
+  }
+}
+
+__device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
+
+// Warp-aggregated append: every lane with pred=true gets a unique slot in out (order within a
+// warp follows lane order; across warps it is unordered).
+__device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t *out, int32_t *count) {
+  const unsigned mask = __activemask();
+  const unsigned ballot = __ballot_sync(mask, pred);
+  if (!ballot) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(ballot) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(ballot));
+  base = __shfl_sync(mask, base, leader);
+  if (pred) out[base + __popc(ballot & ((1u << lane) - 1u))] = value;
+}
+
+inline int ceil_div_i(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+inline int next_pow2(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// kernels.auto_group (dynlp/kernels.py:365-370): power-of-two lanes near the mean degree, in [2, 32].
+inline int auto_group(double avg_deg) {
+  int g = 2;
+  double d = avg_deg > 1.0 ? avg_deg : 1.0;
+  while (g < 32 && g * 2 <= d) g *= 2;
+  return g;
+}
+
+}  // namespace dlp

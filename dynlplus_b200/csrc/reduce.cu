@@ -1,0 +1,230 @@
+// Ordered stream compaction (numpy.flatnonzero semantics) and deterministic column reductions.
+#include "common.cuh"
+
+namespace dlp {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kTile = kScanThreads * kScanItems;
+
+static inline int n_tiles(int32_t n) { return (int)((n + kTile - 1) / kTile); }
+
+// Block-wide exclusive scan of one int per thread (256 threads). Returns the block total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int &excl) {
+  __shared__ int warp_tot[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int inc = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, inc, off);
+    if (lane >= off) inc += t;
+  }
+  if (lane == 31) warp_tot[wid] = inc;
+  __syncthreads();
+  int wpre = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    const int t = warp_tot[w];
+    if (w < wid) wpre += t;
+    total += t;
+  }
+  excl = wpre + inc - v;
+  __syncthreads();
+  return total;
+}
+
+template <typename Pred>
+__global__ void __launch_bounds__(kScanThreads) k_tile_count(Pred pred, int32_t n, int32_t *tile_cnt) {
+  const long long base = (long long)blockIdx.x * kTile + (long long)threadIdx.x * kScanItems;
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const long long g = base + i;
+    if (g < n && pred(g)) ++c;
+  }
+  int excl;
+  const int tot = block_exclusive_scan(c, excl);
+  if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
+}
+
+// Single-block exclusive scan of tile counts in place; total to *count (and *count2 if given).
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t *tile, int nt, int32_t *count) {
+  int carry = 0;
+  for (int base = 0; base < nt; base += kScanThreads) {
+    const int i = base + threadIdx.x;
+    const int v = i < nt ? tile[i] : 0;
+    int excl;
+    const int tot = block_exclusive_scan(v, excl);
+    if (i < nt) tile[i] = carry + excl;
+    carry += tot;
+  }
+  if (threadIdx.x == 0 && count) *count = carry;
+}
+
+template <typename Pred>
+__global__ void __launch_bounds__(kScanThreads)
+    k_tile_write(Pred pred, int32_t n, const int32_t *__restrict__ tile_off, const int32_t *__restrict__ idx,
+                 int32_t *out, int32_t *pos) {
+  const long long base = (long long)blockIdx.x * kTile + (long long)threadIdx.x * kScanItems;
+  bool f[kScanItems];
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const long long g = base + i;
+    f[i] = g < n && pred(g);
+    c += f[i];
+  }
+  int excl;
+  block_exclusive_scan(c, excl);
+  int o = tile_off[blockIdx.x] + excl;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (f[i]) {
+      const long long g = base + i;
+      if (out) out[o] = idx ? idx[g] : (int32_t)g;
+      if (pos) pos[g] = o;
+      ++o;
+    }
+  }
+}
+
+struct FlagPred {
+  const uint8_t *flag;
+  __device__ bool operator()(long long g) const { return flag[g] != 0; }
+};
+struct RootPred {
+  const int32_t *parent;
+  __device__ bool operator()(long long g) const { return parent[g] == (int32_t)g; }
+};
+
+template <typename Pred>
+static int compact_impl(Pred pred, const int32_t *idx, int32_t n, int32_t *out, int32_t *pos, int32_t *count,
+                        void *ws, size_t ws_bytes, cudaStream_t s) {
+  const int nt = n_tiles(n);
+  if (n == 0) {
+    if (count) DLP_CUDA(cudaMemsetAsync(count, 0, sizeof(int32_t), s));
+    return DLP_OK;
+  }
+  if (!ws || ws_bytes < (size_t)nt * sizeof(int32_t)) return DLP_ERR_WORKSPACE;
+  int32_t *tile = (int32_t *)ws;
+  k_tile_count<<<nt, kScanThreads, 0, s>>>(pred, n, tile);
+  k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile, nt, count);
+  k_tile_write<<<nt, kScanThreads, 0, s>>>(pred, n, tile, idx, out, pos);
+  return check_launch();
+}
+
+size_t compact_ws_bytes(int32_t n) { return ((size_t)n_tiles(n) * sizeof(int32_t) + 255) / 256 * 256 + 256; }
+
+int compact_roots(const int32_t *parent, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
+                  cudaStream_t s) {
+  return compact_impl(RootPred{parent}, nullptr, n, nullptr, pos, count, ws, ws_bytes, s);
+}
+
+// ------------------------------------------------------------------------------------------------
+// column reductions: per-block partials over a fixed grid, then an ordered final pass
+// ------------------------------------------------------------------------------------------------
+constexpr int kRedBlocks = 296;
+constexpr int kRedCols = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_colreduce_partial(int kind, int32_t n, int32_t C, const T *__restrict__ X, int64_t ldx,
+                        const T *__restrict__ Y, int64_t ldy, const T *__restrict__ diag,
+                        const uint8_t *__restrict__ mask, double *partial) {
+  __shared__ double sm[8][kRedCols];
+  const long long chunk = ((long long)n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * chunk;
+  const long long r1 = r0 + chunk < n ? r0 + chunk : n;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool is_max = kind == 0 || kind == 3;
+  for (int c0 = 0; c0 < C; c0 += kRedCols) {
+    double acc[kRedCols];
+#pragma unroll
+    for (int i = 0; i < kRedCols; ++i) acc[i] = 0.0;
+    for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      if (mask && !mask[r]) continue;
+      double dinv = 1.0;
+      if (kind == 0) dinv = 1.0 / (double)diag[r];
+#pragma unroll
+      for (int i = 0; i < kRedCols; ++i) {
+        const int c = c0 + i;
+        if (c < C) {
+          const double x = (double)X[r * ldx + c];
+          if (kind == 0) acc[i] = fmax(acc[i], fabs(x) * dinv);
+          else if (kind == 1) acc[i] = fma(x, (double)Y[r * ldy + c], acc[i]);
+          else if (kind == 2) acc[i] = fma(x, x, acc[i]);
+          else acc[i] = fmax(acc[i], fabs(x));
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kRedCols; ++i) {
+      double v = acc[i];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, v, off);
+        v = is_max ? fmax(v, t) : v + t;
+      }
+      if (lane == 0) sm[wid][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kRedCols && c0 + threadIdx.x < C) {
+      double v = sm[0][threadIdx.x];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = is_max ? fmax(v, sm[w][threadIdx.x]) : v + sm[w][threadIdx.x];
+      partial[(long long)blockIdx.x * C + c0 + threadIdx.x] = v;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_colreduce_final(int kind, int32_t C, int nb, const double *__restrict__ partial, double *out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  const bool is_max = kind == 0 || kind == 3;
+  double v = 0.0;
+  for (int b = 0; b < nb; ++b) v = is_max ? fmax(v, partial[(long long)b * C + c]) : v + partial[(long long)b * C + c];
+  out[c] = v;
+}
+
+}  // namespace dlp
+
+using namespace dlp;
+
+extern "C" {
+
+size_t dlp_compact_workspace_bytes(int32_t n) { return compact_ws_bytes(n < 0 ? 0 : n); }
+
+int dlp_compact(const uint8_t *flag, const int32_t *idx, int32_t n, int32_t *out, int32_t *count, void *ws,
+                size_t ws_bytes, dlp_stream_t stream) {
+  if (n < 0 || (n > 0 && (!flag || !out || !count))) return DLP_ERR_INVALID;
+  return compact_impl(FlagPred{flag}, idx, n, out, nullptr, count, ws, ws_bytes, (cudaStream_t)stream);
+}
+
+size_t dlp_colreduce_workspace_bytes(int32_t C) { return (size_t)kRedBlocks * (C > 0 ? C : 1) * sizeof(double); }
+
+int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
+                  const void *diag, int dtype, const uint8_t *mask, double *out, void *ws, size_t ws_bytes,
+                  dlp_stream_t stream) {
+  if (kind < 0 || kind > 3 || n < 0 || C <= 0 || ldx < C || !out) return DLP_ERR_INVALID;
+  if (n > 0 && !X) return DLP_ERR_INVALID;
+  if (kind == 0 && n > 0 && !diag) return DLP_ERR_INVALID;
+  if (kind == 1 && n > 0 && (!Y || ldy < C)) return DLP_ERR_INVALID;
+  if (!ws || ws_bytes < dlp_colreduce_workspace_bytes(C)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  double *partial = (double *)ws;
+  const int nb = n > 0 ? (n < kRedBlocks ? (n + 255) / 256 : kRedBlocks) : 0;
+  if (nb > 0) {
+    if (dtype == DLP_F32)
+      k_colreduce_partial<float><<<nb, 256, 0, s>>>(kind, n, C, (const float *)X, ldx, (const float *)Y, ldy,
+                                                    (const float *)diag, mask, partial);
+    else if (dtype == DLP_F64)
+      k_colreduce_partial<double><<<nb, 256, 0, s>>>(kind, n, C, (const double *)X, ldx, (const double *)Y, ldy,
+                                                     (const double *)diag, mask, partial);
+    else
+      return DLP_ERR_DTYPE;
+  }
+  k_colreduce_final<<<(C + 63) / 64, 64, 0, s>>>(kind, C, nb, partial, out);
+  return check_launch();
+}
+
+}  // extern "C"

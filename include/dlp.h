@@ -1,0 +1,152 @@
+/*
+ * dlp.h - C ABI of libdlp.so, the sm_100a kernels behind the dynlp-compatible Python API.
+ *
+ * Conventions (shared by every entry point):
+ *   - All pointers are device pointers owned by the caller; no entry point allocates device
+ *     memory. Scratch comes from a caller-provided workspace whose size a *_workspace_bytes
+ *     query returns.
+ *   - Every function returns an int status (DLP_OK = 0). Launches are asynchronous on the
+ *     given stream (a cudaStream_t; NULL = legacy default stream) unless documented otherwise.
+ *   - Rows of a sparse matrix are given as [rbeg[r], rend[r]) ranges into col/w. Plain CSR
+ *     passes rbeg = indptr, rend = indptr + 1. Row ranges with slack capacity (the resident
+ *     edge-updatable graph) pass separate begin/end arrays. Stored entries with weight 0 are
+ *     "inert" (deleted edges or edges leaving the solved set), as in the reference
+ *     (dynlp/kernels.py:323, dynlp/stream.py:202-204).
+ *   - Dense n x C score/residual matrices are row-major with a leading dimension ld >= C
+ *     (in elements). Index arrays are int32, as in the reference (dynlp/stream.py:161).
+ *   - Precision codes: DLP_F32, DLP_F64, DLP_BF16. Supported (weights, X, Y) combinations for
+ *     the row kernels: (f32,f32,f32), (f64,f64,f64), (f32,f64,f64) [fp64 residual over fp32-
+ *     stored weights], (bf16,bf16,f32) and (bf16,bf16,bf16) [fp32 accumulation]. The dense
+ *     vectors a/diag/rhs use the Y precision (fp32 when Y is bf16).
+ */
+#ifndef DLP_H
+#define DLP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DLP_OK = 0,
+  DLP_ERR_INVALID = 1,   /* bad pointer, size, shape or leading dimension */
+  DLP_ERR_DTYPE = 2,     /* unsupported precision combination */
+  DLP_ERR_CUDA = 3,      /* a CUDA runtime call failed; dlp_last_cuda_error() has the code */
+  DLP_ERR_CAP = 4,       /* iteration cap reached before convergence */
+  DLP_ERR_CANCELLED = 5, /* the host cancel flag was set */
+  DLP_ERR_WORKSPACE = 6, /* workspace missing or too small */
+  DLP_ERR_OVERFLOW = 7,  /* a row of the resident graph ran out of slack; rebuild needed */
+  DLP_ERR_DEVICE = 8     /* a device-side check failed (bad index or bounded wait ran out) */
+};
+
+enum { DLP_F32 = 0, DLP_F64 = 1, DLP_BF16 = 2 };
+
+typedef struct CUstream_st *dlp_stream_t;
+
+/* ---- library ---------------------------------------------------------------------------- */
+int dlp_version(void);
+const char *dlp_status_string(int status);
+int dlp_last_cuda_error(void);
+/* number of SMs of the current device (used for persistent grid sizes) */
+int dlp_sm_count(void);
+
+/* ---- (a) row-major SpMM with fused axpy / residual epilogue -------------------------------
+ * Replaces kernels.spmm_axpy (dynlp/kernels.py:140-166, :240-266, launcher :377-393),
+ * solvers.apply_A (dynlp/solvers.py:46-49) and the changed-row residual refresh of
+ * IncrementalLP.solve (dynlp/solvers.py:404-407).
+ *   for each output row i (rows == NULL: i = r = 0..n_rows-1; else r = rows[i]):
+ *     acc       = sum_{j in [rbeg[r], rend[r])} w[j] * X[col[j], :]
+ *     Y[o, c]   = cr * RHS[r, c] + alpha * a[r] * X[r, c] + b * acc[c]
+ *   with o = i when compact_out != 0, else o = r. a == NULL drops the a-term, RHS == NULL the
+ *   RHS-term. group = edge lanes per row (power of two <= 32; <= 0 picks from the mean degree
+ *   avg_deg, like kernels.auto_group, dynlp/kernels.py:365-370). */
+int dlp_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype,
+             int32_t n_rows, const int32_t *rows, int32_t C, const void *X, int64_t ldx, int x_dtype,
+             const void *a, double alpha, double b, const void *RHS, int64_t ldr, double cr, void *Y,
+             int64_t ldy, int y_dtype, int compact_out, int32_t group, double avg_deg, dlp_stream_t stream);
+
+/* ---- (b) frontier Jacobi ------------------------------------------------------------------
+ * Replaces the frontier_jacobi kernels (dynlp/kernels.py:31-103, :186-220; FrontierOps.jacobi
+ * :464-474): for g < nf, r = frontier[g]:
+ *   Y[g, c] = (rhs[r, c] + sum_j w_j X[col_j, c]) / diag[r];  changed[g] = any_c |Y[g,c]-X[r,c]| > delta
+ * changed may be NULL. When out_list != NULL the rows with changed[g] are appended to out_list
+ * (unordered, warp-aggregated atomics) and *out_count (device int, caller-zeroed) counts them.
+ * X, rhs, diag, Y share one precision (f32 or f64); w is f32 or matches it. */
+int dlp_frontier_jacobi(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                        int w_dtype, const int32_t *frontier, int32_t nf, int32_t C, const void *X,
+                        int64_t ldx, const void *rhs, int64_t ldr, const void *diag, double delta, void *Y,
+                        int64_t ldy, int dtype, uint8_t *changed, int32_t *out_list, int32_t *out_count,
+                        int32_t group, double avg_deg, dlp_stream_t stream);
+
+/* ---- (b) residual push scatter and neighbour marking --------------------------------------
+ * Replaces push_scatter (dynlp/kernels.py:105-126, :222-238; FrontierOps.push :476-486):
+ *   R[col_j, :] += w_j * D[g, :] for every stored entry j of row frontier[g]; mark[col_j] = 1.
+ * mark may be NULL. R and D share one precision (f32 or f64). */
+int dlp_push_scatter(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype,
+                     const int32_t *frontier, int32_t nf, int32_t C, const void *D, int64_t ldd, void *R,
+                     int64_t ldr, int dtype, uint8_t *mark, int32_t group, double avg_deg,
+                     dlp_stream_t stream);
+
+/* Replaces mark_neighbors (dynlp/kernels.py:128-138): mark[col_j] = 1 for entries of rows[0..nr). */
+int dlp_mark_neighbors(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const int32_t *rows,
+                       int32_t nr, uint8_t *mark, dlp_stream_t stream);
+
+/* ---- synchronous push round helpers (solvers.push, dynlp/solvers.py:100-125) -------------
+ * take: for g < nc, r = cand[g]: D[g,:] = R[r,:] / diag[r]; Z[r,:] += D[g,:]; R[r,:] = 0; mark[r] = 1. */
+int dlp_push_take(const int32_t *cand, int32_t nc, int32_t C, void *Z, int64_t ldz, void *R, int64_t ldr,
+                  const void *diag, void *D, int64_t ldd, int dtype, uint8_t *mark, dlp_stream_t stream);
+
+/* Violating filter of a vertex list: keep[g] = any_c |R[r,c]| > eps[c] * diag[r] for r = idx[g]
+ * (idx == NULL: r = g, g < n). eps is fp64. Optionally clears mark[r]. Output is a uint8 flag per g. */
+int dlp_violating(const int32_t *idx, int32_t n, int32_t C, const void *R, int64_t ldr, const void *diag,
+                  int dtype, const double *eps, uint8_t *flag, uint8_t *clear_mark, dlp_stream_t stream);
+
+/* ---- ordered stream compaction ------------------------------------------------------------
+ * out[0..*count) = the g < n with flag[g] != 0, ascending (numpy flatnonzero); idx != NULL maps
+ * g -> idx[g]. *count is a device int32. Needs dlp_compact_workspace_bytes(n) of workspace. */
+size_t dlp_compact_workspace_bytes(int32_t n);
+int dlp_compact(const uint8_t *flag, const int32_t *idx, int32_t n, int32_t *out, int32_t *count, void *ws,
+                size_t ws_bytes, dlp_stream_t stream);
+
+/* ---- column reductions (fp64 results) -----------------------------------------------------
+ * kind 0: out[c] = max_r |X[r,c]| / diag[r]            (rho_cols, dynlp/solvers.py:52-54)
+ * kind 1: out[c] = sum_r X[r,c] * Y[r,c]                (PCG dots, dynlp/solvers.py:76,79,94)
+ * kind 2: out[c] = sum_r X[r,c]^2                       (2-norms for the relative residual)
+ * kind 3: out[c] = max_r |X[r,c]|
+ * diag/Y may be NULL when unused. out is a device double[C]; rows restricted by mask when
+ * mask != NULL (mask[r] != 0). Partial sums per block over a fixed grid, then an ordered final
+ * pass: the result does not depend on scheduling. Workspace: dlp_colreduce_workspace_bytes(C). */
+size_t dlp_colreduce_workspace_bytes(int32_t C);
+int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
+                  const void *diag, int dtype, const uint8_t *mask, double *out, void *ws, size_t ws_bytes,
+                  dlp_stream_t stream);
+
+/* ---- (f) connected components ---------------------------------------------------------------
+ * Replaces cc.connected_components (dynlp/cc.py:8-23). parent[0..n) receives, for every vertex,
+ * the smallest vertex id of its component (hook-larger-under-smaller union-find with path
+ * halving, then full compression). Edges: m entries (rows[i], cols[i]); endpoints outside
+ * [0, n) are rejected with DLP_ERR_DEVICE via *err (device int, caller-zeroed; may be NULL). */
+int dlp_cc_edges(int32_t n, const int32_t *rows, const int32_t *cols, int64_t m, int32_t *parent, int32_t *err,
+                 dlp_stream_t stream);
+
+/* Graph form used by the grounding checks (dynlp/stream.py:150-159, :275-280): vertices 0..n-1
+ * plus a sink vertex n. An entry (u, v) of the row ranges joins u and v when vmask[u] and
+ * w != 0 (w may be NULL: all entries live) and vmask[v]; it joins u and the sink when vmask[u]
+ * and sink[v]. parent has n + 1 entries. vmask/sink may be NULL (all 1 / all 0). */
+int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                 int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err,
+                 dlp_stream_t stream);
+
+/* Canonical relabel: label[i] = rank of parent[i] among the roots (parent[r] == r; parent must be
+ * fully compressed, as dlp_cc_edges/dlp_cc_graph leave it), i.e. the
+ * labels numpy.unique(parent, return_inverse=True) gives (dynlp/cc.py:22-23); *n_comp = number
+ * of roots (device int). Needs dlp_compact_workspace_bytes(n). */
+int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,
+                   dlp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DLP_H */

@@ -1,0 +1,308 @@
+"""NumPy/SciPy restatement of the reference's hot path (TEST INFRASTRUCTURE ONLY: the checker).
+
+Each function cites the reference (shishir9159/DynLPlus) file:line it restates. Arrays are NumPy,
+sparse matrices SciPy CSR. Pinned against the reference's own outputs in tests/golden/*.npz.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as ssp
+import scipy.sparse.csgraph as csg
+
+
+# ---------------------------------------------------------------------------------------------
+# graphs (dynlp/graphs.py)
+# ---------------------------------------------------------------------------------------------
+def coalesce(rows, cols, vals, n, dtype):
+    """Canonical CSR: duplicates summed, self-loops dropped (dynlp/graphs.py:92-100)."""
+    keep = rows != cols
+    coo = ssp.coo_matrix((np.asarray(vals)[keep].astype(dtype),
+                          (np.asarray(rows)[keep].astype(np.int32), np.asarray(cols)[keep].astype(np.int32))),
+                         shape=(n, n))
+    coo.sum_duplicates()
+    A = coo.tocsr()
+    A.sum_duplicates()
+    return A
+
+
+def symmetric_from_pairs(u, v, w, n, dtype):
+    """dynlp/graphs.py:103-104."""
+    return coalesce(np.concatenate([u, v]), np.concatenate([v, u]), np.concatenate([w, w]), n, dtype)
+
+
+def csr_rows(A):
+    """Row index of every stored entry (dynlp/graphs.py:118-120)."""
+    return np.repeat(np.arange(A.shape[0], dtype=np.int32), np.diff(A.indptr))
+
+
+# ---------------------------------------------------------------------------------------------
+# connected components (dynlp/cc.py:8-23)
+# ---------------------------------------------------------------------------------------------
+def connected_components(n, rows, cols):
+    """Hook (scatter-min of the larger root to the smaller) + full pointer jumping until no edge
+    crosses two labels, then the rank relabel by unique (dynlp/cc.py:8-23)."""
+    if n == 0:
+        return np.zeros(0, dtype=np.int32), 0
+    lab = np.arange(n, dtype=np.int32)
+    rows, cols = np.asarray(rows, dtype=np.int32), np.asarray(cols, dtype=np.int32)
+    while True:
+        lr, lc = lab[rows], lab[cols]
+        diff = lr != lc
+        if not diff.any():
+            break
+        lr, lc = lr[diff], lc[diff]
+        np.minimum.at(lab, np.maximum(lr, lc), np.minimum(lr, lc))
+        while True:
+            nxt = lab[lab]
+            if (nxt == lab).all():
+                break
+            lab = nxt
+    uniq, inv = np.unique(lab, return_inverse=True)
+    return inv.astype(np.int32).ravel(), int(uniq.shape[0])
+
+
+def connected_components_fast(n, rows, cols):
+    """Same labels as connected_components for large inputs: SciPy labels components in the order
+    of their first vertex when scanning 0..n-1, which is the rank of the minimum vertex id."""
+    if n == 0:
+        return np.zeros(0, dtype=np.int32), 0
+    G = ssp.coo_matrix((np.ones(len(rows), dtype=np.int8), (np.asarray(rows), np.asarray(cols))), shape=(n, n))
+    nc, lab = csg.connected_components(G, directed=False)
+    return lab.astype(np.int32), int(nc)
+
+
+def min_vertex_roots(labels):
+    """parent[v] = smallest vertex of v's component, from rank labels."""
+    n = labels.shape[0]
+    first = np.full(labels.max() + 1 if n else 0, n, dtype=np.int64)
+    np.minimum.at(first, labels, np.arange(n))
+    return first[labels].astype(np.int32)
+
+
+# ---------------------------------------------------------------------------------------------
+# kernels (dynlp/kernels.py) -- the kernels' definitions, as the reference's fallbacks state them
+# ---------------------------------------------------------------------------------------------
+def spmm_axpy(W, X, a=None, b=1.0):
+    """Y = a*X + b*(W@X) (dynlp/kernels.py:140-166, :240-266)."""
+    Y = b * (W @ X)
+    if a is not None:
+        Y = a[:, None] * X + Y
+    return Y.astype(X.dtype)
+
+
+def frontier_jacobi(W, frontier, X, rhs, diag, delta):
+    """(rhs[f] + W[f] @ X) / diag[f] and the changed flag (dynlp/kernels.py:473-474)."""
+    Y = (rhs[frontier] + W[frontier] @ X) / diag[frontier][:, None]
+    return Y, (np.abs(Y - X[frontier]) > delta).any(axis=1)
+
+
+def push_scatter(W, frontier, D, R, mark):
+    """R += W[:, frontier] @ D for symmetric W; mark touched (dynlp/kernels.py:483-486)."""
+    sub = W[frontier]
+    seg = np.searchsorted(sub.indptr[1:], np.arange(sub.nnz), side="right")
+    np.add.at(R, sub.indices, sub.data[:, None] * D[seg])
+    mark[sub.indices] = 1
+
+
+def mark_neighbors(W, rows, mark):
+    """dynlp/kernels.py:492."""
+    mark[W[rows].indices] = 1
+
+
+# ---------------------------------------------------------------------------------------------
+# solvers (dynlp/solvers.py)
+# ---------------------------------------------------------------------------------------------
+def apply_A(W, diag, X):
+    """diag*X - W@X (dynlp/solvers.py:46-49)."""
+    return diag[:, None] * X - W @ X
+
+
+def rho_cols(diag, R):
+    """max_u |R_uc| / diag_u (dynlp/solvers.py:52-54)."""
+    return (np.abs(R) / diag[:, None]).max(axis=0) if R.shape[0] else np.zeros(R.shape[1])
+
+
+def violation(diag, R, eps_d):
+    """max |R_uc| / (eps_c diag_u) (dynlp/solvers.py:57-59)."""
+    return float((np.abs(R) / (eps_d[None, :] * diag[:, None])).max()) if R.shape[0] else 0.0
+
+
+def pcg(W, diag, Z, rhs, eps, M=None, max_iter=100_000, patience=400):
+    """Block PCG, one CG per column, until |r_c| <= eps_c diag (dynlp/solvers.py:66-97).
+    Returns (Z, iterations)."""
+    M = M or (lambda R: R / diag[:, None])
+    eps_d = np.asarray(eps, dtype=Z.dtype)
+    R = rhs - apply_A(W, diag, Z)
+    best = violation(diag, R, eps_d)
+    it = 0
+    if best <= 1:
+        return Z, it
+    P = Y = M(R)
+    rz, stall = (R * Y).sum(axis=0), 0
+    for _ in range(max_iter):
+        AP = apply_A(W, diag, P)
+        pAp = (P * AP).sum(axis=0)
+        alpha = np.where(pAp > 0, rz / np.where(pAp > 0, pAp, 1), 0)
+        Z += alpha[None, :] * P
+        R -= alpha[None, :] * AP
+        it += 1
+        v = violation(diag, R, eps_d)
+        if v <= 1:
+            R = rhs - apply_A(W, diag, Z)
+            if (v := violation(diag, R, eps_d)) <= 1:
+                break
+        best, stall = (v, 0) if v < 0.9 * best else (best, stall + 1)
+        if stall >= patience:
+            break
+        Y = M(R)
+        rz_new = (R * Y).sum(axis=0)
+        P = Y + np.where(rz > 0, rz_new / np.where(rz > 0, rz, 1), 0)[None, :] * P
+        rz = rz_new
+    return Z, it
+
+
+def push(W, diag, Z, R, eps, budget_edges=None, max_iter=10**7, record=False):
+    """Synchronous residual push = Jacobi on the violating set (dynlp/solvers.py:100-125).
+
+    Returns (Z, R, converged, iterations, rounds) where rounds lists, per round, the sorted
+    candidate set that pushed and the sorted touched set (when record=True)."""
+    eps_d = np.asarray(eps, dtype=Z.dtype)
+    n = W.shape[0]
+
+    def violating(idx):
+        return (np.abs(R[idx]) > eps_d[None, :] * diag[idx][:, None]).any(axis=1)
+
+    all_idx = np.arange(n, dtype=np.int32)
+    cand, edges, it, best, stall = all_idx[violating(all_idx)], 0, 0, float("inf"), 0
+    rounds = []
+    indptr = W.indptr
+    while cand.shape[0] and it < max_iter:
+        D = R[cand] / diag[cand][:, None]
+        Z[cand] += D
+        R[cand] = 0
+        mark = np.zeros(n, dtype=np.uint8)
+        mark[cand] = 1
+        edges += int((indptr[cand + 1] - indptr[cand]).sum())
+        push_scatter(W, cand, D, R, mark)
+        touched = np.flatnonzero(mark).astype(np.int32)
+        if record:
+            rounds.append((cand.copy(), touched.copy()))
+        cand, it = touched[violating(touched)], it + 1
+        if it % 32 == 0:
+            if budget_edges is not None and edges > budget_edges:
+                break
+            v = violation(diag, R, eps_d)
+            best, stall = (v, 0) if v < 0.99 * best else (best, stall + 1)
+            if stall >= 8:
+                break
+    return Z, R, cand.shape[0] == 0, it, rounds
+
+
+def dynlp_frontier(W, diag, rhs, X, seed_rows, delta, max_iter=10**7, record=False):
+    """DynLP's frontier Jacobi loop (dynlp/solvers.py:227-238): returns (X, iterations, frontiers)."""
+    frontier = np.asarray(seed_rows, dtype=np.int32)
+    it, fronts = 0, []
+    n = W.shape[0]
+    while frontier.shape[0] and it < max_iter:
+        if record:
+            fronts.append(frontier.copy())
+        Y, ch = frontier_jacobi(W, frontier, X, rhs, diag, delta)
+        it += 1
+        upd = frontier[ch]
+        if not upd.shape[0]:
+            break
+        X[upd] = Y[ch]
+        mark = np.zeros(n, dtype=np.uint8)
+        mark[upd] = 1
+        mark_neighbors(W, upd, mark)
+        frontier = np.flatnonzero(mark).astype(np.int32)
+    return X, it, fronts
+
+
+def predict(F, K):
+    """dynlp/solvers.py:166-167."""
+    return (F[:, 0] > 0.5).astype(np.int32) if K == 2 else F.argmax(axis=1).astype(np.int32)
+
+
+# ---------------------------------------------------------------------------------------------
+# system assembly (dynlp/stream.py:142-177)
+# ---------------------------------------------------------------------------------------------
+def build_system(A, y, K, active, labeled, eta=0.0, dtype=np.float64):
+    """The grounded harmonic system of one batch (dynlp/stream.py:142-167, without the new-vertex
+    components): U = active unlabelled vertices whose component (within active unlabelled) holds
+    label weight; W = A[U,U] in CSR order; B = A @ onehot(y_L); s = sum(B)+eta; diag = s+rowsum(W);
+    rhs = B (class 1 only when K == 2)."""
+    n = A.shape[0]
+    rows, cols = csr_rows(A), A.indices
+    prior = np.full(1 if K == 2 else K, 0.5 if K == 2 else 1.0 / K)
+    onehot = np.zeros((n, K), dtype=dtype)
+    li = np.flatnonzero(active & labeled)
+    onehot[li, y[li]] = 1
+    Bfull = A.astype(dtype) @ onehot
+    Um = active & ~labeled
+    U0 = np.flatnonzero(Um)
+    loc = np.full(n, -1, dtype=np.int32)
+    loc[U0] = np.arange(U0.shape[0], dtype=np.int32)
+    keep = Um[rows] & Um[cols]
+    lab, ncomp = connected_components_fast(int(U0.shape[0]), loc[rows[keep]], loc[cols[keep]])
+    gw = np.zeros(ncomp, dtype=dtype)
+    np.add.at(gw, lab, Bfull[U0].sum(axis=1))
+    grounded = gw[lab] > 0
+    Um = Um.copy()
+    Um[U0[~grounded]] = False
+    U = np.flatnonzero(Um)
+    n_u = U.shape[0]
+    loc = np.full(n, -1, dtype=np.int32)
+    loc[U] = np.arange(n_u, dtype=np.int32)
+    keep = Um[rows] & Um[cols]
+    indptr = np.zeros(n_u + 1, dtype=np.int32)
+    indptr[1:] = np.cumsum(np.bincount(loc[rows[keep]], minlength=n_u))
+    W = ssp.csr_matrix((A.data[keep].astype(dtype), loc[cols[keep]], indptr), shape=(n_u, n_u))
+    Bm = Bfull[U]
+    s = Bm.sum(axis=1) + eta
+    diag = s + np.asarray(W.sum(axis=1)).ravel()
+    rhs = (Bm[:, 1:2] if K == 2 else Bm) + eta * prior[None, :]
+    return dict(U=U, W=W, s=s, diag=diag, B=Bm, rhs=rhs, prior=prior, n_ungrounded=int((~grounded).sum()))
+
+
+# ---------------------------------------------------------------------------------------------
+# edge batches (new functionality; set semantics on the symmetric graph)
+# ---------------------------------------------------------------------------------------------
+def apply_edges(A, ins_u, ins_v, ins_w, del_u, del_v):
+    """A' = A with the undirected edges (del_u, del_v) removed, then (ins_u, ins_v, ins_w) set.
+    Deletions of absent edges and self-loops are ignored; an insertion of a present edge sets its
+    weight; within a batch deletions apply before insertions, and a repeated insertion keeps the
+    last weight given."""
+    n = A.shape[0]
+    A = A.tocoo()
+    key = A.row.astype(np.int64) * n + A.col
+    val = A.data.copy()
+    du, dv = np.asarray(del_u, dtype=np.int64), np.asarray(del_v, dtype=np.int64)
+    dkeys = np.concatenate([du * n + dv, dv * n + du])
+    live = ~np.isin(key, dkeys)
+    key, val = key[live], val[live]
+    iu, iv = np.asarray(ins_u, dtype=np.int64), np.asarray(ins_v, dtype=np.int64)
+    iw = np.asarray(ins_w, dtype=A.dtype)
+    ok = iu != iv
+    iu, iv, iw = iu[ok], iv[ok], iw[ok]
+    ikeys = np.concatenate([iu * n + iv, iv * n + iu])
+    iw2 = np.concatenate([iw, iw])
+    # last occurrence wins for repeated keys
+    order = np.arange(ikeys.shape[0])
+    uk, first_rev = np.unique(ikeys[::-1], return_index=True)
+    last = order[::-1][first_rev]
+    keep = ~np.isin(key, uk)
+    key = np.concatenate([key[keep], uk])
+    val = np.concatenate([val[keep], iw2[last]])
+    o = np.argsort(key, kind="stable")
+    key, val = key[o], val[o]
+    return ssp.csr_matrix((val, (key // n, key % n)), shape=(n, n))
+
+
+def relres(W, diag, Z, rhs):
+    """max_c ||rhs_c - A Z_c||_2 / ||rhs_c||_2 in float64."""
+    W64 = W.astype(np.float64)
+    R = rhs.astype(np.float64) - apply_A(W64, diag.astype(np.float64), Z.astype(np.float64))
+    num = np.sqrt((R * R).sum(axis=0))
+    den = np.sqrt((rhs.astype(np.float64) ** 2).sum(axis=0))
+    return float((num / np.where(den > 0, den, 1)).max())

@@ -1,0 +1,169 @@
+"""Generate the golden fixtures by running the REFERENCE (shishir9159/DynLPlus) on the CPU.
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+The reference is pure Python over CuPy; `cupy_shim.install` maps CuPy onto NumPy/SciPy and routes
+its three NVRTC-kernel entry points to its own vectorised fallbacks (see cupy_shim.py). Each
+fixture stores small seeded inputs and the reference's outputs for them; the oracle (oracle/) is
+pinned against these, and the GPU tests compare the CUDA path with both. The reference tree is
+not needed at test time: only these .npz files are read.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import random
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+
+def csr_parts(prefix, A):
+    return {f"{prefix}_indptr": np.asarray(A.indptr, dtype=np.int32), f"{prefix}_indices": np.asarray(A.indices, dtype=np.int32),
+            f"{prefix}_data": np.asarray(A.data), f"{prefix}_shape": np.asarray(A.shape, dtype=np.int64)}
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e3:.0f} kB)")
+
+
+def gen_cc(dl):
+    from dynlp.cc import connected_components
+    out = {}
+    rnd = random.Random(0)  # the reference's own test case (tests/test_dynlp.py:41-46)
+    pairs = [(rnd.randrange(400), rnd.randrange(400)) for _ in range(300)]
+    cases = [(400, np.array([a for a, _ in pairs]), np.array([b for _, b in pairs]))]
+    rs = np.random.RandomState(11)
+    cases.append((5000, rs.randint(0, 5000, 4000), rs.randint(0, 5000, 4000)))   # many components
+    cases.append((3000, rs.randint(0, 3000, 30000), rs.randint(0, 3000, 30000)))  # one giant
+    path = np.arange(2047)
+    cases.append((2048, path[::-1], path[::-1] + 1))  # a long path, hooked from the far end
+    cases.append((17, np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.int64)))  # no edges
+    for i, (n, r, c) in enumerate(cases):
+        lab, nc = connected_components(n, np.asarray(r), np.asarray(c))
+        out.update({f"c{i}_n": np.int64(n), f"c{i}_rows": np.asarray(r, np.int32), f"c{i}_cols": np.asarray(c, np.int32),
+                    f"c{i}_labels": np.asarray(lab, np.int32), f"c{i}_ncomp": np.int64(nc)})
+    out["ncases"] = np.int64(len(cases))
+    save("cc.npz", **out)
+
+
+def gen_kernels(dl):
+    from dynlp import graphs, kernels, solvers
+    out = {}
+    # the reference's kernel-test graph family (tests/test_dynlp.py:199,249), at n=1500 to keep
+    # the fixture small; inputs are float32-representable so they compress
+    ds = graphs.sbm(1500, K=2, deg=12, seed=8, dtype="float64")
+    W, n = ds.A, ds.n
+    out.update(csr_parts("W", W))
+    rs = np.random.RandomState(0)
+    f32 = lambda x: x.astype(np.float32).astype(np.float64)  # noqa: E731
+    frontier = np.sort(rs.choice(n, 350, replace=False)).astype(np.int32)
+    out["frontier"] = frontier
+    diag = (W @ np.ones(n) + 1)
+    out["diag"] = diag
+    for C in (1, 3, 9, 17):
+        X, rhs = f32(rs.random_sample((n, C))), f32(rs.random_sample((n, C)))
+        a = f32(rs.random_sample(n))
+        D = f32(rs.standard_normal((frontier.size, C)))
+        ops = kernels.FrontierOps(W, C, 8)
+        Y, ch = ops.jacobi(frontier, X, rhs, diag, 1e-2)
+        R = np.zeros((n, C))
+        mark = np.zeros(n, dtype=np.uint8)
+        ops.push(frontier, D, R, mark)
+        mk = np.zeros(n, dtype=np.uint8)
+        ops.mark_neighbors(frontier, mk)
+        out.update({f"C{C}_X": X, f"C{C}_rhs": rhs, f"C{C}_a": a, f"C{C}_D": D, f"C{C}_jacY": Y,
+                    f"C{C}_jacch": np.asarray(ch, np.uint8), f"C{C}_pushR": R, f"C{C}_pushmark": mark,
+                    f"C{C}_marknb": mk, f"C{C}_edges": np.int64(int(ops.edges)),
+                    f"C{C}_spmm": solvers.spmm(W, X),
+                    f"C{C}_applyA": solvers.apply_A(type("S", (), {"W": W, "diag": a})(), X)})
+    save("kernels.npz", **out)
+
+
+def _stream_system(dl, n=3000, K=3, deg=8, seed=3, init_frac=0.2, label_frac=0.02, dtype="float64", batch=0):
+    from dynlp import graphs
+    from dynlp.stream import Stream
+    ds = graphs.sbm(n, K=K, deg=deg, seed=seed, dtype=dtype)
+    st = Stream(ds, init_frac=init_frac, n_batches=3, label_frac=label_frac, dtype=dtype)
+    active = np.zeros(ds.n, dtype=bool)
+    for t, sys_ in enumerate(st.batches()):
+        ins, dele = st.schedule[t]
+        active[ins], active[dele] = True, False
+        if t == batch:
+            return ds, st, sys_, active.copy()
+    raise ValueError(batch)
+
+
+def gen_system(dl):
+    out = {}
+    for b in (0, 2):
+        ds, st, s, active = _stream_system(dl, batch=b)
+        p = f"b{b}"
+        out.update(csr_parts(f"{p}_A", ds.A))
+        out.update(csr_parts(f"{p}_W", s.W))
+        out.update({f"{p}_y": np.asarray(ds.y, np.int32), f"{p}_K": np.int64(ds.K),
+                    f"{p}_active": active, f"{p}_labeled": np.asarray(st.labeled),
+                    f"{p}_U": np.asarray(s.U, np.int64), f"{p}_s": s.s, f"{p}_diag": s.diag, f"{p}_B": s.B,
+                    f"{p}_rhs": s.rhs, f"{p}_n_ungrounded": np.int64(s.n_ungrounded)})
+    save("system.npz", **out)
+
+
+def gen_solvers(dl):
+    from dynlp import kernels, solvers
+    out = {}
+    ds, st, s, active = _stream_system(dl, n=3000, K=3, deg=8, seed=3, batch=1)
+    out.update(csr_parts("W", s.W))
+    out.update({"diag": s.diag, "rhs": s.rhs})
+    # pcg with the Jacobi preconditioner (dynlp/solvers.py:66-97)
+    for tag, eps in (("pcg_loose", [1e-4] * 3), ("pcg_tight", [1e-10] * 3)):
+        st_ = solvers.Stats()
+        Z = solvers.pcg(s, np.zeros((s.n_u, 3)), s.rhs.copy(), eps, solvers.jacobi_M(s), 10_000, st_)
+        out.update({f"{tag}_eps": np.asarray(eps), f"{tag}_Z": Z, f"{tag}_iters": np.int64(st_.iters)})
+    # synchronous push from a perturbed warm start, with every round's candidate set recorded
+    Zstar = solvers.pcg(s, np.zeros((s.n_u, 3)), s.rhs.copy(), [1e-12] * 3, solvers.jacobi_M(s), 10_000,
+                        solvers.Stats())
+    rs = np.random.RandomState(5)
+    Z0 = Zstar.copy()
+    hit = rs.choice(s.n_u, 40, replace=False)
+    Z0[hit] += rs.standard_normal((40, 3)) * 0.05
+    R0 = s.rhs - solvers.apply_A(s, Z0)
+    rounds = []
+    orig = kernels.FrontierOps.push
+
+    def rec(self, frontier, D, R, mark):
+        rounds.append(np.asarray(frontier).copy())
+        return orig(self, frontier, D, R, mark)
+
+    kernels.FrontierOps.push = rec
+    try:
+        ops = kernels.FrontierOps(s.W, 3)
+        Z1, R1, ok = solvers.push(s, Z0.copy(), R0.copy(), [1e-7] * 3, ops, solvers.Stats())
+    finally:
+        kernels.FrontierOps.push = orig
+    out.update({"push_Z0": Z0, "push_R0": R0, "push_eps": np.asarray([1e-7] * 3), "push_Z": Z1, "push_R": R1,
+                "push_ok": np.int64(ok), "push_rounds": np.int64(len(rounds)),
+                "push_cand": np.concatenate(rounds).astype(np.int32),
+                "push_cand_off": np.cumsum([0] + [len(r) for r in rounds]).astype(np.int64)})
+    save("solvers.npz", **out)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default="")
+    a = ap.parse_args(argv)
+    import cupy_shim
+    dl = cupy_shim.install(a.reference)
+    gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers}
+    for name, fn in gens.items():
+        if not a.only or name in a.only.split(","):
+            fn(dl)
+
+
+if __name__ == "__main__":
+    main()
