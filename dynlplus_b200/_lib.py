@@ -38,6 +38,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cc_edges": ("ippqppp", ct.c_int),
     "dlp_cc_graph": ("ippppippppp", ct.c_int),
     "dlp_cc_relabel": ("ippppzp", ct.c_int),
+    "dlp_pcg_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_pcg": ("ppppiiippqpqpqpqpqippdiiiiidpzppppp", ct.c_int),
 }
 
 _lib = None

@@ -1,0 +1,97 @@
+// Row-gather machinery shared by the SpMM-shaped kernels (rowops.cu, pcg.cu).
+#pragma once
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace dlp {
+
+template <typename TW_, typename TX_, typename TY_, typename TV_, typename TA_>
+struct Types {
+  using TW = TW_;
+  using TX = TX_;
+  using TY = TY_;
+  using TV = TV_;
+  using TA = TA_;
+};
+using T_F32 = Types<float, float, float, float, float>;
+using T_F64 = Types<double, double, double, double, double>;
+using T_W32X64 = Types<float, double, double, double, double>;
+using T_BF16F = Types<bf16, bf16, float, float, float>;
+using T_BF16B = Types<bf16, bf16, bf16, float, float>;
+
+__device__ __forceinline__ float fmaa(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmaa(double a, double b, double c) { return fma(a, b, c); }
+
+struct Layout {
+  int G, LV, NV, VW, VPL;
+};
+
+constexpr int kThreads = 256;
+
+// Host: pick the lane layout for a k-wide gather of `elem`-byte values at X with leading dim ld.
+static inline int choose_layout(int C, size_t elem, const void *X, int64_t ld, int group, double avg_deg, Layout *L) {
+  const int vwv = (int)(16 / elem);
+  const bool vec = C > 1 && ((uintptr_t)X % 16 == 0) && ((ld * (int64_t)elem) % 16 == 0) &&
+                   ld >= (int64_t)((C + vwv - 1) / vwv) * vwv;
+  L->VW = vec ? vwv : 1;
+  L->NV = (C + L->VW - 1) / L->VW;
+  L->LV = L->NV <= 4 ? 1 : std::min(32, next_pow2((L->NV + 3) / 4));
+  int vpl = (L->NV + L->LV - 1) / L->LV;
+  if (vpl > 4) vpl = vpl <= 8 ? 8 : -1;
+  if (vpl < 0) return DLP_ERR_INVALID;
+  L->VPL = vpl;
+  int es = group > 0 ? std::min(group, 32) : auto_group(avg_deg);
+  int p = 1;
+  while (p * 2 <= es) p *= 2;  // power of two
+  es = std::min(p, 32 / L->LV);
+  if (es < 1) es = 1;
+  L->G = L->LV * es;
+  return DLP_OK;
+}
+
+static inline int grid_for(long long groups, int G) {
+  long long threads = groups * G;
+  long long blocks = (threads + kThreads - 1) / kThreads;
+  long long cap = (long long)sm_count() * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+
+// Sum over the stored entries of one row of w_j * X[col_j, :] for the lane's vectors, reduced
+// over the group's edge slots (every lane of the warp must call this: it shuffles).
+template <typename TW, typename TX, typename TA, int VW, int VPL>
+__device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, const TW *__restrict__ w,
+                                           const TX *__restrict__ X, int64_t ldx, int beg, int end, int es,
+                                           int ES, int cl, int LV, int NV, int G, TA (&acc)[VPL][VW]) {
+#pragma unroll
+  for (int k = 0; k < VPL; ++k)
+#pragma unroll
+    for (int i = 0; i < VW; ++i) acc[k][i] = TA(0);
+  for (int j = beg + es; j < end; j += ES) {
+    const long long v = ld_stream(col + j);
+    const TA wv = cvt<TA>(ld_stream(w + j));
+    const TX *xr = X + v * ldx;
+#pragma unroll
+    for (int k = 0; k < VPL; ++k) {
+      const int vi = cl + k * LV;
+      if (vi < NV) {
+        TA t[VW];
+        load_vec<TX, VW, TA>(xr + (long long)vi * VW, t);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv, t[i], acc[k][i]);
+      }
+    }
+  }
+  for (int off = LV; off < G; off <<= 1) {
+#pragma unroll
+    for (int k = 0; k < VPL; ++k)
+#pragma unroll
+      for (int i = 0; i < VW; ++i) acc[k][i] += __shfl_xor_sync(0xffffffffu, acc[k][i], off);
+  }
+}
+
+}  // namespace dlp

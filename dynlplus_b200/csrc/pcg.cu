@@ -1,0 +1,573 @@
+// Block PCG with the Jacobi preconditioner, one CG per column (dynlp/solvers.py:66-97), fused for
+// B200: three kernels per iteration, fp64 inner products, convergence decided on the device, and
+// the iteration chunk replayed as a CUDA graph (no host round trip per iteration).
+//
+//   K1 apply  : AP = diag*P - W P (row gather), pAp_c partials; last block: alpha_c = rz_c / pAp_c
+//   K2 update : R -= alpha AP; rz_c = sum R^2/diag, ss_c = sum R^2, viol = max |R|/(eps_c diag);
+//               last block: beta_c, stop decision (violation <= 1 and/or max_c ||R_c||/||rhs_c|| <=
+//               target), patience, iteration cap
+//   K3 dir    : Z += alpha P; P = R/diag + beta P   (P update skipped once a stop is proposed)
+//
+// A proposed stop is confirmed on the host against the true residual rhs - A Z, as the reference
+// does (solvers.py:85-89); a failed recheck resumes the iteration from the true residual.
+// Sums over rows go through per-block partials over a fixed grid and an ordered final pass, so
+// the iterates do not depend on scheduling.
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "gather.cuh"
+
+namespace dlp {
+
+struct PcgCtl {
+  int32_t iters;
+  int32_t done;   // 0 running, 1 stop proposed, 2 stalled, 3 iteration cap, 5 converged (confirmed)
+  int32_t stall;
+  int32_t go;     // set by K1 for the iteration in flight
+  uint32_t cnt1, cnt2;
+  int32_t mode, patience;
+  int32_t max_iter, pad0;
+  double best, viol, relres, target;
+};
+
+struct PcgBufs {
+  PcgCtl *ctl;
+  double *alpha, *beta, *rz, *eps, *rhsn, *part1, *part2, *partv;
+};
+
+constexpr int kUpdBlocksPerSM = 4;
+
+static int upd_blocks() { return sm_count() * kUpdBlocksPerSM; }
+static int apply_blocks() { return sm_count() * 8; }
+
+static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+static size_t pcg_ws_bytes(int C) {
+  const size_t nb = (size_t)std::max(upd_blocks(), apply_blocks());
+  size_t b = align256(sizeof(PcgCtl));
+  b += 5 * align256(sizeof(double) * C);
+  b += align256(sizeof(double) * nb * C);      // part1
+  b += align256(sizeof(double) * nb * C * 2);  // part2 (rz, ss)
+  b += align256(sizeof(double) * nb);          // partv
+  return b;
+}
+
+static PcgBufs carve(void *ws, int C) {
+  const size_t nb = (size_t)std::max(upd_blocks(), apply_blocks());
+  char *p = (char *)ws;
+  PcgBufs B;
+  B.ctl = (PcgCtl *)p;
+  p += align256(sizeof(PcgCtl));
+  double **vecs[5] = {&B.alpha, &B.beta, &B.rz, &B.eps, &B.rhsn};
+  for (auto v : vecs) {
+    *v = (double *)p;
+    p += align256(sizeof(double) * C);
+  }
+  B.part1 = (double *)p;
+  p += align256(sizeof(double) * nb * C);
+  B.part2 = (double *)p;
+  p += align256(sizeof(double) * nb * C * 2);
+  B.partv = (double *)p;
+  return B;
+}
+
+// Last block of the grid to finish gets true (after a device-wide fence).
+__device__ __forceinline__ bool last_block(uint32_t *counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const uint32_t t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+// ------------------------------------------------------------------------------------------------
+// K1: AP = diag*P - W P and pAp partials
+// ------------------------------------------------------------------------------------------------
+template <class T>
+struct ApplyArgs {
+  const int32_t *rbeg, *rend, *col;
+  const typename T::TW *w;
+  int32_t n, C;
+  const typename T::TX *P;
+  int64_t ldp;
+  const typename T::TV *diag;
+  typename T::TY *AP;
+  int64_t ldap;
+  PcgBufs B;
+  int G, LV, NV;
+};
+
+template <class T, int VW, int VPL>
+__global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
+  using TA = typename T::TA;
+  PcgCtl *ctl = p.B.ctl;
+  if (ctl->done != 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->go = 0;
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->go = 1;
+  __shared__ double sm[kThreads / 32][256];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int G = p.G, LV = p.LV, NV = p.NV;
+  const int gl = lane & (G - 1);
+  const int cl = gl & (LV - 1);
+  const int es = gl / LV;
+  const int ES = G / LV;
+  const int gpw = 32 / G;
+  double dot[VPL][VW];
+#pragma unroll
+  for (int k = 0; k < VPL; ++k)
+#pragma unroll
+    for (int i = 0; i < VW; ++i) dot[k][i] = 0.0;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long g0 = warp * gpw; g0 < p.n; g0 += nwarps * gpw) {
+    const long long r = g0 + lane / G;
+    const bool valid = r < p.n;
+    const int beg = valid ? p.rbeg[r] : 0;
+    const int end = valid ? p.rend[r] : 0;
+    TA acc[VPL][VW];
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL>(p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV,
+                                                              G, acc);
+    if (valid && es == 0) {
+      const TA d = cvt<TA>(p.diag[r]);
+#pragma unroll
+      for (int k = 0; k < VPL; ++k) {
+        const int vi = cl + k * LV;
+        if (vi < NV) {
+#pragma unroll
+          for (int i = 0; i < VW; ++i) {
+            const int c = vi * VW + i;
+            if (c < p.C) {
+              const TA pv = cvt<TA>(p.P[r * p.ldp + c]);
+              const TA ap = d * pv - acc[k][i];
+              p.AP[r * p.ldap + c] = cvt<typename T::TY>(ap);
+              dot[k][i] += (double)pv * (double)ap;
+            }
+          }
+        }
+      }
+    }
+  }
+  // lanes sharing a vector lane (same cl) hold the same columns: reduce over the other bits
+#pragma unroll
+  for (int k = 0; k < VPL; ++k)
+#pragma unroll
+    for (int i = 0; i < VW; ++i)
+      for (int off = LV; off < 32; off <<= 1) dot[k][i] += __shfl_xor_sync(0xffffffffu, dot[k][i], off);
+  if (lane < LV) {
+#pragma unroll
+    for (int k = 0; k < VPL; ++k) {
+      const int vi = lane + k * LV;
+      if (vi < NV) {
+#pragma unroll
+        for (int i = 0; i < VW; ++i) {
+          const int c = vi * VW + i;
+          if (c < p.C) sm[wid][c] = dot[k][i];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += sm[w][c];
+    p.B.part1[(long long)blockIdx.x * p.C + c] = s;
+  }
+  if (last_block(&ctl->cnt1)) {
+    for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
+      double s = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += p.B.part1[(long long)b * p.C + c];
+      p.B.alpha[c] = s > 0.0 ? p.B.rz[c] / s : 0.0;
+    }
+    if (threadIdx.x == 0) ctl->cnt1 = 0;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// K2: residual update + reductions + stop decision
+//   phase 0: iteration (R -= alpha AP)      phase 1: recheck of a true residual
+//   phase 2: initial residual (sets best, rz)
+// ------------------------------------------------------------------------------------------------
+constexpr int kMaxColChunks = 8;  // C <= 256 with 32 column lanes
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_t C, T *__restrict__ R, int64_t ldr,
+                                                    const T *__restrict__ AP, int64_t ldap,
+                                                    const T *__restrict__ diag, PcgBufs B) {
+  PcgCtl *ctl = B.ctl;
+  if (phase == 0 && !ctl->go) return;
+  const int CX = blockDim.x, RY = blockDim.y;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  __shared__ double s_rz[256], s_ss[256], s_v[256];
+  double rz[kMaxColChunks], ss[kMaxColChunks];
+  double vmax = 0.0;
+  const int nch = (C + CX - 1) / CX;
+#pragma unroll
+  for (int m = 0; m < kMaxColChunks; ++m) rz[m] = ss[m] = 0.0;
+  for (long long r = (long long)blockIdx.x * RY + ty; r < n; r += (long long)gridDim.x * RY) {
+    const double d = (double)diag[r];
+#pragma unroll
+    for (int m = 0; m < kMaxColChunks; ++m) {
+      const int c = tx + m * CX;
+      if (m < nch && c < C) {
+        T rv = R[r * ldr + c];
+        if (phase == 0) {
+          rv = rv - (T)B.alpha[c] * AP[r * ldap + c];
+          R[r * ldr + c] = rv;
+        }
+        const double r64 = (double)rv;
+        rz[m] += r64 * r64 / d;
+        ss[m] += r64 * r64;
+        vmax = fmax(vmax, fabs(r64) / (B.eps[c] * d));
+      }
+    }
+  }
+  // block reduction: per column over ty (fixed order), max over all
+  const int tid = ty * CX + tx;
+  s_v[tid] = vmax;
+  for (int m = 0; m < nch; ++m) {
+    s_rz[tid] = rz[m];
+    s_ss[tid] = ss[m];
+    __syncthreads();
+    if (ty == 0) {
+      const int c = tx + m * CX;
+      double a = 0.0, b = 0.0;
+      for (int y = 0; y < RY; ++y) {
+        a += s_rz[y * CX + tx];
+        b += s_ss[y * CX + tx];
+      }
+      if (c < C) {
+        B.part2[((long long)blockIdx.x * C + c) * 2 + 0] = a;
+        B.part2[((long long)blockIdx.x * C + c) * 2 + 1] = b;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double v = 0.0;
+    for (int t = 0; t < CX * RY; ++t) v = fmax(v, s_v[t]);
+    B.partv[blockIdx.x] = v;
+  }
+  if (last_block(&ctl->cnt2)) {
+    __shared__ double s_rel;
+    if (tid == 0) s_rel = 0.0;
+    __syncthreads();
+    for (int c = tid; c < C; c += CX * RY) {
+      double a = 0.0, b = 0.0;
+      for (int bb = 0; bb < (int)gridDim.x; ++bb) {
+        a += B.part2[((long long)bb * C + c) * 2 + 0];
+        b += B.part2[((long long)bb * C + c) * 2 + 1];
+      }
+      const double rzo = B.rz[c];
+      B.beta[c] = (phase != 2 && rzo > 0.0) ? a / rzo : 0.0;
+      B.rz[c] = a;
+      const double rel = B.rhsn[c] > 0.0 ? sqrt(b) / B.rhsn[c] : sqrt(b);
+      // fmax over non-negative doubles: the int64 view is monotone
+      atomicMax((unsigned long long *)&s_rel, __double_as_longlong(rel));
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double v = 0.0;
+      for (int bb = 0; bb < (int)gridDim.x; ++bb) v = fmax(v, B.partv[bb]);
+      const double rel = s_rel;
+      ctl->viol = v;
+      ctl->relres = rel;
+      double m = 0.0;
+      if (ctl->mode & 1) m = fmax(m, v);
+      if (ctl->mode & 2) m = fmax(m, ctl->target > 0.0 ? rel / ctl->target : rel);
+      const bool conv = m <= 1.0;
+      if (phase == 0) ctl->iters += 1;
+      if (phase == 2) {
+        ctl->best = m;
+        ctl->stall = 0;
+        ctl->done = conv ? 5 : 0;
+      } else if (phase == 0 && conv) {
+        ctl->done = 1;  // proposed: confirmed against the true residual by the host
+      } else if (phase == 1 && conv) {
+        ctl->done = 5;
+      } else {
+        if (m < 0.9 * ctl->best) {
+          ctl->best = m;
+          ctl->stall = 0;
+        } else {
+          ctl->stall += 1;
+        }
+        if (ctl->stall >= ctl->patience) ctl->done = 2;
+        else if (phase == 1) ctl->done = 0;
+      }
+      if (ctl->done == 0 && ctl->iters >= ctl->max_iter) ctl->done = 3;
+      ctl->cnt2 = 0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// K3: Z += alpha P; P = R/diag + beta P
+//   mode 0: both (skipping the P update when a stop was proposed)   mode 1: P update only
+//   mode 2: P = R/diag
+// ------------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z, int64_t ldz,
+                                                 T *__restrict__ P, int64_t ldp, const T *__restrict__ R, int64_t ldr,
+                                                 const T *__restrict__ diag, PcgBufs B) {
+  PcgCtl *ctl = B.ctl;
+  if (mode == 0 && !ctl->go) return;
+  const bool upd_p = mode != 0 || ctl->done == 0;
+  const int CX = blockDim.x, RY = blockDim.y;
+  const int nch = (C + CX - 1) / CX;
+  for (long long r = (long long)blockIdx.x * RY + threadIdx.y; r < n; r += (long long)gridDim.x * RY) {
+    const T dv = diag[r];
+    for (int m = 0; m < nch; ++m) {
+      const int c = threadIdx.x + m * CX;
+      if (c >= C) break;
+      const T pv = P[r * ldp + c];
+      if (mode == 0) Z[r * ldz + c] += (T)B.alpha[c] * pv;
+      if (upd_p) {
+        const T y = R[r * ldr + c] / dv;
+        P[r * ldp + c] = mode == 2 ? y : y + (T)B.beta[c] * pv;
+      }
+    }
+  }
+}
+
+static dim3 upd_block(int C) {
+  const int cx = std::min(32, next_pow2(std::max(C, 1)));
+  return dim3(cx, 256 / cx);
+}
+
+// ------------------------------------------------------------------------------------------------
+// host driver
+// ------------------------------------------------------------------------------------------------
+struct PcgProblem {
+  const int32_t *rbeg, *rend, *col;
+  const void *w;
+  int w_dtype;
+  int32_t n, C;
+  const void *diag, *rhs;
+  int64_t ldrhs;
+  void *Z;
+  int64_t ldz;
+  void *R;
+  int64_t ldr;
+  void *P;
+  int64_t ldp;
+  void *AP;
+  int64_t ldap;
+  int dtype;
+  double avg_deg;
+};
+
+template <class T>
+static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  Layout L;
+  DLP_TRY(choose_layout(q.C, sizeof(typename T::TX), q.P, q.ldp, 0, q.avg_deg, &L));
+  ApplyArgs<T> a{q.rbeg, q.rend, q.col, (const typename T::TW *)q.w, q.n, q.C, (const typename T::TX *)q.P, q.ldp,
+                 (const typename T::TV *)q.diag, (typename T::TY *)q.AP, q.ldap, B, L.G, L.LV, L.NV};
+  const int grid = apply_blocks();
+  constexpr int VWV = 16 / sizeof(typename T::TX);
+#define DLP_APPLY_CASE(VW_)                                                           \
+  switch (L.VPL) {                                                                    \
+    case 1: k_pcg_apply<T, VW_, 1><<<grid, kThreads, 0, s>>>(a); break;              \
+    case 2: k_pcg_apply<T, VW_, 2><<<grid, kThreads, 0, s>>>(a); break;              \
+    case 3: k_pcg_apply<T, VW_, 3><<<grid, kThreads, 0, s>>>(a); break;              \
+    case 4: k_pcg_apply<T, VW_, 4><<<grid, kThreads, 0, s>>>(a); break;              \
+    case 8: k_pcg_apply<T, VW_, 8><<<grid, kThreads, 0, s>>>(a); break;              \
+    default: return DLP_ERR_INVALID;                                                  \
+  }
+  if (L.VW == 1) {
+    DLP_APPLY_CASE(1)
+  } else {
+    DLP_APPLY_CASE(VWV)
+  }
+#undef DLP_APPLY_CASE
+  return check_launch();
+}
+
+template <typename TS>
+static int launch_update(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  k_pcg_update<TS><<<upd_blocks(), upd_block(q.C), 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, (const TS *)q.AP,
+                                                            q.ldap, (const TS *)q.diag, B);
+  return check_launch();
+}
+
+template <typename TS>
+static int launch_dir(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  k_pcg_dir<TS><<<upd_blocks(), upd_block(q.C), 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
+                                                         (const TS *)q.R, q.ldr, (const TS *)q.diag, B);
+  return check_launch();
+}
+
+static int iteration(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  if (q.dtype == DLP_F32) {
+    DLP_TRY(launch_apply<T_F32>(q, B, s));
+    DLP_TRY(launch_update<float>(0, q, B, s));
+    return launch_dir<float>(0, q, B, s);
+  }
+  if (q.w_dtype == DLP_F64) DLP_TRY(launch_apply<T_F64>(q, B, s));
+  else DLP_TRY(launch_apply<T_W32X64>(q, B, s));
+  DLP_TRY(launch_update<double>(0, q, B, s));
+  return launch_dir<double>(0, q, B, s);
+}
+
+static int true_residual(const PcgProblem &q, cudaStream_t s) {
+  // R = rhs - diag*Z + W Z
+  return dlp_spmm(q.rbeg, q.rend, q.col, q.w, q.w_dtype, q.n, nullptr, q.C, q.Z, q.ldz, q.dtype, q.diag, -1.0,
+                  1.0, q.rhs, q.ldrhs, 1.0, q.R, q.ldr, q.dtype, 0, 0, q.avg_deg, (dlp_stream_t)s);
+}
+
+static int update_phase(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  return q.dtype == DLP_F32 ? launch_update<float>(phase, q, B, s) : launch_update<double>(phase, q, B, s);
+}
+
+static int dir_phase(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  return q.dtype == DLP_F32 ? launch_dir<float>(mode, q, B, s) : launch_dir<double>(mode, q, B, s);
+}
+
+// Graph cache: one instantiated chunk of `k` iterations per problem signature.
+struct GraphKey {
+  std::vector<uintptr_t> v;
+  bool operator==(const GraphKey &o) const { return v == o.v; }
+};
+struct GraphKeyHash {
+  size_t operator()(const GraphKey &k) const {
+    size_t h = 1469598103934665603ull;
+    for (auto x : k.v) h = (h ^ x) * 1099511628211ull;
+    return h;
+  }
+};
+
+static std::mutex g_graph_mu;
+static std::unordered_map<GraphKey, cudaGraphExec_t, GraphKeyHash> g_graphs;
+static cudaStream_t g_capture_stream[64];
+
+static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, cudaGraphExec_t *out) {
+  int dev = 0;
+  DLP_CUDA(cudaGetDevice(&dev));
+  GraphKey key{{(uintptr_t)dev, (uintptr_t)q.rbeg, (uintptr_t)q.rend, (uintptr_t)q.col, (uintptr_t)q.w,
+                (uintptr_t)q.w_dtype, (uintptr_t)q.n, (uintptr_t)q.C, (uintptr_t)q.diag, (uintptr_t)q.Z,
+                (uintptr_t)q.ldz, (uintptr_t)q.R, (uintptr_t)q.ldr, (uintptr_t)q.P, (uintptr_t)q.ldp, (uintptr_t)q.AP,
+                (uintptr_t)q.ldap, (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)k,
+                (uintptr_t)(q.avg_deg * 1024)}};
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  auto it = g_graphs.find(key);
+  if (it != g_graphs.end()) {
+    *out = it->second;
+    return DLP_OK;
+  }
+  if (dev < 0 || dev >= 64) return DLP_ERR_INVALID;
+  if (!g_capture_stream[dev]) DLP_CUDA(cudaStreamCreateWithFlags(&g_capture_stream[dev], cudaStreamNonBlocking));
+  cudaStream_t cs = g_capture_stream[dev];
+  DLP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int st = DLP_OK;
+  for (int i = 0; i < k && st == DLP_OK; ++i) st = iteration(q, B, cs);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(cs, &g);
+  if (st != DLP_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (e != cudaSuccess) {
+    set_cuda_error(e);
+    return DLP_ERR_CUDA;
+  }
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    set_cuda_error(e);
+    return DLP_ERR_CUDA;
+  }
+  if (g_graphs.size() >= 32) {  // bounded cache
+    for (auto &kv : g_graphs) cudaGraphExecDestroy(kv.second);
+    g_graphs.clear();
+  }
+  g_graphs.emplace(key, ex);
+  *out = ex;
+  return DLP_OK;
+}
+
+}  // namespace dlp
+
+using namespace dlp;
+
+extern "C" {
+
+size_t dlp_pcg_workspace_bytes(int32_t C) { return pcg_ws_bytes(C > 0 ? C : 1); }
+
+int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype, int32_t n,
+            int32_t C, const void *diag, const void *rhs, int64_t ldrhs, void *Z, int64_t ldz, void *R, int64_t ldr,
+            void *P, int64_t ldp, void *AP, int64_t ldap, int dtype, const double *eps, const double *rhs_norm,
+            double target_relres, int32_t mode, int32_t max_iter, int32_t patience, int32_t check_every,
+            int32_t use_graph, double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, double *viol_out,
+            double *relres_out, int32_t *status_out, dlp_stream_t stream) {
+  if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
+  if (mode < 1 || mode > 3 || !eps) return DLP_ERR_INVALID;
+  if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
+    return DLP_ERR_DTYPE;
+  if (!ws || ws_bytes < pcg_ws_bytes(C)) return DLP_ERR_WORKSPACE;
+  if (n == 0) {
+    if (iters_out) *iters_out = 0;
+    if (status_out) *status_out = 5;
+    return DLP_OK;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  PcgProblem q{rbeg, rend, col, w, w_dtype, n, C, diag, rhs, ldrhs, Z, ldz, R, ldr, P, ldp, AP, ldap, dtype, avg_deg};
+  PcgBufs B = carve(ws, C);
+  PcgCtl h{};
+  h.mode = mode;
+  h.patience = patience > 0 ? patience : 400;
+  h.max_iter = max_iter;
+  h.target = target_relres;
+  DLP_CUDA(cudaMemcpyAsync(B.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  DLP_CUDA(cudaMemcpyAsync(B.eps, eps, sizeof(double) * C, cudaMemcpyHostToDevice, s));
+  if (rhs_norm) {
+    DLP_CUDA(cudaMemcpyAsync(B.rhsn, rhs_norm, sizeof(double) * C, cudaMemcpyHostToDevice, s));
+  } else {
+    DLP_CUDA(cudaMemsetAsync(B.rhsn, 0, sizeof(double) * C, s));
+  }
+  DLP_CUDA(cudaMemsetAsync(B.rz, 0, sizeof(double) * C, s));
+  // R = rhs - A Z; best = violation; P = R/diag; rz = R.(R/diag)
+  DLP_TRY(true_residual(q, s));
+  DLP_TRY(update_phase(2, q, B, s));
+  DLP_TRY(dir_phase(2, q, B, s));
+  const int k = check_every > 0 ? check_every : 8;
+  cudaGraphExec_t ex = nullptr;
+  if (use_graph) DLP_TRY(get_chunk_graph(q, B, k, &ex));
+  PcgCtl cur{};
+  DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+  DLP_CUDA(cudaStreamSynchronize(s));
+  if (max_iter <= 0 && cur.done == 0) cur.done = 3;
+  while (cur.done == 0 || cur.done == 1) {
+    if (cur.done == 0) {
+      if (ex) {
+        DLP_CUDA(cudaGraphLaunch(ex, s));
+      } else {
+        for (int i = 0; i < k; ++i) DLP_TRY(iteration(q, B, s));
+      }
+    } else {
+      // a stop was proposed: recheck on the true residual (dynlp/solvers.py:85-89)
+      DLP_TRY(true_residual(q, s));
+      DLP_TRY(update_phase(1, q, B, s));
+      DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+      DLP_CUDA(cudaStreamSynchronize(s));
+      if (cur.done != 0) break;
+      DLP_TRY(dir_phase(1, q, B, s));  // resume from the true residual
+    }
+    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    DLP_CUDA(cudaStreamSynchronize(s));
+  }
+  if (iters_out) *iters_out = cur.iters;
+  if (viol_out) *viol_out = cur.viol;
+  if (relres_out) *relres_out = cur.relres;
+  if (status_out) *status_out = cur.done;
+  return DLP_OK;
+}
+
+}  // extern "C"

@@ -13,7 +13,7 @@ import torch
 from . import _lib
 from .backend import CSR, code, ld, ptr, stream, workspace
 
-MAX_KERNEL_COLS = 256  # widest score matrix the gather kernels take (32 vector lanes x 8 vectors)
+MAX_KERNEL_COLS = 256  # widest score matrix every layout takes (scalar path: 32 lanes x 8 columns)
 COLS_MIN = 17
 
 

@@ -146,6 +146,28 @@ int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int3
 int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,
                    dlp_stream_t stream);
 
+
+/* ---- (d) fused block PCG, Jacobi preconditioner --------------------------------------------
+ * Replaces solvers.pcg with jacobi_M (dynlp/solvers.py:62-97): one CG per column of
+ * (diag - W) Z = rhs, starting from the Z given. Per iteration three kernels (SpMM + pAp, residual
+ * update + rz/norms/violation, direction update); all inner products and norms in fp64, reduced
+ * in a fixed order. Stop rule `mode`: bit 0 = the reference's max_uc |R_uc|/(eps_c diag_u) <= 1,
+ * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold). A proposed
+ * stop is confirmed on the true residual rhs - A Z (solvers.py:85-89); `patience` iterations
+ * without a 10% improvement stop the solve as the reference's stall rule does (:90-92).
+ * eps and rhs_norm are HOST arrays of C doubles (rhs_norm may be NULL when bit 1 is unused).
+ * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual). The chunk of
+ * check_every iterations is replayed as a CUDA graph when use_graph != 0 (cached per problem).
+ * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap.
+ * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C). */
+size_t dlp_pcg_workspace_bytes(int32_t C);
+int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype, int32_t n,
+            int32_t C, const void *diag, const void *rhs, int64_t ldrhs, void *Z, int64_t ldz, void *R, int64_t ldr,
+            void *P, int64_t ldp, void *AP, int64_t ldap, int dtype, const double *eps, const double *rhs_norm,
+            double target_relres, int32_t mode, int32_t max_iter, int32_t patience, int32_t check_every,
+            int32_t use_graph, double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, double *viol_out,
+            double *relres_out, int32_t *status_out, dlp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

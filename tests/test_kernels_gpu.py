@@ -204,6 +204,10 @@ def test_push_take_and_violating(dt):
 
 
 def test_invalid_arguments_raise():
+    A = O.symmetric_from_pairs(np.array([0]), np.array([1]), np.ones(1), 4, np.float32)
+    # 1100 fp32 columns = 275 vectors: beyond 32 vector lanes x 8 vectors per lane
     with pytest.raises(_lib.DLPError):
-        A = O.symmetric_from_pairs(np.array([0]), np.array([1]), np.ones(1), 4, np.float32)
-        kernels.spmm_axpy(CSR.from_scipy(A), T(np.zeros((4, 300), np.float32)))  # wider than 256 columns
+        kernels.spmm_axpy(CSR.from_scipy(A), T(np.zeros((4, 1100), np.float32)))
+    # 300 columns fit (75 vectors) and are exact
+    X = np.random.RandomState(0).rand(4, 300).astype(np.float32)
+    np.testing.assert_allclose(kernels.spmm_axpy(CSR.from_scipy(A), T(X)).cpu().numpy(), A @ X, rtol=1e-6)
