@@ -25,6 +25,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_status_string": ("i", ct.c_char_p),
     "dlp_last_cuda_error": ("", ct.c_int),
     "dlp_sm_count": ("", ct.c_int),
+    "dlp_launch_count": ("", ct.c_ulonglong),
     "dlp_spmm": ("ppppiipipqipddpqdpqiiidp", ct.c_int),
     "dlp_frontier_jacobi": ("ppppipiipqpqpdpqipppidp", ct.c_int),
     "dlp_push_scatter": ("ppppipiipqpqipidp", ct.c_int),
@@ -40,6 +41,15 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cc_relabel": ("ippppzp", ct.c_int),
     "dlp_pcg_workspace_bytes": ("i", ct.c_size_t),
     "dlp_pcg": ("ppppiiippqpqpqpqpqippdiiiiidpzppppp", ct.c_int),
+    "dlp_graph_delete": ("ipppppppipppipppppp", ct.c_int),
+    "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
+    "dlp_graph_toggle": ("ppppppippppp", ct.c_int),
+    "dlp_graph_rowsum": ("ppppipp", ct.c_int),
+    "dlp_system_rows": ("pippipdpiiippqppqp", ct.c_int),
+    "dlp_park_rows": ("pipiipdpqpqp", ct.c_int),
+    "dlp_cols_scale": ("iipqipipqip", ct.c_int),
+    "dlp_ground_update": ("ipppppp", ct.c_int),
 }
 
 _lib = None

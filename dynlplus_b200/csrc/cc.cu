@@ -148,7 +148,7 @@ int dlp_cc_edges(int32_t n, const int32_t *rows, const int32_t *cols, int64_t m,
   k_cc_init<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n);
   if (m > 0) k_cc_edges<<<grid_persist(m), kCcThreads, 0, s>>>(n, rows, cols, m, parent, err);
   k_cc_compress<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n, err);
-  return check_launch();
+  return check_launch(m > 0 ? 3 : 2);
 }
 
 int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
@@ -171,7 +171,7 @@ int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int3
       return DLP_ERR_DTYPE;
   }
   k_cc_compress<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1, err);
-  return check_launch();
+  return check_launch(n > 0 ? 3 : 2);
 }
 
 int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,
@@ -181,7 +181,7 @@ int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_
   // label[root] = rank of the root among roots; then every vertex copies its root's rank.
   DLP_TRY(compact_roots(parent, n, label, n_comp, ws, ws_bytes, s));
   if (n > 0) k_cc_gather_rank<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n, label);
-  return check_launch();
+  return check_launch(n > 0 ? 1 : 0);
 }
 
 }  // extern "C"

@@ -13,8 +13,9 @@ using bf16 = __nv_bfloat16;
 
 // ---- status plumbing --------------------------------------------------------------------------
 void set_cuda_error(cudaError_t e);
-int check_launch();  // cudaGetLastError -> status
+int check_launch(int kernels = 1);  // cudaGetLastError -> status; counts `kernels` launches
 int sm_count();
+void note_launches(unsigned long long k);  // kernels launched outside check_launch (graph replays)
 
 #define DLP_TRY(expr)                 \
   do {                                \

@@ -548,6 +548,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
     if (cur.done == 0) {
       if (ex) {
         DLP_CUDA(cudaGraphLaunch(ex, s));
+        note_launches(3ull * k);
       } else {
         for (int i = 0; i < k; ++i) DLP_TRY(iteration(q, B, s));
       }

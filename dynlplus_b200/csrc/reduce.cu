@@ -110,7 +110,7 @@ static int compact_impl(Pred pred, const int32_t *idx, int32_t n, int32_t *out, 
   k_tile_count<<<nt, kScanThreads, 0, s>>>(pred, n, tile);
   k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile, nt, count);
   k_tile_write<<<nt, kScanThreads, 0, s>>>(pred, n, tile, idx, out, pos);
-  return check_launch();
+  return check_launch(3);
 }
 
 size_t compact_ws_bytes(int32_t n) { return ((size_t)n_tiles(n) * sizeof(int32_t) + 255) / 256 * 256 + 256; }
@@ -224,7 +224,7 @@ int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, co
       return DLP_ERR_DTYPE;
   }
   k_colreduce_final<<<(C + 63) / 64, 64, 0, s>>>(kind, C, nb, partial, out);
-  return check_launch();
+  return check_launch(nb > 0 ? 2 : 1);
 }
 
 }  // extern "C"

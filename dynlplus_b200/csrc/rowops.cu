@@ -8,6 +8,7 @@
 // (dynlp/kernels.py:141-166), LV > 1 its class-parallel map (:240-266), here with 16-byte
 // vector gathers of X when the leading dimension allows it.
 #include <algorithm>
+#include <atomic>
 
 #include "gather.cuh"
 
@@ -15,11 +16,15 @@ namespace dlp {
 
 namespace {
 cudaError_t g_last_cuda = cudaSuccess;
+std::atomic<unsigned long long> g_launches{0};
 }
 
 void set_cuda_error(cudaError_t e) { g_last_cuda = e; }
 
-int check_launch() {
+void note_launches(unsigned long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+int check_launch(int kernels) {
+  g_launches.fetch_add((unsigned long long)kernels, std::memory_order_relaxed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_cuda_error(e);
@@ -382,6 +387,8 @@ const char *dlp_status_string(int st) {
 }
 
 int dlp_last_cuda_error(void) { return (int)g_last_cuda; }
+
+unsigned long long dlp_launch_count(void) { return g_launches.load(); }
 
 int dlp_sm_count(void) { return sm_count(); }
 

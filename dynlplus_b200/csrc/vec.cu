@@ -1,0 +1,71 @@
+// Column-scaled vector updates of the refinement loop and the grounding update.
+#include "common.cuh"
+
+namespace dlp {
+
+// op 0: Y = X / scale[c]   op 1: Y += X * scale[c]   op 2: Y = X * scale[c]
+template <typename TX, typename TY>
+__global__ void k_cols_scale(int32_t n, int32_t C, const TX *__restrict__ X, int64_t ldx,
+                             const double *__restrict__ scale, int op, TY *Y, int64_t ldy) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * C) return;
+  const long long r = t / C;
+  const int c = (int)(t % C);
+  const double x = (double)X[r * ldx + c];
+  const double s = scale[c];
+  if (op == 0) Y[r * ldy + c] = (TY)(x / s);
+  else if (op == 1) Y[r * ldy + c] = (TY)((double)Y[r * ldy + c] + x * s);
+  else Y[r * ldy + c] = (TY)(x * s);
+}
+
+// umask[v] = vmask[v] && root(v) == root(sink); in_t[v] = membership changed; counts[0] += |changed|
+__global__ void k_ground_update(int32_t n, const int32_t *__restrict__ parent, const uint8_t *__restrict__ vmask,
+                                uint8_t *umask, uint8_t *in_t, int32_t *counts) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool ch = false;
+  if (v < n) {
+    const bool nu = vmask[v] && parent[v] == parent[n];
+    const bool ou = umask[v] != 0;
+    ch = nu != ou;
+    umask[v] = nu ? 1 : 0;
+    in_t[v] = ch ? 1 : 0;
+  }
+  const unsigned b = __ballot_sync(0xffffffffu, ch);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(counts, __popc(b));
+}
+
+}  // namespace dlp
+
+using namespace dlp;
+
+extern "C" {
+
+int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
+                   void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream) {
+  if (n < 0 || C <= 0 || ldx < C || ldy < C || op < 0 || op > 2) return DLP_ERR_INVALID;
+  if (n == 0) return DLP_OK;
+  if (!X || !Y || !scale) return DLP_ERR_INVALID;
+  const int grid = ceil_div_i((long long)n * C, 256);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (x_dtype == DLP_F64 && y_dtype == DLP_F32)
+    k_cols_scale<double, float><<<grid, 256, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (float *)Y, ldy);
+  else if (x_dtype == DLP_F32 && y_dtype == DLP_F64)
+    k_cols_scale<float, double><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (double *)Y, ldy);
+  else if (x_dtype == DLP_F64 && y_dtype == DLP_F64)
+    k_cols_scale<double, double><<<grid, 256, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (double *)Y, ldy);
+  else if (x_dtype == DLP_F32 && y_dtype == DLP_F32)
+    k_cols_scale<float, float><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (float *)Y, ldy);
+  else
+    return DLP_ERR_DTYPE;
+  return check_launch();
+}
+
+int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, uint8_t *umask, uint8_t *in_t,
+                      int32_t *count, dlp_stream_t stream) {
+  if (n < 0 || !parent || !vmask || !umask || !in_t || !count) return DLP_ERR_INVALID;
+  if (n == 0) return DLP_OK;
+  k_ground_update<<<ceil_div_i(n, 256), 256, 0, (cudaStream_t)stream>>>(n, parent, vmask, umask, in_t, count);
+  return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,572 @@
+"""Label-propagation solvers (mirrors dynlp/solvers.py).
+
+DynLP+ (certified): A = diag - W is a nonsingular M-matrix, so |r| <= rho * diag implies
+|F - F*| <= rho * h with A h = diag (dynlp/solvers.py:10-12); h rides along as one extra column.
+The iterations run in libdlp's kernels: Jacobi-PCG is one fused C call (three kernels per
+iteration, CUDA-graph chunks, device-side stop rule), push and frontier Jacobi use the row
+kernels, and the fp64 refinement (solvers.py:322-337) uses fp64 residual SpMMs.
+
+Extension over the reference: `target_relres` adds a second stop rule, the relative residual
+max_c ||rhs_c - A F_c||_2 / ||rhs_c||_2 in fp64, which the certified loops must also meet.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib, kernels
+from .backend import Timer, code, ld, ptr, stream, workspace
+from .kernels import FrontierOps
+from .stream import System
+
+F64 = torch.float64
+
+
+@dataclass
+class Stats:
+    iters: int = 0
+    edges: int = 0              # edge visits: hardware-independent work
+    ms: float = 0.0             # init + setup + solve
+    setup_ms: float = 0.0       # AMG setup (included in ms)
+    path: str = ""
+    cert: float = float("nan")  # bound the solver certified itself
+    hmax: float = float("nan")
+    relres: float = float("nan")  # fp64 relative residual of the F columns at return
+
+
+def _pad(C, dt):
+    q = 16 // torch.tensor([], dtype=dt).element_size()
+    return (C + q - 1) // q * q
+
+
+def padded_empty(n, C, dt, dev, fill=None):
+    """n x C view of an n x ld buffer whose rows start on 16-byte boundaries (vector gathers)."""
+    buf = torch.empty((n, _pad(C, dt)), dtype=dt, device=dev) if fill is None else \
+        torch.full((n, _pad(C, dt)), fill, dtype=dt, device=dev)
+    return buf[:, :C]
+
+
+_SCRATCH: dict = {}
+
+
+def _scratch(tag, n, C, dt, dev, padded=False):
+    key = (tag, n, C, dt, dev)
+    t = _SCRATCH.get(key)
+    if t is None:
+        t = padded_empty(n, C, dt, dev, 0.0) if padded else torch.zeros((n, C), dtype=dt, device=dev)
+        _SCRATCH[key] = t
+    return t
+
+
+def spmm(W, X):
+    """W @ X (dynlp/solvers.py:40-43)."""
+    return kernels.spmm_axpy(W, X)
+
+
+def apply_A(sys: System, X):
+    """diag * X - W X (dynlp/solvers.py:46-49)."""
+    return kernels.spmm_axpy(sys.W, X, a=sys.diag, b=-1.0)
+
+
+def residual(sys: System, X, rhs, out=None, rows=None):
+    """rhs - A X in one fused pass (fp64 when X is fp64)."""
+    return kernels.spmm_axpy(sys.W, X, a=sys.diag.to(X.dtype), alpha=-1.0, b=1.0, rhs=rhs, out=out, rows=rows)
+
+
+def rho_cols(sys: System, R):
+    """max_u |R_uc| / diag_u per column (dynlp/solvers.py:52-54), fp64 on the device."""
+    if R.shape[0] == 0:
+        return torch.zeros(R.shape[1], dtype=F64, device=R.device)
+    return kernels.colreduce(0, R, diag=sys.diag.to(R.dtype))
+
+
+def violation(sys: System, R, eps_d):
+    """max |R_uc| / (eps_c diag_u); <= 1 means converged (dynlp/solvers.py:57-59)."""
+    if R.shape[0] == 0:
+        return 0.0
+    return float((rho_cols(sys, R) / torch.as_tensor(eps_d, dtype=F64, device=R.device)).max().item())
+
+
+def col_norms(X):
+    return kernels.colreduce(2, X).sqrt()
+
+
+class JacobiM:
+    """R / diag (dynlp/solvers.py:62-63); recognised by `pcg`, which then runs the fused kernels."""
+
+    def __init__(self, sys):
+        self.sys = sys
+
+    def __call__(self, R):
+        return R / self.sys.diag.to(R.dtype)[:, None]
+
+
+def jacobi_M(sys):
+    return JacobiM(sys)
+
+
+def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400, *, target_relres=None,
+        rhs_norm=None, check_every=8, use_graph=True):
+    """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
+
+    Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
+    residual ||R_c|| / rhs_norm_c <= target must hold as well (rhs_norm defaults to ||rhs_c||)."""
+    if M is not None and not isinstance(M, JacobiM):
+        return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm)
+    n, C = Z.shape
+    if n == 0:
+        return Z
+    dt, dev = Z.dtype, Z.device
+    diag = sys.diag.to(dt).contiguous()
+    W = sys.W
+    wdt = W.data.dtype
+    if dt == torch.float32 and wdt != torch.float32:
+        raise TypeError("fp32 PCG needs fp32 weights")
+    R = _scratch("pcg_R", n, C, dt, dev)
+    P = _scratch("pcg_P", n, C, dt, dev, padded=True)
+    AP = _scratch("pcg_AP", n, C, dt, dev)
+    eps_h = (ct.c_double * C)(*[float(e) for e in eps])
+    mode = 1
+    rn = None
+    if target_relres is not None:
+        mode = 3
+        if rhs_norm is None:
+            rhs_norm = col_norms(rhs.to(dt)).cpu().tolist()
+        rn = (ct.c_double * C)(*[float(x) for x in rhs_norm])
+    ws = workspace("pcg").get(_lib.lib().dlp_pcg_workspace_bytes(C))
+    it, viol, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_double(0), ct.c_int32(0)
+    rhs = rhs.to(dt)
+    _lib.call("dlp_pcg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C, ptr(diag),
+              ptr(rhs), ld(rhs), ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), code(Z), eps_h, rn,
+              float(target_relres or 0.0), mode, int(max_iter), int(patience), int(check_every), int(bool(use_graph)),
+              W.nnz / max(n, 1), ptr(ws), ws.numel(), ct.byref(it), ct.byref(viol), ct.byref(rel), ct.byref(status),
+              stream())
+    st.iters += it.value
+    st.edges += (it.value + 2) * W.nnz + work_M * it.value
+    st.relres = rel.value
+    return Z
+
+
+def _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm):
+    """PCG with a general preconditioner M (the AMG V-cycle): the reference loop
+    (dynlp/solvers.py:66-97) over libdlp's SpMM and fp64 column reductions."""
+    dt = Z.dtype
+    eps_d = torch.as_tensor(eps, dtype=F64, device=Z.device)
+    rn = None
+    if target_relres is not None:
+        rn = (col_norms(rhs.to(dt)) if rhs_norm is None else torch.as_tensor(rhs_norm, dtype=F64, device=Z.device))
+
+    def stop_metric(R):
+        m = (rho_cols(sys, R) / eps_d).max()
+        if rn is not None:
+            m = torch.maximum(m, (col_norms(R) / torch.where(rn > 0, rn, torch.ones_like(rn))).max() / target_relres)
+        return float(m.item())
+
+    R = residual(sys, Z, rhs.to(dt))
+    st.edges += sys.nnz
+    best = stop_metric(R)
+    if best <= 1:
+        return Z
+    P = Y = M(R)
+    rz, stall = kernels.colreduce(1, R, Y=Y), 0
+    for _ in range(max_iter):
+        AP = apply_A(sys, P)
+        pAp = kernels.colreduce(1, P, Y=AP)
+        alpha = torch.where(pAp > 0, rz / torch.where(pAp > 0, pAp, torch.ones_like(pAp)), torch.zeros_like(pAp))
+        Z += alpha.to(dt)[None, :] * P
+        R -= alpha.to(dt)[None, :] * AP
+        st.iters, st.edges = st.iters + 1, st.edges + sys.nnz + work_M
+        v = stop_metric(R)
+        if v <= 1:
+            R = residual(sys, Z, rhs.to(dt))
+            st.edges += sys.nnz
+            if (v := stop_metric(R)) <= 1:
+                break
+        best, stall = (v, 0) if v < 0.9 * best else (best, stall + 1)
+        if stall >= patience:
+            break
+        Y = M(R)
+        rz_new = kernels.colreduce(1, R, Y=Y)
+        beta = torch.where(rz > 0, rz_new / torch.where(rz > 0, rz, torch.ones_like(rz)), torch.zeros_like(rz))
+        P = Y + beta.to(dt)[None, :] * P
+        rz = rz_new
+    return Z
+
+
+def push(sys: System, Z, R, eps, ops: FrontierOps, st: Stats, budget_edges=None, max_iter=10**7, record=None):
+    """Residual push (Jacobi on the violating set) until |r_c| <= eps_c * diag (solvers.py:100-125).
+
+    One round: D = R[cand]/diag; Z[cand] += D; R[cand] = 0; R[N(cand)] += W D (atomics); the next
+    candidates are the touched rows that violate. Sets are compacted in ascending order, so the
+    candidate set of every round equals the reference's (up to float ties at the threshold).
+    `record`, a list, receives (cand, touched) per round. Returns (Z, R, converged)."""
+    n = Z.shape[0]
+    dev, dt = Z.device, Z.dtype
+    diag = sys.diag.to(dt).contiguous()
+    eps_d = torch.as_tensor(eps, dtype=F64, device=dev)
+    flags = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+    mark = torch.zeros(max(n, 1), dtype=torch.uint8, device=dev)
+    cand = kernels.flatnonzero(kernels.violating(R, diag, eps_d, out=flags))
+    e0, it, best, stall = int(ops.edges), 0, float("inf"), 0
+    D = torch.empty((max(n, 1), Z.shape[1]), dtype=dt, device=dev)
+    while cand.numel() and it < max_iter:
+        kernels.push_take(cand, Z, R, diag, D[: cand.numel()], mark)
+        ops.push(cand, D[: cand.numel()], R, mark)
+        touched = kernels.flatnonzero(mark)
+        viol = kernels.violating(R, diag, eps_d, idx=touched, clear_mark=mark, out=flags)
+        if record is not None:
+            record.append((cand.clone(), touched.clone()))
+        cand = kernels.flatnonzero(viol, idx=touched)
+        it += 1
+        if it % 32 == 0:
+            if budget_edges is not None and int(ops.edges) - e0 > budget_edges:
+                break
+            v = violation(sys, R, eps_d)
+            best, stall = (v, 0) if v < 0.99 * best else (best, stall + 1)
+            if stall >= 8:
+                break
+    st.iters += it
+    return Z, R, cand.numel() == 0
+
+
+def predict(F, K):
+    """dynlp/solvers.py:166-167."""
+    return (F[:, 0] > 0.5).to(torch.int32) if K == 2 else F.argmax(dim=1).to(torch.int32)
+
+
+class Solver:
+    name = "base"
+
+    def __init__(self, n_total, K, dtype="float32", store_dtype=None):
+        from .backend import to_dtype
+        self.n_total, self.K, self.dtype = n_total, K, to_dtype(dtype)
+        self.store_dtype, self.C, self.F = to_dtype(store_dtype or dtype), 1 if K == 2 else K, None
+
+    def _warm(self, sys: System):
+        if self.F is None:
+            self.F = torch.empty((self.n_total, self.C), dtype=self.store_dtype, device=sys.diag.device)
+            self.F[:] = sys.prior.to(self.store_dtype)
+        return self.F[sys.U].to(self.dtype)
+
+    def _store(self, sys: System, X):
+        self.F[sys.U] = X.to(self.store_dtype)
+
+    def scores(self, sys: System):
+        return self.F[sys.U]
+
+
+class DynLP(Solver):
+    """DynLP's frontier Jacobi (Algorithm 2, dynlp/solvers.py:213-241) on the frontier kernels: the
+    frontier starts at the seed rows; each round updates the rows that changed by more than delta
+    and the next frontier is their neighbourhood. (The paper's tau-component initialisation of new
+    vertices is not run: new rows start at the prior.)"""
+
+    def __init__(self, n_total, K, dtype="float32", delta=1e-4, group="auto", comp="tau", max_iter=10**7):
+        super().__init__(n_total, K, dtype)
+        self.delta, self.group, self.comp, self.max_iter = delta, group, comp, max_iter
+        self.name = "dynlp" if comp == "tau" else f"dynlp-{comp}"
+
+    def solve(self, sys, record=None):
+        st, sys = Stats(path="frontier-jacobi"), sys.astype(self.dtype)
+        with Timer() as tm:
+            X = self._warm(sys).contiguous()
+            ops = FrontierOps(sys.W, self.C, self.group)
+            n = X.shape[0]
+            frontier = kernels.flatnonzero(sys.seed.to(torch.uint8))
+            mark = torch.zeros(max(n, 1), dtype=torch.uint8, device=X.device)
+            while frontier.numel() and st.iters < self.max_iter:
+                if record is not None:
+                    record.append(frontier.clone())
+                Y, ch = ops.jacobi(frontier, X, sys.rhs, sys.diag, self.delta)
+                st.iters += 1
+                chu = ch.to(torch.uint8)
+                upd = kernels.flatnonzero(chu, idx=frontier)
+                if not upd.numel():
+                    break
+                X[upd.long()] = Y[ch]
+                mark.zero_()
+                mark[upd.long()] = 1
+                ops.mark_neighbors(upd, mark)
+                frontier = kernels.flatnonzero(mark)
+            self._store(sys, X)
+        st.edges, st.ms = int(ops.edges), tm.ms
+        return st
+
+
+class DynLPPlus(Solver):
+    """Certified DynLP+: guarantees ||F - F*||_inf <= tol on every batch (dynlp/solvers.py:244-343)."""
+
+    def __init__(self, n_total, K, dtype="float32", method="auto", tol=1e-3, eps_h=0.05, group="auto",
+                 push_frac=0.05, push_budget=30.0, amg_hmax=2000.0, max_iter=100_000, amg_opts=None,
+                 target_relres=None):
+        super().__init__(n_total, K, dtype, store_dtype="float64")  # float64 master copy of F and h
+        self.method, self.tol, self.eps_h, self.group = method, tol, eps_h, group
+        self.push_frac, self.push_budget, self.amg_hmax = push_frac, push_budget, amg_hmax
+        self.max_iter, self.amg_opts = max_iter, amg_opts or {}
+        self.target_relres = target_relres
+        self.name, self.H, self.hmax = f"dynlp+{method}", None, None
+
+    def _use_amg(self):
+        return self.method == "amg" or (self.method == "auto" and (self.hmax or float("inf")) > self.amg_hmax)
+
+    def _precond(self, sys, st, amg_box):
+        if not self._use_amg():
+            return jacobi_M(sys), 0
+        if amg_box[0] is None:
+            from .amg import AMG
+            with Timer() as t:
+                amg_box[0] = AMG(sys.W, sys.s, **self.amg_opts)
+            st.setup_ms += t.ms
+            st.edges += 10 * sys.nnz
+        return amg_box[0], amg_box[0].work_per_apply
+
+    def _global(self, sys, Z, rhs, eps, st, amg_box, **kw):
+        M, wm = self._precond(sys, st, amg_box)
+        return pcg(sys, Z, rhs, eps, M, self.max_iter, st, wm, **kw)
+
+    def _run(self, sys, Z, rhs, eps, ops, st, amg_box, **kw):
+        """auto: push when few rows violate, else PCG/AMG (dynlp/solvers.py:272-288)."""
+        if self.method != "auto":
+            st.path = self.method
+            return self._global(sys, Z, rhs, eps, st, amg_box, **kw)
+        R = residual(sys, Z, rhs)
+        st.edges += sys.nnz
+        n = Z.shape[0]
+        eps_d = torch.as_tensor(eps, dtype=F64, device=Z.device)
+        frac = int(kernels.flatnonzero(kernels.violating(R, sys.diag, eps_d)).numel()) / max(n, 1)
+        if n and frac > self.push_frac:
+            st.path = "amg" if self._use_amg() else "pcg"
+            return self._global(sys, Z, rhs, eps, st, amg_box, **kw)
+        Z, R, ok = push(sys, Z, R, eps, ops, st, self.push_budget * max(sys.nnz, 1))
+        st.path = "push"
+        if ok and not kw.get("target_relres"):
+            return Z
+        st.path = "push+amg" if self._use_amg() else "push+pcg"
+        return self._global(sys, Z, rhs, eps, st, amg_box, **kw)
+
+    def _floor(self, scale=1.0):
+        """Smallest residual ratio the working precision resolves (dynlp/solvers.py:290-293)."""
+        u = 1e-7 if self.dtype == torch.float32 else 2e-16
+        return min(0.5, max(20 * u, 10 * u * scale))
+
+    def _bound(self, rc, h_est):
+        """(hmax, bound) from the column residual ratios (dynlp/solvers.py:295-301)."""
+        C = self.C
+        if rc[C] > self.eps_h:
+            return h_est, float("inf")
+        hmax = h_est / (1 - float(rc[C]))
+        return hmax, float(max(rc[:C])) * hmax
+
+    def _relres_ok(self, R64, rhs_norm):
+        if self.target_relres is None:
+            return True, float("nan")
+        rel = (col_norms(R64[:, : self.C]) / rhs_norm).max().item()
+        return rel <= self.target_relres, rel
+
+    def _refine(self, sw, s64, Z64, rhs64, ops, st, amg_box, rounds, rhs_norm, R64=None):
+        """fp64 certification and refinement (dynlp/solvers.py:322-337): R64 = rhs - A Z64; if the
+        certificate (or the relative residual) falls short, solve A D = R64 / scale in the working
+        precision and add D * scale. Returns (Z64, R64, hmax, bound, relres)."""
+        C = self.C
+        hmax, bound, rel = self.hmax, float("inf"), float("nan")
+        dev = Z64.device
+        for _ in range(rounds):
+            if R64 is None:
+                R64 = residual(s64, Z64, rhs64)
+                st.edges += s64.nnz
+            rc = rho_cols(s64, R64).cpu().tolist()
+            h_est = float(kernels.colreduce(3, Z64[:, C:]).item())
+            hmax, bound = self._bound(rc, h_est)
+            ok_rel, rel = self._relres_ok(R64, rhs_norm)
+            if bound <= self.tol and ok_rel:
+                break
+            scale = [r if r > 0 else 1.0 for r in rc]
+            sc = torch.tensor(scale, dtype=F64, device=dev)
+            eps_c = [min(max(e / s, self._floor(h_est)), 1.0) for e, s in
+                     zip([self.tol / (1.25 * hmax)] * C + [self.eps_h], scale)]
+            kw = {}
+            if self.target_relres is not None:
+                # the correction must bring the fp64 residual of every F column under the target, or
+                # as far as the working precision resolves in one round (the next round continues)
+                rnR = col_norms(R64[:, :C]).cpu().tolist()
+                fl = 3e-6 if self.dtype == torch.float32 else 1e-13
+                allowed = [max(0.5 * self.target_relres * float(rhs_norm[c]), fl * rnR[c], 1e-300) / scale[c]
+                           for c in range(C)]
+                kw = dict(target_relres=1.0, rhs_norm=allowed + [1e300])
+            Rs = _scratch("ref_Rs", Z64.shape[0], C + 1, self.dtype, dev)
+            _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs), ld(Rs),
+                      code(Rs), stream())
+            D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)
+            D.zero_()
+            D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, **kw)
+            _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(D), ld(D), code(D), ptr(sc), 1, ptr(Z64), ld(Z64),
+                      code(Z64), stream())
+            R64 = None
+        if R64 is None:
+            R64 = residual(s64, Z64, rhs64)
+            st.edges += s64.nnz
+            rc = rho_cols(s64, R64).cpu().tolist()
+            hmax, bound = self._bound(rc, float(kernels.colreduce(3, Z64[:, C:]).item()))
+            _, rel = self._relres_ok(R64, rhs_norm)
+        return Z64, R64, hmax, bound, rel
+
+    def _rhs_h(self, sys):
+        if sys.rhs_h is not None:
+            return sys.rhs_h
+        return torch.cat([sys.rhs, sys.diag[:, None]], dim=1).contiguous()
+
+    def solve(self, sys):
+        st, C, tol = Stats(), self.C, self.tol
+        sw, s64 = sys.astype(self.dtype), sys.astype(F64)
+        with Timer() as tm:
+            dev = sw.diag.device
+            n = sys.n_u
+            if self.H is None:
+                self.H = torch.zeros((self.n_total, 1), dtype=self.store_dtype, device=dev)
+            X = self._warm(sw)
+            Hc = self.H[sw.U].to(self.dtype)
+            Z = padded_empty(n, C + 1, self.dtype, dev)
+            Z[:, :C] = X
+            Z[:, C:] = Hc
+            rhs = self._rhs_h(sw)
+            ops, amg_box, hmax = FrontierOps(sw.W, C + 1, self.group), [None], self.hmax
+            if hmax is None and n:  # first batch: get h before choosing the label tolerance
+                M, wm = self._precond(sw, st, amg_box) if self.method == "amg" else (jacobi_M(sw), 0)
+                Zh = padded_empty(n, 1, self.dtype, dev)
+                Zh.copy_(Z[:, C:])
+                Zh = pcg(sw, Zh, rhs[:, C:].contiguous(), [self.eps_h], M, self.max_iter, st, wm)
+                Z[:, C:] = Zh
+                hmax = float(Zh.max().item()) / (1 - self.eps_h)
+            self.hmax = hmax = hmax or 1.0
+            eps = [max(tol / (1.25 * hmax), self._floor())] * C + [max(self.eps_h, self._floor(hmax))]
+            rhs64 = self._rhs_h(s64)
+            rn = col_norms(rhs64[:, :C]) if self.target_relres is not None else None
+            kw = {}
+            if self.target_relres is not None:
+                kw = dict(target_relres=self.target_relres, rhs_norm=rn.cpu().tolist() + [1e300])
+            Z = self._run(sw, Z, rhs, eps, ops, st, amg_box, **kw)
+            Z64 = padded_empty(n, C + 1, F64, dev)
+            Z64.copy_(Z)
+            if n:
+                Z64, R64, hmax, bound, rel = self._refine(sw, s64, Z64, rhs64, ops, st, amg_box,
+                                                          10 if self.dtype == torch.float32 else 2, rn)
+            else:
+                R64, bound, rel = None, 0.0, 0.0
+            st.cert, st.hmax, self.hmax, st.relres = bound, hmax, hmax, rel
+            self._store(sw, Z64[:, :C])
+            self.H[sw.U] = Z64[:, C:]
+            self._Z64, self._R64 = Z64, R64
+        st.edges += int(ops.edges)
+        st.ms = tm.ms
+        return st
+
+
+class IncrementalLP(DynLPPlus):
+    """Certified DynLP+ with resident state on a global-index system (dynlp/solvers.py:346-434).
+
+    Keeps Z = [F, h] and its fp64 residual R between batches; a batch refreshes R on its changed
+    rows only (one fused SpMM over those rows), small changes are repaired by push and larger ones
+    by the working-precision PCG correction with fp64 refinement; R is recomputed in full every
+    `full_every` batches to bound drift."""
+
+    def __init__(self, n_total, K, dtype="float32", tol=1e-3, full_every=16, max_rounds=50_000, method="auto",
+                 **kw):
+        super().__init__(n_total, K, dtype, method=method, tol=tol, **kw)
+        self.name, self.full_every, self.max_rounds = "dynlp+inc", full_every, max_rounds
+        self.Z = self.R = None
+        self.since_full = 0
+
+    def _full_residual(self, s64, st):
+        self.R = residual(s64, self.Z, self._rhs_h(s64), out=self.R)
+        st.edges += s64.nnz
+        self.since_full = 0
+
+    def _park(self, s64, rows):
+        if rows is not None and rows.numel():
+            h0 = float(self.hmax or 1.0)
+            _lib.call("dlp_park_rows", ptr(rows), int(rows.numel()), ptr(s64.solved.to(torch.uint8)), self.C, 1,
+                      ptr(s64.prior.to(F64).contiguous()), h0, ptr(self.Z), ld(self.Z), ptr(self.R), ld(self.R),
+                      stream())
+
+    def solve(self, sys):
+        if sys.solved is None:
+            raise ValueError("dynlp+inc needs a global-index system (EdgeStream)")
+        s64, C, tol, st = sys.astype(F64), self.C, self.tol, Stats(path="inc-push")
+        sw = sys.astype(self.dtype)
+        with Timer() as tm:
+            rhs64 = self._rhs_h(s64)
+            rn = col_norms(rhs64[:, :C]) if self.target_relres is not None else None
+            if self.Z is None:
+                inner = DynLPPlus.solve(self, sys)
+                st.iters, st.edges, st.setup_ms, st.path = inner.iters, inner.edges, inner.setup_ms, "inc-" + inner.path
+                self.Z, self.R = self._Z64, self._R64
+                st.cert, st.hmax, st.relres = inner.cert, inner.hmax, inner.relres
+                self.since_full = 0
+            else:
+                self._park(s64, sys.moved)
+                Q = sys.changed
+                if Q is not None and Q.numel():
+                    residual(s64, self.Z, rhs64, out=self.R, rows=Q)
+                    st.edges += int(Q.numel()) * max(int(s64.nnz / max(s64.n_u, 1)), 1)
+                self.since_full += 1
+                if self.since_full >= self.full_every:
+                    self._full_residual(s64, st)
+                amg_box = [None]
+                ops = FrontierOps(sw.W, C + 1, self.group)
+                rc = rho_cols(s64, self.R).cpu().tolist()
+                h_est = float(kernels.colreduce(3, self.Z[:, C:]).item())
+                hmax, bound = self._bound(rc, h_est)
+                ok_rel, rel = self._relres_ok(self.R, rn)
+                st.path = "inc-none"
+                if not (bound <= tol and ok_rel):
+                    eps = [tol / (1.25 * (self.hmax or 1.0))] * C + [self.eps_h]
+                    eps_d = torch.as_tensor(eps, dtype=F64, device=self.Z.device)
+                    nviol = int(kernels.flatnonzero(kernels.violating(self.R, s64.diag, eps_d)).numel())
+                    small = nviol / max(s64.n_solved, 1) <= self.push_frac and self.method in ("auto", "push")
+                    if small and self.target_relres is None:
+                        st.path = "inc-push"
+                        for _ in range(4):
+                            _, _, ok = push(s64, self.Z, self.R, eps, FrontierOps(s64.W, C + 1, self.group), st,
+                                            max_iter=self.max_rounds)
+                            hmax, bound = self._bound(rho_cols(s64, self.R).cpu().tolist(),
+                                                      float(kernels.colreduce(3, self.Z[:, C:]).item()))
+                            if ok and bound <= tol:
+                                break
+                            eps = [tol / (1.25 * hmax)] * C + [self.eps_h]
+                        rel = float("nan")
+                    if not (bound <= tol and (small and self.target_relres is None)):
+                        st.path = "inc-" + ("pcg" if self.method in ("auto", "pcg", "push") else self.method)
+                        self.Z, self.R, hmax, bound, rel = self._refine(sw, s64, self.Z, rhs64, ops, st, amg_box, 10,
+                                                                        rn, R64=self.R)
+                st.cert, st.hmax, self.hmax, st.relres = bound, hmax, hmax, rel
+            self.F, self.H = self.Z[:, :C], self.Z[:, C:]
+        st.ms = tm.ms
+        return st
+
+
+class Reference:
+    """High-accuracy float64 solution F* and absorption bound (dynlp/solvers.py:437-445)."""
+
+    def __init__(self, n_total, K, tol=1e-8, method="pcg"):
+        self.inner = DynLPPlus(n_total, K, "float64", method=method, tol=tol, eps_h=1e-6, max_iter=100_000)
+
+    def solve(self, sys):
+        st = self.inner.solve(sys)
+        return self.inner.scores(sys), self.inner.hmax, st
+
+
+def make(name, n_total, K, *, dtype, delta, tol, group, max_iter=None):
+    """dynlp/solvers.py:448-458."""
+    kw = {} if max_iter is None else {"max_iter": max_iter}
+    if name in ("dynlp", "dynlp-fh"):
+        return DynLP(n_total, K, dtype, delta, group, comp="fh" if name == "dynlp-fh" else "tau", **kw)
+    if name == "dynlp+inc":
+        return IncrementalLP(n_total, K, dtype, tol=tol, group=group, **kw)
+    if name.startswith("dynlp+"):
+        return DynLPPlus(n_total, K, dtype, method=name.split("+", 1)[1], tol=tol, group=group, **kw)
+    raise ValueError(f"unknown solver {name!r}")
+
+
+SOLVERS = ["dynlp", "dynlp-fh", "dynlp+pcg", "dynlp+amg", "dynlp+auto", "dynlp+inc"]

@@ -1,0 +1,378 @@
+"""The per-batch linear system and the edge-update stream (mirrors dynlp/stream.py).
+
+Per batch, the harmonic system on the active unlabelled set U (dynlp/stream.py:1-6):
+    (diag - W_UU) F_U = rhs,   diag = s + rowsum(W_UU),   s = w(u, L) + eta
+Binary problems solve one column (class 1); K classes solve K columns.
+
+* `System`: the reference's dataclass (stream.py:17-58) with torch tensors.
+* `build_system`: `Stream._build` (stream.py:142-177) on the device: grounding by connected
+  components with the labelled vertices as a sink, U x U filter in CSR order, B = A @ onehot.
+* `ResidentGraph`: the graph kept on the device with per-row slack so edges can be inserted in
+  place; it is accepted as `W` by every row kernel.
+* `EdgeStream`: the resident global-index system (the `IncrementalStream` form, stream.py:180-346:
+  inert rows have diag 1, rhs 0 and no live entries) updated by edge batches through
+  `apply_edges`, the new entry point of the edge-update workload.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+import torch
+
+from . import _lib, cc, kernels
+from .backend import CSR, code, ld, ptr, stream, to_dtype, workspace
+from .graphs import Dataset, csr_rows
+
+
+@dataclass
+class System:
+    t: int
+    U: torch.Tensor          # global ids of the rows (sorted)
+    W: object                # CSR U x U (or the resident graph for global-index systems)
+    s: torch.Tensor          # grounding
+    diag: torch.Tensor       # s + rowsum(W)
+    B: torch.Tensor          # (n_u, K) weight to labelled neighbours per class
+    rhs: torch.Tensor        # (n_u, C)
+    prior: torch.Tensor      # (C,)
+    is_new: torch.Tensor     # rows not in U at the previous batch
+    seed: torch.Tensor       # rows whose equation changed (DynLP's affected set)
+    comps: dict
+    K: int
+    C: int
+    eta: float
+    n_inserted: int
+    n_deleted: int
+    n_active: int
+    n_ungrounded: int = 0
+    solved: object = None    # global-index systems: rows really solved (others inert)
+    changed: object = None   # global-index systems: rows whose equation changed
+    moved: object = None     # global-index systems: rows that entered or left U this batch
+    rhs_h: object = None     # (n, C+1) [rhs | diag], the DynLP+ right-hand side with the h column
+    _conv: dict = field(default_factory=dict, repr=False, compare=False)
+
+    n_u = property(lambda self: int(self.U.numel()))
+    nnz = property(lambda self: int(self.W.nnz))
+
+    @property
+    def n_solved(self) -> int:
+        return self.n_u if self.solved is None else int(self.solved.sum().item())
+
+    def label_cols(self, M):
+        """Columns of a (., K) class matrix that are solved (class 1 if binary)."""
+        return M[:, 1:2] if self.K == 2 else M
+
+    def astype(self, dtype) -> "System":
+        """Same system in another precision (cached; index arrays shared) (stream.py:49-58)."""
+        dt = to_dtype(dtype)
+        if dt == self.diag.dtype:
+            return self
+        if dt not in self._conv:
+            cast = {k: getattr(self, k).to(dt) for k in ("s", "diag", "B", "rhs", "prior")}
+            W = self.W.astype(dt) if isinstance(self.W, CSR) and dt != torch.float64 else self.W
+            rh = self.rhs_h.to(dt) if self.rhs_h is not None else None
+            self._conv[dt] = replace(self, W=W, rhs_h=rh, _conv={}, **cast)
+        return self._conv[dt]
+
+
+def _onehot_labels(y, lab_mask, K, dev):
+    n = y.numel()
+    X = torch.zeros((n, K), dtype=torch.float64, device=dev)
+    li = torch.nonzero(lab_mask, as_tuple=False).flatten()
+    X[li, y[li].long()] = 1.0
+    return X
+
+
+def build_system(ds: Dataset, active, labeled, *, eta=0.0, dtype="float32", t=0, prev_U=None, ins=0, dele=0):
+    """The grounded system of one batch (Stream._build, dynlp/stream.py:142-177), on the device.
+
+    U = active unlabelled vertices whose component (within the active unlabelled subgraph) holds
+    label weight; W = A[U, U] in CSR order; B = A @ onehot(y_L); s = sum(B) + eta; diag = s +
+    rowsum(W); rhs = B (class 1 when K == 2) + eta * prior. The new-vertex components and DynLP's
+    seed set are not built (they serve the vertex-arrival warm start)."""
+    A, K = ds.A, ds.K
+    dev = A.indices.device
+    n = A.shape[0]
+    dt = to_dtype(dtype)
+    active = active.to(torch.bool)
+    labeled = labeled.to(torch.bool)
+    al = active & labeled
+    Bfull = kernels.spmm_axpy(A, _onehot_labels(ds.y, al, K, dev))  # fp64 (fp32 weights x fp64 onehot)
+    vmask = (active & ~labeled).to(torch.uint8)
+    parent, err = cc.graph_components(A, vmask, al.to(torch.uint8))
+    root = parent[n]
+    Um = vmask.bool() & (parent[:n] == root)
+    n_ungrounded = int((vmask.bool() & ~Um).sum().item())
+    U = torch.nonzero(Um, as_tuple=False).flatten()
+    n_u = int(U.numel())
+    loc = torch.full((n,), -1, dtype=torch.int64, device=dev)
+    loc[U] = torch.arange(n_u, device=dev)
+    rows = csr_rows(A).long()
+    cols = A.indices.long()
+    keep = Um[rows] & Um[cols]
+    indptr = torch.zeros(n_u + 1, dtype=torch.int64, device=dev)
+    indptr[1:] = torch.cumsum(torch.bincount(loc[rows[keep]], minlength=n_u), 0)
+    W = CSR(A.data[keep].to(dt), loc[cols[keep]].to(torch.int32), indptr.to(torch.int32), (n_u, n_u))
+    Bm = Bfull[U]
+    s = Bm.sum(dim=1) + eta
+    rowsum = torch.zeros(n_u, dtype=torch.float64, device=dev)
+    if n_u:
+        _lib.call("dlp_graph_rowsum", ptr(W.rbeg), ptr(W.rend), ptr(W.data.float() if dt != torch.float32 else W.data),
+                  None, n_u, ptr(rowsum), stream())
+    diag = s + rowsum
+    prior = torch.full((1 if K == 2 else K,), 0.5 if K == 2 else 1.0 / K, dtype=torch.float64, device=dev)
+    rhs = (Bm[:, 1:2] if K == 2 else Bm) + eta * prior[None, :]
+    is_new = torch.ones(n_u, dtype=torch.bool, device=dev) if prev_U is None else ~prev_U[U]
+    sysd = dict(t=t, U=U, W=W, s=s.to(dt), diag=diag.to(dt), B=Bm.to(dt), rhs=rhs.to(dt).contiguous(),
+                prior=prior.to(dt), is_new=is_new, seed=is_new.clone(), comps={}, K=K, C=1 if K == 2 else K, eta=eta,
+                n_inserted=ins, n_deleted=dele, n_active=int(active.sum().item()), n_ungrounded=n_ungrounded)
+    sysd["rhs_h"] = torch.cat([sysd["rhs"], sysd["diag"][:, None]], dim=1).contiguous()
+    S = System(**sysd)
+    if dt != torch.float64:
+        S._conv[torch.float64] = System(**{**sysd, "W": CSR(W.data.to(torch.float32), W.indices, W.indptr, W.shape),
+                                           "s": s, "diag": diag, "B": Bm, "rhs": rhs.contiguous(),
+                                           "prior": prior, "rhs_h": torch.cat([rhs, diag[:, None]], 1).contiguous()})
+    return S
+
+
+class ResidentGraph:
+    """Slack-padded rows on the device. Row r owns slots [rbeg[r], rcap[r]); [rbeg[r], rend[r]) are
+    stored entries. `aw` = edge weights (0 = deleted), `data` = the solver operator W_UU."""
+
+    def __init__(self, A: CSR, slack_frac=0.25, slack_min=4):
+        self._build_from(A.indptr, A.indices, A.data.to(torch.float32), A.shape[0], slack_frac, slack_min)
+
+    def _build_from(self, indptr, indices, aw, n, slack_frac, slack_min):
+        dev = indices.device
+        indptr = indptr.long()
+        deg = torch.diff(indptr)
+        cap = deg + torch.clamp((deg.double() * slack_frac).ceil().long(), min=slack_min)
+        rbeg = torch.zeros(n, dtype=torch.int64, device=dev)
+        if n > 1:
+            rbeg[1:] = torch.cumsum(cap, 0)[:-1]
+        total = int(cap.sum().item()) if n else 0
+        if total >= 2**31:
+            raise ValueError("graph too large for int32 slot offsets")
+        rows = torch.repeat_interleave(torch.arange(n, device=dev), deg)
+        pos = rbeg[rows] + (torch.arange(indices.numel(), device=dev) - indptr[rows])
+        self.indices = torch.full((max(total, 1),), -1, dtype=torch.int32, device=dev)
+        self.aw = torch.zeros(max(total, 1), dtype=torch.float32, device=dev)
+        self.indices[pos] = indices.to(torch.int32)
+        self.aw[pos] = aw
+        self.data = torch.zeros_like(self.aw)
+        self.rbeg = rbeg.to(torch.int32)
+        self.rend = (rbeg + deg).to(torch.int32)
+        self.rcap = (rbeg + cap).to(torch.int32)
+        self.shape = (n, n)
+        self.slack_frac, self.slack_min = slack_frac, slack_min
+        self._slot_rows = None
+
+    @property
+    def nnz(self) -> int:
+        return int((self.rend - self.rbeg).sum().item())
+
+    @property
+    def dtype(self):
+        return self.data.dtype
+
+    def astype(self, dtype):
+        return self
+
+    def slot_rows(self):
+        """Row of every slot (for setup-time masking)."""
+        cap = (self.rcap - self.rbeg).long()
+        return torch.repeat_interleave(torch.arange(self.shape[0], device=self.rbeg.device), cap)
+
+    def rebuild(self, grow=2.0):
+        """Repack with more slack (after a row overflowed); tombstones are dropped."""
+        n = self.shape[0]
+        slots = self.slot_rows()
+        rbeg_l = self.rbeg.long()[slots]
+        j = torch.arange(slots.numel(), device=slots.device)
+        live = (j < self.rend.long()[slots]) & (self.aw[: slots.numel()] != 0)
+        rows = slots[live]
+        deg = torch.bincount(rows, minlength=n)
+        indptr = torch.zeros(n + 1, dtype=torch.int64, device=slots.device)
+        indptr[1:] = torch.cumsum(deg, 0)
+        del rbeg_l
+        w_live = self.data[: slots.numel()][live]
+        self._build_from(indptr, self.indices[: slots.numel()][live], self.aw[: slots.numel()][live], n,
+                         self.slack_frac * grow + 0.25, self.slack_min * 2)
+        slots = self.slot_rows()
+        j = torch.arange(slots.numel(), device=slots.device)
+        live_new = j < self.rend.long()[slots]
+        self.data[: slots.numel()][live_new] = w_live
+
+    def to_csr(self, which="aw", drop_zero=True) -> CSR:
+        """Compact CSR of the stored entries (column order within rows as stored)."""
+        n = self.shape[0]
+        slots = self.slot_rows()
+        j = torch.arange(slots.numel(), device=slots.device)
+        vals = (self.aw if which == "aw" else self.data)[: slots.numel()]
+        live = j < self.rend.long()[slots]
+        if drop_zero:
+            live &= vals != 0
+        rows = slots[live]
+        indptr = torch.zeros(n + 1, dtype=torch.int64, device=slots.device)
+        indptr[1:] = torch.cumsum(torch.bincount(rows, minlength=n), 0)
+        return CSR(vals[live].clone(), self.indices[: slots.numel()][live].clone(), indptr.to(torch.int32), (n, n))
+
+
+class EdgeStream:
+    """The resident grounded system under edge-update batches (global vertex ids).
+
+    Mirrors IncrementalStream (dynlp/stream.py:180-346) for an edge stream: every vertex keeps its
+    global id, rows outside U (labelled or in a component without labels) are inert (diag 1, rhs 0,
+    no live solver entries), and each batch is applied in place on the device:
+      1. deletions, then insertions, into the resident graph (weights, row sums, label weights);
+      2. connected components of the unlabelled subgraph with the labelled vertices as a sink: the
+         vertices whose component holds no label leave U, newly grounded ones enter it;
+      3. the equations (s, diag, rhs and the h column's rhs) of every changed row are rebuilt.
+    `system` is a System whose arrays stay live until the next batch; `changed` lists the rows whose
+    equation changed and `moved` the rows that entered or left U.
+    """
+
+    def __init__(self, ds: Dataset, labeled, *, eta_rel=0.0, dtype="float32", with_h=True, slack_frac=0.25,
+                 active=None):
+        A, K = ds.A, ds.K
+        self.ds, self.K, self.dtype = ds, K, to_dtype(dtype)
+        self.C = 1 if K == 2 else K
+        self.col0 = 1 if K == 2 else 0
+        self.with_h = with_h
+        n = A.shape[0]
+        dev = A.indices.device
+        self.n, self.dev = n, dev
+        self.G = ResidentGraph(A, slack_frac=slack_frac)
+        labeled = labeled.to(torch.bool)
+        active = torch.ones(n, dtype=torch.bool, device=dev) if active is None else active.to(torch.bool)
+        self.labeled = (labeled & active).to(torch.uint8)
+        self.vmask = (active & ~labeled).to(torch.uint8)
+        self.y = ds.y.to(torch.int32).contiguous()
+        self.eta = float(eta_rel * float(A.data.double().sum().item()) / max(n, 1))
+        self.prior64 = torch.full((self.C,), 0.5 if K == 2 else 1.0 / K, dtype=torch.float64, device=dev)
+        # label weights B = A @ onehot(y_L) (fp64)
+        self.B = kernels.spmm_axpy(A, _onehot_labels(self.y, self.labeled.bool(), K, dev)).contiguous()
+        # grounding and the masked operator
+        self.umask = torch.zeros(n, dtype=torch.uint8, device=dev)
+        self.in_t = torch.zeros(n, dtype=torch.uint8, device=dev)
+        self.changed = torch.zeros(n, dtype=torch.uint8, device=dev)
+        self._stat = torch.zeros(8, dtype=torch.int32, device=dev)
+        self._ground()
+        sr = self.G.slot_rows()
+        um = self.umask.bool()
+        colv = self.G.indices[: sr.numel()].long().clamp(min=0)
+        self.G.data[: sr.numel()] = torch.where(um[sr] & um[colv], self.G.aw[: sr.numel()],
+                                                torch.zeros_like(self.G.aw[: sr.numel()]))
+        self.rowsum = torch.zeros(n, dtype=torch.float64, device=dev)
+        _lib.call("dlp_graph_rowsum", ptr(self.G.rbeg), ptr(self.G.rend), ptr(self.G.data), None, n,
+                  ptr(self.rowsum), stream())
+        ch = self.C + (1 if with_h else 0)
+        self.ld64 = ch + (ch & 1)
+        self.ld32 = (ch + 3) // 4 * 4
+        self.diag64 = torch.empty(n, dtype=torch.float64, device=dev)
+        self.rhs64 = torch.zeros((n, self.ld64), dtype=torch.float64, device=dev)
+        self.diag32 = torch.empty(n, dtype=torch.float32, device=dev)
+        self.rhs32 = torch.zeros((n, self.ld32), dtype=torch.float32, device=dev)
+        self._system_rows(None, n)
+        self.t = 0
+        self.last_changed = torch.arange(n, dtype=torch.int32, device=dev)
+        self.last_moved = torch.zeros(0, dtype=torch.int32, device=dev)
+        self.counters = {"rebuilds": 0, "ground_changes": 0, "applied": 0}
+        self.n_ins = self.n_del = 0
+
+    # -- helpers -------------------------------------------------------------------------------
+    def _ground(self):
+        """umask = grounded unlabelled vertices; in_t flags membership changes; returns #changes."""
+        parent, err = cc.graph_components(self.G, self.vmask, self.labeled, w=self.G.aw)
+        self._stat[4].zero_()
+        _lib.call("dlp_ground_update", self.n, ptr(parent), ptr(self.vmask), ptr(self.umask), ptr(self.in_t),
+                  ptr(self._stat[4:5]), stream())
+        return parent
+
+    def _system_rows(self, rows, nr):
+        ch = self.C + (1 if self.with_h else 0)
+        _lib.call("dlp_system_rows", ptr(rows), nr, ptr(self.umask), ptr(self.B), self.K, ptr(self.rowsum),
+                  self.eta, ptr(self.prior64), self.C, self.col0, int(self.with_h), ptr(self.diag64),
+                  ptr(self.rhs64), self.ld64, ptr(self.diag32), ptr(self.rhs32), self.ld32, stream())
+        del ch
+
+    def _upload(self, x, dt):
+        if x is None:
+            return None
+        if torch.is_tensor(x):
+            return x.to(device=self.dev, dtype=dt, non_blocking=True).contiguous()
+        t = torch.from_numpy(np.ascontiguousarray(x)).to(dt)
+        if torch.cuda.is_available():
+            t = t.pin_memory()
+        return t.to(self.dev, non_blocking=True)
+
+    # -- the batch -----------------------------------------------------------------------------
+    def apply_edges(self, ins_u=None, ins_v=None, ins_w=None, del_u=None, del_v=None) -> System:
+        """Apply one edge batch (deletions, then insertions) and return the updated system."""
+        G, n = self.G, self.n
+        du, dv = self._upload(del_u, torch.int32), self._upload(del_v, torch.int32)
+        iu, iv = self._upload(ins_u, torch.int32), self._upload(ins_v, torch.int32)
+        iw = self._upload(ins_w, torch.float32)
+        nd = int(du.numel()) if du is not None else 0
+        ni = int(iu.numel()) if iu is not None else 0
+        self.changed.zero_()
+        self._stat.zero_()
+        st = self._stat
+        s = stream()
+        if nd:
+            _lib.call("dlp_graph_delete", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(du),
+                      ptr(dv), nd, ptr(self.umask), ptr(self.labeled), ptr(self.y), self.K, ptr(self.rowsum),
+                      ptr(self.B), ptr(self.changed), ptr(st[2:3]), ptr(st[0:1]), s)
+        if ni:
+            for attempt in range(4):
+                ws = workspace("insert").get(_lib.lib().dlp_graph_insert_workspace_bytes(ni))
+                st[1].zero_()
+                _lib.call("dlp_graph_insert", n, ptr(G.rbeg), ptr(G.rend), ptr(G.rcap), ptr(G.indices), ptr(G.aw),
+                          ptr(G.data), ptr(iu), ptr(iv), ptr(iw), ni, ptr(self.umask), ptr(self.labeled), ptr(self.y),
+                          self.K, ptr(self.rowsum), ptr(self.B), ptr(self.changed), ptr(st[1:2]), ptr(st[3:4]),
+                          ptr(st[0:1]), ptr(ws), ws.numel(), s)
+                if int(st[1].item()) == 0:
+                    break
+                G.rebuild()  # a row ran out of slack: repack with more and apply the batch again
+                self.counters["rebuilds"] += 1
+            else:
+                raise RuntimeError("edge insertion kept overflowing after repacking")
+        if int(st[0].item()):
+            raise ValueError(f"edge batch rejected: {_lib.STATUS.get(int(st[0].item()))} (vertex id out of range?)")
+        # grounding: components of the unlabelled subgraph with the labelled vertices as a sink
+        self._ground()
+        nmoved = int(st[4].item())
+        moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
+        if nmoved:
+            moved = kernels.flatnonzero(self.in_t)
+            _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(moved),
+                      int(moved.numel()), ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), s)
+            self.counters["ground_changes"] += nmoved
+        Q = kernels.flatnonzero(self.changed)
+        self._system_rows(Q, int(Q.numel()))
+        self.t += 1
+        self.last_changed, self.last_moved = Q, moved
+        self.n_ins, self.n_del = ni, nd
+        self.counters["applied"] += int(st[2].item()) + int(st[3].item())
+        return self.system
+
+    @property
+    def system(self) -> System:
+        """Global-index system of the current batch (arrays live until the next batch)."""
+        n, C, dev = self.n, self.C, self.dev
+        um = self.umask.bool()
+        s64 = self.diag64 - self.rowsum
+        common = dict(t=self.t, U=torch.arange(n, device=dev), W=self.G, is_new=torch.zeros(n, dtype=torch.bool,
+                      device=dev), seed=self.changed.bool(), comps={}, K=self.K, C=C, eta=self.eta,
+                      n_inserted=self.n_ins, n_deleted=self.n_del, n_active=int(self.vmask.sum().item() +
+                                                                               self.labeled.sum().item()),
+                      n_ungrounded=int((self.vmask.bool() & ~um).sum().item()), solved=um,
+                      changed=self.last_changed, moved=self.last_moved)
+        ch = C + (1 if self.with_h else 0)
+        S = System(s=s64.to(self.dtype), diag=self.diag32 if self.dtype == torch.float32 else self.diag64.to(self.dtype),
+                   B=self.B, rhs=self.rhs32[:, :C] if self.dtype == torch.float32 else self.rhs64[:, :C].to(self.dtype),
+                   prior=self.prior64.to(self.dtype), rhs_h=self.rhs32[:, :ch] if self.dtype == torch.float32 else None,
+                   **common)
+        S._conv[torch.float64] = System(s=s64, diag=self.diag64, B=self.B, rhs=self.rhs64[:, :C], prior=self.prior64,
+                                        rhs_h=self.rhs64[:, :ch], **common)
+        return S

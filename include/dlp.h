@@ -51,6 +51,8 @@ const char *dlp_status_string(int status);
 int dlp_last_cuda_error(void);
 /* number of SMs of the current device (used for persistent grid sizes) */
 int dlp_sm_count(void);
+/* kernels this library has launched in the process so far (graph replays count their kernels) */
+unsigned long long dlp_launch_count(void);
 
 /* ---- (a) row-major SpMM with fused axpy / residual epilogue -------------------------------
  * Replaces kernels.spmm_axpy (dynlp/kernels.py:140-166, :240-266, launcher :377-393),
@@ -167,6 +169,73 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
             double target_relres, int32_t mode, int32_t max_iter, int32_t patience, int32_t check_every,
             int32_t use_graph, double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, double *viol_out,
             double *relres_out, int32_t *status_out, dlp_stream_t stream);
+
+
+/* ---- (c) resident graph: edge-batch patch of the grounded system ---------------------------
+ * No reference counterpart for edge updates (the reference streams vertices); closest are
+ * IncrementalStream._toggle / _label_update (dynlp/stream.py:206-235). Row r owns slots
+ * [rbeg[r], rcap[r]) of col/aw/w, of which [rbeg[r], rend[r]) are stored entries. aw = graph edge
+ * weights (0 = deleted: a tombstone, revived by a later insertion of the edge); w = the solver
+ * operator W_UU (aw masked to 0 unless both ends are in U = umask). Each applied change updates
+ * rowsum[u] = sum_v w(u,v) and B[u, y_l] = sum of aw(u,l) over labelled l (both fp64, B n x K)
+ * and flags changed[u] for every solved row whose equation changed. Deletions (du, dv) and
+ * insertions (iu, iv, iw; iw == NULL: weight 1) are undirected; self-loops and absent deletions
+ * are ignored, an insertion of a present edge sets its weight, and among repeated insertions of
+ * one edge the largest batch index wins. *err (device int, caller-zeroed) reports endpoints out of
+ * range; *overflow = 1 when a row ran out of slack (the edges that did not fit are not applied
+ * and the graph stays consistent: rebuild with more slack and run the insertions again).
+ * *n_applied (device int, may be NULL) counts applied updates. */
+int dlp_graph_delete(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, float *aw, float *w,
+                     const int32_t *du, const int32_t *dv, int32_t nd, const uint8_t *umask, const uint8_t *labeled,
+                     const int32_t *y, int32_t K, double *rowsum, double *B, uint8_t *changed, int32_t *n_applied,
+                     int32_t *err, dlp_stream_t stream);
+size_t dlp_graph_insert_workspace_bytes(int32_t ni);
+int dlp_graph_insert(int32_t n, const int32_t *rbeg, int32_t *rend, const int32_t *rcap, int32_t *col, float *aw,
+                     float *w, const int32_t *iu, const int32_t *iv, const float *iw, int32_t ni,
+                     const uint8_t *umask, const uint8_t *labeled, const int32_t *y, int32_t K, double *rowsum,
+                     double *B, uint8_t *changed, int32_t *overflow, int32_t *n_applied, int32_t *err, void *ws,
+                     size_t ws_bytes, dlp_stream_t stream);
+
+/* Membership change of the vertices T[0..nt) (in_t[v] = 1 marks them; umask already holds the new
+ * U): solver weights of their entries and mirror entries follow umask, neighbours' row sums move
+ * by the difference and are flagged changed, and the row sums of T are recomputed
+ * (IncrementalStream._toggle, dynlp/stream.py:206-228). */
+int dlp_graph_toggle(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *aw, float *w,
+                     const int32_t *T, int32_t nt, const uint8_t *in_t, const uint8_t *umask, double *rowsum,
+                     uint8_t *changed, dlp_stream_t stream);
+
+/* rowsum[r] = sum of w over the stored entries of r, for r = rows[g] (rows == NULL: all nr rows). */
+int dlp_graph_rowsum(const int32_t *rbeg, const int32_t *rend, const float *w, const int32_t *rows, int32_t nr,
+                     double *rowsum, dlp_stream_t stream);
+
+/* The equations of the listed rows (rows == NULL: rows 0..nr-1) in the resident global-index form
+ * (dynlp/stream.py:329-331): solved rows (umask) get s = sum_c B[u,c] + eta, diag = s + rowsum[u],
+ * rhs[u, 0..C) = B[u, col0 .. col0+C) + eta * prior[0..C) (col0 = 1, C = 1 for the binary case,
+ * stream.py:331) and, with with_h, rhs[u, C] = diag (the h column, solvers.py:312-313); inert rows
+ * get diag = 1, rhs = 0 (rhs[u, C] = 1). prior is a device double[C]. fp32 copies optional. */
+int dlp_system_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, const double *B, int32_t K,
+                    const double *rowsum, double eta, const double *prior, int32_t C, int32_t col0, int32_t with_h,
+                    double *diag64, double *rhs64, int64_t ldr64, float *diag32, float *rhs32, int64_t ldr32,
+                    dlp_stream_t stream);
+
+/* Scores of rows whose membership changed: solved rows start at (prior, h0); inert rows get their
+ * exact values F = 0, h = 1 (IncrementalLP._park, dynlp/solvers.py:365-368); R rows are zeroed. */
+int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t C, int32_t with_h,
+                  const double *prior, double h0, double *Z, int64_t ldz, double *R, int64_t ldr,
+                  dlp_stream_t stream);
+
+
+/* ---- vector helpers of the refinement loop (dynlp/solvers.py:333-337) and grounding ---------
+ * op 0: Y = X / scale[c] (the scaled residual, cast to Y's precision); op 1: Y += X * scale[c]
+ * (Z64 += D * scale); op 2: Y = X * scale[c]. scale is a device double[C]. Precisions: f32/f64. */
+int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
+                   void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream);
+
+/* After dlp_cc_graph with the labelled vertices as sink: umask[v] = vmask[v] && parent[v] ==
+ * parent[n] (the grounded vertices, dynlp/stream.py:150-159, :275-280); in_t[v] = 1 where membership
+ * changed; *count (device int, caller-zeroed) += number of changes. */
+int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, uint8_t *umask, uint8_t *in_t,
+                      int32_t *count, dlp_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -27,7 +27,7 @@ def _header_functions():
                     codes += "q"
                 elif a.startswith("double"):
                     codes += "d"
-                elif a.startswith("size_t"):
+                elif a.startswith(("size_t", "unsigned long long")):
                     codes += "z"
                 else:
                     raise AssertionError(f"unhandled parameter type in {name}: {a}")

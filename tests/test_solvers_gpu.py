@@ -1,0 +1,202 @@
+"""Solvers, system assembly and the edge stream against the reference's outputs (golden fixtures)
+and the oracle (GPU)."""
+import numpy as np
+import pytest
+import scipy.sparse as ssp
+import scipy.sparse.linalg as sla
+import torch
+
+from conftest import golden_csr, load_golden
+from dynlplus_b200 import graphs, kernels, solvers, stream
+from dynlplus_b200.backend import CSR
+from oracle import ref_np as O
+
+pytestmark = pytest.mark.gpu
+
+
+def T(x, dt=None):
+    t = torch.as_tensor(np.ascontiguousarray(x))
+    return (t.to(dt) if dt is not None else t).cuda()
+
+
+def golden_system(dt=torch.float64):
+    g = load_golden("solvers.npz")
+    A = golden_csr(g, "W")
+    n = A.shape[0]
+    S = stream.System(t=0, U=torch.arange(n, device="cuda"), W=CSR.from_scipy(A, dtype=dt), s=T(g["diag"], dt),
+                      diag=T(g["diag"], dt), B=T(g["rhs"], dt), rhs=T(g["rhs"], dt), prior=T(np.full(3, 1 / 3), dt),
+                      is_new=torch.zeros(n, dtype=torch.bool, device="cuda"),
+                      seed=torch.zeros(n, dtype=torch.bool, device="cuda"), comps={}, K=3, C=3, eta=0.0,
+                      n_inserted=0, n_deleted=0, n_active=n)
+    return g, A, S
+
+
+@pytest.mark.parametrize("b", [0, 2])
+def test_build_system_matches_reference(b):
+    g = load_golden("system.npz")
+    p = f"b{b}"
+    A = golden_csr(g, f"{p}_A")
+    ds = graphs.Dataset("fixture", CSR.from_scipy(A), T(g[f"{p}_y"]), int(g[f"{p}_K"]),
+                        torch.arange(A.shape[0], device="cuda"))
+    S = stream.build_system(ds, T(g[f"{p}_active"]), T(g[f"{p}_labeled"]), dtype="float64")
+    np.testing.assert_array_equal(S.U.cpu().numpy(), g[f"{p}_U"])
+    Wg = golden_csr(g, f"{p}_W")
+    np.testing.assert_array_equal(S.W.indptr.cpu().numpy(), Wg.indptr)
+    np.testing.assert_array_equal(S.W.indices.cpu().numpy(), Wg.indices)
+    np.testing.assert_array_equal(S.W.data.cpu().numpy(), Wg.data)
+    for k in ("s", "diag", "B", "rhs"):
+        np.testing.assert_allclose(getattr(S, k).cpu().numpy(), g[f"{p}_{k}"], rtol=1e-12, err_msg=k)
+    assert S.n_ungrounded == int(g[f"{p}_n_ungrounded"])
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_fused_pcg_matches_reference(graph):
+    """Same iteration counts as the reference's pcg (dynlp/solvers.py:66-97) and the same iterate."""
+    g, A, S = golden_system()
+    for tag in ("pcg_loose", "pcg_tight"):
+        Z = torch.zeros((A.shape[0], 3), dtype=torch.float64, device="cuda")
+        st = solvers.Stats()
+        solvers.pcg(S, Z, S.rhs, g[f"{tag}_eps"].tolist(), solvers.jacobi_M(S), 10_000, st, use_graph=graph)
+        assert st.iters == int(g[f"{tag}_iters"]), (tag, st.iters, int(g[f"{tag}_iters"]))
+        np.testing.assert_allclose(Z.cpu().numpy(), g[f"{tag}_Z"], rtol=1e-8, atol=1e-11)
+
+
+def test_fused_pcg_fp32_and_relres_target():
+    g, A, S = golden_system()
+    S32 = S.astype(torch.float32)
+    Z = solvers.padded_empty(A.shape[0], 3, torch.float32, "cuda")
+    Z.zero_()
+    st = solvers.Stats()
+    solvers.pcg(S32, Z, S32.rhs, [1e-30] * 3, solvers.jacobi_M(S32), 10_000, st, target_relres=1e-5)
+    rel = O.relres(A, g["diag"], Z.double().cpu().numpy(), g["rhs"])
+    assert rel <= 1e-5 * 1.01 and st.iters < 200, (rel, st.iters)
+
+
+def test_push_rounds_match_reference():
+    g, A, S = golden_system()
+    Z, R = T(g["push_Z0"]), T(g["push_R0"])
+    ops = kernels.FrontierOps(S.W, 3)
+    rec = []
+    Z, R, ok = solvers.push(S, Z, R, g["push_eps"].tolist(), ops, solvers.Stats(), record=rec)
+    assert ok == bool(g["push_ok"]) and len(rec) == int(g["push_rounds"])
+    off, cand = g["push_cand_off"], g["push_cand"]
+    for k, (c, _t) in enumerate(rec):
+        np.testing.assert_array_equal(c.cpu().numpy(), cand[off[k]:off[k + 1]])
+    np.testing.assert_allclose(Z.cpu().numpy(), g["push_Z"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(R.cpu().numpy(), g["push_R"], rtol=1e-6, atol=1e-13)
+    # touched sets equal the oracle's too
+    Zo, Ro, oko, ito, rounds = O.push(A, g["diag"], g["push_Z0"].copy(), g["push_R0"].copy(), g["push_eps"], record=True)
+    for (c, t), (co, to) in zip(rec, rounds):
+        np.testing.assert_array_equal(t.cpu().numpy(), to)
+
+
+def test_dynlp_frontier_matches_oracle():
+    g, A, S = golden_system()
+    rs = np.random.RandomState(3)
+    seed = np.zeros(A.shape[0], dtype=bool)
+    seed[rs.choice(A.shape[0], 50, replace=False)] = True
+    S.seed = T(seed)
+    solver = solvers.DynLP(A.shape[0], 3, "float64", delta=1e-6)
+    rec = []
+    solver.solve(S, record=rec)
+    X0 = np.full((A.shape[0], 3), 1 / 3)
+    Xo, it, fronts = O.dynlp_frontier(A, g["diag"], g["rhs"], X0, np.flatnonzero(seed), 1e-6, record=True)
+    assert len(rec) == len(fronts)
+    for a, b in zip(rec, fronts):
+        np.testing.assert_array_equal(a.cpu().numpy(), b)
+    np.testing.assert_allclose(solver.F.cpu().numpy(), Xo, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("method", ["pcg", "auto"])
+@pytest.mark.parametrize("K", [2, 3])
+def test_dynlp_plus_certificate_holds(method, K):
+    """tests/test_dynlp.py:109-120 on our stack: cert <= tol and err <= 1.05 cert."""
+    ds = graphs.sbm(3000, K=K, deg=8, seed=3, dtype="float32")
+    rs = np.random.RandomState(0)
+    lab = np.zeros(3000, bool)
+    lab[rs.choice(3000, 60, replace=False)] = True
+    S = stream.build_system(ds, torch.ones(3000, dtype=torch.bool, device="cuda"), T(lab), dtype="float32")
+    solver = solvers.DynLPPlus(3000, K, "float32", method=method, tol=1e-3)
+    st = solver.solve(S)
+    S64 = S.astype(torch.float64)
+    Wd = S64.W.to_scipy().astype(np.float64)
+    Ad = ssp.diags(S64.diag.cpu().numpy()) - Wd
+    Fd = sla.spsolve(Ad.tocsc(), S64.rhs.cpu().numpy())
+    Fd = Fd.reshape(-1, 1) if Fd.ndim == 1 else Fd
+    err = np.abs(solver.scores(S).cpu().numpy() - Fd).max()
+    assert st.cert <= 1e-3 * 1.0001
+    assert err <= st.cert * 1.05 + 1e-6, (err, st.cert)
+
+
+def test_dynlp_plus_relres_target_fp32():
+    ds = graphs.er_graph(20_000, 10, 8, seed=1)
+    lab = graphs.label_mask(20_000, 0.005, seed=1)
+    S = stream.build_system(ds, torch.ones(20_000, dtype=torch.bool, device="cuda"), lab, dtype="float32")
+    solver = solvers.DynLPPlus(20_000, 8, "float32", method="pcg", tol=1e-3, target_relres=1e-8)
+    st = solver.solve(S)
+    S64 = S.astype(torch.float64)
+    A = S64.W.to_scipy().astype(np.float64)
+    rel = O.relres(A, S64.diag.cpu().numpy(), solver.scores(S).cpu().numpy(), S64.rhs.cpu().numpy())
+    assert rel <= 1e-8 and st.relres <= 1e-8, (rel, st.relres)
+
+
+def _oracle_edge_system(A_sc, y, K, lab):
+    n = A_sc.shape[0]
+    return O.build_system(A_sc, y, K, np.ones(n, bool), lab)
+
+
+@pytest.mark.parametrize("weights", ["unit", "lognormal"])
+def test_edge_stream_matches_rebuilt_system(weights):
+    """After every edge batch the resident system equals the system rebuilt from scratch on the
+    updated graph (the oracle's apply_edges + build_system), on its solved rows; inert rows carry
+    no live entries, diag 1 and rhs 0 (tests/test_incremental.py:18-41 for edge batches)."""
+    n, K = 4000, 3
+    ds = graphs.planted_partition(n, K, 3.0, 1.0, weights=weights, seed=2)  # sparse: splits and regrounding
+    lab = graphs.label_mask(n, 0.01, seed=2)
+    es = stream.EdgeStream(ds, lab, slack_frac=0.0)  # no slack: forces repacking
+    up = graphs.EdgeUpdates(ds.A, seed=3, weights=weights)
+    A_sc = ds.A.to_scipy().astype(np.float64)
+    y, labn = ds.y.cpu().numpy(), lab.cpu().numpy()
+    for t in range(6):
+        b = up.next(300 if t % 2 else 1200, ins_frac=0.3 if t < 3 else 0.7)
+        S = es.apply_edges(**b)
+        A_sc = O.apply_edges(A_sc, b["ins_u"], b["ins_v"], b["ins_w"].astype(np.float64), b["del_u"], b["del_v"])
+        # graph equality
+        G = es.G.to_csr("aw").to_scipy().astype(np.float64)
+        assert abs(G - A_sc.astype(np.float32).astype(np.float64)).max() == 0
+        ref = _oracle_edge_system(A_sc.astype(np.float32).astype(np.float64), y, K, labn)
+        U = S.solved.cpu().numpy()
+        np.testing.assert_array_equal(np.flatnonzero(U), ref["U"])
+        S64 = S.astype(torch.float64)
+        Wd = es.G.to_csr("w").to_scipy().astype(np.float64)
+        Uidx = ref["U"]
+        assert abs(Wd[Uidx][:, Uidx] - ref["W"]).max() < 1e-12
+        out = ~U
+        assert abs(Wd[out]).sum() == 0 and abs(Wd[:, out]).sum() == 0
+        np.testing.assert_allclose(S64.diag.cpu().numpy()[Uidx], ref["diag"], rtol=1e-10)
+        np.testing.assert_allclose(S64.rhs.cpu().numpy()[Uidx], ref["rhs"], rtol=1e-10, atol=1e-12)
+        assert (S64.diag.cpu().numpy()[out] == 1).all() and (S64.rhs.cpu().numpy()[out] == 0).all()
+    assert es.counters["rebuilds"] >= 1 and es.counters["ground_changes"] >= 1
+
+
+def test_incremental_solver_relres_on_edge_batches():
+    n, K = 20_000, 4
+    ds = graphs.er_graph(n, 10, K, seed=5)
+    lab = graphs.label_mask(n, 0.01, seed=5)
+    es = stream.EdgeStream(ds, lab)
+    up = graphs.EdgeUpdates(ds.A, seed=5)
+    solver = solvers.IncrementalLP(n, K, "float32", tol=1e-3, method="pcg", target_relres=1e-6, full_every=4)
+    st = solver.solve(es.system)
+    assert st.relres <= 1e-6
+    for t in range(5):
+        S = es.apply_edges(**up.next(400))
+        st = solver.solve(S)
+        S64 = S.astype(torch.float64)
+        A = es.G.to_csr("w").to_scipy().astype(np.float64)
+        F = solver.Z.cpu().numpy()[:, :K]
+        rel = O.relres(A, S64.diag.cpu().numpy(), F, S64.rhs.cpu().numpy())
+        assert rel <= 1e-6 and st.relres <= 1e-6, (t, rel, st.relres, st.path)
+        # kept residual equals a fresh one (drift)
+        R_true = S64.rhs_h.cpu().numpy() - (S64.diag.cpu().numpy()[:, None] * solver.Z.cpu().numpy() - A @ solver.Z.cpu().numpy())
+        drift = np.abs(R_true - solver.R.cpu().numpy()).max() / S64.diag.cpu().numpy().min()
+        assert drift < 1e-9, drift
