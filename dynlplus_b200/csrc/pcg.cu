@@ -27,7 +27,7 @@ struct PcgCtl {
   int32_t go;     // set by K1 for the iteration in flight
   uint32_t cnt1, cnt2;
   int32_t mode, patience;
-  int32_t max_iter, pad0;
+  int32_t max_iter, bad;  // bad: non-finite residual entries seen (breakdown)
   double best, viol, relres, target;
 };
 
@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
     for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
       double s = 0.0;
       for (int b = 0; b < (int)gridDim.x; ++b) s += p.B.part1[(long long)b * p.C + c];
-      p.B.alpha[c] = s > 0.0 ? p.B.rz[c] / s : 0.0;
+      const double al = s > 0.0 ? p.B.rz[c] / s : 0.0;
+      p.B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
     }
     if (threadIdx.x == 0) ctl->cnt1 = 0;
   }
@@ -194,6 +195,8 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
 // K2: residual update + reductions + stop decision
 //   phase 0: iteration (R -= alpha AP)      phase 1: recheck of a true residual
 //   phase 2: initial residual (sets best, rz)
+// A non-finite residual entry stops the solve with status 4 (breakdown) instead of letting the
+// max-reductions (which skip NaN) read it as convergence.
 // ------------------------------------------------------------------------------------------------
 constexpr int kMaxColChunks = 8;  // C <= 256 with 32 column lanes
 
@@ -223,6 +226,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
           R[r * ldr + c] = rv;
         }
         const double r64 = (double)rv;
+        if (!isfinite(r64)) ctl->bad = 1;
         rz[m] += r64 * r64 / d;
         ss[m] += r64 * r64;
         vmax = fmax(vmax, fabs(r64) / (B.eps[c] * d));
@@ -266,7 +270,8 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
         b += B.part2[((long long)bb * C + c) * 2 + 1];
       }
       const double rzo = B.rz[c];
-      B.beta[c] = (phase != 2 && rzo > 0.0) ? a / rzo : 0.0;
+      const double be = (phase != 2 && rzo > 0.0) ? a / rzo : 0.0;
+      B.beta[c] = isfinite(be) && fabs(be) < 1e30 ? be : 0.0;
       B.rz[c] = a;
       const double rel = B.rhsn[c] > 0.0 ? sqrt(b) / B.rhsn[c] : sqrt(b);
       // fmax over non-negative doubles: the int64 view is monotone
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
       double m = 0.0;
       if (ctl->mode & 1) m = fmax(m, v);
       if (ctl->mode & 2) m = fmax(m, ctl->target > 0.0 ? rel / ctl->target : rel);
-      const bool conv = m <= 1.0;
+      const bool conv = m <= 1.0 && !ctl->bad;
       if (phase == 0) ctl->iters += 1;
       if (phase == 2) {
         ctl->best = m;
@@ -303,6 +308,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
         else if (phase == 1) ctl->done = 0;
       }
       if (ctl->done == 0 && ctl->iters >= ctl->max_iter) ctl->done = 3;
+      if (ctl->bad) ctl->done = 4;
       ctl->cnt2 = 0;
     }
   }
@@ -508,7 +514,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
             int32_t use_graph, double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, double *viol_out,
             double *relres_out, int32_t *status_out, dlp_stream_t stream) {
   if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
-  if (mode < 1 || mode > 3 || !eps) return DLP_ERR_INVALID;
+  if (mode < 1 || mode > 3 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
     return DLP_ERR_DTYPE;
   if (!ws || ws_bytes < pcg_ws_bytes(C)) return DLP_ERR_WORKSPACE;
@@ -526,7 +532,12 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   h.max_iter = max_iter;
   h.target = target_relres;
   DLP_CUDA(cudaMemcpyAsync(B.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-  DLP_CUDA(cudaMemcpyAsync(B.eps, eps, sizeof(double) * C, cudaMemcpyHostToDevice, s));
+  if (eps) {
+    DLP_CUDA(cudaMemcpyAsync(B.eps, eps, sizeof(double) * C, cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<double> big((size_t)C, 1e300);
+    DLP_CUDA(cudaMemcpy(B.eps, big.data(), sizeof(double) * C, cudaMemcpyHostToDevice));
+  }
   if (rhs_norm) {
     DLP_CUDA(cudaMemcpyAsync(B.rhsn, rhs_norm, sizeof(double) * C, cudaMemcpyHostToDevice, s));
   } else {
@@ -544,7 +555,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
   DLP_CUDA(cudaStreamSynchronize(s));
   if (max_iter <= 0 && cur.done == 0) cur.done = 3;
-  while (cur.done == 0 || cur.done == 1) {
+  while ((cur.done == 0 || cur.done == 1) && !cur.bad) {
     if (cur.done == 0) {
       if (ex) {
         DLP_CUDA(cudaGraphLaunch(ex, s));

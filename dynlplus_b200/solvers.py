@@ -113,6 +113,8 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
 
     Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
     residual ||R_c|| / rhs_norm_c <= target must hold as well (rhs_norm defaults to ||rhs_c||)."""
+    if eps is None and target_relres is None:
+        raise ValueError("pcg needs eps and/or target_relres")
     if M is not None and not isinstance(M, JacobiM):
         return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm)
     n, C = Z.shape
@@ -127,11 +129,11 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     R = _scratch("pcg_R", n, C, dt, dev)
     P = _scratch("pcg_P", n, C, dt, dev, padded=True)
     AP = _scratch("pcg_AP", n, C, dt, dev)
-    eps_h = (ct.c_double * C)(*[float(e) for e in eps])
-    mode = 1
+    eps_h = (ct.c_double * C)(*[float(e) for e in eps]) if eps is not None else None
+    mode = 1 if eps is not None else 0
     rn = None
     if target_relres is not None:
-        mode = 3
+        mode |= 2
         if rhs_norm is None:
             rhs_norm = col_norms(rhs.to(dt)).cpu().tolist()
         rn = (ct.c_double * C)(*[float(x) for x in rhs_norm])
@@ -146,6 +148,8 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     st.iters += it.value
     st.edges += (it.value + 2) * W.nnz + work_M * it.value
     st.relres = rel.value
+    if status.value == 4:
+        raise FloatingPointError("PCG breakdown: non-finite residual")
     return Z
 
 

@@ -115,10 +115,9 @@ def build_system(ds: Dataset, active, labeled, *, eta=0.0, dtype="float32", t=0,
     W = CSR(A.data[keep].to(dt), loc[cols[keep]].to(torch.int32), indptr.to(torch.int32), (n_u, n_u))
     Bm = Bfull[U]
     s = Bm.sum(dim=1) + eta
-    rowsum = torch.zeros(n_u, dtype=torch.float64, device=dev)
-    if n_u:
-        _lib.call("dlp_graph_rowsum", ptr(W.rbeg), ptr(W.rend), ptr(W.data.float() if dt != torch.float32 else W.data),
-                  None, n_u, ptr(rowsum), stream())
+    ones = torch.ones((n_u, 1), dtype=torch.float64, device=dev)
+    rowsum = kernels.spmm_axpy(W if dt != torch.bfloat16 else W.astype(torch.float32), ones)[:, 0] if n_u else \
+        torch.zeros(0, dtype=torch.float64, device=dev)
     diag = s + rowsum
     prior = torch.full((1 if K == 2 else K,), 0.5 if K == 2 else 1.0 / K, dtype=torch.float64, device=dev)
     rhs = (Bm[:, 1:2] if K == 2 else Bm) + eta * prior[None, :]

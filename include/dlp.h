@@ -160,7 +160,8 @@ int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_
  * eps and rhs_norm are HOST arrays of C doubles (rhs_norm may be NULL when bit 1 is unused).
  * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual). The chunk of
  * check_every iterations is replayed as a CUDA graph when use_graph != 0 (cached per problem).
- * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap.
+ * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap,
+ * 4 breakdown (a non-finite residual entry). eps may be NULL when bit 0 is unused.
  * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C). */
 size_t dlp_pcg_workspace_bytes(int32_t C);
 int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype, int32_t n,

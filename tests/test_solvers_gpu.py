@@ -67,7 +67,7 @@ def test_fused_pcg_fp32_and_relres_target():
     Z = solvers.padded_empty(A.shape[0], 3, torch.float32, "cuda")
     Z.zero_()
     st = solvers.Stats()
-    solvers.pcg(S32, Z, S32.rhs, [1e-30] * 3, solvers.jacobi_M(S32), 10_000, st, target_relres=1e-5)
+    solvers.pcg(S32, Z, S32.rhs, None, solvers.jacobi_M(S32), 10_000, st, target_relres=1e-5)
     rel = O.relres(A, g["diag"], Z.double().cpu().numpy(), g["rhs"])
     assert rel <= 1e-5 * 1.01 and st.iters < 200, (rel, st.iters)
 
