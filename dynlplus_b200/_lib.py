@@ -45,10 +45,14 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
     "dlp_graph_toggle": ("ppppppippppp", ct.c_int),
+    "dlp_graph_to_csr_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_graph_to_csr": ("ippppppppzp", ct.c_int),
     "dlp_graph_rowsum": ("ppppipp", ct.c_int),
     "dlp_system_rows": ("pippipdpiiippqppqp", ct.c_int),
     "dlp_park_rows": ("pipiipdpqpqp", ct.c_int),
     "dlp_cols_scale": ("iipqipipqip", ct.c_int),
+    "dlp_fused_push_workspace_bytes": ("ii", ct.c_size_t),
+    "dlp_fused_push": ("ppppiiippqpqippiiiipzpppp", ct.c_int),
     "dlp_ground_update": ("ipppppp", ct.c_int),
 }
 

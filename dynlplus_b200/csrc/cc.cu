@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kCcThreads)
         continue;
       }
       if (!vmask || vmask[v]) {
-        if (u != v) unite(parent, u, v, err);
+        if (u < v) unite(parent, u, v, err);  // the mirror entry (v, u) covers the pair once
       } else if (sink && sink[v]) {
         unite(parent, u, n, err);
       }

@@ -99,6 +99,23 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t *o
   if (pred) out[base + __popc(ballot & ((1u << lane) - 1u))] = value;
 }
 
+// Deterministic warp-wide sum (or max) of base[b * stride] over b < nb: lane l takes b = l, l+32,
+// ... (independent loads, so the latency overlaps), then a fixed xor tree. All lanes get the result.
+__device__ __forceinline__ double warp_strided_reduce(const double *base, long long stride, int nb, bool is_max) {
+  const int lane = threadIdx.x & 31;
+  double v = 0.0;
+  for (int b = lane; b < nb; b += 32) {
+    const double x = base[(long long)b * stride];
+    v = is_max ? fmax(v, x) : v + x;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double t = __shfl_xor_sync(0xffffffffu, v, off);
+    v = is_max ? fmax(v, t) : v + t;
+  }
+  return v;
+}
+
 inline int ceil_div_i(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 inline int next_pow2(int x) {

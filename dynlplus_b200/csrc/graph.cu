@@ -16,6 +16,9 @@
 
 namespace dlp {
 
+int exclusive_scan_i32(const int32_t *in, int32_t n, int32_t *out, void *ws, size_t ws_bytes, cudaStream_t s);
+size_t compact_ws_bytes(int32_t n);
+
 constexpr int kGThreads = 256;
 constexpr unsigned long long kEmpty = ~0ull;
 
@@ -260,6 +263,32 @@ __global__ void k_park(const int32_t *__restrict__ rows, int32_t nr, const uint8
   }
 }
 
+// Compact CSR of the solver operator: the entries with w != 0 of every row, in stored order.
+__global__ void k_live_count(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+                             const float *__restrict__ w, int32_t *cnt) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int c = 0;
+  for (int j = rbeg[r]; j < rend[r]; ++j) c += w[j] != 0.0f;
+  cnt[r] = c;
+}
+
+__global__ void k_live_copy(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+                            const int32_t *__restrict__ col, const float *__restrict__ w,
+                            const int32_t *__restrict__ indptr, int32_t *col_out, float *w_out) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int o = indptr[r];
+  for (int j = rbeg[r]; j < rend[r]; ++j) {
+    const float x = w[j];
+    if (x != 0.0f) {
+      col_out[o] = col[j];
+      w_out[o] = x;
+      ++o;
+    }
+  }
+}
+
 static int grid1(long long work) { return ceil_div_i(work > 0 ? work : 1, kGThreads); }
 
 static uint32_t table_size(int32_t ni) {
@@ -329,6 +358,23 @@ int dlp_graph_toggle(const int32_t *rbeg, const int32_t *rend, const int32_t *co
                                                                  changed);
   k_rowsum<<<grid1(nt), kGThreads, 0, s>>>(rbeg, rend, w, T, nt, rowsum);
   return check_launch(2);
+}
+
+size_t dlp_graph_to_csr_workspace_bytes(int32_t n) { return compact_ws_bytes(n) + sizeof(int32_t) * (size_t)(n > 0 ? n : 1) + 256; }
+
+int dlp_graph_to_csr(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *w,
+                     int32_t *indptr, int32_t *col_out, float *w_out, void *ws, size_t ws_bytes, dlp_stream_t stream) {
+  if (n < 0 || !indptr) return DLP_ERR_INVALID;
+  if (n > 0 && (!rbeg || !rend || !col || !w || !col_out || !w_out)) return DLP_ERR_INVALID;
+  if (!ws || ws_bytes < dlp_graph_to_csr_workspace_bytes(n)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t *cnt = (int32_t *)ws;
+  void *scan_ws = (char *)ws + ((sizeof(int32_t) * (size_t)(n > 0 ? n : 1) + 255) / 256 * 256);
+  const size_t scan_bytes = ws_bytes - ((sizeof(int32_t) * (size_t)(n > 0 ? n : 1) + 255) / 256 * 256);
+  if (n > 0) k_live_count<<<grid1(n), kGThreads, 0, s>>>(n, rbeg, rend, w, cnt);
+  DLP_TRY(exclusive_scan_i32(cnt, n, indptr, scan_ws, scan_bytes, s));
+  if (n > 0) k_live_copy<<<grid1(n), kGThreads, 0, s>>>(n, rbeg, rend, col, w, indptr, col_out, w_out);
+  return check_launch(n > 0 ? 2 : 0);
 }
 
 int dlp_graph_rowsum(const int32_t *rbeg, const int32_t *rend, const float *w, const int32_t *rows, int32_t nr,

@@ -33,10 +33,10 @@ struct PcgCtl {
 
 struct PcgBufs {
   PcgCtl *ctl;
-  double *alpha, *beta, *rz, *eps, *rhsn, *part1, *part2, *partv;
+  double *alpha, *beta, *rz, *eps, *rhsn, *epsinv, *part1, *part2, *partv;
 };
 
-constexpr int kUpdBlocksPerSM = 4;
+constexpr int kUpdBlocksPerSM = 8;
 
 static int upd_blocks() { return sm_count() * kUpdBlocksPerSM; }
 static int apply_blocks() { return sm_count() * 8; }
@@ -46,7 +46,7 @@ static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 static size_t pcg_ws_bytes(int C) {
   const size_t nb = (size_t)std::max(upd_blocks(), apply_blocks());
   size_t b = align256(sizeof(PcgCtl));
-  b += 5 * align256(sizeof(double) * C);
+  b += 6 * align256(sizeof(double) * C);
   b += align256(sizeof(double) * nb * C);      // part1
   b += align256(sizeof(double) * nb * C * 2);  // part2 (rz, ss)
   b += align256(sizeof(double) * nb);          // partv
@@ -59,7 +59,7 @@ static PcgBufs carve(void *ws, int C) {
   PcgBufs B;
   B.ctl = (PcgCtl *)p;
   p += align256(sizeof(PcgCtl));
-  double **vecs[5] = {&B.alpha, &B.beta, &B.rz, &B.eps, &B.rhsn};
+  double **vecs[6] = {&B.alpha, &B.beta, &B.rz, &B.eps, &B.rhsn, &B.epsinv};
   for (auto v : vecs) {
     *v = (double *)p;
     p += align256(sizeof(double) * C);
@@ -181,11 +181,13 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
     p.B.part1[(long long)blockIdx.x * p.C + c] = s;
   }
   if (last_block(&ctl->cnt1)) {
-    for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
-      double s = 0.0;
-      for (int b = 0; b < (int)gridDim.x; ++b) s += p.B.part1[(long long)b * p.C + c];
-      const double al = s > 0.0 ? p.B.rz[c] / s : 0.0;
-      p.B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
+    // one warp per column: lane-strided loads over the block partials, fixed-order tree
+    for (int c = wid; c < p.C; c += kThreads / 32) {
+      const double s = warp_strided_reduce(p.B.part1 + c, p.C, (int)gridDim.x, false);
+      if (lane == 0) {
+        const double al = s > 0.0 ? p.B.rz[c] / s : 0.0;
+        p.B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
+      }
     }
     if (threadIdx.x == 0) ctl->cnt1 = 0;
   }
@@ -199,6 +201,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
 // max-reductions (which skip NaN) read it as convergence.
 // ------------------------------------------------------------------------------------------------
 constexpr int kMaxColChunks = 8;  // C <= 256 with 32 column lanes
+constexpr int kRowsPerThread = 4;
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_t C, T *__restrict__ R, int64_t ldr,
@@ -214,22 +217,29 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
   const int nch = (C + CX - 1) / CX;
 #pragma unroll
   for (int m = 0; m < kMaxColChunks; ++m) rz[m] = ss[m] = 0.0;
-  for (long long r = (long long)blockIdx.x * RY + ty; r < n; r += (long long)gridDim.x * RY) {
-    const double d = (double)diag[r];
+  // kRowsPerThread rows in flight per thread and iteration (memory-level parallelism)
+  const long long step = (long long)gridDim.x * RY * kRowsPerThread;
+  for (long long r0 = (long long)blockIdx.x * RY * kRowsPerThread + ty; r0 < n; r0 += step) {
 #pragma unroll
-    for (int m = 0; m < kMaxColChunks; ++m) {
-      const int c = tx + m * CX;
-      if (m < nch && c < C) {
-        T rv = R[r * ldr + c];
-        if (phase == 0) {
-          rv = rv - (T)B.alpha[c] * AP[r * ldap + c];
-          R[r * ldr + c] = rv;
+    for (int u = 0; u < kRowsPerThread; ++u) {
+      const long long r = r0 + (long long)u * RY;
+      if (r >= n) break;
+      const double dinv = 1.0 / (double)diag[r];
+#pragma unroll
+      for (int m = 0; m < kMaxColChunks; ++m) {
+        const int c = tx + m * CX;
+        if (m < nch && c < C) {
+          T rv = R[r * ldr + c];
+          if (phase == 0) {
+            rv = rv - (T)B.alpha[c] * AP[r * ldap + c];
+            R[r * ldr + c] = rv;
+          }
+          const double r64 = (double)rv;
+          if (!isfinite(r64)) ctl->bad = 1;
+          rz[m] += r64 * r64 * dinv;
+          ss[m] += r64 * r64;
+          vmax = fmax(vmax, fabs(r64) * dinv * B.epsinv[c]);
         }
-        const double r64 = (double)rv;
-        if (!isfinite(r64)) ctl->bad = 1;
-        rz[m] += r64 * r64 / d;
-        ss[m] += r64 * r64;
-        vmax = fmax(vmax, fabs(r64) / (B.eps[c] * d));
       }
     }
   }
@@ -263,12 +273,11 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
     __shared__ double s_rel;
     if (tid == 0) s_rel = 0.0;
     __syncthreads();
-    for (int c = tid; c < C; c += CX * RY) {
-      double a = 0.0, b = 0.0;
-      for (int bb = 0; bb < (int)gridDim.x; ++bb) {
-        a += B.part2[((long long)bb * C + c) * 2 + 0];
-        b += B.part2[((long long)bb * C + c) * 2 + 1];
-      }
+    const int wid = tid >> 5, lane = tid & 31;
+    for (int c = wid; c < C; c += (CX * RY) >> 5) {
+      const double a = warp_strided_reduce(B.part2 + (long long)c * 2 + 0, (long long)C * 2, (int)gridDim.x, false);
+      const double b = warp_strided_reduce(B.part2 + (long long)c * 2 + 1, (long long)C * 2, (int)gridDim.x, false);
+      if (lane != 0) continue;
       const double rzo = B.rz[c];
       const double be = (phase != 2 && rzo > 0.0) ? a / rzo : 0.0;
       B.beta[c] = isfinite(be) && fabs(be) < 1e30 ? be : 0.0;
@@ -278,9 +287,14 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
       atomicMax((unsigned long long *)&s_rel, __double_as_longlong(rel));
     }
     __syncthreads();
+    __shared__ double s_vmax;
+    if (wid == 0) {
+      const double v = warp_strided_reduce(B.partv, 1, (int)gridDim.x, true);
+      if (lane == 0) s_vmax = v;
+    }
+    __syncthreads();
     if (tid == 0) {
-      double v = 0.0;
-      for (int bb = 0; bb < (int)gridDim.x; ++bb) v = fmax(v, B.partv[bb]);
+      const double v = s_vmax;
       const double rel = s_rel;
       ctl->viol = v;
       ctl->relres = rel;
@@ -328,16 +342,22 @@ __global__ void __launch_bounds__(256) k_pcg_dir(int mode, int32_t n, int32_t C,
   const bool upd_p = mode != 0 || ctl->done == 0;
   const int CX = blockDim.x, RY = blockDim.y;
   const int nch = (C + CX - 1) / CX;
-  for (long long r = (long long)blockIdx.x * RY + threadIdx.y; r < n; r += (long long)gridDim.x * RY) {
-    const T dv = diag[r];
-    for (int m = 0; m < nch; ++m) {
-      const int c = threadIdx.x + m * CX;
-      if (c >= C) break;
-      const T pv = P[r * ldp + c];
-      if (mode == 0) Z[r * ldz + c] += (T)B.alpha[c] * pv;
-      if (upd_p) {
-        const T y = R[r * ldr + c] / dv;
-        P[r * ldp + c] = mode == 2 ? y : y + (T)B.beta[c] * pv;
+  const long long step = (long long)gridDim.x * RY * kRowsPerThread;
+  for (long long r0 = (long long)blockIdx.x * RY * kRowsPerThread + threadIdx.y; r0 < n; r0 += step) {
+#pragma unroll
+    for (int u = 0; u < kRowsPerThread; ++u) {
+      const long long r = r0 + (long long)u * RY;
+      if (r >= n) break;
+      const T dv = diag[r];
+      for (int m = 0; m < nch; ++m) {
+        const int c = threadIdx.x + m * CX;
+        if (c >= C) break;
+        const T pv = P[r * ldp + c];
+        if (mode == 0) Z[r * ldz + c] += (T)B.alpha[c] * pv;
+        if (upd_p) {
+          const T y = R[r * ldr + c] / dv;
+          P[r * ldp + c] = mode == 2 ? y : y + (T)B.beta[c] * pv;
+        }
       }
     }
   }
@@ -532,11 +552,14 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   h.max_iter = max_iter;
   h.target = target_relres;
   DLP_CUDA(cudaMemcpyAsync(B.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-  if (eps) {
-    DLP_CUDA(cudaMemcpyAsync(B.eps, eps, sizeof(double) * C, cudaMemcpyHostToDevice, s));
-  } else {
-    std::vector<double> big((size_t)C, 1e300);
-    DLP_CUDA(cudaMemcpy(B.eps, big.data(), sizeof(double) * C, cudaMemcpyHostToDevice));
+  {
+    std::vector<double> e2((size_t)C * 2);
+    for (int c = 0; c < C; ++c) {
+      e2[c] = eps ? eps[c] : 1e300;
+      e2[C + c] = 1.0 / e2[c];
+    }
+    DLP_CUDA(cudaMemcpy(B.eps, e2.data(), sizeof(double) * C, cudaMemcpyHostToDevice));
+    DLP_CUDA(cudaMemcpy(B.epsinv, e2.data() + C, sizeof(double) * C, cudaMemcpyHostToDevice));
   }
   if (rhs_norm) {
     DLP_CUDA(cudaMemcpyAsync(B.rhsn, rhs_norm, sizeof(double) * C, cudaMemcpyHostToDevice, s));

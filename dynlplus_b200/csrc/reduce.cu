@@ -113,6 +113,54 @@ static int compact_impl(Pred pred, const int32_t *idx, int32_t n, int32_t *out, 
   return check_launch(3);
 }
 
+// Exclusive scan of int32 counts: out[0] = 0, out[i+1] = sum_{j<=i} in[j] (out has n + 1 entries).
+__global__ void __launch_bounds__(kScanThreads) k_tile_sum_i32(const int32_t *__restrict__ in, int32_t n,
+                                                               int32_t *tile_sum) {
+  const long long base = (long long)blockIdx.x * kTile + (long long)threadIdx.x * kScanItems;
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i)
+    if (base + i < n) c += in[base + i];
+  int excl;
+  const int tot = block_exclusive_scan(c, excl);
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_scan_i32(const int32_t *__restrict__ in, int32_t n,
+                                                                const int32_t *__restrict__ tile_off, int32_t *out) {
+  const long long base = (long long)blockIdx.x * kTile + (long long)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = base + i < n ? in[base + i] : 0;
+    c += v[i];
+  }
+  int excl;
+  block_exclusive_scan(c, excl);
+  int o = tile_off[blockIdx.x] + excl;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) out[base + i] = o;
+    o += v[i];
+  }
+  if (base + kScanItems >= n && base < n) out[n] = o;  // the thread holding the last element
+}
+
+int exclusive_scan_i32(const int32_t *in, int32_t n, int32_t *out, void *ws, size_t ws_bytes, cudaStream_t s) {
+  const int nt = n_tiles(n);
+  if (n == 0) {
+    DLP_CUDA(cudaMemsetAsync(out, 0, sizeof(int32_t), s));
+    return DLP_OK;
+  }
+  if (!ws || ws_bytes < (size_t)nt * sizeof(int32_t)) return DLP_ERR_WORKSPACE;
+  int32_t *tile = (int32_t *)ws;
+  k_tile_sum_i32<<<nt, kScanThreads, 0, s>>>(in, n, tile);
+  k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile, nt, nullptr);
+  k_tile_scan_i32<<<nt, kScanThreads, 0, s>>>(in, n, tile, out);
+  return check_launch(3);
+}
+
 size_t compact_ws_bytes(int32_t n) { return ((size_t)n_tiles(n) * sizeof(int32_t) + 255) / 256 * 256 + 256; }
 
 int compact_roots(const int32_t *parent, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
@@ -177,13 +225,12 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// One warp per column (lane-strided partials, fixed-order tree): deterministic.
 __global__ void k_colreduce_final(int kind, int32_t C, int nb, const double *__restrict__ partial, double *out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (c >= C) return;
-  const bool is_max = kind == 0 || kind == 3;
-  double v = 0.0;
-  for (int b = 0; b < nb; ++b) v = is_max ? fmax(v, partial[(long long)b * C + c]) : v + partial[(long long)b * C + c];
-  out[c] = v;
+  const double v = warp_strided_reduce(partial + c, C, nb, kind == 0 || kind == 3);
+  if ((threadIdx.x & 31) == 0) out[c] = v;
 }
 
 }  // namespace dlp
@@ -223,7 +270,7 @@ int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, co
     else
       return DLP_ERR_DTYPE;
   }
-  k_colreduce_final<<<(C + 63) / 64, 64, 0, s>>>(kind, C, nb, partial, out);
+  k_colreduce_final<<<(C + 7) / 8, 256, 0, s>>>(kind, C, nb, partial, out);
   return check_launch(nb > 0 ? 2 : 1);
 }
 

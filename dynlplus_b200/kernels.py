@@ -76,6 +76,35 @@ def spmm_axpy(W, X, a=None, b=1.0, group="auto", *, rhs=None, cr=1.0, alpha=1.0,
     return out
 
 
+class FusedPush:
+    """Asynchronous residual push with device-resident frontiers (dynlp/kernels.py:396-433).
+
+    Takes the residual of every violating vertex (|r_u| > eps_c * diag_u), adds r_u / diag_u to z_u
+    and scatters it to the neighbours, keeping r exact; converges for this M-matrix despite the
+    asynchrony (chaotic relaxation). C <= 33."""
+
+    def __init__(self, W, C, group="auto", threads=256, blocks_per_sm=8):
+        if C > 33:
+            raise ValueError("FusedPush takes at most 33 columns")
+        self.W, self.C = W, C
+        self.edges = 0
+
+    def run(self, Z, R, diag, eps, cand, max_rounds, check_every=8, use_graph=True):
+        """Push until no vertex violates; returns (rounds, converged, edge visits) (:415-433)."""
+        import ctypes as ct
+        W, n, C = self.W, self.W.shape[0], self.C
+        cand = cand.to(torch.int32).contiguous()
+        eps_h = (ct.c_double * C)(*[float(e) for e in (eps.tolist() if torch.is_tensor(eps) else eps)])
+        ws = workspace("fused_push").get(_lib.lib().dlp_fused_push_workspace_bytes(n, C))
+        rounds, ok, edges = ct.c_int32(0), ct.c_int32(0), ct.c_ulonglong(0)
+        _lib.call("dlp_fused_push", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C,
+                  ptr(diag.to(Z.dtype).contiguous()), ptr(Z), ld(Z), ptr(R), ld(R), code(Z), eps_h, ptr(cand),
+                  int(cand.numel()), int(max_rounds), int(check_every), int(bool(use_graph)), ptr(ws), ws.numel(),
+                  ct.byref(rounds), ct.byref(ok), ct.byref(edges), stream())
+        self.edges = int(edges.value)
+        return int(rounds.value), bool(ok.value), int(edges.value)
+
+
 class FrontierOps:
     """Frontier primitives bound to one sparse matrix and column count (dynlp/kernels.py:436-492)."""
 

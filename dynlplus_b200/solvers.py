@@ -487,6 +487,23 @@ class IncrementalLP(DynLPPlus):
         st.edges += s64.nnz
         self.since_full = 0
 
+    def _push(self, s64, eps, st):
+        """Repair the violating rows of R (dynlp/solvers.py:375-389): the fused asynchronous push
+        for up to 33 columns, the synchronous vectorised push beyond."""
+        Z, R = self.Z, self.R
+        eps_d = torch.as_tensor(eps, dtype=F64, device=Z.device)
+        if Z.shape[1] <= 33:
+            if getattr(self, "_fused", None) is None or self._fused.W is not s64.W:
+                self._fused = kernels.FusedPush(s64.W, Z.shape[1], self.group)
+            cand = kernels.flatnonzero(kernels.violating(R, s64.diag, eps_d))
+            rounds, ok, edges = self._fused.run(Z, R, s64.diag, eps_d, cand, self.max_rounds)
+            st.iters, st.edges = st.iters + rounds, st.edges + edges
+            return ok
+        ops = FrontierOps(s64.W, Z.shape[1], self.group)
+        ok = push(s64, Z, R, eps, ops, st, max_iter=self.max_rounds)[2]
+        st.edges += int(ops.edges)
+        return ok
+
     def _park(self, s64, rows):
         if rows is not None and rows.numel():
             h0 = float(self.hmax or 1.0)
@@ -532,8 +549,7 @@ class IncrementalLP(DynLPPlus):
                     if small and self.target_relres is None:
                         st.path = "inc-push"
                         for _ in range(4):
-                            _, _, ok = push(s64, self.Z, self.R, eps, FrontierOps(s64.W, C + 1, self.group), st,
-                                            max_iter=self.max_rounds)
+                            ok = self._push(s64, eps, st)
                             hmax, bound = self._bound(rho_cols(s64, self.R).cpu().tolist(),
                                                       float(kernels.colreduce(3, self.Z[:, C:]).item()))
                             if ok and bound <= tol:

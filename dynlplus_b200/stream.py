@@ -355,13 +355,32 @@ class EdgeStream:
         self.counters["applied"] += int(st[2].item()) + int(st[3].item())
         return self.system
 
+    def solver_csr(self) -> CSR:
+        """Compact CSR of W_UU (live solver entries only) for the current batch (cached)."""
+        if getattr(self, "_csr_t", None) == (self.t, id(self.G.indices)):
+            return self._csr
+        n, G = self.n, self.G
+        cap = int(G.indices.numel())
+        if getattr(self, "_csr_cap", 0) < cap:
+            self._csr_col = torch.empty(cap, dtype=torch.int32, device=self.dev)
+            self._csr_w = torch.empty(cap, dtype=torch.float32, device=self.dev)
+            self._csr_ptr = torch.empty(n + 1, dtype=torch.int32, device=self.dev)
+            self._csr_cap = cap
+        ws = workspace("to_csr").get(_lib.lib().dlp_graph_to_csr_workspace_bytes(n))
+        _lib.call("dlp_graph_to_csr", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.data), ptr(self._csr_ptr),
+                  ptr(self._csr_col), ptr(self._csr_w), ptr(ws), ws.numel(), stream())
+        nnz = int(self._csr_ptr[n].item())
+        self._csr = CSR(self._csr_w[:nnz], self._csr_col[:nnz], self._csr_ptr, (n, n))
+        self._csr_t = (self.t, id(G.indices))
+        return self._csr
+
     @property
     def system(self) -> System:
         """Global-index system of the current batch (arrays live until the next batch)."""
         n, C, dev = self.n, self.C, self.dev
         um = self.umask.bool()
         s64 = self.diag64 - self.rowsum
-        common = dict(t=self.t, U=torch.arange(n, device=dev), W=self.G, is_new=torch.zeros(n, dtype=torch.bool,
+        common = dict(t=self.t, U=torch.arange(n, device=dev), W=self.solver_csr(), is_new=torch.zeros(n, dtype=torch.bool,
                       device=dev), seed=self.changed.bool(), comps={}, K=self.K, C=C, eta=self.eta,
                       n_inserted=self.n_ins, n_deleted=self.n_del, n_active=int(self.vmask.sum().item() +
                                                                                self.labeled.sum().item()),

@@ -121,6 +121,7 @@ int dlp_compact(const uint8_t *flag, const int32_t *idx, int32_t n, int32_t *out
  * mask != NULL (mask[r] != 0). Partial sums per block over a fixed grid, then an ordered final
  * pass: the result does not depend on scheduling. Workspace: dlp_colreduce_workspace_bytes(C). */
 size_t dlp_colreduce_workspace_bytes(int32_t C);
+
 int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
                   const void *diag, int dtype, const uint8_t *mask, double *out, void *ws, size_t ws_bytes,
                   dlp_stream_t stream);
@@ -205,6 +206,13 @@ int dlp_graph_toggle(const int32_t *rbeg, const int32_t *rend, const int32_t *co
                      const int32_t *T, int32_t nt, const uint8_t *in_t, const uint8_t *umask, double *rowsum,
                      uint8_t *changed, dlp_stream_t stream);
 
+/* Compact CSR of the solver operator: indptr[0..n] and the entries with w != 0 of every row, in
+ * stored order (col_out/w_out must hold the number of such entries; the total slot count is a safe
+ * capacity). The solver iterates on this copy, so no slack slot or inert entry is streamed. */
+size_t dlp_graph_to_csr_workspace_bytes(int32_t n);
+int dlp_graph_to_csr(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *w,
+                     int32_t *indptr, int32_t *col_out, float *w_out, void *ws, size_t ws_bytes, dlp_stream_t stream);
+
 /* rowsum[r] = sum of w over the stored entries of r, for r = rows[g] (rows == NULL: all nr rows). */
 int dlp_graph_rowsum(const int32_t *rbeg, const int32_t *rend, const float *w, const int32_t *rows, int32_t nr,
                      double *rowsum, dlp_stream_t stream);
@@ -237,6 +245,23 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
  * changed; *count (device int, caller-zeroed) += number of changes. */
 int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, uint8_t *umask, uint8_t *in_t,
                       int32_t *count, dlp_stream_t stream);
+
+
+/* ---- (b) asynchronous residual push with device-resident frontiers ---------------------------
+ * Replaces FusedPush (push_round + compact_frontier, dynlp/kernels.py:269-350; run :415-433):
+ * starting from the candidate rows cand[0..ncand) (device), repeat rounds of
+ *   r = atomicExch(R[u,:], 0); d = r / diag[u]; Z[u,:] += d; R[v,:] += w_uv d (live entries only)
+ * and keep the touched rows with any_c |R[v,c]| > eps[c] * diag[v] as the next frontier, until the
+ * frontier is empty or max_rounds rounds ran. The host reads one counter every check_every rounds
+ * (chunks replayed as a CUDA graph when use_graph != 0). eps is a HOST array of C doubles. C <= 33.
+ * (dtype, w_dtype) in {(f32,f32), (f64,f32), (f64,f64)}. Workspace: dlp_fused_push_workspace_bytes.
+ * Synchronous: *rounds_out, *converged_out (1 = no row violates), *edges_out (edge visits). */
+size_t dlp_fused_push_workspace_bytes(int32_t n, int32_t C);
+int dlp_fused_push(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype,
+                   int32_t n, int32_t C, const void *diag, void *Z, int64_t ldz, void *R, int64_t ldr, int dtype,
+                   const double *eps, const int32_t *cand, int32_t ncand, int32_t max_rounds, int32_t check_every,
+                   int32_t use_graph, void *ws, size_t ws_bytes, int32_t *rounds_out, int32_t *converged_out,
+                   unsigned long long *edges_out, dlp_stream_t stream);
 
 #ifdef __cplusplus
 }

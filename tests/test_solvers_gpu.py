@@ -200,3 +200,52 @@ def test_incremental_solver_relres_on_edge_batches():
         R_true = S64.rhs_h.cpu().numpy() - (S64.diag.cpu().numpy()[:, None] * solver.Z.cpu().numpy() - A @ solver.Z.cpu().numpy())
         drift = np.abs(R_true - solver.R.cpu().numpy()).max() / S64.diag.cpu().numpy().min()
         assert drift < 1e-9, drift
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("C", [2, 4, 9])
+def test_fused_push_reaches_tolerance(dtype, C):
+    """tests/test_incremental.py:66-81: the asynchronous push converges, its kept residual is the
+    true one (up to rounding) and meets eps everywhere."""
+    ds = graphs.sbm(4000, K=2, deg=8.0, seed=9, dtype="float32")
+    lab = graphs.label_mask(4000, 0.03, seed=9)
+    es = stream.EdgeStream(ds, lab)
+    s = es.system.astype(dtype)
+    rs = np.random.RandomState(0)
+    solved = s.solved.cpu().numpy()
+    rhs = T(rs.random_sample((4000, C)) * solved[:, None], dtype)
+    Z = torch.zeros((4000, C), dtype=dtype, device="cuda")
+    R = solvers.residual(s, Z, rhs)
+    eps = [1e-5 if dtype == torch.float64 else 1e-4] * C
+    cand = kernels.flatnonzero((R.abs() > 0).any(dim=1).to(torch.uint8))
+    fp = kernels.FusedPush(s.W, C)
+    rounds, ok, edges = fp.run(Z, R, s.diag, eps, cand, 100_000)
+    assert ok and rounds > 0 and edges > 0
+    R_true = solvers.residual(s, Z, rhs)
+    np.testing.assert_allclose(R.cpu().numpy(), R_true.cpu().numpy(), atol=1e-4 if dtype == torch.float32 else 1e-10)
+    viol = (R_true.abs() / s.diag.to(dtype)[:, None]).max().item() / eps[0]
+    assert viol <= 1.0 + (0.05 if dtype == torch.float32 else 1e-6), viol
+
+
+def test_incremental_push_path_on_small_batches():
+    """IncrementalLP's small-batch branch (dynlp/solvers.py:414-422) certifies with the fused push."""
+    n, K = 6000, 3
+    ds = graphs.planted_partition(n, K, 6.0, 2.0, seed=4)
+    lab = graphs.label_mask(n, 0.02, seed=4)
+    es = stream.EdgeStream(ds, lab)
+    up = graphs.EdgeUpdates(ds.A, seed=4)
+    solver = solvers.IncrementalLP(n, K, "float32", tol=1e-3, push_frac=0.2)
+    solver.solve(es.system)
+    paths = []
+    for _ in range(4):
+        S = es.apply_edges(**up.next(40))
+        st = solver.solve(S)
+        paths.append(st.path)
+        S64 = S.astype(torch.float64)
+        A = es.G.to_csr("w").to_scipy().astype(np.float64)
+        U = S.solved.cpu().numpy()
+        Ad = ssp.diags(S64.diag.cpu().numpy()) - A
+        Fd = sla.spsolve(Ad.tocsc(), S64.rhs.cpu().numpy())
+        err = np.abs(solver.Z.cpu().numpy()[U, :K] - Fd[U]).max()
+        assert st.cert <= 1e-3 * 1.0001 and err <= st.cert * 1.05 + 1e-9, (st.path, err, st.cert)
+    assert "inc-push" in paths, paths
