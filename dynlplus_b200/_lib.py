@@ -53,6 +53,17 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cols_scale": ("iipqipipqip", ct.c_int),
     "dlp_fused_push_workspace_bytes": ("ii", ct.c_size_t),
     "dlp_fused_push": ("ppppiiippqpqippiiiipzpppp", ct.c_int),
+    "dlp_amg_match_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_amg_match": ("ipppipppzp", ct.c_int),
+    "dlp_amg_members_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_amg_members": ("iippppzp", ct.c_int),
+    "dlp_amg_coarse_plan": ("ipppppzp", ct.c_int),
+    "dlp_amg_coarsen": ("ipppppppppqppppppzp", ct.c_int),
+    "dlp_amg_restrict": ("iipppqpqip", ct.c_int),
+    "dlp_amg_prolong_add": ("iippqpqip", ct.c_int),
+    "dlp_amg_scale_rows": ("iidpqppqip", ct.c_int),
+    "dlp_amg_jacobi_sweep": ("iippppqpqpdpqip", ct.c_int),
+    "dlp_dense_apply": ("iippqpqip", ct.c_int),
     "dlp_ground_update": ("ipppppp", ct.c_int),
 }
 

@@ -85,13 +85,20 @@ __device__ __forceinline__ void load_vec_coherent(const T *p, TA (&out)[VW]) {
 __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
 
+// Hardware lane id (correct for 1-D and multi-dimensional blocks alike).
+__device__ __forceinline__ int lane_id() {
+  unsigned l;
+  asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+  return (int)l;
+}
+
 // Warp-aggregated append: every lane with pred=true gets a unique slot in out (order within a
 // warp follows lane order; across warps it is unordered).
 __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t *out, int32_t *count) {
   const unsigned mask = __activemask();
   const unsigned ballot = __ballot_sync(mask, pred);
   if (!ballot) return;
-  const int lane = threadIdx.x & 31;
+  const int lane = lane_id();
   const int leader = __ffs(ballot) - 1;
   int base = 0;
   if (lane == leader) base = atomicAdd(count, __popc(ballot));
@@ -102,7 +109,7 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t *o
 // Deterministic warp-wide sum (or max) of base[b * stride] over b < nb: lane l takes b = l, l+32,
 // ... (independent loads, so the latency overlaps), then a fixed xor tree. All lanes get the result.
 __device__ __forceinline__ double warp_strided_reduce(const double *base, long long stride, int nb, bool is_max) {
-  const int lane = threadIdx.x & 31;
+  const int lane = lane_id();
   double v = 0.0;
   for (int b = lane; b < nb; b += 32) {
     const double x = base[(long long)b * stride];

@@ -3,7 +3,7 @@
 
 namespace dlp {
 
-// op 0: Y = X / scale[c]   op 1: Y += X * scale[c]   op 2: Y = X * scale[c]
+// op 0: Y = X / scale[c]   op 1: Y += X * scale[c]   op 2: Y = X * scale[c]   op 3: Y = X + Y * scale[c]
 template <typename TX, typename TY>
 __global__ void k_cols_scale(int32_t n, int32_t C, const TX *__restrict__ X, int64_t ldx,
                              const double *__restrict__ scale, int op, TY *Y, int64_t ldy) {
@@ -15,7 +15,8 @@ __global__ void k_cols_scale(int32_t n, int32_t C, const TX *__restrict__ X, int
   const double s = scale[c];
   if (op == 0) Y[r * ldy + c] = (TY)(x / s);
   else if (op == 1) Y[r * ldy + c] = (TY)((double)Y[r * ldy + c] + x * s);
-  else Y[r * ldy + c] = (TY)(x * s);
+  else if (op == 2) Y[r * ldy + c] = (TY)(x * s);
+  else Y[r * ldy + c] = (TY)(x + (double)Y[r * ldy + c] * s);
 }
 
 // umask[v] = vmask[v] && root(v) == root(sink); in_t[v] = membership changed; counts[0] += |changed|
@@ -42,7 +43,7 @@ extern "C" {
 
 int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
                    void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream) {
-  if (n < 0 || C <= 0 || ldx < C || ldy < C || op < 0 || op > 2) return DLP_ERR_INVALID;
+  if (n < 0 || C <= 0 || ldx < C || ldy < C || op < 0 || op > 3) return DLP_ERR_INVALID;
   if (n == 0) return DLP_OK;
   if (!X || !Y || !scale) return DLP_ERR_INVALID;
   const int grid = ceil_div_i((long long)n * C, 256);

@@ -236,7 +236,8 @@ int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t
 
 /* ---- vector helpers of the refinement loop (dynlp/solvers.py:333-337) and grounding ---------
  * op 0: Y = X / scale[c] (the scaled residual, cast to Y's precision); op 1: Y += X * scale[c]
- * (Z64 += D * scale); op 2: Y = X * scale[c]. scale is a device double[C]. Precisions: f32/f64. */
+ * (Z64 += D * scale); op 2: Y = X * scale[c]; op 3: Y = X + Y * scale[c] (P = Y + beta P).
+ * scale is a device double[C]. Precisions: f32/f64. */
 int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
                    void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream);
 
@@ -262,6 +263,46 @@ int dlp_fused_push(const int32_t *rbeg, const int32_t *rend, const int32_t *col,
                    const double *eps, const int32_t *cand, int32_t ncand, int32_t max_rounds, int32_t check_every,
                    int32_t use_graph, void *ws, size_t ws_bytes, int32_t *rounds_out, int32_t *converged_out,
                    unsigned long long *edges_out, dlp_stream_t stream);
+
+
+/* ---- (e) aggregation AMG: setup and V-cycle (dynlp/amg.py) ---------------------------------
+ * Heavy-edge handshake matching (amg.py:32-64) on a plain CSR (indptr/col/w fp32): `rounds`
+ * rounds of mutual heaviest-admissible-neighbour choices (ties: smallest id), then unmatched
+ * vertices join their heaviest matched neighbour, the rest stay single; agg[u] = rank of the
+ * aggregate's representative (numpy.unique's inverse); *n_agg (device int) = number of aggregates. */
+size_t dlp_amg_match_workspace_bytes(int32_t n);
+int dlp_amg_match(int32_t n, const int32_t *indptr, const int32_t *col, const float *w, int32_t rounds, int32_t *agg,
+                  int32_t *n_agg, void *ws, size_t ws_bytes, dlp_stream_t stream);
+/* Members of each aggregate in ascending fine id: off[0..nc] and members[0..n). */
+size_t dlp_amg_members_workspace_bytes(int32_t nc);
+int dlp_amg_members(int32_t n, int32_t nc, const int32_t *agg, int32_t *off, int32_t *members, void *ws,
+                    size_t ws_bytes, dlp_stream_t stream);
+/* Galerkin coarse operator of the piecewise-constant prolongation (amg.py:67-74), in two steps:
+ * plan (per-coarse-row table offsets toff[0..nc], toff[nc] = slots to provide), then coarsen:
+ * W_c[a, b] = sum of w(u, v) over u in a, v in b, a != b (sorted rows, fp64 sums in a fixed order,
+ * stored fp32), s_c[a] = sum of s over a (s_fine may be NULL). tkey/tval: toff[nc] slots each.
+ * Both take dlp_amg_members_workspace_bytes(nc) of workspace. */
+int dlp_amg_coarse_plan(int32_t nc, const int32_t *off, const int32_t *members, const int32_t *indptr, int32_t *toff,
+                        void *ws, size_t ws_bytes, dlp_stream_t stream);
+int dlp_amg_coarsen(int32_t nc, const int32_t *off, const int32_t *members, const int32_t *indptr, const int32_t *col,
+                    const float *w, const int32_t *agg, const int32_t *toff, int32_t *tkey, double *tval,
+                    int64_t total_slots, const double *s_fine, double *s_coarse, int32_t *indptr_c, int32_t *col_c,
+                    float *w_c, void *ws, size_t ws_bytes, dlp_stream_t stream);
+/* V-cycle pieces (amg.py:460-480 region, Level.apply / _smooth / _cycle):
+ * restrict Rc[a,:] = sum over members of R (ordered); prolong X[u,:] += Xc[agg[u],:];
+ * scale_rows X = omega R / diag; jacobi_sweep Y = X + omega ((RHS + W X) / diag - X);
+ * dense_apply Y = M X with M a row-major fp64 nc x nc matrix (the coarsest-level inverse). */
+int dlp_amg_restrict(int32_t nc, int32_t C, const int32_t *off, const int32_t *members, const void *R, int64_t ldr,
+                     void *Rc, int64_t ldc, int dtype, dlp_stream_t stream);
+int dlp_amg_prolong_add(int32_t n, int32_t C, const int32_t *agg, const void *Xc, int64_t ldc, void *X, int64_t ldx,
+                        int dtype, dlp_stream_t stream);
+int dlp_amg_scale_rows(int32_t n, int32_t C, double omega, const void *R, int64_t ldr, const void *diag, void *X,
+                       int64_t ldx, int dtype, dlp_stream_t stream);
+int dlp_amg_jacobi_sweep(int32_t n, int32_t C, const int32_t *indptr, const int32_t *col, const float *w,
+                         const void *X, int64_t ldx, const void *RHS, int64_t ldr, const void *diag, double omega,
+                         void *Y, int64_t ldy, int dtype, dlp_stream_t stream);
+int dlp_dense_apply(int32_t nc, int32_t C, const double *M, const void *X, int64_t ldx, void *Y, int64_t ldy,
+                    int dtype, dlp_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -306,3 +306,114 @@ def relres(W, diag, Z, rhs):
     num = np.sqrt((R * R).sum(axis=0))
     den = np.sqrt((rhs.astype(np.float64) ** 2).sum(axis=0))
     return float((num / np.where(den > 0, den, 1)).max())
+
+
+# ---------------------------------------------------------------------------------------------
+# aggregation AMG (dynlp/amg.py)
+# ---------------------------------------------------------------------------------------------
+def handshake(n, rows, cols, w, rounds):
+    """Heavy-edge handshake matching; unmatched vertices join a matched neighbour (amg.py:32-64)."""
+    agg = np.full(n, -1, dtype=np.int64)
+    matched = np.zeros(n, dtype=bool)
+    ar = np.arange(n, dtype=np.int64)
+
+    def best_choice(er, ec, ew):
+        best = np.full(n, -np.inf, dtype=ew.dtype)
+        np.maximum.at(best, er, ew)
+        tie = ew >= best[er]
+        choice = np.full(n, n, dtype=np.int64)
+        np.minimum.at(choice, er[tie], ec[tie].astype(np.int64))
+        return choice
+
+    for _ in range(rounds):
+        ok = ~matched[rows] & ~matched[cols]
+        if not ok.any():
+            break
+        choice = best_choice(rows[ok], cols[ok], w[ok])
+        has = choice < n
+        partner = np.where(has, choice, 0)
+        mutual = has & (choice[partner] == ar)
+        matched |= mutual
+        agg = np.where(mutual, np.minimum(ar, partner), agg)
+    ok = ~matched[rows] & matched[cols]
+    if ok.any():
+        choice = best_choice(rows[ok], cols[ok], w[ok])
+        has = choice < n
+        agg[has] = agg[choice[has]]
+    left = agg < 0
+    agg[left] = ar[left]
+    uniq, inv = np.unique(agg, return_inverse=True)
+    return inv.ravel().astype(np.int64), int(uniq.shape[0])
+
+
+def coarsen(W, s, agg, nc):
+    """W_c sums the inter-aggregate weights, s_c the grounding (amg.py:67-74)."""
+    rows = csr_rows(W)
+    rc, cc = agg[rows], agg[W.indices]
+    off = rc != cc
+    Wc = coalesce(rc[off], cc[off], W.data[off], nc, W.data.dtype)
+    sc = np.zeros(nc, dtype=s.dtype)
+    np.add.at(sc, agg, s)
+    return Wc, sc
+
+
+class AMGOracle:
+    """V-cycle preconditioner (amg.py:77-134), same defaults."""
+
+    def __init__(self, W, s, *, max_coarse=1500, passes=2, rounds=3, omega=0.7, nu=1, max_levels=25, min_ratio=0.85,
+                 coarse_sweeps=20):
+        self.omega, self.nu, self.coarse_sweeps = omega, nu, coarse_sweeps
+        self.levels = []
+        dt = W.data.dtype
+        n = W.shape[0]
+        cur = dict(W=W, s=s, diag=s + W @ np.ones(n, dtype=dt))
+        while n > max_coarse and len(self.levels) < max_levels:
+            agg = np.arange(n, dtype=np.int64)
+            nc, Wp = n, cur["W"]
+            for _ in range(passes):
+                a2, nc2 = handshake(Wp.shape[0], csr_rows(Wp), Wp.indices, Wp.data, rounds)
+                agg = a2[agg]
+                Wp, _ = coarsen(Wp, np.zeros(Wp.shape[0], dtype=dt), a2, nc2)
+                nc = nc2
+            if nc > min_ratio * n:
+                break
+            Wc, sc = coarsen(cur["W"], cur["s"], agg, nc)
+            cur["agg"] = agg
+            self.levels.append(cur)
+            cur = dict(W=Wc, s=sc, diag=sc + Wc @ np.ones(nc, dtype=dt))
+            n = nc
+        self.coarse = cur
+        self.inv = None
+        if n <= 4 * max_coarse:
+            Ad = -cur["W"].toarray().astype(np.float64)
+            Ad[np.arange(n), np.arange(n)] += cur["diag"].astype(np.float64)
+            self.inv = np.linalg.inv(Ad)
+        self.sizes = [L["W"].shape[0] for L in self.levels] + [n]
+
+    def _apply(self, L, X):
+        return L["diag"][:, None] * X - L["W"] @ X
+
+    def _smooth(self, L, X, R, sweeps):
+        for _ in range(sweeps):
+            X = X + self.omega * (R - self._apply(L, X)) / L["diag"][:, None]
+        return X
+
+    def _cycle(self, lvl, R):
+        if lvl == len(self.levels):
+            L = self.coarse
+            if self.inv is not None:
+                return self.inv @ R
+            X = self.omega * R / L["diag"][:, None]
+            return self._smooth(L, X, R, self.coarse_sweeps - 1)
+        L = self.levels[lvl]
+        X = self.omega * R / L["diag"][:, None]
+        X = self._smooth(L, X, R, self.nu - 1)
+        nc = (self.levels[lvl + 1]["W"] if lvl + 1 < len(self.levels) else self.coarse["W"]).shape[0]
+        Rr = R - self._apply(L, X)
+        Rc = np.zeros((nc, R.shape[1]))
+        np.add.at(Rc, L["agg"], Rr)
+        X = X + self._cycle(lvl + 1, Rc)[L["agg"]]
+        return self._smooth(L, X, R, self.nu)
+
+    def __call__(self, R):
+        return self._cycle(0, R)

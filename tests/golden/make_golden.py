@@ -152,6 +152,31 @@ def gen_solvers(dl):
     save("solvers.npz", **out)
 
 
+def gen_amg(dl):
+    """AMG setup and one V-cycle of the reference (dynlp/amg.py) on a float32 system."""
+    from dynlp.amg import AMG, _handshake, _coarsen
+    from dynlp.graphs import csr_rows
+    out = {}
+    ds, st, s, active = _stream_system(dl, n=3000, K=3, deg=8, seed=3, batch=2, dtype="float32")
+    out.update(csr_parts("W", s.W))
+    out["s"] = np.asarray(s.s, dtype=np.float64)
+    W = s.W
+    a2, nc2 = _handshake(W.shape[0], csr_rows(W), W.indices, W.data, 3)
+    out.update({"match_agg": np.asarray(a2, np.int32), "match_nc": np.int64(nc2)})
+    Wc, sc = _coarsen(W, s.s, a2, nc2)
+    out.update(csr_parts("match_Wc", Wc))
+    out["match_sc"] = np.asarray(sc, np.float64)
+    amg = AMG(W, s.s, max_coarse=50)
+    out["sizes"] = np.asarray(amg.sizes, np.int64)
+    for i, L in enumerate(amg.levels):
+        out[f"L{i}_agg"] = np.asarray(L.agg, np.int32)
+    rs = np.random.RandomState(4)
+    R = rs.standard_normal((W.shape[0], 3)).astype(np.float32)
+    out["R"] = R
+    out["MR"] = np.asarray(amg(R), np.float64)
+    save("amg.npz", **out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", default="/root/reference")
@@ -159,7 +184,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     import cupy_shim
     dl = cupy_shim.install(a.reference)
-    gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers}
+    gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg}
     for name, fn in gens.items():
         if not a.only or name in a.only.split(","):
             fn(dl)

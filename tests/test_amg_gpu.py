@@ -1,0 +1,68 @@
+"""Aggregation AMG on the device against the reference's outputs (GPU)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_csr, load_golden
+from dynlplus_b200 import amg, graphs, solvers, stream
+from dynlplus_b200.backend import CSR
+from oracle import ref_np as O
+
+pytestmark = pytest.mark.gpu
+
+
+def test_handshake_and_coarsen_match_reference():
+    g = load_golden("amg.npz")
+    W = CSR.from_scipy(golden_csr(g, "W"), dtype=torch.float32)
+    agg, nc = amg.handshake(W, 3)
+    np.testing.assert_array_equal(agg.cpu().numpy(), g["match_agg"])
+    assert nc == int(g["match_nc"])
+    Wc, sc = amg.coarsen(W, torch.as_tensor(g["s"]).cuda(), agg, nc)
+    Wg = golden_csr(g, "match_Wc")
+    got = Wc.to_scipy()
+    np.testing.assert_array_equal(got.indptr, Wg.indptr)
+    np.testing.assert_array_equal(got.indices, Wg.indices)
+    np.testing.assert_allclose(got.data, Wg.data, rtol=1e-6)
+    np.testing.assert_allclose(sc.cpu().numpy(), g["match_sc"], rtol=1e-6)  # reference: fp32 sums
+
+
+def test_hierarchy_and_vcycle_match_reference():
+    g = load_golden("amg.npz")
+    W = CSR.from_scipy(golden_csr(g, "W"), dtype=torch.float32)
+    M = amg.AMG(W, torch.as_tensor(g["s"]).cuda(), max_coarse=50)
+    assert M.sizes == list(g["sizes"])
+    for i, L in enumerate(M.levels):
+        np.testing.assert_array_equal(L.agg.cpu().numpy(), g[f"L{i}_agg"])
+    R = torch.as_tensor(g["R"]).cuda()
+    Y = M(R).double().cpu().numpy()
+    np.testing.assert_allclose(Y, g["MR"], rtol=1e-4, atol=1e-5 * abs(g["MR"]).max())
+
+
+def test_amg_is_symmetric_positive_definite():
+    """tests/test_dynlp.py:159-166: the V-cycle operator is symmetric with positive eigenvalues."""
+    ds = graphs.sbm(1200, K=2, deg=6, seed=7, dtype="float64")
+    lab = graphs.label_mask(1200, 0.02, seed=7)
+    S = stream.build_system(ds, torch.ones(1200, dtype=torch.bool, device="cuda"), lab, dtype="float64")
+    M = amg.AMG(S.W, S.s, max_coarse=50)
+    assert len(M.levels) >= 2
+    Mi = M(torch.eye(S.n_u, dtype=torch.float64, device="cuda")).cpu().numpy()
+    np.testing.assert_allclose(Mi, Mi.T, atol=1e-6)  # fp32 weights on the levels: 1e-6 instead of 1e-10
+    assert np.linalg.eigvalsh((Mi + Mi.T) / 2).min() > 0
+
+
+@pytest.mark.parametrize("K", [2, 3])
+def test_dynlp_plus_amg_certificate(K):
+    ds = graphs.sbm(3000, K=K, deg=8, seed=3, dtype="float32")
+    lab = graphs.label_mask(3000, 0.02, seed=3)
+    S = stream.build_system(ds, torch.ones(3000, dtype=torch.bool, device="cuda"), lab, dtype="float32")
+    solver = solvers.DynLPPlus(3000, K, "float32", method="amg", tol=1e-3)
+    st = solver.solve(S)
+    S64 = S.astype(torch.float64)
+    import scipy.sparse as ssp
+    import scipy.sparse.linalg as sla
+    A = ssp.diags(S64.diag.cpu().numpy()) - S64.W.to_scipy().astype(np.float64)
+    Fd = sla.spsolve(A.tocsc(), S64.rhs.cpu().numpy())
+    Fd = Fd.reshape(-1, 1) if Fd.ndim == 1 else Fd
+    err = np.abs(solver.scores(S).cpu().numpy() - Fd).max()
+    assert st.cert <= 1e-3 * 1.0001 and err <= st.cert * 1.05 + 1e-6, (err, st.cert, st.iters)
+    assert st.iters < 60

@@ -90,3 +90,20 @@ def test_apply_edges_set_semantics():
     assert D[1, 2] == D[2, 1] == 7.0             # deleted then re-inserted in the same batch
     assert D[0, 1] == 1.0                        # untouched
     assert (D == D.T).all()
+
+
+def test_amg_matches_reference():
+    g = load_golden("amg.npz")
+    W = golden_csr(g, "W")
+    a2, nc = O.handshake(W.shape[0], O.csr_rows(W), W.indices, W.data, 3)
+    np.testing.assert_array_equal(a2, g["match_agg"])
+    assert nc == int(g["match_nc"])
+    Wc, sc = O.coarsen(W, g["s"], a2, nc)
+    Wg = golden_csr(g, "match_Wc")
+    assert abs(Wc - Wg).max() <= 1e-6 * abs(Wg).max()
+    np.testing.assert_allclose(sc, g["match_sc"], rtol=1e-6)  # the reference sums fp32 groundings in fp32
+    amg = O.AMGOracle(W, g["s"].astype(np.float32), max_coarse=50)
+    assert amg.sizes == list(g["sizes"])
+    for i, L in enumerate(amg.levels):
+        np.testing.assert_array_equal(L["agg"], g[f"L{i}_agg"])
+    np.testing.assert_allclose(amg(g["R"].astype(np.float64)), g["MR"], rtol=1e-4, atol=1e-5 * abs(g["MR"]).max())
