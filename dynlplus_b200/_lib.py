@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libdlp.so")
 DLP_F32, DLP_F64, DLP_BF16 = 0, 1, 2
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported precision combination", 3: "CUDA runtime error",
           4: "iteration cap reached", 5: "cancelled", 6: "workspace too small", 7: "row capacity exceeded",
-          8: "device-side check failed"}
+          8: "device-side check failed", 9: "size exceeds the fixed scratch of an allocation-free entry point"}
 
 _P, _I, _Q, _D, _Z = ct.c_void_p, ct.c_int32, ct.c_int64, ct.c_double, ct.c_size_t
 _CODES = {"p": _P, "i": _I, "q": _Q, "d": _D, "z": _Z}
@@ -36,6 +36,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_compact": ("ppipppzp", ct.c_int),
     "dlp_colreduce_workspace_bytes": ("i", ct.c_size_t),
     "dlp_colreduce": ("iiipqpqpipppzp", ct.c_int),
+    "dlp_colreduce_noalloc": ("iiipqpqpippp", ct.c_int),
     "dlp_cc_edges": ("ippqppp", ct.c_int),
     "dlp_cc_graph": ("ippppippppp", ct.c_int),
     "dlp_cc_relabel": ("ippppzp", ct.c_int),

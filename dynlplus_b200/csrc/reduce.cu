@@ -1,4 +1,6 @@
 // Ordered stream compaction (numpy.flatnonzero semantics) and deterministic column reductions.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace dlp {
@@ -233,11 +235,74 @@ __global__ void k_colreduce_final(int kind, int32_t C, int nb, const double *__r
   if ((threadIdx.x & 31) == 0) out[c] = v;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Allocation-free column reduction. Some callers cannot allocate device memory at the point where
+// they need a reduction: a serving process that reserved all of HBM for its own pool up front, a
+// host runtime reached through a foreign-function bridge that has no device allocator wired in,
+// or code that must not trigger the implicit synchronisation an allocation can cause. For them
+// the per-block partial sums live in this fixed file-scope array instead of a caller workspace.
+// Every GPU that loads the library holds it (kRedBlocks x kStaticMaxCols doubles = 151,552 bytes)
+// until the process exits. All calls on a device share it, so calls that overlap on the GPU (on
+// different streams, or from different host threads) race and must be serialised by the caller.
+// Nothing in it has to start at zero: each call writes every partial it later reads.
+// ------------------------------------------------------------------------------------------------
+constexpr int kStaticMaxCols = 64;
+static __device__ __align__(256) double g_colreduce_scratch[kRedBlocks * kStaticMaxCols];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_scratch_mu;
+static double *g_scratch_addr[kMaxDevices];
+
+// Device address of the array on the current device, looked up once per device. The name
+// g_colreduce_scratch on the host is only a stand-in for the symbol, not a device address.
+static int scratch_address(double **out) {
+  int dev = 0;
+  DLP_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return DLP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_colreduce_scratch);
+    if (e != cudaSuccess) {
+      set_cuda_error(e);
+      return DLP_ERR_CUDA;
+    }
+    g_scratch_addr[dev] = (double *)p;
+  }
+  *out = g_scratch_addr[dev];
+  return DLP_OK;
+}
+
 }  // namespace dlp
 
 using namespace dlp;
 
 extern "C" {
+
+int dlp_colreduce_noalloc(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
+                          const void *diag, int dtype, const uint8_t *mask, double *out, dlp_stream_t stream) {
+  if (kind < 0 || kind > 3 || n < 0 || C <= 0 || ldx < C || !out) return DLP_ERR_INVALID;
+  if (C > kStaticMaxCols) return DLP_ERR_SCRATCH_LIMIT;
+  if (n > 0 && !X) return DLP_ERR_INVALID;
+  if (kind == 0 && n > 0 && !diag) return DLP_ERR_INVALID;
+  if (kind == 1 && n > 0 && (!Y || ldy < C)) return DLP_ERR_INVALID;
+  double *partial = nullptr;
+  DLP_TRY(scratch_address(&partial));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = n > 0 ? (n < kRedBlocks ? (n + 255) / 256 : kRedBlocks) : 0;
+  if (nb > 0) {
+    if (dtype == DLP_F32)
+      k_colreduce_partial<float><<<nb, 256, 0, s>>>(kind, n, C, (const float *)X, ldx, (const float *)Y, ldy,
+                                                    (const float *)diag, mask, partial);
+    else if (dtype == DLP_F64)
+      k_colreduce_partial<double><<<nb, 256, 0, s>>>(kind, n, C, (const double *)X, ldx, (const double *)Y, ldy,
+                                                     (const double *)diag, mask, partial);
+    else
+      return DLP_ERR_DTYPE;
+  }
+  k_colreduce_final<<<(C + 7) / 8, 256, 0, s>>>(kind, C, nb, partial, out);
+  return check_launch(nb > 0 ? 2 : 1);
+}
 
 size_t dlp_compact_workspace_bytes(int32_t n) { return compact_ws_bytes(n < 0 ? 0 : n); }
 

@@ -382,6 +382,7 @@ const char *dlp_status_string(int st) {
     case DLP_ERR_WORKSPACE: return "workspace too small";
     case DLP_ERR_OVERFLOW: return "row capacity exceeded";
     case DLP_ERR_DEVICE: return "device-side check failed";
+    case DLP_ERR_SCRATCH_LIMIT: return "size exceeds the fixed scratch of an allocation-free entry point";
     default: return "unknown status";
   }
 }

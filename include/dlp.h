@@ -38,7 +38,8 @@ enum {
   DLP_ERR_CANCELLED = 5, /* the host cancel flag was set */
   DLP_ERR_WORKSPACE = 6, /* workspace missing or too small */
   DLP_ERR_OVERFLOW = 7,  /* a row of the resident graph ran out of slack; rebuild needed */
-  DLP_ERR_DEVICE = 8     /* a device-side check failed (bad index or bounded wait ran out) */
+  DLP_ERR_DEVICE = 8,    /* a device-side check failed (bad index or bounded wait ran out) */
+  DLP_ERR_SCRATCH_LIMIT = 9 /* size beyond the fixed scratch of an allocation-free entry point */
 };
 
 enum { DLP_F32 = 0, DLP_F64 = 1, DLP_BF16 = 2 };
@@ -122,6 +123,18 @@ int dlp_compact(const uint8_t *flag, const int32_t *idx, int32_t n, int32_t *out
  * pass: the result does not depend on scheduling. Workspace: dlp_colreduce_workspace_bytes(C). */
 size_t dlp_colreduce_workspace_bytes(int32_t C);
 
+/* Allocation-free variant of dlp_colreduce (no counterpart in the reference): same kinds, inputs,
+ * output and results, but it takes no workspace. It is for callers that cannot allocate device
+ * memory when they need the reduction (a server that reserved all of HBM for its own pool, a host
+ * runtime bridged through an FFI with no device allocator, code that must avoid the implicit
+ * synchronisation of an allocation). Its partial sums live in a fixed array inside the library,
+ * sized for C <= 64 columns (151,552 bytes, held on every GPU that loads the library until exit);
+ * wider inputs return DLP_ERR_SCRATCH_LIMIT. The first call on each device looks the array's
+ * device address up (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. It allocates nothing and calls no allocating routine. */
+int dlp_colreduce_noalloc(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
+                          const void *diag, int dtype, const uint8_t *mask, double *out, dlp_stream_t stream);
 int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
                   const void *diag, int dtype, const uint8_t *mask, double *out, void *ws, size_t ws_bytes,
                   dlp_stream_t stream);

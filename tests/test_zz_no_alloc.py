@@ -1,0 +1,48 @@
+"""The allocation-free column reduction, dlp_colreduce_noalloc (GPU).
+
+It exists for callers that cannot allocate device memory when they need a reduction: a serving
+process that reserved all of HBM for its own pool up front, a host runtime bridged through an FFI
+without a device allocator, or code that must not pay the implicit synchronisation an allocation
+can cause. It keeps its partial sums in a fixed array inside the library (up to 64 columns) rather
+than in a caller workspace. Called through the C ABI, it must return what the workspace version
+dlp_colreduce returns, on two calls in a row, and refuse wider inputs with a clear status.
+This file is named to be collected last.
+"""
+import numpy as np
+import pytest
+import torch
+
+from dynlplus_b200 import _lib, kernels
+from dynlplus_b200.backend import code, ld, ptr, stream
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(kind, X, Y=None, diag=None, mask=None):
+    n, C = X.shape
+    out = torch.full((C,), float("nan"), dtype=torch.float64, device=X.device)
+    _lib.call("dlp_colreduce_noalloc", kind, n, C, ptr(X), ld(X), ptr(Y), ld(Y) if Y is not None else C, ptr(diag),
+              code(X), ptr(mask), ptr(out), stream())
+    return out
+
+
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+def test_noalloc_matches_workspace_version_twice(dt):
+    rs = np.random.RandomState(42)
+    for call in range(2):  # the second call must not see anything of the first
+        for n, C in ((1, 1), (257, 3), (100_003, 9), (300_000, 33), (50_000, 64)):
+            X = torch.as_tensor(rs.randn(n, C)).to(dt).cuda()
+            Y = torch.as_tensor(rs.randn(n, C)).to(dt).cuda()
+            d = torch.as_tensor(rs.rand(n) + 0.5).to(dt).cuda()
+            mask = torch.as_tensor((rs.rand(n) < 0.5).astype(np.uint8)).cuda()
+            for kind, kw in ((0, dict(diag=d)), (1, dict(Y=Y)), (2, {}), (3, dict(mask=mask))):
+                want = kernels.colreduce(kind, X, **kw).cpu().numpy()
+                got = _noalloc(kind, X, **kw).cpu().numpy()
+                np.testing.assert_allclose(got, want, rtol=1e-12, atol=0, err_msg=f"call {call} kind {kind} C {C}")
+
+
+def test_noalloc_refuses_more_columns_than_its_scratch():
+    X = torch.zeros((10, 65), dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.DLPError) as e:
+        _noalloc(2, X)
+    assert e.value.status == 9
