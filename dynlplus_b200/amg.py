@@ -191,6 +191,12 @@ class AMG:
         return self._smooth(L, X, R, self.nu, lvl)
 
     def __call__(self, R):
-        """M(R): one V-cycle; returns a new tensor (the cycle's buffers are reused across calls)."""
+        """M(R): one V-cycle; returns a new tensor (the cycle's buffers are reused across calls).
+        Inputs wider than 64 columns are cycled 64 columns at a time (the columns are independent)."""
         R = R.contiguous()
-        return self._cycle(0, R).clone()
+        if R.shape[1] <= 64:
+            return self._cycle(0, R).clone()
+        out = torch.empty_like(R)
+        for c0 in range(0, R.shape[1], 64):
+            out[:, c0:c0 + 64] = self._cycle(0, R[:, c0:c0 + 64].contiguous())
+        return out

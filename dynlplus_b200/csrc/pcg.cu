@@ -246,23 +246,26 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
   // block reduction: per column over ty (fixed order), max over all
   const int tid = ty * CX + tx;
   s_v[tid] = vmax;
-  for (int m = 0; m < nch; ++m) {
-    s_rz[tid] = rz[m];
-    s_ss[tid] = ss[m];
-    __syncthreads();
-    if (ty == 0) {
-      const int c = tx + m * CX;
-      double a = 0.0, b = 0.0;
-      for (int y = 0; y < RY; ++y) {
-        a += s_rz[y * CX + tx];
-        b += s_ss[y * CX + tx];
+#pragma unroll
+  for (int m = 0; m < kMaxColChunks; ++m) {  // compile-time indices keep rz/ss in registers
+    if (m < nch) {                            // nch is uniform over the block
+      s_rz[tid] = rz[m];
+      s_ss[tid] = ss[m];
+      __syncthreads();
+      if (ty == 0) {
+        const int c = tx + m * CX;
+        double a = 0.0, b = 0.0;
+        for (int y = 0; y < RY; ++y) {
+          a += s_rz[y * CX + tx];
+          b += s_ss[y * CX + tx];
+        }
+        if (c < C) {
+          B.part2[((long long)blockIdx.x * C + c) * 2 + 0] = a;
+          B.part2[((long long)blockIdx.x * C + c) * 2 + 1] = b;
+        }
       }
-      if (c < C) {
-        B.part2[((long long)blockIdx.x * C + c) * 2 + 0] = a;
-        B.part2[((long long)blockIdx.x * C + c) * 2 + 1] = b;
-      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   if (tid == 0) {
     double v = 0.0;
