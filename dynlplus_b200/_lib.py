@@ -65,6 +65,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_amg_scale_rows": ("iidpqppqip", ct.c_int),
     "dlp_amg_jacobi_sweep": ("iippppqpqpdpqip", ct.c_int),
     "dlp_dense_apply": ("iippqpqip", ct.c_int),
+    "dlp_pcg_batched_workspace_bytes": ("iii", ct.c_size_t),
+    "dlp_pcg_batched": ("pppiippqpqpqpqpqiiippppppdiiiiiidpzpppp", ct.c_int),
     "dlp_ground_update": ("ipppppp", ct.c_int),
 }
 

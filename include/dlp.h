@@ -317,6 +317,28 @@ int dlp_amg_jacobi_sweep(int32_t n, int32_t C, const int32_t *indptr, const int3
 int dlp_dense_apply(int32_t nc, int32_t C, const double *M, const void *X, int64_t ldx, void *Y, int64_t ldy,
                     int dtype, dlp_stream_t stream);
 
+
+/* ---- batched independent solves (config: many instances in one launch sequence) -------------
+ * No reference counterpart (the reference solves one system at a time). Block PCG with the Jacobi
+ * preconditioner over a concatenated block-diagonal CSR (indptr/col/w fp32, N rows, C <= 64
+ * columns) holding `ninst` independent systems. Rows are cut into `ntiles` tiles that never
+ * straddle two instances: tile t covers rows [tile_beg[t], tile_end[t]) of instance tile_inst[t],
+ * and instance i owns tiles [inst_tiles[i], inst_tiles[i+1]) (inst_tiles has ninst + 1 entries).
+ * Every instance runs its own CG (its own alpha, beta and stop state; reductions per instance in
+ * a fixed tile order, so an instance gets the iterates it would get alone) until the stop rule
+ * `mode` (as in dlp_pcg; eps_dev and rhs_norm_dev are DEVICE arrays of ninst x C doubles) holds,
+ * confirmed on its true residual. Synchronous: per-instance iterations, status (5 converged,
+ * 2 stalled, 3 cap, 4 breakdown) and relative residuals are written to HOST arrays of ninst. */
+size_t dlp_pcg_batched_workspace_bytes(int32_t ninst, int32_t ntiles, int32_t C);
+int dlp_pcg_batched(const int32_t *indptr, const int32_t *col, const float *w, int32_t N, int32_t C, const void *diag,
+                    const void *rhs, int64_t ldrhs, void *Z, int64_t ldz, void *R, int64_t ldr, void *P, int64_t ldp,
+                    void *AP, int64_t ldap, int dtype, int32_t ninst, int32_t ntiles, const int32_t *tile_inst,
+                    const int32_t *tile_beg, const int32_t *tile_end, const int32_t *inst_tiles,
+                    const double *eps_dev, const double *rhs_norm_dev, double target_relres, int32_t mode,
+                    int32_t max_iter, int32_t patience, int32_t check_every, int32_t use_graph, int32_t group,
+                    double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, int32_t *status_out,
+                    double *relres_out, dlp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
