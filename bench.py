@@ -50,6 +50,13 @@ def parse(argv=None):
     ap.add_argument("--cpu-budget-s", type=float, default=150.0, help="wall budget of the CPU reference legs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--workload", default="edge-stream",
+                    choices=["edge-stream", "static", "amg", "batched", "serving"],
+                    help="edge-stream: the headline (ER 1M edge batches); static: SBM 100k solve + one "
+                         "1000-update batch; amg: SBM 1M lognormal, AMG-PCG to rel-res 1e-8; batched: 256 SBM "
+                         "instances in one batched solve; serving: resident SBM with mixed Poisson requests")
+    ap.add_argument("--requests", type=int, default=200, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: offered load (requests/s)")
     return ap.parse_args(argv)
 
 
@@ -334,10 +341,152 @@ def ours(a):
     return 0
 
 
+# ---------------------------------------------------------------------------------------------
+# the other workloads (one JSON line each; the driver's headline is edge-stream)
+# ---------------------------------------------------------------------------------------------
+def _line(a, metric, value, unit, ms, cfg, hib=True, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+         "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+         "data": "synthetic", "config": cfg}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def _events(fn):
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    out = fn()
+    e.record()
+    e.synchronize()
+    return s.elapsed_time(e), out
+
+
+def wl_static(a):
+    """Config 1: SBM n=100,000 (4 blocks, degree 12 in + 4 cross, unit weights), 1% labelled, k=4:
+    the static solve by Jacobi-PCG to rel-res 1e-6, then one batch of 1,000 edge updates."""
+    import torch
+    from dynlplus_b200 import graphs, solvers, stream
+    ms_s, ms_u, rel = [], [], []
+    for rep in range(a.warmup + a.steps):
+        ds = graphs.planted_partition(100_000, 4, 12.0, 4.0, seed=rep)
+        lab = graphs.label_mask(100_000, 0.01, seed=rep)
+        es = stream.EdgeStream(ds, lab)
+        solver = solvers.IncrementalLP(100_000, 4, "float32", tol=1e-3, method="pcg", target_relres=1e-6)
+        b = graphs.EdgeUpdates(ds.A, seed=rep).next(1000)
+        t0, st0 = _events(lambda: solver.solve(es.system))
+        t1, st1 = _events(lambda: solver.solve(es.apply_edges(**b)))
+        if rep >= a.warmup:
+            ms_s.append(t0)
+            ms_u.append(t1)
+            rel.append(max(st0.relres, st1.relres))
+    _line(a, "edge-updates/s of the 1,000-update batch after the static solve (rel-res 1e-6)",
+          1000 / (np.mean(ms_u) * 1e-3), "edge-updates/s", float(np.mean(ms_s) + np.mean(ms_u)),
+          {"workload": "sbm-n100000-b4-d12+4-unit-lab0.01-k4", "static_solve_ms": float(np.mean(ms_s)),
+           "update_batch_ms": float(np.mean(ms_u)), "l2": "not flushed (fresh graph per repetition)"},
+          relres_max=float(max(rel)))
+
+
+def wl_amg(a):
+    """Config 3: SBM n=1,000,000, 16 blocks, degree 24 in + 8 cross, lognormal(0, 0.5) weights,
+    1% labelled, k=16: AMG-preconditioned PCG (fp32 sweeps) with fp64 refinement to rel-res 1e-8."""
+    import torch
+    from dynlplus_b200 import graphs, solvers, stream
+    ds = graphs.planted_partition(1_000_000, 16, 24.0, 8.0, weights="lognormal", seed=3)
+    lab = graphs.label_mask(1_000_000, 0.01, seed=3)
+    S = stream.build_system(ds, torch.ones(ds.n, dtype=torch.bool, device="cuda"), lab, dtype="float32")
+    times, rels, iters, setups = [], [], [], []
+    for rep in range(a.warmup + a.steps):
+        solver = solvers.DynLPPlus(ds.n, 16, "float32", method="amg", tol=1e-3, target_relres=1e-8)
+        t, st = _events(lambda: solver.solve(S))
+        if rep >= a.warmup:
+            times.append(t)
+            rels.append(st.relres)
+            iters.append(st.iters)
+            setups.append(st.setup_ms)
+    _line(a, "AMG-PCG solve time to rel-res 1e-8 (fp32 sweeps, fp64 refinement)", float(np.mean(times)), "ms",
+          float(np.mean(times)), {"workload": "sbm-n1000000-b16-d24+8-lognormal-lab0.01-k16"}, hib=False,
+          relres_max=float(max(rels)), pcg_iters=float(np.mean(iters)), amg_setup_ms=float(np.mean(setups)))
+
+
+def wl_batched(a):
+    """Config 4: 256 SBM graphs, n log-uniform in [2,000, 200,000], blocks = k in {2,4,8}, mean degree
+    U[8,24] (3:1 in:cross), unit weights, 1% labelled: all solves batched, rel-res 1e-6."""
+    import torch
+    from dynlplus_b200 import batched, graphs, stream
+    rng = np.random.default_rng(4)
+    systems = []
+    for i in range(256):
+        n = int(np.exp(rng.uniform(np.log(2000), np.log(200_000))))
+        k = int(rng.choice([2, 4, 8]))
+        deg = float(rng.uniform(8, 24))
+        ds = graphs.planted_partition(n, k, 0.75 * deg, 0.25 * deg, seed=1000 + i)
+        lab = graphs.label_mask(n, 0.01, seed=1000 + i)
+        systems.append(stream.build_system(ds, torch.ones(n, dtype=torch.bool, device="cuda"), lab, dtype="float32"))
+    times = []
+    info = None
+    for rep in range(a.warmup + a.steps):
+        t, (Fs, info) = _events(lambda: batched.solve_many(systems, target_relres=1e-6, autotune=True))
+        if rep >= a.warmup:
+            times.append(t)
+    rows = sum(s.n_u for s in systems)
+    _line(a, "independent harmonic solves per second, 256 instances batched (rel-res 1e-6)",
+          256 / (np.mean(times) * 1e-3), "solves/s", float(np.mean(times)),
+          {"workload": "256x sbm n~logU[2e3,2e5] k in {2,4,8} deg~U[8,24] lab0.01", "rows": int(rows)},
+          relres_max=float(max(r for _, _, r in info)), converged=int(sum(s == 5 for _, s, _ in info)))
+
+
+def wl_serving(a):
+    """Config 5: resident SBM n=4,000,000, 32 blocks, degree 16 (12 in + 4 cross), lognormal weights,
+    1% labelled, k=32; Poisson arrivals at `--rate`: 60% edge-update batches (size log-uniform in
+    [10, 50,000]), 30% label queries (1 to 10,000 ids), 10% fresh solves (n log-uniform in
+    [10,000, 500,000], k=32)."""
+    import time as _t
+    import torch
+    from dynlplus_b200 import graphs, serve
+    n = 4_000_000
+    ds = graphs.planted_partition(n, 32, 12.0, 4.0, weights="lognormal", seed=5)
+    lab = graphs.label_mask(n, 0.01, seed=5)
+    srv = serve.Server(ds, lab, target_relres=1e-6)
+    up = graphs.EdgeUpdates(ds.A, seed=5, weights="lognormal")
+    rng = np.random.default_rng(5)
+    reqs = []
+    for i in range(a.requests):
+        u = rng.random()
+        if u < 0.6:
+            b = up.next(int(np.exp(rng.uniform(np.log(10), np.log(50_000)))))
+            reqs.append(serve.EdgeUpdate(b["ins_u"], b["ins_v"], b["ins_w"], b["del_u"], b["del_v"]))
+        elif u < 0.9:
+            reqs.append(serve.LabelQuery(rng.integers(0, n, int(rng.integers(1, 10_001)))))
+        else:
+            m = int(np.exp(rng.uniform(np.log(10_000), np.log(500_000))))
+            reqs.append(serve.FreshSolve(graphs.planted_partition(m, 32, 12.0, 4.0, weights="lognormal", seed=i),
+                                         graphs.label_mask(m, 0.01, seed=i)))
+    gaps = rng.exponential(1.0 / a.rate, len(reqs))
+    t0 = _t.perf_counter()
+    futs = []
+    for r, g in zip(reqs, gaps):
+        _t.sleep(g)
+        futs.append(srv.submit(r))
+    for f in futs:
+        f.result(timeout=1200)
+    wall = _t.perf_counter() - t0
+    updates = sum(r.size for r in reqs if isinstance(r, serve.EdgeUpdate))
+    lat = {k: srv.latency(k) for k in ("update", "query", "fresh")}
+    srv.close()
+    _line(a, "served edge-updates/s under mixed Poisson load (p50/p99 per request kind)", updates / wall,
+          "edge-updates/s", 1e3 * wall / len(reqs),
+          {"workload": "serving sbm-n4000000-b32-d12+4-lognormal-lab0.01-k32", "rate_req_s": a.rate,
+           "requests": len(reqs)}, latency_ms=lat, requests_per_s=len(reqs) / wall)
+
+
 def main(argv=None):
     a = parse(argv)
     if a.impl == "reference":
         return reference_arm(a)
+    if a.workload != "edge-stream":
+        return {"static": wl_static, "amg": wl_amg, "batched": wl_batched, "serving": wl_serving}[a.workload](a) or 0
     return ours(a)
 
 

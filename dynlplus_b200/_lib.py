@@ -27,6 +27,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_sm_count": ("", ct.c_int),
     "dlp_launch_count": ("", ct.c_ulonglong),
     "dlp_spmm": ("ppppiipipqipddpqdpqiiidp", ct.c_int),
+    "dlp_spmm_lowp": ("ppppiipqpqpddpqidp", ct.c_int),
     "dlp_frontier_jacobi": ("ppppipiipqpqpdpqipppidp", ct.c_int),
     "dlp_push_scatter": ("ppppipiipqpqipidp", ct.c_int),
     "dlp_mark_neighbors": ("ppppipp", ct.c_int),
@@ -41,7 +42,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cc_graph": ("ippppippppp", ct.c_int),
     "dlp_cc_relabel": ("ippppzp", ct.c_int),
     "dlp_pcg_workspace_bytes": ("i", ct.c_size_t),
-    "dlp_pcg": ("ppppiiippqpqpqpqpqippdiiiiidpzppppp", ct.c_int),
+    "dlp_pcg": ("ppppiiippqpqpqpqpqippdiiiiidpzpppppppq", ct.c_int),
     "dlp_graph_delete": ("ipppppppipppipppppp", ct.c_int),
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),

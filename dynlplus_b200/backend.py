@@ -101,7 +101,10 @@ _WS: dict = {}
 
 
 def workspace(tag: str = "default") -> Workspace:
-    key = (tag, torch.cuda.current_device() if torch.cuda.is_available() else -1)
+    """Scratch buffer per (tag, device, current stream): work on different streams (the serving
+    loop's workers) never shares a buffer."""
+    key = (tag, torch.cuda.current_device() if torch.cuda.is_available() else -1,
+           torch.cuda.current_stream().cuda_stream if torch.cuda.is_available() else 0)
     if key not in _WS:
         _WS[key] = Workspace()
     return _WS[key]

@@ -101,6 +101,8 @@ struct ApplyArgs {
   int64_t ldap;
   PcgBufs B;
   int G, LV, NV;
+  const typename T::TV *Pown;  // own-row P for the diagonal term and pAp (NULL: P itself)
+  int64_t ldpo;
 };
 
 template <class T, int VW, int VPL>
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
           for (int i = 0; i < VW; ++i) {
             const int c = vi * VW + i;
             if (c < p.C) {
-              const TA pv = cvt<TA>(p.P[r * p.ldp + c]);
+              const TA pv = p.Pown ? cvt<TA>(p.Pown[r * p.ldpo + c]) : cvt<TA>(p.P[r * p.ldp + c]);
               const TA ap = d * pv - acc[k][i];
               p.AP[r * p.ldap + c] = cvt<typename T::TY>(ap);
               dot[k][i] += (double)pv * (double)ap;
@@ -339,7 +341,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
 template <typename T>
 __global__ void __launch_bounds__(256) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z, int64_t ldz,
                                                  T *__restrict__ P, int64_t ldp, const T *__restrict__ R, int64_t ldr,
-                                                 const T *__restrict__ diag, PcgBufs B) {
+                                                 const T *__restrict__ diag, PcgBufs B, bf16 *P_lo, int64_t ld_lo) {
   PcgCtl *ctl = B.ctl;
   if (mode == 0 && !ctl->go) return;
   const bool upd_p = mode != 0 || ctl->done == 0;
@@ -359,7 +361,9 @@ __global__ void __launch_bounds__(256) k_pcg_dir(int mode, int32_t n, int32_t C,
         if (mode == 0) Z[r * ldz + c] += (T)B.alpha[c] * pv;
         if (upd_p) {
           const T y = R[r * ldr + c] / dv;
-          P[r * ldp + c] = mode == 2 ? y : y + (T)B.beta[c] * pv;
+          const T pn = mode == 2 ? y : y + (T)B.beta[c] * pv;
+          P[r * ldp + c] = pn;
+          if (P_lo) P_lo[r * ld_lo + c] = cvt<bf16>(pn);
         }
       }
     }
@@ -391,14 +395,21 @@ struct PcgProblem {
   int64_t ldap;
   int dtype;
   double avg_deg;
+  const void *w_lo;  // bf16 weights and the bf16 mirror of P (NULL: full precision gathers)
+  void *P_lo;
+  int64_t ld_lo;
 };
 
 template <class T>
 static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   Layout L;
-  DLP_TRY(choose_layout(q.C, sizeof(typename T::TX), q.P, q.ldp, 0, q.avg_deg, &L));
-  ApplyArgs<T> a{q.rbeg, q.rend, q.col, (const typename T::TW *)q.w, q.n, q.C, (const typename T::TX *)q.P, q.ldp,
-                 (const typename T::TV *)q.diag, (typename T::TY *)q.AP, q.ldap, B, L.G, L.LV, L.NV};
+  const bool lo = sizeof(typename T::TX) == 2;
+  const void *X = lo ? q.P_lo : q.P;
+  const int64_t ldx = lo ? q.ld_lo : q.ldp;
+  DLP_TRY(choose_layout(q.C, sizeof(typename T::TX), X, ldx, 0, q.avg_deg, &L));
+  ApplyArgs<T> a{q.rbeg, q.rend, q.col, (const typename T::TW *)(lo ? q.w_lo : q.w), q.n, q.C,
+                 (const typename T::TX *)X, ldx, (const typename T::TV *)q.diag, (typename T::TY *)q.AP, q.ldap, B,
+                 L.G, L.LV, L.NV, lo ? (const typename T::TV *)q.P : nullptr, q.ldp};
   const int grid = apply_blocks();
   constexpr int VWV = 16 / sizeof(typename T::TX);
 #define DLP_APPLY_CASE(VW_)                                                           \
@@ -429,13 +440,15 @@ static int launch_update(int phase, const PcgProblem &q, const PcgBufs &B, cudaS
 template <typename TS>
 static int launch_dir(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   k_pcg_dir<TS><<<upd_blocks(), upd_block(q.C), 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
-                                                         (const TS *)q.R, q.ldr, (const TS *)q.diag, B);
+                                                         (const TS *)q.R, q.ldr, (const TS *)q.diag, B,
+                                                         (bf16 *)q.P_lo, q.ld_lo);
   return check_launch();
 }
 
 static int iteration(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   if (q.dtype == DLP_F32) {
-    DLP_TRY(launch_apply<T_F32>(q, B, s));
+    if (q.w_lo) DLP_TRY(launch_apply<T_BF16F>(q, B, s));
+    else DLP_TRY(launch_apply<T_F32>(q, B, s));
     DLP_TRY(launch_update<float>(0, q, B, s));
     return launch_dir<float>(0, q, B, s);
   }
@@ -482,7 +495,8 @@ static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, cudaGra
   GraphKey key{{(uintptr_t)dev, (uintptr_t)q.rbeg, (uintptr_t)q.rend, (uintptr_t)q.col, (uintptr_t)q.w,
                 (uintptr_t)q.w_dtype, (uintptr_t)q.n, (uintptr_t)q.C, (uintptr_t)q.diag, (uintptr_t)q.Z,
                 (uintptr_t)q.ldz, (uintptr_t)q.R, (uintptr_t)q.ldr, (uintptr_t)q.P, (uintptr_t)q.ldp, (uintptr_t)q.AP,
-                (uintptr_t)q.ldap, (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)k,
+                (uintptr_t)q.ldap, (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)k, (uintptr_t)q.w_lo,
+                (uintptr_t)q.P_lo, (uintptr_t)q.ld_lo,
                 (uintptr_t)(q.avg_deg * 1024)}};
   std::lock_guard<std::mutex> lk(g_graph_mu);
   auto it = g_graphs.find(key);
@@ -535,8 +549,10 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
             void *P, int64_t ldp, void *AP, int64_t ldap, int dtype, const double *eps, const double *rhs_norm,
             double target_relres, int32_t mode, int32_t max_iter, int32_t patience, int32_t check_every,
             int32_t use_graph, double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, double *viol_out,
-            double *relres_out, int32_t *status_out, dlp_stream_t stream) {
+            double *relres_out, int32_t *status_out, dlp_stream_t stream, const void *w_lo, void *P_lo,
+            int64_t ld_lo) {
   if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
+  if ((w_lo || P_lo) && (!w_lo || !P_lo || ld_lo < C || dtype != DLP_F32)) return DLP_ERR_INVALID;
   if (mode < 1 || mode > 3 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
     return DLP_ERR_DTYPE;
@@ -547,7 +563,8 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
     return DLP_OK;
   }
   cudaStream_t s = (cudaStream_t)stream;
-  PcgProblem q{rbeg, rend, col, w, w_dtype, n, C, diag, rhs, ldrhs, Z, ldz, R, ldr, P, ldp, AP, ldap, dtype, avg_deg};
+  PcgProblem q{rbeg, rend, col, w, w_dtype, n, C, diag, rhs, ldrhs, Z, ldz, R, ldr, P, ldp, AP, ldap, dtype, avg_deg,
+               w_lo, P_lo, ld_lo};
   PcgBufs B = carve(ws, C);
   PcgCtl h{};
   h.mode = mode;

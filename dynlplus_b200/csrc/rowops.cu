@@ -65,6 +65,8 @@ struct SpmmArgs {
   int64_t ldy;
   int compact;
   int G, LV, NV;
+  const typename T::TV *Xo;  // own-row values for the a-term (NULL: X itself)
+  int64_t ldxo;
 };
 
 template <class T, int VW, int VPL>
@@ -124,7 +126,9 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
             const int c = vi * VW + i;
             if (c < p.C) {
               TA y = (TA)p.b * acc[k][i];
-              if (p.a) y = fmaa(av, cvt<TA>(p.X[(long long)r * p.ldx + c]), y);
+              if (p.a)
+                y = fmaa(av, p.Xo ? cvt<TA>(p.Xo[(long long)r * p.ldxo + c]) : cvt<TA>(p.X[(long long)r * p.ldx + c]),
+                         y);
               if (p.rhs) y += (TA)p.cr * cvt<TA>(p.rhs[(long long)r * p.ldr + c]);
               p.Y[orow * p.ldy + c] = cvt<typename T::TY>(y);
             }
@@ -153,12 +157,12 @@ template <class T>
 static int run_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int32_t n_rows,
                     const int32_t *rows, int32_t C, const void *X, int64_t ldx, const void *a, double alpha,
                     double b, const void *RHS, int64_t ldr, double cr, void *Y, int64_t ldy, int compact,
-                    int32_t group, double avg_deg, dlp_stream_t s) {
+                    int32_t group, double avg_deg, dlp_stream_t s, const void *Xo = nullptr, int64_t ldxo = 0) {
   Layout L;
   DLP_TRY(choose_layout(C, sizeof(typename T::TX), X, ldx, group, avg_deg, &L));
   SpmmArgs<T> p{rbeg, rend, col, (const typename T::TW *)w, n_rows, rows, C, (const typename T::TX *)X, ldx,
                 (const typename T::TV *)a, alpha, b, (const typename T::TV *)RHS, ldr, cr,
-                (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV};
+                (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV, (const typename T::TV *)Xo, ldxo};
   constexpr int VWV = 16 / sizeof(typename T::TX);
   if (L.VW == 1) return launch_spmm_vw<T, 1>(p, L.VPL, s);
   return launch_spmm_vw<T, VWV>(p, L.VPL, s);
@@ -409,6 +413,16 @@ int dlp_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const
   if (w_dtype == DLP_BF16 && x_dtype == DLP_BF16 && y_dtype == DLP_BF16) return run_spmm<T_BF16B>(DLP_SPMM_ARGS);
 #undef DLP_SPMM_ARGS
   return DLP_ERR_DTYPE;
+}
+
+int dlp_spmm_lowp(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w_lo, int32_t n_rows,
+                  int32_t C, const void *X_lo, int64_t ld_lo, const void *X_own, int64_t ld_own, const void *a,
+                  double alpha, double b, void *Y, int64_t ldy, int32_t group, double avg_deg, dlp_stream_t stream) {
+  if (n_rows < 0 || C <= 0 || ld_lo < C || ldy < C || (X_own && ld_own < C)) return DLP_ERR_INVALID;
+  if (n_rows == 0) return DLP_OK;
+  if (!rbeg || !rend || !col || !w_lo || !X_lo || !Y) return DLP_ERR_INVALID;
+  return run_spmm<T_BF16F>(rbeg, rend, col, w_lo, n_rows, nullptr, C, X_lo, ld_lo, a, alpha, b, nullptr, C, 0.0, Y,
+                           ldy, 0, group, avg_deg, stream, X_own, ld_own);
 }
 
 int dlp_frontier_jacobi(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,

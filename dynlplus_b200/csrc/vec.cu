@@ -13,10 +13,14 @@ __global__ void k_cols_scale(int32_t n, int32_t C, const TX *__restrict__ X, int
   const int c = (int)(t % C);
   const double x = (double)X[r * ldx + c];
   const double s = scale[c];
-  if (op == 0) Y[r * ldy + c] = (TY)(x / s);
-  else if (op == 1) Y[r * ldy + c] = (TY)((double)Y[r * ldy + c] + x * s);
-  else if (op == 2) Y[r * ldy + c] = (TY)(x * s);
-  else Y[r * ldy + c] = (TY)(x + (double)Y[r * ldy + c] * s);
+  if constexpr (sizeof(TY) == 2) {
+    Y[r * ldy + c] = cvt<TY>(x * s);  // the bf16 mirror: op 2 only
+  } else {
+    if (op == 0) Y[r * ldy + c] = (TY)(x / s);
+    else if (op == 1) Y[r * ldy + c] = (TY)((double)Y[r * ldy + c] + x * s);
+    else if (op == 2) Y[r * ldy + c] = (TY)(x * s);
+    else Y[r * ldy + c] = (TY)(x + (double)Y[r * ldy + c] * s);
+  }
 }
 
 // umask[v] = vmask[v] && root(v) == root(sink); in_t[v] = membership changed; counts[0] += |changed|
@@ -56,6 +60,8 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
     k_cols_scale<double, double><<<grid, 256, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (double *)Y, ldy);
   else if (x_dtype == DLP_F32 && y_dtype == DLP_F32)
     k_cols_scale<float, float><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (float *)Y, ldy);
+  else if (x_dtype == DLP_F32 && y_dtype == DLP_BF16 && op == 2)
+    k_cols_scale<float, bf16><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (bf16 *)Y, ldy);
   else
     return DLP_ERR_DTYPE;
   return check_launch();

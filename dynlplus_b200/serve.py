@@ -1,0 +1,231 @@
+"""Continuous-batching serving loop over a resident graph (no reference counterpart; the closest
+is the reference's batch loop, dynlp/bench.py:93-118).
+
+The server keeps the resident system (graph, scores, residual) on the device and answers three
+request kinds as they arrive:
+
+* `EdgeUpdate`: edge insertions/deletions. Every queued update is patched into the resident graph
+  in arrival order (so the final graph is the sequential one), then ONE certified solve brings the
+  scores back to the target relative residual for all of them; the request completes when its
+  scores are current. Updates arriving while a solve runs are admitted into the next one.
+* `LabelQuery`: argmax labels of the given vertices, read from the label snapshot published after
+  the last completed update (queries never see scores that are being solved).
+* `FreshSolve`: the harmonic solve of a new graph. Pending fresh solves are admitted while their
+  estimated HBM footprint fits the budget and solved together in one batched launch (per-instance
+  CG, so every result equals what it would be alone); requests arriving meanwhile wait for the next
+  batch. A request larger than the whole budget is refused.
+
+Each kind has its own worker thread and CUDA stream, so their device work overlaps; libdlp calls
+release the GIL. Every request records its submit and completion times (p50/p99 latency).
+"""
+from __future__ import annotations
+
+import queue
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import batched, solvers, stream
+
+
+@dataclass
+class EdgeUpdate:
+    ins_u: np.ndarray
+    ins_v: np.ndarray
+    ins_w: np.ndarray | None = None
+    del_u: np.ndarray | None = None
+    del_v: np.ndarray | None = None
+
+    @property
+    def size(self):
+        return len(self.ins_u) + (len(self.del_u) if self.del_u is not None else 0)
+
+
+@dataclass
+class LabelQuery:
+    ids: np.ndarray
+
+
+@dataclass
+class FreshSolve:
+    ds: object            # graphs.Dataset
+    labeled: torch.Tensor
+
+    def hbm_bytes(self, C):
+        n, nnz = self.ds.n, self.ds.nnz
+        return int(nnz * 12 + n * (C + 1) * 8 * 7 + n * 64)
+
+
+@dataclass
+class _Item:
+    req: object
+    fut: Future
+    t_submit: float
+    kind: str
+    t_done: float = 0.0
+    extra: dict = field(default_factory=dict)
+
+
+class AdmissionError(RuntimeError):
+    """The request cannot fit the HBM budget."""
+
+
+class Server:
+    def __init__(self, ds, labeled, *, dtype="float32", target_relres=1e-6, tol=1e-3, hbm_budget_bytes=None,
+                 max_fresh_batch=64, fresh_dtype=torch.float64):
+        self.target = target_relres
+        self.K = ds.K
+        self.fresh_dtype = fresh_dtype
+        self.es = stream.EdgeStream(ds, labeled, dtype=dtype)
+        self.solver = solvers.IncrementalLP(ds.n, ds.K, dtype, tol=tol, method="pcg", target_relres=target_relres,
+                                            full_every=16)
+        self.solver.solve(self.es.system)
+        self.labels = self._snapshot()
+        self.version = 0
+        free, total = torch.cuda.mem_get_info()
+        self.budget = int(hbm_budget_bytes if hbm_budget_bytes is not None else 0.5 * free)
+        self.max_fresh_batch = max_fresh_batch
+        self._q = {"update": queue.Queue(), "query": queue.Queue(), "fresh": queue.Queue()}
+        self._streams = {k: torch.cuda.Stream() for k in self._q}
+        self._stop = threading.Event()
+        self._lock = threading.Lock()
+        self.done: list[_Item] = []
+        self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in self._q]
+        self._dev = torch.cuda.current_device()
+        for t in self._threads:
+            t.start()
+
+    # -- client side ---------------------------------------------------------------------------
+    def submit(self, req) -> Future:
+        kind = "update" if isinstance(req, EdgeUpdate) else "query" if isinstance(req, LabelQuery) else "fresh"
+        fut = Future()
+        if kind == "fresh":
+            C = 1 if req.ds.K == 2 else req.ds.K
+            if req.hbm_bytes(C) > self.budget:
+                fut.set_exception(AdmissionError(f"fresh solve needs ~{req.hbm_bytes(C) / 1e9:.2f} GB, "
+                                                 f"budget {self.budget / 1e9:.2f} GB"))
+                return fut
+        self._q[kind].put(_Item(req, fut, time.perf_counter(), kind))
+        return fut
+
+    def close(self):
+        self._stop.set()
+        for q in self._q.values():
+            q.put(None)
+        for t in self._threads:
+            t.join(timeout=60)
+
+    def latency(self, kind=None):
+        with self._lock:
+            lat = [1e3 * (it.t_done - it.t_submit) for it in self.done if kind in (None, it.kind)]
+        if not lat:
+            return {}
+        return {"n": len(lat), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+    # -- workers -------------------------------------------------------------------------------
+    def _snapshot(self):
+        Z = self.solver.Z
+        return solvers.predict(Z[:, : self.solver.C], self.K).clone()
+
+    def _finish(self, items, results):
+        t = time.perf_counter()
+        with self._lock:
+            for it, r in zip(items, results):
+                it.t_done = t
+                self.done.append(it)
+        for it, r in zip(items, results):
+            if isinstance(r, BaseException):
+                it.fut.set_exception(r)
+            else:
+                it.fut.set_result(r)
+
+    def _drain(self, kind, first, limit=None):
+        items = [first]
+        q = self._q[kind]
+        while limit is None or len(items) < limit:
+            try:
+                nxt = q.get_nowait()
+            except queue.Empty:
+                break
+            if nxt is None:
+                q.put(None)
+                break
+            items.append(nxt)
+        return items
+
+    def _worker(self, kind):
+        torch.cuda.set_device(self._dev)
+        with torch.cuda.stream(self._streams[kind]):
+            while not self._stop.is_set():
+                first = self._q[kind].get()
+                if first is None:
+                    break
+                try:
+                    getattr(self, "_do_" + kind)(first)
+                except BaseException as e:  # a failing batch fails its requests, not the server
+                    self._finish([first], [e])
+
+    def _do_update(self, first):
+        items = self._drain("update", first)
+        try:
+            for it in items:  # sequential patch semantics
+                r = it.req
+                self.es.apply_edges(r.ins_u, r.ins_v, r.ins_w, r.del_u, r.del_v)
+            st = self.solver.solve(self.es.system)
+            labels = self._snapshot()
+            torch.cuda.current_stream().synchronize()
+            with self._lock:
+                self.labels, self.version = labels, self.version + 1
+            res = {"relres": st.relres, "cert": st.cert, "path": st.path, "coalesced": len(items),
+                   "version": self.version}
+            self._finish(items, [res] * len(items))
+        except BaseException as e:
+            self._finish(items, [e] * len(items))
+
+    def _do_query(self, first):
+        items = self._drain("query", first)
+        with self._lock:
+            labels = self.labels
+        outs = []
+        for it in items:
+            ids = torch.as_tensor(np.asarray(it.req.ids, dtype=np.int64)).to(labels.device, non_blocking=True)
+            outs.append(labels.index_select(0, ids))
+        torch.cuda.current_stream().synchronize()
+        self._finish(items, [o.cpu().numpy() for o in outs])
+
+    def _do_fresh(self, first):
+        items, used = [first], first.req.hbm_bytes(1 if first.req.ds.K == 2 else first.req.ds.K)
+        q = self._q["fresh"]
+        while len(items) < self.max_fresh_batch:
+            try:
+                nxt = q.get_nowait()
+            except queue.Empty:
+                break
+            if nxt is None:
+                q.put(None)
+                break
+            need = nxt.req.hbm_bytes(1 if nxt.req.ds.K == 2 else nxt.req.ds.K)
+            if used + need > self.budget:  # admit later, when this batch has freed its memory
+                q.put(nxt)
+                break
+            items.append(nxt)
+            used += need
+        try:
+            systems = []
+            for it in items:
+                ds = it.req.ds
+                systems.append(stream.build_system(ds, torch.ones(ds.n, dtype=torch.bool, device=ds.A.indices.device),
+                                                   it.req.labeled, dtype="float32"))
+            Fs, info = batched.solve_many(systems, target_relres=self.target, dtype=self.fresh_dtype)
+            outs = []
+            for S, F, (iters, status, rel) in zip(systems, Fs, info):
+                outs.append({"U": S.U, "F": F, "labels": solvers.predict(F, S.K), "iters": iters, "status": status,
+                             "relres": rel, "batch": len(items)})
+            torch.cuda.current_stream().synchronize()
+            self._finish(items, outs)
+        except BaseException as e:
+            self._finish(items, [e] * len(items))

@@ -52,7 +52,7 @@ _SCRATCH: dict = {}
 
 
 def _scratch(tag, n, C, dt, dev, padded=False):
-    key = (tag, n, C, dt, dev)
+    key = (tag, n, C, dt, dev, torch.cuda.current_stream().cuda_stream)  # per stream, like the workspaces
     t = _SCRATCH.get(key)
     if t is None:
         t = padded_empty(n, C, dt, dev, 0.0) if padded else torch.zeros((n, C), dtype=dt, device=dev)
@@ -107,8 +107,20 @@ def jacobi_M(sys):
     return JacobiM(sys)
 
 
+def bf16_weights(W):
+    """bf16 copy of a sparse operator's weights, cached on the object (the BF16 sweeps)."""
+    wb = getattr(W, "_w_bf16", None)
+    if wb is None or wb.numel() != W.data.numel():
+        wb = W.data.to(torch.bfloat16)
+        try:
+            W._w_bf16 = wb
+        except AttributeError:
+            pass
+    return wb
+
+
 def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400, *, target_relres=None,
-        rhs_norm=None, check_every=8, use_graph=True):
+        rhs_norm=None, check_every=8, use_graph=True, lowp=False):
     """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
 
     Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
@@ -116,7 +128,7 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     if eps is None and target_relres is None:
         raise ValueError("pcg needs eps and/or target_relres")
     if M is not None and not isinstance(M, JacobiM):
-        return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm)
+        return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, lowp)
     n, C = Z.shape
     if n == 0:
         return Z
@@ -140,11 +152,17 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     ws = workspace("pcg").get(_lib.lib().dlp_pcg_workspace_bytes(C))
     it, viol, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_double(0), ct.c_int32(0)
     rhs = rhs.to(dt)
+    w_lo = P_lo = None
+    if lowp:
+        if dt != torch.float32:
+            raise TypeError("the BF16 sweeps run inside the fp32 working precision")
+        w_lo = bf16_weights(W)
+        P_lo = _scratch("pcg_Plo", n, C, torch.bfloat16, dev, padded=True)
     _lib.call("dlp_pcg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C, ptr(diag),
               ptr(rhs), ld(rhs), ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), code(Z), eps_h, rn,
               float(target_relres or 0.0), mode, int(max_iter), int(patience), int(check_every), int(bool(use_graph)),
               W.nnz / max(n, 1), ptr(ws), ws.numel(), ct.byref(it), ct.byref(viol), ct.byref(rel), ct.byref(status),
-              stream())
+              stream(), ptr(w_lo), ptr(P_lo), ld(P_lo) if P_lo is not None else 0)
     st.iters += it.value
     st.edges += (it.value + 2) * W.nnz + work_M * it.value
     st.relres = rel.value
@@ -153,10 +171,30 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     return Z
 
 
-def _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm):
+def _apply_lowp(sys, P, W, wb, Pb, ones):
+    """A P with the SpMM on bf16 weights and a bf16 mirror of P (fp32 accumulation and diagonal)."""
+    n, C = P.shape
+    _lib.call("dlp_cols_scale", n, C, ptr(P), ld(P), code(P), ptr(ones), 2, ptr(Pb), ld(Pb), code(Pb), stream())
+    AP = torch.empty_like(P)
+    _lib.call("dlp_spmm_lowp", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(wb), n, C, ptr(Pb), ld(Pb), ptr(P),
+              ld(P), ptr(sys.diag.to(torch.float32).contiguous()), 1.0, -1.0, ptr(AP), ld(AP), 0,
+              W.nnz / max(n, 1), stream())
+    return AP
+
+
+def _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, lowp=False):
     """PCG with a general preconditioner M (the AMG V-cycle): the reference loop
     (dynlp/solvers.py:66-97) over libdlp's SpMM and fp64 column reductions."""
     dt = Z.dtype
+    if lowp:
+        if dt != torch.float32:
+            raise TypeError("the BF16 sweeps run inside the fp32 working precision")
+        wb = bf16_weights(sys.W)
+        Pb = _scratch("gen_Plo", Z.shape[0], Z.shape[1], torch.bfloat16, Z.device, padded=True)
+        ones = torch.ones(Z.shape[1], dtype=F64, device=Z.device)
+        applyA = lambda X: _apply_lowp(sys, X.contiguous(), sys.W, wb, Pb, ones)  # noqa: E731
+    else:
+        applyA = lambda X: apply_A(sys, X)  # noqa: E731
     eps_d = torch.as_tensor(eps, dtype=F64, device=Z.device)
     rn = None
     if target_relres is not None:
@@ -176,7 +214,7 @@ def _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_rel
     P = Y = M(R)
     rz, stall = kernels.colreduce(1, R, Y=Y), 0
     for _ in range(max_iter):
-        AP = apply_A(sys, P)
+        AP = applyA(P)
         pAp = kernels.colreduce(1, P, Y=AP)
         alpha = torch.where(pAp > 0, rz / torch.where(pAp > 0, pAp, torch.ones_like(pAp)), torch.zeros_like(pAp))
         Z += alpha.to(dt)[None, :] * P
@@ -304,12 +342,13 @@ class DynLPPlus(Solver):
 
     def __init__(self, n_total, K, dtype="float32", method="auto", tol=1e-3, eps_h=0.05, group="auto",
                  push_frac=0.05, push_budget=30.0, amg_hmax=2000.0, max_iter=100_000, amg_opts=None,
-                 target_relres=None):
+                 target_relres=None, lowp=False):
         super().__init__(n_total, K, dtype, store_dtype="float64")  # float64 master copy of F and h
         self.method, self.tol, self.eps_h, self.group = method, tol, eps_h, group
         self.push_frac, self.push_budget, self.amg_hmax = push_frac, push_budget, amg_hmax
         self.max_iter, self.amg_opts = max_iter, amg_opts or {}
         self.target_relres = target_relres
+        self.lowp = lowp  # SpMM sweeps on bf16 weights and scores (fp32 accumulation)
         self.name, self.H, self.hmax = f"dynlp+{method}", None, None
 
     def _use_amg(self):
@@ -328,7 +367,7 @@ class DynLPPlus(Solver):
 
     def _global(self, sys, Z, rhs, eps, st, amg_box, **kw):
         M, wm = self._precond(sys, st, amg_box)
-        return pcg(sys, Z, rhs, eps, M, self.max_iter, st, wm, **kw)
+        return pcg(sys, Z, rhs, eps, M, self.max_iter, st, wm, lowp=self.lowp and Z.dtype == torch.float32, **kw)
 
     def _run(self, sys, Z, rhs, eps, ops, st, amg_box, **kw):
         """auto: push when few rows violate, else PCG/AMG (dynlp/solvers.py:272-288)."""

@@ -309,6 +309,9 @@ class EdgeStream:
     def apply_edges(self, ins_u=None, ins_v=None, ins_w=None, del_u=None, del_v=None) -> System:
         """Apply one edge batch (deletions, then insertions) and return the updated system."""
         G, n = self.G, self.n
+        for name, x in (("ins_u", ins_u), ("ins_v", ins_v), ("del_u", del_u), ("del_v", del_v)):
+            if x is not None and not torch.is_tensor(x) and len(x) and (np.min(x) < 0 or np.max(x) >= n):
+                raise ValueError(f"edge batch rejected: {name} has vertex ids outside [0, {n})")
         du, dv = self._upload(del_u, torch.int32), self._upload(del_v, torch.int32)
         iu, iv = self._upload(ins_u, torch.int32), self._upload(ins_v, torch.int32)
         iw = self._upload(ins_w, torch.float32)

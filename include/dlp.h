@@ -70,6 +70,13 @@ int dlp_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const
              const void *a, double alpha, double b, const void *RHS, int64_t ldr, double cr, void *Y,
              int64_t ldy, int y_dtype, int compact_out, int32_t group, double avg_deg, dlp_stream_t stream);
 
+/* Mixed-precision SpMM in the apply_A form: Y = alpha * a[r] * X_own[r, :] + b * sum_j w_lo[j] *
+ * X_lo[col_j, :], with bf16 weights and gathered rows, fp32 accumulation, the own-row term from the
+ * fp32 X_own (NULL: from X_lo) and fp32 a / Y (config: SpMM on BF16 weights/scores). */
+int dlp_spmm_lowp(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w_lo, int32_t n_rows,
+                  int32_t C, const void *X_lo, int64_t ld_lo, const void *X_own, int64_t ld_own, const void *a,
+                  double alpha, double b, void *Y, int64_t ldy, int32_t group, double avg_deg, dlp_stream_t stream);
+
 /* ---- (b) frontier Jacobi ------------------------------------------------------------------
  * Replaces the frontier_jacobi kernels (dynlp/kernels.py:31-103, :186-220; FrontierOps.jacobi
  * :464-474): for g < nf, r = frontier[g]:
@@ -176,14 +183,18 @@ int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_
  * check_every iterations is replayed as a CUDA graph when use_graph != 0 (cached per problem).
  * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap,
  * 4 breakdown (a non-finite residual entry). eps may be NULL when bit 0 is unused.
- * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C). */
+ * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C).
+ * Mixed precision (fp32 only): with w_lo (bf16 copy of w) and P_lo (a bf16 n x C buffer, ld_lo) the
+ * SpMM gathers the bf16 mirror of P that the direction update keeps (fp32 accumulation), while the
+ * diagonal term, pAp and every vector update stay fp32; NULL for both = full-precision gathers. */
 size_t dlp_pcg_workspace_bytes(int32_t C);
 int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype, int32_t n,
             int32_t C, const void *diag, const void *rhs, int64_t ldrhs, void *Z, int64_t ldz, void *R, int64_t ldr,
             void *P, int64_t ldp, void *AP, int64_t ldap, int dtype, const double *eps, const double *rhs_norm,
             double target_relres, int32_t mode, int32_t max_iter, int32_t patience, int32_t check_every,
             int32_t use_graph, double avg_deg, void *ws, size_t ws_bytes, int32_t *iters_out, double *viol_out,
-            double *relres_out, int32_t *status_out, dlp_stream_t stream);
+            double *relres_out, int32_t *status_out, dlp_stream_t stream, const void *w_lo, void *P_lo,
+            int64_t ld_lo);
 
 
 /* ---- (c) resident graph: edge-batch patch of the grounded system ---------------------------

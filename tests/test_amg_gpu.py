@@ -66,3 +66,23 @@ def test_dynlp_plus_amg_certificate(K):
     err = np.abs(solver.scores(S).cpu().numpy() - Fd).max()
     assert st.cert <= 1e-3 * 1.0001 and err <= st.cert * 1.05 + 1e-6, (err, st.cert, st.iters)
     assert st.iters < 60
+
+
+@pytest.mark.parametrize("method", ["pcg", "amg"])
+def test_bf16_sweeps_with_fp64_refinement_reach_1e8(method):
+    """Config 3's precision scheme: SpMM on bf16 weights/scores (fp32 accumulation) inside fp32 PCG,
+    fp64 residual refinement to rel-res 1e-8; the result is checked against a direct fp64 solve."""
+    ds = graphs.planted_partition(20_000, 8, 18.0, 6.0, weights="lognormal", seed=5)
+    lab = graphs.label_mask(20_000, 0.01, seed=5)
+    S = stream.build_system(ds, torch.ones(20_000, dtype=torch.bool, device="cuda"), lab, dtype="float32")
+    solver = solvers.DynLPPlus(20_000, 8, "float32", method=method, tol=1e-3, target_relres=1e-8, lowp=True)
+    st = solver.solve(S)
+    S64 = S.astype(torch.float64)
+    A = S64.W.to_scipy().astype(np.float64)
+    F = solver.scores(S).cpu().numpy()
+    rel = O.relres(A, S64.diag.cpu().numpy(), F, S64.rhs.cpu().numpy())
+    assert rel <= 1e-8 and st.relres <= 1e-8, (rel, st.relres)
+    import scipy.sparse as ssp
+    import scipy.sparse.linalg as sla
+    Fd = sla.spsolve((ssp.diags(S64.diag.cpu().numpy()) - A).tocsc(), S64.rhs.cpu().numpy())
+    assert np.abs(F - Fd).max() <= max(st.cert, 1e-6)

@@ -1,0 +1,83 @@
+"""Serving loop (GPU): results are the same alone and in a mix of concurrent requests."""
+import numpy as np
+import pytest
+import torch
+
+from dynlplus_b200 import batched, graphs, serve, solvers, stream
+
+pytestmark = pytest.mark.gpu
+
+
+def _fresh(i):
+    n = 2000 + 700 * i
+    ds = graphs.planted_partition(n, 4, 9.0, 3.0, seed=100 + i)
+    return serve.FreshSolve(ds, graphs.label_mask(n, 0.02, seed=100 + i))
+
+
+def _alone_fresh(req):
+    S = stream.build_system(req.ds, torch.ones(req.ds.n, dtype=torch.bool, device="cuda"), req.labeled,
+                            dtype="float32")
+    Fs, info = batched.solve_many([S], target_relres=1e-6)
+    return Fs[0]
+
+
+def test_results_alone_equal_results_in_the_mix():
+    n, K = 20_000, 4
+    ds = graphs.er_graph(n, 10, K, seed=7)
+    lab = graphs.label_mask(n, 0.01, seed=7)
+    up = graphs.EdgeUpdates(ds.A, seed=7)
+    batches = [up.next(int(s)) for s in (50, 400, 10, 1200, 300)]
+    fresh = [_fresh(i) for i in range(5)]
+
+    srv = serve.Server(ds, lab, target_relres=1e-6)
+    futs = []
+    for i, b in enumerate(batches):  # interleave updates, fresh solves and queries
+        futs.append(srv.submit(serve.EdgeUpdate(b["ins_u"], b["ins_v"], b["ins_w"], b["del_u"], b["del_v"])))
+        futs.append(srv.submit(fresh[i]))
+        futs.append(srv.submit(serve.LabelQuery(np.arange(0, n, 97))))
+    res = [f.result(timeout=300) for f in futs]
+    final_q = srv.submit(serve.LabelQuery(np.arange(n))).result(timeout=60)
+    Z_mix = srv.solver.Z[:, :K].clone()
+    lat = srv.latency()
+    srv.close()
+    assert lat["n"] == len(futs) + 1
+    # fresh solves: same scores as the same request solved alone
+    for i, r in enumerate(res[1::3]):
+        assert r["status"] == 5 and r["relres"] <= 1e-6
+        np.testing.assert_allclose(r["F"].cpu().numpy(), _alone_fresh(fresh[i]).cpu().numpy(), rtol=1e-9, atol=1e-12)
+    # updates: the same final state as applying the batches one by one without the server
+    es = stream.EdgeStream(ds, lab)
+    solver = solvers.IncrementalLP(n, K, "float32", tol=1e-3, method="pcg", target_relres=1e-6, full_every=16)
+    solver.solve(es.system)
+    for b in batches:
+        solver.solve(es.apply_edges(**b))
+    Z_alone = solver.Z[:, :K]
+    for r in res[0::3]:
+        assert r["relres"] <= 1e-6
+    diff = (Z_mix - Z_alone).abs().max().item()
+    assert diff < 1e-5, diff
+    # the final query reads the published labels of the final state
+    want = solvers.predict(Z_mix, K).cpu().numpy()
+    np.testing.assert_array_equal(final_q, want)
+
+
+def test_admission_and_malformed_requests():
+    n, K = 5000, 3
+    ds = graphs.er_graph(n, 8, K, seed=3)
+    lab = graphs.label_mask(n, 0.02, seed=3)
+    srv = serve.Server(ds, lab, hbm_budget_bytes=2_000_000)  # room for small fresh solves only
+    big = serve.FreshSolve(graphs.er_graph(200_000, 10, 4, seed=1), graphs.label_mask(200_000, 0.01, seed=1))
+    with pytest.raises(serve.AdmissionError):
+        srv.submit(big).result(timeout=60)
+    bad = serve.EdgeUpdate(np.array([0, n + 5], np.int32), np.array([1, 2], np.int32), np.ones(2, np.float32),
+                           np.zeros(0, np.int32), np.zeros(0, np.int32))
+    with pytest.raises(ValueError):
+        srv.submit(bad).result(timeout=60)
+    up = graphs.EdgeUpdates(ds.A, seed=3)
+    b = up.next(100)
+    ok = srv.submit(serve.EdgeUpdate(b["ins_u"], b["ins_v"], b["ins_w"], b["del_u"], b["del_v"])).result(timeout=120)
+    assert ok["relres"] <= 1e-6
+    small = serve.FreshSolve(graphs.er_graph(1000, 8, 3, seed=9), graphs.label_mask(1000, 0.03, seed=9))
+    r = srv.submit(small).result(timeout=120)
+    assert r["status"] == 5
+    srv.close()
