@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import golden_csr, load_golden
+from conftest import direct_solve, golden_csr, load_golden
 from dynlplus_b200 import amg, graphs, solvers, stream
 from dynlplus_b200.backend import CSR
 from oracle import ref_np as O
@@ -61,7 +61,7 @@ def test_dynlp_plus_amg_certificate(K):
     import scipy.sparse as ssp
     import scipy.sparse.linalg as sla
     A = ssp.diags(S64.diag.cpu().numpy()) - S64.W.to_scipy().astype(np.float64)
-    Fd = sla.spsolve(A.tocsc(), S64.rhs.cpu().numpy())
+    Fd = direct_solve(A, S64.rhs.cpu().numpy())
     Fd = Fd.reshape(-1, 1) if Fd.ndim == 1 else Fd
     err = np.abs(solver.scores(S).cpu().numpy() - Fd).max()
     assert st.cert <= 1e-3 * 1.0001 and err <= st.cert * 1.05 + 1e-6, (err, st.cert, st.iters)
@@ -84,5 +84,5 @@ def test_bf16_sweeps_with_fp64_refinement_reach_1e8(method):
     assert rel <= 1e-8 and st.relres <= 1e-8, (rel, st.relres)
     import scipy.sparse as ssp
     import scipy.sparse.linalg as sla
-    Fd = sla.spsolve((ssp.diags(S64.diag.cpu().numpy()) - A).tocsc(), S64.rhs.cpu().numpy())
+    Fd = direct_solve(ssp.diags(S64.diag.cpu().numpy()) - A, S64.rhs.cpu().numpy())
     assert np.abs(F - Fd).max() <= max(st.cert, 1e-6)

@@ -6,7 +6,7 @@ import scipy.sparse as ssp
 import scipy.sparse.linalg as sla
 import torch
 
-from conftest import golden_csr, load_golden
+from conftest import direct_solve, golden_csr, load_golden
 from dynlplus_b200 import graphs, kernels, solvers, stream
 from dynlplus_b200.backend import CSR
 from oracle import ref_np as O
@@ -121,7 +121,7 @@ def test_dynlp_plus_certificate_holds(method, K):
     S64 = S.astype(torch.float64)
     Wd = S64.W.to_scipy().astype(np.float64)
     Ad = ssp.diags(S64.diag.cpu().numpy()) - Wd
-    Fd = sla.spsolve(Ad.tocsc(), S64.rhs.cpu().numpy())
+    Fd = direct_solve(Ad, S64.rhs.cpu().numpy())
     Fd = Fd.reshape(-1, 1) if Fd.ndim == 1 else Fd
     err = np.abs(solver.scores(S).cpu().numpy() - Fd).max()
     assert st.cert <= 1e-3 * 1.0001
@@ -245,7 +245,7 @@ def test_incremental_push_path_on_small_batches():
         A = es.G.to_csr("w").to_scipy().astype(np.float64)
         U = S.solved.cpu().numpy()
         Ad = ssp.diags(S64.diag.cpu().numpy()) - A
-        Fd = sla.spsolve(Ad.tocsc(), S64.rhs.cpu().numpy())
+        Fd = direct_solve(Ad, S64.rhs.cpu().numpy())
         err = np.abs(solver.Z.cpu().numpy()[U, :K] - Fd[U]).max()
         assert st.cert <= 1e-3 * 1.0001 and err <= st.cert * 1.05 + 1e-9, (st.path, err, st.cert)
     assert "inc-push" in paths, paths
