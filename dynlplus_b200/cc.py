@@ -56,6 +56,8 @@ def graph_components(G, vmask=None, sink=None, w=None):
     dev = G.indices.device
     parent = torch.empty(n + 1, dtype=torch.int32, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
+    ws = workspace("cc_graph").get(_lib.lib().dlp_cc_graph_workspace_bytes())
     _lib.call("dlp_cc_graph", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(w),
-              code(w) if w is not None else 0, ptr(vmask), ptr(sink), ptr(parent), ptr(err), stream())
+              code(w) if w is not None else 0, ptr(vmask), ptr(sink), ptr(parent), ptr(err), ptr(ws), ws.numel(),
+              stream())
     return parent, err

@@ -73,30 +73,113 @@ __global__ void __launch_bounds__(kCcThreads)
   }
 }
 
-// 8 lanes per row over the row ranges; sink vertex id = n.
+// Graph form, in the sampling-then-skip order of Afforest (Sutton, Ben-Nun, Barak, IPDPS 2018):
+//   1. kCcSample rounds: every vertex hooks its k-th live in-mask neighbour, then compress;
+//   2. the most frequent root L among a fixed sample of vertices is taken as the big component;
+//   3. the rows of every vertex outside L are hooked in full (both directions, so an edge whose
+//      other end lies in L is still seen); rows of L are skipped, except for their sink entries
+//      until L is joined to the sink.
+// Any edge skipped in 3 has both ends in L, so the partition is the full one; and since every hook
+// puts a larger root under a smaller one, each root is still its component's minimum vertex id.
+constexpr int kCcSample = 2;
+constexpr int kCcModeSample = 1024;
+
+template <typename TW>
+__device__ __forceinline__ bool live(const TW *w, int j) {
+  return !w || cvt<float>(w[j]) != 0.0f;
+}
+
+// Sampling round k: every vertex of the mask hooks its k-th live in-mask neighbour (CSR order).
+// One neighbour per round with a compression in between keeps every find one or two hops long.
+template <typename TW>
+__global__ void __launch_bounds__(kCcThreads)
+    k_cc_sample(int32_t n, int k, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+                const int32_t *__restrict__ col, const TW *__restrict__ w, const uint8_t *__restrict__ vmask,
+                int32_t *parent, int32_t *err) {
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (long long)gridDim.x * blockDim.x) {
+    if (vmask && !vmask[u]) continue;
+    const int end = rend[u];
+    int seen = 0;
+    for (int j = rbeg[u]; j < end; ++j) {
+      if (!live(w, j)) continue;
+      const int32_t v = col[j];
+      if ((unsigned)v >= (unsigned)n) {
+        if (err) atomicExch(err, DLP_ERR_DEVICE);
+        continue;
+      }
+      if (vmask && !vmask[v]) continue;
+      if (seen++ == k) {
+        unite(parent, (int32_t)u, v, err);
+        break;
+      }
+    }
+  }
+}
+
+// One block: the most frequent root among kCcModeSample in-mask vertices spread over [0, n)
+// (ties: the smaller root); -1 when no sampled vertex is in the mask. scratch[1] = 0 (L not yet
+// joined to the sink).
+__global__ void __launch_bounds__(kCcModeSample) k_cc_big(int32_t n, const uint8_t *__restrict__ vmask,
+                                                          const int32_t *__restrict__ parent, int32_t *scratch) {
+  __shared__ int32_t root[kCcModeSample];
+  __shared__ unsigned long long best;
+  const int k = threadIdx.x;
+  const int S = n < kCcModeSample ? n : kCcModeSample;
+  int32_t r = -1;
+  if (k < S) {
+    const int32_t i = (int32_t)(((long long)k * n) / S);
+    if (!vmask || vmask[i]) r = parent[i];
+  }
+  root[k] = r;
+  if (k == 0) best = 0ull;
+  __syncthreads();
+  if (r >= 0) {
+    unsigned cnt = 0;
+    for (int j = 0; j < S; ++j) cnt += root[j] == r;
+    // larger count first, then smaller root
+    const unsigned long long key = ((unsigned long long)cnt << 32) | (0xffffffffu - (unsigned)r);
+    atomicMax(&best, key);
+  }
+  __syncthreads();
+  if (k == 0) {
+    scratch[0] = best ? (int32_t)(0xffffffffu - (unsigned)(best & 0xffffffffu)) : -1;
+    scratch[1] = 0;
+  }
+}
+
+// 8 lanes per row; sink vertex id = n. With scratch == NULL every row is hooked in full (entry
+// (u, v) once, from the smaller end).
 template <typename TW>
 __global__ void __launch_bounds__(kCcThreads)
     k_cc_graph(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
                const int32_t *__restrict__ col, const TW *__restrict__ w, const uint8_t *__restrict__ vmask,
-               const uint8_t *__restrict__ sink, int32_t *parent, int32_t *err) {
+               const uint8_t *__restrict__ sink, int32_t *parent, int32_t *err, int32_t *scratch) {
   const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
+  const int32_t big = scratch ? scratch[0] : -1;
+  volatile int32_t *grounded = scratch ? scratch + 1 : nullptr;
   for (long long t = t0; t < (long long)n * 8; t += stride) {
     const int32_t u = (int32_t)(t >> 3);
     const int l = (int)(t & 7);
     if (vmask && !vmask[u]) continue;
+    const bool inL = big >= 0 && ((volatile int32_t *)parent)[u] == big;
+    if (inL && (!sink || *grounded)) continue;
     const int beg = rbeg[u], end = rend[u];
     for (int j = beg + l; j < end; j += 8) {
-      if (w && cvt<float>(w[j]) == 0.0f) continue;
+      if (!live(w, j)) continue;
       const int32_t v = col[j];
       if ((unsigned)v >= (unsigned)n) {
         if (err) atomicExch(err, DLP_ERR_DEVICE);
         continue;
       }
       if (!vmask || vmask[v]) {
-        if (u < v) unite(parent, u, v, err);  // the mirror entry (v, u) covers the pair once
+        // skipped rows (L) are covered from the other end; without a sample pass the mirror
+        // entry (v, u) covers the pair once
+        if (!inL && (scratch || u < v)) unite(parent, u, v, err);
       } else if (sink && sink[v]) {
         unite(parent, u, n, err);
+        if (inL) *grounded = 1;
       }
     }
   }
@@ -151,27 +234,44 @@ int dlp_cc_edges(int32_t n, const int32_t *rows, const int32_t *cols, int64_t m,
   return check_launch(m > 0 ? 3 : 2);
 }
 
+size_t dlp_cc_graph_workspace_bytes(void) { return 256; }
+
 int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
-                 int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err,
-                 dlp_stream_t stream) {
+                 int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err, void *ws,
+                 size_t ws_bytes, dlp_stream_t stream) {
   if (n < 0 || !parent) return DLP_ERR_INVALID;
+  if (ws && ws_bytes < dlp_cc_graph_workspace_bytes()) return DLP_ERR_WORKSPACE;
+  if (n > 0 && (!rbeg || !rend || !col)) return DLP_ERR_INVALID;
+  if (w && w_dtype != DLP_F32 && w_dtype != DLP_F64 && w_dtype != DLP_BF16) return DLP_ERR_DTYPE;
   cudaStream_t s = (cudaStream_t)stream;
+  int32_t *scratch = (int32_t *)ws;
+  int launches = 2;
   k_cc_init<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1);
   if (n > 0) {
-    if (!rbeg || !rend || !col) return DLP_ERR_INVALID;
     const int grid = grid_persist((long long)n * 8);
-    if (!w || w_dtype == DLP_F32)
-      k_cc_graph<float><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const float *)w, vmask, sink, parent, err);
-    else if (w_dtype == DLP_F64)
-      k_cc_graph<double><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const double *)w, vmask, sink, parent,
-                                                     err);
-    else if (w_dtype == DLP_BF16)
-      k_cc_graph<bf16><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const bf16 *)w, vmask, sink, parent, err);
-    else
-      return DLP_ERR_DTYPE;
+    const int grid1 = grid_persist(n);
+#define DLP_CC_PASSES(TW)                                                                                      \
+  if (scratch) {                                                                                               \
+    for (int k = 0; k < kCcSample; ++k) {                                                                     \
+      k_cc_sample<TW><<<grid1, kCcThreads, 0, s>>>(n, k, rbeg, rend, col, (const TW *)w, vmask, parent, err);   \
+      k_cc_compress<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(parent, n, err);                         \
+    }                                                                                                          \
+    k_cc_big<<<1, kCcModeSample, 0, s>>>(n, vmask, parent, scratch);                                           \
+    launches += 2 * kCcSample + 1;                                                                             \
+  }                                                                                                            \
+  k_cc_graph<TW><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const TW *)w, vmask, sink, parent, err, scratch); \
+  launches += 1;
+    if (!w || w_dtype == DLP_F32) {
+      DLP_CC_PASSES(float)
+    } else if (w_dtype == DLP_F64) {
+      DLP_CC_PASSES(double)
+    } else {
+      DLP_CC_PASSES(bf16)
+    }
+#undef DLP_CC_PASSES
   }
   k_cc_compress<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1, err);
-  return check_launch(n > 0 ? 3 : 2);
+  return check_launch(launches);
 }
 
 int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,

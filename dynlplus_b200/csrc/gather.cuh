@@ -64,29 +64,51 @@ static inline int grid_for(long long groups, int G) {
 
 
 // Sum over the stored entries of one row of w_j * X[col_j, :] for the lane's vectors, reduced
-// over the group's edge slots (every lane of the warp must call this: it shuffles).
+// over the group's edge slots (every lane of the warp must call this: it shuffles). Each lane
+// takes its entries in batches of U: the U column indices and weights are loaded first, then the
+// U neighbour rows, then the U multiply-adds, so U row gathers are in flight per lane instead of
+// one. The per-lane accumulation order (entries beg+es, beg+es+ES, ...) is that of a plain loop.
 template <typename TW, typename TX, typename TA, int VW, int VPL>
 __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, const TW *__restrict__ w,
                                            const TX *__restrict__ X, int64_t ldx, int beg, int end, int es,
                                            int ES, int cl, int LV, int NV, int G, TA (&acc)[VPL][VW]) {
+  // batch size: about 48 registers of gathered values per lane
+  constexpr int kWords = VPL * VW * (int)(sizeof(TA) / 4);
+  constexpr int U = kWords <= 12 ? 4 : kWords <= 24 ? 2 : 1;
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
     for (int i = 0; i < VW; ++i) acc[k][i] = TA(0);
-  for (int j = beg + es; j < end; j += ES) {
-    const long long v = ld_stream(col + j);
-    const TA wv = cvt<TA>(ld_stream(w + j));
-    const TX *xr = X + v * ldx;
+  for (int j0 = beg + es; j0 < end; j0 += U * ES) {
+    int v[U];
+    TA wv[U];
 #pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      const int vi = cl + k * LV;
-      if (vi < NV) {
-        TA t[VW];
-        load_vec<TX, VW, TA>(xr + (long long)vi * VW, t);
+    for (int u = 0; u < U; ++u) {
+      const int j = j0 + u * ES;
+      v[u] = j < end ? ld_stream(col + j) : -1;
+      wv[u] = j < end ? cvt<TA>(ld_stream(w + j)) : TA(0);
+    }
+    TA t[U][VPL][VW];
 #pragma unroll
-        for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv, t[i], acc[k][i]);
+    for (int u = 0; u < U; ++u) {
+      const TX *xr = X + (long long)(v[u] < 0 ? 0 : v[u]) * ldx;
+#pragma unroll
+      for (int k = 0; k < VPL; ++k) {
+        const int vi = cl + k * LV;
+        if (v[u] >= 0 && vi < NV) {
+          load_vec<TX, VW, TA>(xr + (long long)vi * VW, t[u][k]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < VW; ++i) t[u][k][i] = TA(0);
+        }
       }
     }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int k = 0; k < VPL; ++k)
+#pragma unroll
+        for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv[u], t[u][k][i], acc[k][i]);
   }
   for (int off = LV; off < G; off <<= 1) {
 #pragma unroll

@@ -196,90 +196,118 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
 }
 
 // ------------------------------------------------------------------------------------------------
+// Element sweeps (K2, K3). Thread t of the grid owns column c = t mod ld of the rows t/ld,
+// t/ld + RS, t/ld + 2 RS, ... with RS = (threads in the grid) / ld: its column never changes, so its
+// per-column sums are scalars, and consecutive threads touch consecutive addresses of the
+// row-major n x ld block. kSweepUnroll rows per batch are loaded before any is used.
+// ------------------------------------------------------------------------------------------------
+constexpr int kSweepUnroll = 4;
+constexpr int kSweepThreads = 256;
+
+struct SweepIdx {
+  long long r0, RS;
+  int c;
+  bool on;  // thread owns a column < C
+};
+
+__device__ __forceinline__ SweepIdx sweep_index(int64_t ld, int32_t C) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)gridDim.x * blockDim.x;
+  SweepIdx s;
+  s.RS = total / ld;
+  s.r0 = t / ld;
+  s.c = (int)(t - s.r0 * ld);
+  s.on = s.r0 < s.RS && s.c < C;
+  return s;
+}
+
+// Deterministic per-column block sums of the per-thread values v[tid] (thread tid of this block
+// owns column (blockIdx.x * blockDim.x + tid) mod ld): warp w handles columns w, w+8, ...; the
+// lanes take the column's threads in a fixed strided order, then a fixed xor tree.
+__device__ __forceinline__ double block_column_sum(const double *v, int c, int64_t ld) {
+  const long long base = (long long)blockIdx.x * blockDim.x;
+  const int first = (int)(((c - base % ld) % ld + ld) % ld);
+  const int lane = lane_id();
+  double s = 0.0;
+  for (long long tid = first + (long long)lane * ld; tid < blockDim.x; tid += 32 * ld) s += v[tid];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  return s;
+}
+
 // K2: residual update + reductions + stop decision
 //   phase 0: iteration (R -= alpha AP)      phase 1: recheck of a true residual
 //   phase 2: initial residual (sets best, rz)
 // A non-finite residual entry stops the solve with status 4 (breakdown) instead of letting the
 // max-reductions (which skip NaN) read it as convergence.
-// ------------------------------------------------------------------------------------------------
-constexpr int kMaxColChunks = 8;  // C <= 256 with 32 column lanes
-constexpr int kRowsPerThread = 4;
-
 template <typename T>
-__global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_t C, T *__restrict__ R, int64_t ldr,
-                                                    const T *__restrict__ AP, int64_t ldap,
-                                                    const T *__restrict__ diag, PcgBufs B) {
+__global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t n, int32_t C, T *__restrict__ R,
+                                                              int64_t ldr, const T *__restrict__ AP, int64_t ldap,
+                                                              const T *__restrict__ diag, PcgBufs B) {
   PcgCtl *ctl = B.ctl;
   if (phase == 0 && !ctl->go) return;
-  const int CX = blockDim.x, RY = blockDim.y;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  __shared__ double s_rz[256], s_ss[256], s_v[256];
-  double rz[kMaxColChunks], ss[kMaxColChunks];
-  double vmax = 0.0;
-  const int nch = (C + CX - 1) / CX;
+  __shared__ double s_rz[kSweepThreads], s_ss[kSweepThreads], s_v[kSweepThreads / 32];
+  const SweepIdx ix = sweep_index(ldr, C);
+  double rz = 0.0, ss = 0.0, vmax = 0.0;
+  bool bad = false;
+  if (ix.on) {
+    const int c = ix.c;
+    const T al = phase == 0 ? (T)B.alpha[c] : T(0);
+    const double einv = B.epsinv[c];
+    for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
+      T rv[kSweepUnroll], ap[kSweepUnroll], dv[kSweepUnroll];
 #pragma unroll
-  for (int m = 0; m < kMaxColChunks; ++m) rz[m] = ss[m] = 0.0;
-  // kRowsPerThread rows in flight per thread and iteration (memory-level parallelism)
-  const long long step = (long long)gridDim.x * RY * kRowsPerThread;
-  for (long long r0 = (long long)blockIdx.x * RY * kRowsPerThread + ty; r0 < n; r0 += step) {
+      for (int u = 0; u < kSweepUnroll; ++u) {
+        const long long rr = r + u * ix.RS;
+        const bool ok = rr < n;
+        rv[u] = ok ? R[rr * ldr + c] : T(0);
+        dv[u] = ok ? diag[rr] : T(1);
+        ap[u] = (ok && phase == 0) ? AP[rr * ldap + c] : T(0);
+      }
 #pragma unroll
-    for (int u = 0; u < kRowsPerThread; ++u) {
-      const long long r = r0 + (long long)u * RY;
-      if (r >= n) break;
-      const double dinv = 1.0 / (double)diag[r];
-#pragma unroll
-      for (int m = 0; m < kMaxColChunks; ++m) {
-        const int c = tx + m * CX;
-        if (m < nch && c < C) {
-          T rv = R[r * ldr + c];
+      for (int u = 0; u < kSweepUnroll; ++u) {
+        const long long rr = r + u * ix.RS;
+        if (rr < n) {
           if (phase == 0) {
-            rv = rv - (T)B.alpha[c] * AP[r * ldap + c];
-            R[r * ldr + c] = rv;
+            rv[u] = rv[u] - al * ap[u];
+            R[rr * ldr + c] = rv[u];
           }
-          const double r64 = (double)rv;
-          if (!isfinite(r64)) ctl->bad = 1;
-          rz[m] += r64 * r64 * dinv;
-          ss[m] += r64 * r64;
-          vmax = fmax(vmax, fabs(r64) * dinv * B.epsinv[c]);
+          const double r64 = (double)rv[u];
+          const double dinv = 1.0 / (double)dv[u];
+          bad |= !isfinite(r64);
+          rz += r64 * r64 * dinv;
+          ss += r64 * r64;
+          vmax = fmax(vmax, fabs(r64) * dinv * einv);
         }
       }
     }
   }
-  // block reduction: per column over ty (fixed order), max over all
-  const int tid = ty * CX + tx;
-  s_v[tid] = vmax;
+  if (bad) ctl->bad = 1;
+  const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  s_rz[tid] = rz;
+  s_ss[tid] = ss;
 #pragma unroll
-  for (int m = 0; m < kMaxColChunks; ++m) {  // compile-time indices keep rz/ss in registers
-    if (m < nch) {                            // nch is uniform over the block
-      s_rz[tid] = rz[m];
-      s_ss[tid] = ss[m];
-      __syncthreads();
-      if (ty == 0) {
-        const int c = tx + m * CX;
-        double a = 0.0, b = 0.0;
-        for (int y = 0; y < RY; ++y) {
-          a += s_rz[y * CX + tx];
-          b += s_ss[y * CX + tx];
-        }
-        if (c < C) {
-          B.part2[((long long)blockIdx.x * C + c) * 2 + 0] = a;
-          B.part2[((long long)blockIdx.x * C + c) * 2 + 1] = b;
-        }
-      }
-      __syncthreads();
+  for (int off = 16; off > 0; off >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+  if (lane == 0) s_v[wid] = vmax;
+  __syncthreads();
+  for (int c = wid; c < C; c += kSweepThreads / 32) {
+    const double a = block_column_sum(s_rz, c, ldr);
+    const double b = block_column_sum(s_ss, c, ldr);
+    if (lane == 0) {
+      B.part2[((long long)blockIdx.x * C + c) * 2 + 0] = a;
+      B.part2[((long long)blockIdx.x * C + c) * 2 + 1] = b;
     }
   }
   if (tid == 0) {
     double v = 0.0;
-    for (int t = 0; t < CX * RY; ++t) v = fmax(v, s_v[t]);
+    for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
     B.partv[blockIdx.x] = v;
   }
   if (last_block(&ctl->cnt2)) {
     __shared__ double s_rel;
     if (tid == 0) s_rel = 0.0;
     __syncthreads();
-    const int wid = tid >> 5, lane = tid & 31;
-    for (int c = wid; c < C; c += (CX * RY) >> 5) {
+    for (int c = wid; c < C; c += kSweepThreads / 32) {
       const double a = warp_strided_reduce(B.part2 + (long long)c * 2 + 0, (long long)C * 2, (int)gridDim.x, false);
       const double b = warp_strided_reduce(B.part2 + (long long)c * 2 + 1, (long long)C * 2, (int)gridDim.x, false);
       if (lane != 0) continue;
@@ -333,47 +361,51 @@ __global__ void __launch_bounds__(256) k_pcg_update(int phase, int32_t n, int32_
   }
 }
 
-// ------------------------------------------------------------------------------------------------
 // K3: Z += alpha P; P = R/diag + beta P
 //   mode 0: both (skipping the P update when a stop was proposed)   mode 1: P update only
 //   mode 2: P = R/diag
-// ------------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z, int64_t ldz,
-                                                 T *__restrict__ P, int64_t ldp, const T *__restrict__ R, int64_t ldr,
-                                                 const T *__restrict__ diag, PcgBufs B, bf16 *P_lo, int64_t ld_lo) {
+__global__ void __launch_bounds__(kSweepThreads) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z,
+                                                           int64_t ldz, T *__restrict__ P, int64_t ldp,
+                                                           const T *__restrict__ R, int64_t ldr,
+                                                           const T *__restrict__ diag, PcgBufs B, bf16 *P_lo,
+                                                           int64_t ld_lo) {
   PcgCtl *ctl = B.ctl;
   if (mode == 0 && !ctl->go) return;
   const bool upd_p = mode != 0 || ctl->done == 0;
-  const int CX = blockDim.x, RY = blockDim.y;
-  const int nch = (C + CX - 1) / CX;
-  const long long step = (long long)gridDim.x * RY * kRowsPerThread;
-  for (long long r0 = (long long)blockIdx.x * RY * kRowsPerThread + threadIdx.y; r0 < n; r0 += step) {
+  const SweepIdx ix = sweep_index(ldr, C);
+  if (!ix.on) return;
+  const int c = ix.c;
+  const T al = mode == 0 ? (T)B.alpha[c] : T(0);
+  const T be = mode == 2 ? T(0) : (T)B.beta[c];
+  for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
+    T pv[kSweepUnroll], rv[kSweepUnroll], dv[kSweepUnroll];
 #pragma unroll
-    for (int u = 0; u < kRowsPerThread; ++u) {
-      const long long r = r0 + (long long)u * RY;
-      if (r >= n) break;
-      const T dv = diag[r];
-      for (int m = 0; m < nch; ++m) {
-        const int c = threadIdx.x + m * CX;
-        if (c >= C) break;
-        const T pv = P[r * ldp + c];
-        if (mode == 0) Z[r * ldz + c] += (T)B.alpha[c] * pv;
+    for (int u = 0; u < kSweepUnroll; ++u) {
+      const long long rr = r + u * ix.RS;
+      const bool ok = rr < n;
+      pv[u] = ok ? P[rr * ldp + c] : T(0);
+      rv[u] = (ok && upd_p) ? R[rr * ldr + c] : T(0);
+      dv[u] = (ok && upd_p) ? diag[rr] : T(1);
+    }
+#pragma unroll
+    for (int u = 0; u < kSweepUnroll; ++u) {
+      const long long rr = r + u * ix.RS;
+      if (rr < n) {
+        if (mode == 0) Z[rr * ldz + c] += al * pv[u];
         if (upd_p) {
-          const T y = R[r * ldr + c] / dv;
-          const T pn = mode == 2 ? y : y + (T)B.beta[c] * pv;
-          P[r * ldp + c] = pn;
-          if (P_lo) P_lo[r * ld_lo + c] = cvt<bf16>(pn);
+          const T y = rv[u] / dv[u];
+          const T pn = mode == 2 ? y : y + be * pv[u];
+          P[rr * ldp + c] = pn;
+          if (P_lo) P_lo[rr * ld_lo + c] = cvt<bf16>(pn);
         }
       }
     }
   }
 }
 
-static dim3 upd_block(int C) {
-  const int cx = std::min(32, next_pow2(std::max(C, 1)));
-  return dim3(cx, 256 / cx);
-}
+// The sweeps need ld <= threads in the grid (at least one row per pass); dlp_pcg checks it.
+static int sweep_blocks(int64_t) { return upd_blocks(); }
 
 // ------------------------------------------------------------------------------------------------
 // host driver
@@ -432,14 +464,14 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
 
 template <typename TS>
 static int launch_update(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
-  k_pcg_update<TS><<<upd_blocks(), upd_block(q.C), 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, (const TS *)q.AP,
+  k_pcg_update<TS><<<sweep_blocks(q.ldr), kSweepThreads, 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, (const TS *)q.AP,
                                                             q.ldap, (const TS *)q.diag, B);
   return check_launch();
 }
 
 template <typename TS>
 static int launch_dir(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
-  k_pcg_dir<TS><<<upd_blocks(), upd_block(q.C), 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
+  k_pcg_dir<TS><<<sweep_blocks(q.ldr), kSweepThreads, 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
                                                          (const TS *)q.R, q.ldr, (const TS *)q.diag, B,
                                                          (bf16 *)q.P_lo, q.ld_lo);
   return check_launch();
@@ -552,6 +584,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
             double *relres_out, int32_t *status_out, dlp_stream_t stream, const void *w_lo, void *P_lo,
             int64_t ld_lo) {
   if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
+  if (ldr > (int64_t)upd_blocks() * kSweepThreads) return DLP_ERR_INVALID;
   if ((w_lo || P_lo) && (!w_lo || !P_lo || ld_lo < C || dtype != DLP_F32)) return DLP_ERR_INVALID;
   if (mode < 1 || mode > 3 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
@@ -578,8 +611,9 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
       e2[c] = eps ? eps[c] : 1e300;
       e2[C + c] = 1.0 / e2[c];
     }
-    DLP_CUDA(cudaMemcpy(B.eps, e2.data(), sizeof(double) * C, cudaMemcpyHostToDevice));
-    DLP_CUDA(cudaMemcpy(B.epsinv, e2.data() + C, sizeof(double) * C, cudaMemcpyHostToDevice));
+    // pageable source: staged before the call returns, so e2 may go out of scope
+    DLP_CUDA(cudaMemcpyAsync(B.eps, e2.data(), sizeof(double) * C, cudaMemcpyHostToDevice, s));
+    DLP_CUDA(cudaMemcpyAsync(B.epsinv, e2.data() + C, sizeof(double) * C, cudaMemcpyHostToDevice, s));
   }
   if (rhs_norm) {
     DLP_CUDA(cudaMemcpyAsync(B.rhsn, rhs_norm, sizeof(double) * C, cudaMemcpyHostToDevice, s));

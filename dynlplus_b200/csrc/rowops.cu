@@ -89,31 +89,7 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-#pragma unroll
-      for (int i = 0; i < VW; ++i) acc[k][i] = TA(0);
-    for (int j = beg + es; j < end; j += ES) {
-      const long long v = ld_stream(p.col + j);
-      const TA wv = cvt<TA>(ld_stream(p.w + j));
-      const TX *xr = p.X + v * p.ldx;
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        const int vi = cl + k * LV;
-        if (vi < NV) {
-          TA t[VW];
-          load_vec<TX, VW, TA>(xr + (long long)vi * VW, t);
-#pragma unroll
-          for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv, t[i], acc[k][i]);
-        }
-      }
-    }
-    for (int off = LV; off < G; off <<= 1) {
-#pragma unroll
-      for (int k = 0; k < VPL; ++k)
-#pragma unroll
-        for (int i = 0; i < VW; ++i) acc[k][i] += __shfl_xor_sync(0xffffffffu, acc[k][i], off);
-    }
+    gather_row<typename T::TW, TX, TA, VW, VPL>(p.col, p.w, p.X, p.ldx, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
       const long long orow = p.compact ? gi : (long long)r;
       const TA av = p.a ? (TA)p.alpha * cvt<TA>(p.a[r]) : TA(0);
@@ -212,31 +188,7 @@ __global__ void __launch_bounds__(kThreads) k_jacobi(JacArgs<T> p) {
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-#pragma unroll
-      for (int i = 0; i < VW; ++i) acc[k][i] = TA(0);
-    for (int j = beg + es; j < end; j += ES) {
-      const long long v = ld_stream(p.col + j);
-      const TA wv = cvt<TA>(ld_stream(p.w + j));
-      const TX *xr = p.X + v * p.ldx;
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        const int vi = cl + k * LV;
-        if (vi < NV) {
-          TA t[VW];
-          load_vec<TX, VW, TA>(xr + (long long)vi * VW, t);
-#pragma unroll
-          for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv, t[i], acc[k][i]);
-        }
-      }
-    }
-    for (int off = LV; off < G; off <<= 1) {
-#pragma unroll
-      for (int k = 0; k < VPL; ++k)
-#pragma unroll
-        for (int i = 0; i < VW; ++i) acc[k][i] += __shfl_xor_sync(0xffffffffu, acc[k][i], off);
-    }
+    gather_row<typename T::TW, TX, TA, VW, VPL>(p.col, p.w, p.X, p.ldx, beg, end, es, ES, cl, LV, NV, G, acc);
     bool ch = false;
     if (valid && es == 0) {
       const TA inv = TA(1) / cvt<TA>(p.diag[r]);

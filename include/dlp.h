@@ -157,10 +157,14 @@ int dlp_cc_edges(int32_t n, const int32_t *rows, const int32_t *cols, int64_t m,
 /* Graph form used by the grounding checks (dynlp/stream.py:150-159, :275-280): vertices 0..n-1
  * plus a sink vertex n. An entry (u, v) of the row ranges joins u and v when vmask[u] and
  * w != 0 (w may be NULL: all entries live) and vmask[v]; it joins u and the sink when vmask[u]
- * and sink[v]. parent has n + 1 entries. vmask/sink may be NULL (all 1 / all 0). */
+ * and sink[v]. parent has n + 1 entries. vmask/sink may be NULL (all 1 / all 0). The row ranges
+ * must be symmetric (entry (u, v) live iff (v, u) is). With a workspace of
+ * dlp_cc_graph_workspace_bytes() the edges go in the sampling-then-skip order (the rows of the
+ * dominant component are not hooked twice); ws = NULL hooks every entry. Same result either way. */
+size_t dlp_cc_graph_workspace_bytes(void);
 int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
-                 int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err,
-                 dlp_stream_t stream);
+                 int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err, void *ws,
+                 size_t ws_bytes, dlp_stream_t stream);
 
 /* Canonical relabel: label[i] = rank of parent[i] among the roots (parent[r] == r; parent must be
  * fully compressed, as dlp_cc_edges/dlp_cc_graph leave it), i.e. the

@@ -59,3 +59,46 @@ def test_graph_components_with_sink_match_grounding():
         U = np.flatnonzero((act & ~lab) & (par[:n] == par[n]))
         np.testing.assert_array_equal(U, g[f"{p}_U"])
         assert par[n] == par[par[n]]  # compressed
+
+
+@pytest.mark.parametrize("n,deg,seed", [(5, 2.0, 0), (50, 1.0, 1), (200_000, 6.0, 2), (300_000, 1.2, 3)])
+def test_graph_components_sampled_order_matches_oracle(n, deg, seed):
+    """The sampling-then-skip order (with a workspace) and the hook-every-entry order (without)
+    give the oracle's min-vertex-id roots, sink included, on masked random graphs: a dense one
+    (one dominant component) and a sparse one (many small components)."""
+    import scipy.sparse as ssp
+    from dynlplus_b200 import _lib
+    from dynlplus_b200.backend import ptr, stream
+    rs = np.random.RandomState(seed)
+    m = int(n * deg / 2)
+    u, v = rs.randint(0, n, m), rs.randint(0, n, m)
+    keep = u != v
+    A = ssp.coo_matrix((np.ones(2 * keep.sum()), (np.r_[u[keep], v[keep]], np.r_[v[keep], u[keep]])),
+                       shape=(n, n)).tocsr()
+    A.sum_duplicates()
+    rows = np.repeat(np.arange(n), np.diff(A.indptr))
+    key = np.minimum(rows, A.indices).astype(np.int64) * n + np.maximum(rows, A.indices)
+    A.data = np.where(key * 2654435761 % 1000 < 50, 0.0, 1.0)  # inert pairs (weight 0), symmetric
+    labeled = rs.rand(n) < 0.01
+    vmask = (rs.rand(n) < 0.97) & ~labeled
+    G = CSR.from_scipy(A, dtype="float32")
+    live = np.asarray(A.data) != 0
+    r, c = rows[live], A.indices[live]
+    inm = vmask[r] & vmask[c]
+    tos = vmask[r] & labeled[c]
+    want = O.min_vertex_roots(O.connected_components_fast(n + 1, np.r_[r[inm], r[tos]],
+                                                          np.r_[c[inm], np.full(tos.sum(), n)])[0])
+    vm, sk = T(vmask.astype(np.uint8)), T(labeled.astype(np.uint8))  # held until the launches are done
+    got = []
+    for use_ws in (True, False):
+        parent = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ws = torch.empty(_lib.lib().dlp_cc_graph_workspace_bytes(), dtype=torch.uint8, device="cuda")
+        indptr = G.indptr
+        _lib.call("dlp_cc_graph", n, ptr(indptr[:-1]), ptr(indptr[1:]), ptr(G.indices), ptr(G.data), 0,
+                  ptr(vm), ptr(sk), ptr(parent), ptr(err),
+                  ptr(ws) if use_ws else None, ws.numel() if use_ws else 0, stream())
+        assert int(err.item()) == 0
+        got.append(parent.cpu().numpy())
+    np.testing.assert_array_equal(got[0], want)
+    np.testing.assert_array_equal(got[1], want)
