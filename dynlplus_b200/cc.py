@@ -61,3 +61,25 @@ def graph_components(G, vmask=None, sink=None, w=None):
               code(w) if w is not None else 0, ptr(vmask), ptr(sink), ptr(parent), ptr(err), ptr(ws), ws.numel(),
               stream())
     return parent, err
+
+
+def ground_reach(G, vmask, sink, umask, in_t, w=None):
+    """Grounded set of the graph form of graph_components, updated in place: umask[u] = 1 iff
+    vmask[u] and u's component reaches the sink (the vertices whose root is the sink's root there);
+    in_t[u] = 1 where membership changed. Bottom-up reachability sweeps; the union-find finishes
+    the job when they do not settle. Returns (number of changes, sweeps run; negative = fallback)."""
+    import ctypes as ct
+    n = G.shape[0]
+    dev = G.indices.device
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    sweeps = ct.c_int32(0)
+    ws = workspace("ground_reach").get(_lib.lib().dlp_ground_reach_workspace_bytes(n))
+    rbeg, rend = (G.rbeg, G.rend) if hasattr(G, "rbeg") else (G.indptr[:-1], G.indptr[1:])
+    _lib.call("dlp_ground_reach", n, ptr(rbeg), ptr(rend), ptr(G.indices), ptr(w), code(w) if w is not None else 0,
+              ptr(vmask), ptr(sink), ptr(umask), ptr(in_t), ptr(cnt), ptr(err), ct.addressof(sweeps), ptr(ws),
+              ws.numel(), stream())
+    if int(err.item()):
+        raise ValueError("ground_reach: entry column outside [0, n)")
+    return int(cnt.item()), int(sweeps.value)
+

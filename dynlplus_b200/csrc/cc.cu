@@ -210,6 +210,60 @@ __global__ void k_cc_gather_rank(const int32_t *__restrict__ parent, int32_t n, 
   if (p != (int32_t)i) label[i] = label[p];
 }
 
+// ------------------------------------------------------------------------------------------------
+// Grounded set by reachability: the vertices of the mask whose component (live in-mask entries)
+// holds an entry to a sink vertex outside the mask -- the set {u : parent[u] == parent[n]} of the
+// graph form above, found by bottom-up sweeps instead of a full union-find: an unreached vertex of
+// the mask joins as soon as one of its live entries leads to a sink vertex or to a reached vertex.
+// Marks are read and written in place, so one sweep carries a mark along many hops; a sweep that
+// marks nothing ends it (the reached set is then closed under adjacency, i.e. whole components).
+// ------------------------------------------------------------------------------------------------
+template <typename TW>
+__global__ void __launch_bounds__(kCcThreads)
+    k_reach_sweep(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+                  const int32_t *__restrict__ col, const TW *__restrict__ w, const uint8_t *__restrict__ vmask,
+                  const uint8_t *__restrict__ sink, uint8_t *reached_, int32_t *flag, int32_t *err) {
+  volatile uint8_t *reached = reached_;
+  bool any = false;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (long long)gridDim.x * blockDim.x) {
+    if ((vmask && !vmask[u]) || reached[u]) continue;
+    const int end = rend[u];
+    for (int j = rbeg[u]; j < end; ++j) {
+      if (!live(w, j)) continue;
+      const int32_t v = col[j];
+      if ((unsigned)v >= (unsigned)n) {
+        if (err) atomicExch(err, DLP_ERR_DEVICE);
+        continue;
+      }
+      const bool inm = !vmask || vmask[v];
+      if (inm ? reached[v] != 0 : (sink && sink[v])) {
+        reached[u] = 1;
+        any = true;
+        break;
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, any) && lane_id() == 0) atomicAdd(flag, 1);
+}
+
+// umask[v] = reached[v] (or root(v) == root(sink) when parent is given); in_t[v] = membership
+// changed; *count += |changed|
+__global__ void k_ground_apply(int32_t n, const uint8_t *__restrict__ reached, const int32_t *__restrict__ parent,
+                               const uint8_t *__restrict__ vmask, uint8_t *umask, uint8_t *in_t, int32_t *count) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool ch = false;
+  if (v < n) {
+    const bool nu = parent ? ((!vmask || vmask[v]) && parent[v] == parent[n]) : reached[v] != 0;
+    const bool ou = umask[v] != 0;
+    ch = nu != ou;
+    umask[v] = nu ? 1 : 0;
+    in_t[v] = ch ? 1 : 0;
+  }
+  const unsigned b = __ballot_sync(0xffffffffu, ch);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
+}
+
 static int grid_persist(long long work) {
   long long blocks = (work + kCcThreads - 1) / kCcThreads;
   const long long cap = (long long)sm_count() * 8;
@@ -272,6 +326,78 @@ int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int3
   }
   k_cc_compress<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1, err);
   return check_launch(launches);
+}
+
+constexpr int kReachBatch = 4;      // sweeps between host checks
+constexpr int kReachMaxSweeps = 32; // then the union-find finishes the job
+
+static size_t reach_ws_layout(int32_t n, size_t *off_flags, size_t *off_parent, size_t *off_cc) {
+  size_t b = ((size_t)n + 255) / 256 * 256;  // reached
+  *off_flags = b;
+  b += 256;                                  // one flag per sweep (kReachMaxSweeps ints)
+  *off_parent = b;
+  b += ((size_t)n + 1 + 63) / 64 * 256;      // parent of the fallback (n + 1 ints)
+  *off_cc = b;
+  return b + 256;                            // dlp_cc_graph workspace
+}
+
+size_t dlp_ground_reach_workspace_bytes(int32_t n) {
+  size_t a, b, c;
+  return reach_ws_layout(n < 0 ? 0 : n, &a, &b, &c);
+}
+
+int dlp_ground_reach(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                     int w_dtype, const uint8_t *vmask, const uint8_t *sink, uint8_t *umask, uint8_t *in_t,
+                     int32_t *count, int32_t *err, int32_t *sweeps_out, void *ws, size_t ws_bytes,
+                     dlp_stream_t stream) {
+  if (n < 0 || (n > 0 && (!rbeg || !rend || !col || !umask || !in_t || !count))) return DLP_ERR_INVALID;
+  if (w && w_dtype != DLP_F32 && w_dtype != DLP_F64 && w_dtype != DLP_BF16) return DLP_ERR_DTYPE;
+  size_t off_flags, off_parent, off_cc;
+  if (!ws || ws_bytes < reach_ws_layout(n, &off_flags, &off_parent, &off_cc)) return DLP_ERR_WORKSPACE;
+  if (sweeps_out) *sweeps_out = 0;
+  if (n == 0) return DLP_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  char *base = (char *)ws;
+  uint8_t *reached = (uint8_t *)base;
+  int32_t *flags = (int32_t *)(base + off_flags);
+  DLP_CUDA(cudaMemsetAsync(reached, 0, (size_t)n, s));
+  DLP_CUDA(cudaMemsetAsync(flags, 0, sizeof(int32_t) * kReachMaxSweeps, s));
+  const int grid = grid_persist(n);
+  int done = 0;
+  bool converged = false;
+  while (!converged && done < kReachMaxSweeps) {
+    for (int k = 0; k < kReachBatch; ++k, ++done) {
+      if (!w || w_dtype == DLP_F32)
+        k_reach_sweep<float><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const float *)w, vmask, sink, reached,
+                                                          flags + done, err);
+      else if (w_dtype == DLP_F64)
+        k_reach_sweep<double><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const double *)w, vmask, sink,
+                                                           reached, flags + done, err);
+      else
+        k_reach_sweep<bf16><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const bf16 *)w, vmask, sink, reached,
+                                                         flags + done, err);
+    }
+    DLP_TRY(check_launch(kReachBatch));
+    int32_t h[kReachBatch];
+    DLP_CUDA(cudaMemcpyAsync(h, flags + done - kReachBatch, sizeof(h), cudaMemcpyDeviceToHost, s));
+    DLP_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < kReachBatch; ++k) {
+      if (h[k] == 0) {
+        converged = true;
+        if (sweeps_out) *sweeps_out = done - kReachBatch + k + 1;
+        break;
+      }
+    }
+  }
+  const int32_t *parent = nullptr;
+  if (!converged) {  // long chains: the union-find settles the rest exactly
+    int32_t *par = (int32_t *)(base + off_parent);
+    DLP_TRY(dlp_cc_graph(n, rbeg, rend, col, w, w_dtype, vmask, sink, par, err, base + off_cc, 256, stream));
+    parent = par;
+    if (sweeps_out) *sweeps_out = -done;
+  }
+  k_ground_apply<<<ceil_div_i(n, 256), 256, 0, s>>>(n, reached, parent, vmask, umask, in_t, count);
+  return check_launch();
 }
 
 int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,

@@ -256,6 +256,7 @@ class EdgeStream:
         self.in_t = torch.zeros(n, dtype=torch.uint8, device=dev)
         self.changed = torch.zeros(n, dtype=torch.uint8, device=dev)
         self._stat = torch.zeros(8, dtype=torch.int32, device=dev)
+        self.counters = {"rebuilds": 0, "ground_changes": 0, "applied": 0, "ground_sweeps": 0, "ground_fallbacks": 0}
         self._ground()
         sr = self.G.slot_rows()
         um = self.umask.bool()
@@ -276,17 +277,20 @@ class EdgeStream:
         self.t = 0
         self.last_changed = torch.arange(n, dtype=torch.int32, device=dev)
         self.last_moved = torch.zeros(0, dtype=torch.int32, device=dev)
-        self.counters = {"rebuilds": 0, "ground_changes": 0, "applied": 0}
         self.n_ins = self.n_del = 0
 
     # -- helpers -------------------------------------------------------------------------------
     def _ground(self):
-        """umask = grounded unlabelled vertices; in_t flags membership changes; returns #changes."""
-        parent, err = cc.graph_components(self.G, self.vmask, self.labeled, w=self.G.aw)
-        self._stat[4].zero_()
-        _lib.call("dlp_ground_update", self.n, ptr(parent), ptr(self.vmask), ptr(self.umask), ptr(self.in_t),
-                  ptr(self._stat[4:5]), stream())
-        return parent
+        """umask = grounded unlabelled vertices; in_t flags membership changes; returns #changes.
+
+        The grounding check of dynlp/stream.py:150-159 (components of the unlabelled subgraph with
+        the labelled vertices as a sink) as reachability from the sink: the same set without a full
+        labelling of the components."""
+        changes, sweeps = cc.ground_reach(self.G, self.vmask, self.labeled, self.umask, self.in_t, w=self.G.aw)
+        self.counters["ground_sweeps"] += abs(sweeps)
+        self.counters["ground_fallbacks"] += sweeps < 0
+        self._stat[4].fill_(changes)
+        return changes
 
     def _system_rows(self, rows, nr):
         ch = self.C + (1 if self.with_h else 0)
@@ -342,8 +346,7 @@ class EdgeStream:
         if int(st[0].item()):
             raise ValueError(f"edge batch rejected: {_lib.STATUS.get(int(st[0].item()))} (vertex id out of range?)")
         # grounding: components of the unlabelled subgraph with the labelled vertices as a sink
-        self._ground()
-        nmoved = int(st[4].item())
+        nmoved = self._ground()
         moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
         if nmoved:
             moved = kernels.flatnonzero(self.in_t)

@@ -166,6 +166,20 @@ int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int3
                  int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err, void *ws,
                  size_t ws_bytes, dlp_stream_t stream);
 
+/* The grounded set (dynlp/stream.py:150-159, :275-280) without a full labelling: on entry umask
+ * holds the previous grounded set; on exit umask[u] = 1 iff vmask[u] and u's component in the
+ * graph form of dlp_cc_graph (same arguments, same symmetric row ranges) reaches the sink, i.e.
+ * exactly the vertices with parent[u] == parent[n] there; in_t[u] = 1 where membership changed;
+ * *count (device int, caller-zeroed) += number of changes. Bottom-up reachability sweeps, checked
+ * on the host every few sweeps; when they have not settled after 32, dlp_cc_graph finishes the
+ * job (same result). *sweeps_out (host, may be NULL) = sweeps run, negated if the fallback ran.
+ * Workspace: dlp_ground_reach_workspace_bytes(n). Synchronises the stream. */
+size_t dlp_ground_reach_workspace_bytes(int32_t n);
+int dlp_ground_reach(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                     int w_dtype, const uint8_t *vmask, const uint8_t *sink, uint8_t *umask, uint8_t *in_t,
+                     int32_t *count, int32_t *err, int32_t *sweeps_out, void *ws, size_t ws_bytes,
+                     dlp_stream_t stream);
+
 /* Canonical relabel: label[i] = rank of parent[i] among the roots (parent[r] == r; parent must be
  * fully compressed, as dlp_cc_edges/dlp_cc_graph leave it), i.e. the
  * labels numpy.unique(parent, return_inverse=True) gives (dynlp/cc.py:22-23); *n_comp = number

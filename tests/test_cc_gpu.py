@@ -102,3 +102,61 @@ def test_graph_components_sampled_order_matches_oracle(n, deg, seed):
         got.append(parent.cpu().numpy())
     np.testing.assert_array_equal(got[0], want)
     np.testing.assert_array_equal(got[1], want)
+
+
+def _grounded_oracle(A, vmask, labeled):
+    n = A.shape[0]
+    rows = np.repeat(np.arange(n), np.diff(A.indptr))
+    live = np.asarray(A.data) != 0
+    r, c = rows[live], A.indices[live]
+    inm = vmask[r] & vmask[c]
+    tos = vmask[r] & ~vmask[c] & labeled[c]
+    par = O.min_vertex_roots(O.connected_components_fast(n + 1, np.r_[r[inm], r[tos]],
+                                                         np.r_[c[inm], np.full(tos.sum(), n)])[0])
+    return vmask & (par[:n] == par[n])
+
+
+@pytest.mark.parametrize("case", ["dense", "sparse", "path"])
+def test_ground_reach_matches_components(case):
+    """Reachability grounding (in place over a previous grounded set) equals the component test of
+    the reference's Stream._build (dynlp/stream.py:150-159): a dense random graph settles in a few
+    sweeps; a long path (label at its far end) exceeds the sweep budget and finishes with the
+    union-find; a near-critical sparse graph takes either route."""
+    import scipy.sparse as ssp
+    rs = np.random.RandomState({"dense": 5, "sparse": 6, "path": 7}[case])
+    if case == "path":
+        n = 5000
+        u = np.arange(n - 1)
+        A = ssp.coo_matrix((np.ones(2 * (n - 1)), (np.r_[u, u + 1], np.r_[u + 1, u])), shape=(n, n)).tocsr()
+        labeled = np.zeros(n, bool)
+        labeled[n - 1] = True
+        vmask = ~labeled
+        vmask[n // 3] = False  # cuts the path: the first third stays ungrounded
+    else:
+        n, deg = (200_000, 6.0) if case == "dense" else (300_000, 1.2)
+        m = int(n * deg / 2)
+        u, v = rs.randint(0, n, m), rs.randint(0, n, m)
+        keep = u != v
+        A = ssp.coo_matrix((np.ones(2 * keep.sum()), (np.r_[u[keep], v[keep]], np.r_[v[keep], u[keep]])),
+                           shape=(n, n)).tocsr()
+        A.sum_duplicates()
+        rows = np.repeat(np.arange(n), np.diff(A.indptr))
+        key = np.minimum(rows, A.indices).astype(np.int64) * n + np.maximum(rows, A.indices)
+        A.data = np.where(key * 2654435761 % 1000 < 50, 0.0, 1.0)
+        labeled = rs.rand(n) < 0.01
+        vmask = (rs.rand(n) < 0.97) & ~labeled
+    want = _grounded_oracle(A, vmask, labeled)
+    G = CSR.from_scipy(A, dtype="float32")
+    old = rs.rand(n) < 0.5
+    umask = T(old.astype(np.uint8))
+    in_t = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    vm, sk = T(vmask.astype(np.uint8)), T(labeled.astype(np.uint8))
+    changes, sweeps = cc.ground_reach(G, vm, sk, umask, in_t, w=G.data)
+    got = umask.cpu().numpy().astype(bool)
+    np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(in_t.cpu().numpy().astype(bool), got != old)
+    assert changes == int((got != old).sum())
+    if case == "path":
+        assert sweeps < 0  # the fallback ran
+    elif case == "dense":
+        assert 0 < sweeps <= 32  # settled by the sweeps (a near-critical sparse graph may need the fallback)
