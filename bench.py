@@ -279,8 +279,9 @@ def ours(a):
     clocks = Clocks(torch.cuda.current_device()) if not a.no_clocks else None
     launches0 = _lib.lib().dlp_launch_count()
     torch.cuda.nvtx.range_push("timed")  # lets a profiler filter the timed steps (--nvtx-include timed/)
-    times, relres, paths, iters = [], [], [], []
-    for b in dev_batches:
+    times, relres, paths, iters, events = [], [], [], [], {}
+    for k, b in enumerate(dev_batches):
+        c0 = dict(es.counters)
         flush.fill_(0.0)
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -292,6 +293,9 @@ def ours(a):
         relres.append(st.relres)
         paths.append(st.path)
         iters.append(st.iters)
+        ev = {c: es.counters[c] - c0[c] for c in ("rebuilds", "ground_fallbacks") if es.counters[c] != c0[c]}
+        if ev:
+            events[k] = ev
     launches = _lib.lib().dlp_launch_count() - launches0
     torch.cuda.nvtx.range_pop()
     clk = clocks.stop() if clocks else None
@@ -331,6 +335,7 @@ def ours(a):
                                "e2e_p50": float(np.percentile(e2e_times, 50)),
                                "e2e_p99": float(np.percentile(e2e_times, 99))},
                 "relres_max": float(max(relres)), "paths": sorted(set(paths)),
+                "stream_events": {str(k): v for k, v in events.items()},
                 "pcg_iters_per_batch": float(np.mean(iters)),
                 "step_ms": [round(t, 3) for t in times],
                 "e2e": {"value": e2e, "unit": "edge-updates/s", "h2d_bytes_per_step": int(h2d),

@@ -44,9 +44,11 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_ground_reach_workspace_bytes": ("i", ct.c_size_t),
     "dlp_ground_reach": ("ippppippppppppzp", ct.c_int),
     "dlp_cc_relabel": ("ippppzp", ct.c_int),
+    "dlp_residual_stats_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_residual_stats": ("iipqpqppqippzp", ct.c_int),
     "dlp_pcg_workspace_bytes": ("i", ct.c_size_t),
     "dlp_pcg": ("ppppiiippqpqpqpqpqippdiiiiidpzpppppppq", ct.c_int),
-    "dlp_graph_delete": ("ipppppppipppipppppp", ct.c_int),
+    "dlp_graph_delete": ("ipppppppipppippppppp", ct.c_int),
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
     "dlp_graph_toggle": ("ppppppippppp", ct.c_int),

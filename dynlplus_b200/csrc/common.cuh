@@ -107,14 +107,34 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t *o
 }
 
 // Deterministic warp-wide sum (or max) of base[b * stride] over b < nb: lane l takes b = l, l+32,
-// ... (independent loads, so the latency overlaps), then a fixed xor tree. All lanes get the result.
+// ... in groups of 8 independent loads (8 accumulators, so 8 loads are in flight per lane), the
+// accumulators are combined in a fixed tree, then a fixed xor tree across lanes. All lanes get the
+// result; the order depends only on nb.
 __device__ __forceinline__ double warp_strided_reduce(const double *base, long long stride, int nb, bool is_max) {
   const int lane = lane_id();
-  double v = 0.0;
-  for (int b = lane; b < nb; b += 32) {
-    const double x = base[(long long)b * stride];
-    v = is_max ? fmax(v, x) : v + x;
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = 0.0;
+  int b = lane;
+  for (; b + 7 * 32 < nb; b += 8 * 32) {
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = base[(long long)(b + 32 * k) * stride];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = is_max ? fmax(a[k], x[k]) : a[k] + x[k];
   }
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {  // the tail: fewer than 8 loads left per lane
+    if (b + 32 * k < nb) {
+      const double x = base[(long long)(b + 32 * k) * stride];
+      a[k] = is_max ? fmax(a[k], x) : a[k] + x;
+    }
+  }
+#pragma unroll
+  for (int w = 4; w > 0; w >>= 1)
+#pragma unroll
+    for (int k = 0; k < w; ++k) a[k] = is_max ? fmax(a[k], a[k + w]) : a[k] + a[k + w];
+  double v = a[0];
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     const double t = __shfl_xor_sync(0xffffffffu, v, off);

@@ -63,18 +63,29 @@ static inline int grid_for(long long groups, int G) {
 }
 
 
+// Entries per batch of a gather_row lane, by the registers the batch holds (VPL x VW values of TA
+// per entry). Measured on B200 (ER n = 1M, degree 10, 9 fp32 columns): the plain SpMM is fastest
+// with four gathers in flight (about 48 registers of batch, one resident block fewer per SM); the
+// PCG apply, which also holds fp64 dot accumulators and is capped at 64 registers for a fourth
+// resident block, with two.
+template <typename TA, int VW, int VPL>
+constexpr int gather_batch_wide() {
+  return VPL * VW * (int)(sizeof(TA) / 4) <= 12 ? 4 : VPL * VW * (int)(sizeof(TA) / 4) <= 24 ? 2 : 1;
+}
+template <typename TA, int VW, int VPL>
+constexpr int gather_batch_lean() {
+  return VPL * VW * (int)(sizeof(TA) / 4) <= 8 ? 4 : VPL * VW * (int)(sizeof(TA) / 4) <= 16 ? 2 : 1;
+}
+
 // Sum over the stored entries of one row of w_j * X[col_j, :] for the lane's vectors, reduced
 // over the group's edge slots (every lane of the warp must call this: it shuffles). Each lane
 // takes its entries in batches of U: the U column indices and weights are loaded first, then the
 // U neighbour rows, then the U multiply-adds, so U row gathers are in flight per lane instead of
 // one. The per-lane accumulation order (entries beg+es, beg+es+ES, ...) is that of a plain loop.
-template <typename TW, typename TX, typename TA, int VW, int VPL>
+template <typename TW, typename TX, typename TA, int VW, int VPL, int U = gather_batch_wide<TA, VW, VPL>()>
 __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, const TW *__restrict__ w,
                                            const TX *__restrict__ X, int64_t ldx, int beg, int end, int es,
                                            int ES, int cl, int LV, int NV, int G, TA (&acc)[VPL][VW]) {
-  // batch size: about 48 registers of gathered values per lane
-  constexpr int kWords = VPL * VW * (int)(sizeof(TA) / 4);
-  constexpr int U = kWords <= 12 ? 4 : kWords <= 24 ? 2 : 1;
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll

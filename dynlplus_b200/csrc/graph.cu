@@ -2,7 +2,7 @@
 //
 // Layout: row r owns slots [rbeg[r], rcap[r]) of col/aw/w; [rbeg[r], rend[r]) are stored entries.
 // aw holds the graph's edge weights (0 = a deleted edge: a tombstone that a later insertion of the
-// same edge revives); w holds the solver's operator W_UU (aw masked to 0 unless both endpoints are
+// same edge revives, unless the deletion squeezed its row); w holds the solver's operator W_UU (aw masked to 0 unless both endpoints are
 // in the solved set U), the in-place masking of dynlp/stream.py:202-228. The patch keeps, for the
 // grounded system (dynlp/stream.py:142-177 in its resident form :300-346):
 //   rowsum[u] = sum_v w(u, v)                        (fp64)
@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kGThreads)
                    float *aw, float *w, const int32_t *__restrict__ du, const int32_t *__restrict__ dv, int32_t nd,
                    const uint8_t *__restrict__ umask, const uint8_t *__restrict__ labeled,
                    const int32_t *__restrict__ y, int32_t K, double *rowsum, double *B, uint8_t *changed,
-                   int32_t *n_applied, int32_t *err) {
+                   int32_t *n_applied, int32_t *err, uint8_t *squeeze) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nd) return;
   int32_t a = du[i], b = dv[i];
@@ -82,7 +82,35 @@ __global__ void __launch_bounds__(kGThreads)
   if (jb >= 0) aw[jb] = 0.0f;
   else atomicExch(err, DLP_ERR_DEVICE);  // asymmetric graph
   account(a, b, ja, jb, 0.0f, -old, w, umask, labeled, y, K, rowsum, B, changed);
+  if (squeeze) {
+    squeeze[a] = 1;
+    squeeze[b] = 1;
+  }
   if (n_applied) atomicAdd(n_applied, 1);
+}
+
+// Rows flagged in squeeze drop their deleted entries (aw == 0): the survivors move down in order
+// (col, aw, w together) and rend shrinks, so the slots are free for later insertions instead of
+// accumulating as tombstones until the row overflows. One thread per row; clears the flag.
+__global__ void __launch_bounds__(kGThreads)
+    k_graph_squeeze(int32_t n, const int32_t *__restrict__ rbeg, int32_t *rend, int32_t *col, float *aw, float *w,
+                    uint8_t *squeeze) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n || !squeeze[r]) return;
+  squeeze[r] = 0;
+  const int end = rend[r];
+  int k = rbeg[r];
+  for (int j = k; j < end; ++j) {
+    const float a = aw[j];
+    if (a == 0.0f) continue;
+    if (j != k) {
+      col[k] = col[j];
+      aw[k] = a;
+      w[k] = w[j];
+    }
+    ++k;
+  }
+  rend[r] = k;
 }
 
 // Dedupe table: key (a << 32 | b) with the largest batch index that inserts it.
@@ -303,10 +331,10 @@ using namespace dlp;
 
 extern "C" {
 
-int dlp_graph_delete(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, float *aw, float *w,
+int dlp_graph_delete(int32_t n, const int32_t *rbeg, int32_t *rend, int32_t *col, float *aw, float *w,
                      const int32_t *du, const int32_t *dv, int32_t nd, const uint8_t *umask, const uint8_t *labeled,
                      const int32_t *y, int32_t K, double *rowsum, double *B, uint8_t *changed, int32_t *n_applied,
-                     int32_t *err, dlp_stream_t stream) {
+                     int32_t *err, uint8_t *squeeze, dlp_stream_t stream) {
   if (n < 0 || nd < 0 || K <= 0) return DLP_ERR_INVALID;
   if (nd == 0) return DLP_OK;
   if (!rbeg || !rend || !col || !aw || !w || !du || !dv || !umask || !labeled || !y || !rowsum || !B || !changed ||
@@ -314,8 +342,9 @@ int dlp_graph_delete(int32_t n, const int32_t *rbeg, const int32_t *rend, const 
     return DLP_ERR_INVALID;
   k_graph_delete<<<grid1(nd), kGThreads, 0, (cudaStream_t)stream>>>(n, rbeg, rend, col, aw, w, du, dv, nd, umask,
                                                                      labeled, y, K, rowsum, B, changed, n_applied,
-                                                                     err);
-  return check_launch();
+                                                                     err, squeeze);
+  if (squeeze) k_graph_squeeze<<<grid1(n), kGThreads, 0, (cudaStream_t)stream>>>(n, rbeg, rend, col, aw, w, squeeze);
+  return check_launch(squeeze ? 2 : 1);
 }
 
 size_t dlp_graph_insert_workspace_bytes(int32_t ni) {

@@ -105,8 +105,15 @@ struct ApplyArgs {
   int64_t ldpo;
 };
 
+// Small fp32 rows fit in 64 registers (4 blocks of 256 threads per SM); the wider or fp64 ones keep
+// the compiler's choice rather than spill.
 template <class T, int VW, int VPL>
-__global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
+constexpr int apply_min_blocks() {
+  return (sizeof(typename T::TA) == 4 && VPL * VW <= 12 && VPL <= 4) ? 4 : 1;
+}
+
+template <class T, int VW, int VPL>
+__global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_pcg_apply(ApplyArgs<T> p) {
   using TA = typename T::TA;
   PcgCtl *ctl = p.B.ctl;
   if (ctl->done != 0) {
@@ -135,8 +142,8 @@ __global__ void __launch_bounds__(kThreads) k_pcg_apply(ApplyArgs<T> p) {
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL>(p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV,
-                                                              G, acc);
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, gather_batch_lean<TA, VW, VPL>()>(
+        p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);
 #pragma unroll
@@ -408,6 +415,85 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_dir(int mode, int32_t n, 
 static int sweep_blocks(int64_t) { return upd_blocks(); }
 
 // ------------------------------------------------------------------------------------------------
+// Certification statistics in one sweep: per column max |R|/diag and sum R^2 (and sum rhs^2), plus
+// max |H|. Per-thread column as in the PCG sweeps; per-block partials, then one warp per output.
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double block_column_max(const double *v, int c, int64_t ld) {
+  const long long base = (long long)blockIdx.x * blockDim.x;
+  const int first = (int)(((c - base % ld) % ld + ld) % ld);
+  const int lane = lane_id();
+  double s = 0.0;
+  for (long long tid = first + (long long)lane * ld; tid < blockDim.x; tid += 32 * ld) s = fmax(s, v[tid]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, off));
+  return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads)
+    k_resid_stats(int32_t n, int32_t C, const T *__restrict__ R, int64_t ldr, const T *__restrict__ rhs,
+                  int64_t ldrhs, const T *__restrict__ diag, const T *__restrict__ H, int64_t ldh, double *part) {
+  __shared__ double s_m[kSweepThreads], s_r[kSweepThreads], s_b[kSweepThreads], s_h[kSweepThreads / 32];
+  const SweepIdx ix = sweep_index(ldr, C);
+  double mx = 0.0, rr = 0.0, bb = 0.0, hm = 0.0;
+  if (ix.on) {
+    const int c = ix.c;
+    for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
+      double x[kSweepUnroll], d[kSweepUnroll], b[kSweepUnroll], h[kSweepUnroll];
+#pragma unroll
+      for (int u = 0; u < kSweepUnroll; ++u) {
+        const long long q = r + u * ix.RS;
+        const bool ok = q < n;
+        x[u] = ok ? (double)R[q * ldr + c] : 0.0;
+        d[u] = ok ? (double)diag[q] : 1.0;
+        b[u] = (ok && rhs) ? (double)rhs[q * ldrhs + c] : 0.0;
+        h[u] = (ok && H && c == 0) ? (double)H[q * ldh] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kSweepUnroll; ++u) {
+        mx = fmax(mx, fabs(x[u]) / d[u]);
+        rr = fma(x[u], x[u], rr);
+        bb = fma(b[u], b[u], bb);
+        hm = fmax(hm, fabs(h[u]));
+      }
+    }
+  }
+  const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  s_m[tid] = mx;
+  s_r[tid] = rr;
+  s_b[tid] = bb;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) hm = fmax(hm, __shfl_xor_sync(0xffffffffu, hm, off));
+  if (lane == 0) s_h[wid] = hm;
+  __syncthreads();
+  const int NO = 3 * C + 1;
+  for (int c = wid; c < C; c += kSweepThreads / 32) {
+    const double a = block_column_max(s_m, c, ldr);
+    const double b = block_column_sum(s_r, c, ldr);
+    const double e = block_column_sum(s_b, c, ldr);
+    if (lane == 0) {
+      part[(long long)blockIdx.x * NO + c] = a;
+      part[(long long)blockIdx.x * NO + C + c] = b;
+      part[(long long)blockIdx.x * NO + 2 * C + c] = e;
+    }
+  }
+  if (tid == 0) {
+    double v = 0.0;
+    for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_h[w]);
+    part[(long long)blockIdx.x * NO + 3 * C] = v;
+  }
+}
+
+__global__ void k_resid_stats_final(int32_t C, int nb, const double *__restrict__ part, double *out) {
+  const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int NO = 3 * C + 1;
+  if (o >= NO) return;
+  const bool is_max = o < C || o == 3 * C;
+  const double v = warp_strided_reduce(part + o, NO, nb, is_max);
+  if ((threadIdx.x & 31) == 0) out[o] = v;
+}
+
+// ------------------------------------------------------------------------------------------------
 // host driver
 // ------------------------------------------------------------------------------------------------
 struct PcgProblem {
@@ -524,12 +610,20 @@ static cudaStream_t g_capture_stream[64];
 static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, cudaGraphExec_t *out) {
   int dev = 0;
   DLP_CUDA(cudaGetDevice(&dev));
+  // the mean degree enters the kernels only through the gather layout it selects: key on that, so
+  // a graph whose entry count drifts from batch to batch keeps its instantiated chunk
+  Layout L;
+  {
+    const bool lo = q.w_lo != nullptr;
+    const size_t xs = lo ? 2 : (q.dtype == DLP_F32 ? 4 : 8);
+    DLP_TRY(choose_layout(q.C, xs, lo ? q.P_lo : q.P, lo ? q.ld_lo : q.ldp, 0, q.avg_deg, &L));
+  }
   GraphKey key{{(uintptr_t)dev, (uintptr_t)q.rbeg, (uintptr_t)q.rend, (uintptr_t)q.col, (uintptr_t)q.w,
                 (uintptr_t)q.w_dtype, (uintptr_t)q.n, (uintptr_t)q.C, (uintptr_t)q.diag, (uintptr_t)q.Z,
                 (uintptr_t)q.ldz, (uintptr_t)q.R, (uintptr_t)q.ldr, (uintptr_t)q.P, (uintptr_t)q.ldp, (uintptr_t)q.AP,
                 (uintptr_t)q.ldap, (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)k, (uintptr_t)q.w_lo,
-                (uintptr_t)q.P_lo, (uintptr_t)q.ld_lo,
-                (uintptr_t)(q.avg_deg * 1024)}};
+                (uintptr_t)q.P_lo, (uintptr_t)q.ld_lo, (uintptr_t)L.G, (uintptr_t)L.LV, (uintptr_t)L.VW,
+                (uintptr_t)L.VPL}};
   std::lock_guard<std::mutex> lk(g_graph_mu);
   auto it = g_graphs.find(key);
   if (it != g_graphs.end()) {
@@ -586,7 +680,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
   if (ldr > (int64_t)upd_blocks() * kSweepThreads) return DLP_ERR_INVALID;
   if ((w_lo || P_lo) && (!w_lo || !P_lo || ld_lo < C || dtype != DLP_F32)) return DLP_ERR_INVALID;
-  if (mode < 1 || mode > 3 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
+  if ((mode & 3) == 0 || mode > 7 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
     return DLP_ERR_DTYPE;
   if (!ws || ws_bytes < pcg_ws_bytes(C)) return DLP_ERR_WORKSPACE;
@@ -600,7 +694,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
                w_lo, P_lo, ld_lo};
   PcgBufs B = carve(ws, C);
   PcgCtl h{};
-  h.mode = mode;
+  h.mode = mode & 3;
   h.patience = patience > 0 ? patience : 400;
   h.max_iter = max_iter;
   h.target = target_relres;
@@ -621,8 +715,14 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
     DLP_CUDA(cudaMemsetAsync(B.rhsn, 0, sizeof(double) * C, s));
   }
   DLP_CUDA(cudaMemsetAsync(B.rz, 0, sizeof(double) * C, s));
-  // R = rhs - A Z; best = violation; P = R/diag; rz = R.(R/diag)
-  DLP_TRY(true_residual(q, s));
+  // R = rhs - A Z (= rhs when Z is known to be zero); best = violation; P = R/diag; rz = R.(R/diag)
+  if (mode & 4) {
+    const size_t es = q.dtype == DLP_F32 ? 4 : 8;
+    DLP_CUDA(cudaMemcpy2DAsync(q.R, (size_t)q.ldr * es, q.rhs, (size_t)q.ldrhs * es, (size_t)q.C * es, (size_t)q.n,
+                               cudaMemcpyDeviceToDevice, s));
+  } else {
+    DLP_TRY(true_residual(q, s));
+  }
   DLP_TRY(update_phase(2, q, B, s));
   DLP_TRY(dir_phase(2, q, B, s));
   const int k = check_every > 0 ? check_every : 8;
@@ -657,6 +757,31 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   if (relres_out) *relres_out = cur.relres;
   if (status_out) *status_out = cur.done;
   return DLP_OK;
+}
+
+size_t dlp_residual_stats_workspace_bytes(int32_t C) {
+  return (size_t)upd_blocks() * (size_t)(3 * (C > 0 ? C : 1) + 1) * sizeof(double);
+}
+
+int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const void *rhs, int64_t ldrhs,
+                       const void *diag, const void *H, int64_t ldh, int dtype, double *out, void *ws,
+                       size_t ws_bytes, dlp_stream_t stream) {
+  if (n < 0 || C <= 0 || ldr < C || (rhs && ldrhs < C) || !out || (n > 0 && (!R || !diag))) return DLP_ERR_INVALID;
+  if (ldr > (int64_t)upd_blocks() * kSweepThreads) return DLP_ERR_INVALID;
+  if (dtype != DLP_F32 && dtype != DLP_F64) return DLP_ERR_DTYPE;
+  if (!ws || ws_bytes < dlp_residual_stats_workspace_bytes(C)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = upd_blocks();
+  double *part = (double *)ws;
+  if (dtype == DLP_F32)
+    k_resid_stats<float><<<nb, kSweepThreads, 0, s>>>(n, C, (const float *)R, ldr, (const float *)rhs, ldrhs,
+                                                       (const float *)diag, (const float *)H, ldh, part);
+  else
+    k_resid_stats<double><<<nb, kSweepThreads, 0, s>>>(n, C, (const double *)R, ldr, (const double *)rhs, ldrhs,
+                                                        (const double *)diag, (const double *)H, ldh, part);
+  const int NO = 3 * C + 1;
+  k_resid_stats_final<<<(NO + 7) / 8, 256, 0, s>>>(C, nb, part, out);
+  return check_launch(2);
 }
 
 }  // extern "C"

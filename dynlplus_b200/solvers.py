@@ -93,6 +93,27 @@ def col_norms(X):
     return kernels.colreduce(2, X).sqrt()
 
 
+def residual_stats(sys: System, R, rhs=None, H=None):
+    """The certification check's reductions in one pass and one device-to-host copy: (rho_cols,
+    column sums of R^2, column sums of rhs^2 or None, max |H| or None) as host lists / floats
+    (dynlp/solvers.py:52-54, :295-301)."""
+    n, C = R.shape
+    dt = R.dtype
+    out = torch.zeros(3 * C + 1, dtype=F64, device=R.device)
+    if n:
+        if rhs is not None:
+            rhs = rhs.to(dt)
+        if H is not None:
+            H = H.to(dt)
+        ws = workspace("resid_stats").get(_lib.lib().dlp_residual_stats_workspace_bytes(C))
+        _lib.call("dlp_residual_stats", n, C, ptr(R), ld(R), ptr(rhs), ld(rhs) if rhs is not None else C,
+                  ptr(sys.diag.to(dt)), ptr(H), ld(H) if H is not None else 1, code(R), ptr(out), ptr(ws), ws.numel(),
+                  stream())
+    v = out.cpu().tolist()
+    return (v[:C], v[C:2 * C], v[2 * C:3 * C] if rhs is not None else None,
+            v[3 * C] if H is not None else None)
+
+
 class JacobiM:
     """R / diag (dynlp/solvers.py:62-63); recognised by `pcg`, which then runs the fused kernels."""
 
@@ -120,7 +141,7 @@ def bf16_weights(W):
 
 
 def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400, *, target_relres=None,
-        rhs_norm=None, check_every=8, use_graph=True, lowp=False):
+        rhs_norm=None, check_every=8, use_graph=True, lowp=False, zero_start=False):
     """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
 
     Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
@@ -149,6 +170,8 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
         if rhs_norm is None:
             rhs_norm = col_norms(rhs.to(dt)).cpu().tolist()
         rn = (ct.c_double * C)(*[float(x) for x in rhs_norm])
+    if zero_start:
+        mode |= 4  # Z == 0 on entry: the initial residual is rhs (no SpMM)
     ws = workspace("pcg").get(_lib.lib().dlp_pcg_workspace_bytes(C))
     it, viol, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_double(0), ct.c_int32(0)
     rhs = rhs.to(dt)
@@ -348,6 +371,9 @@ class DynLPPlus(Solver):
         self.push_frac, self.push_budget, self.amg_hmax = push_frac, push_budget, amg_hmax
         self.max_iter, self.amg_opts = max_iter, amg_opts or {}
         self.target_relres = target_relres
+        # share of the relative-residual target a correction round aims for (the rest absorbs the
+        # working-precision rounding between the PCG's own residual and the fp64 one)
+        self.refine_share = 0.2
         self.lowp = lowp  # SpMM sweeps on bf16 weights and scores (fp32 accumulation)
         self.name, self.H, self.hmax = f"dynlp+{method}", None, None
 
@@ -369,19 +395,25 @@ class DynLPPlus(Solver):
         M, wm = self._precond(sys, st, amg_box)
         return pcg(sys, Z, rhs, eps, M, self.max_iter, st, wm, lowp=self.lowp and Z.dtype == torch.float32, **kw)
 
-    def _run(self, sys, Z, rhs, eps, ops, st, amg_box, **kw):
-        """auto: push when few rows violate, else PCG/AMG (dynlp/solvers.py:272-288)."""
+    def _run(self, sys, Z, rhs, eps, ops, st, amg_box, zero_start=False, **kw):
+        """auto: push when few rows violate, else PCG/AMG (dynlp/solvers.py:272-288). With
+        zero_start (Z == 0 on entry) the residual is rhs itself and is not recomputed."""
         if self.method != "auto":
             st.path = self.method
-            return self._global(sys, Z, rhs, eps, st, amg_box, **kw)
-        R = residual(sys, Z, rhs)
-        st.edges += sys.nnz
+            return self._global(sys, Z, rhs, eps, st, amg_box, zero_start=zero_start, **kw)
+        if zero_start:
+            R = rhs
+        else:
+            R = residual(sys, Z, rhs)
+            st.edges += sys.nnz
         n = Z.shape[0]
         eps_d = torch.as_tensor(eps, dtype=F64, device=Z.device)
-        frac = int(kernels.flatnonzero(kernels.violating(R, sys.diag, eps_d)).numel()) / max(n, 1)
+        frac = int(kernels.violating(R, sys.diag, eps_d).sum().item()) / max(n, 1)
         if n and frac > self.push_frac:
             st.path = "amg" if self._use_amg() else "pcg"
-            return self._global(sys, Z, rhs, eps, st, amg_box, **kw)
+            return self._global(sys, Z, rhs, eps, st, amg_box, zero_start=zero_start, **kw)
+        if zero_start:
+            R = rhs.clone()  # push updates R in place
         Z, R, ok = push(sys, Z, R, eps, ops, st, self.push_budget * max(sys.nnz, 1))
         st.path = "push"
         if ok and not kw.get("target_relres"):
@@ -402,16 +434,18 @@ class DynLPPlus(Solver):
         hmax = h_est / (1 - float(rc[C]))
         return hmax, float(max(rc[:C])) * hmax
 
-    def _relres_ok(self, R64, rhs_norm):
+    def _relres_ok(self, ss, rhs_norm):
+        """max_c ||R_c|| / ||rhs_c|| over the label columns, from the column sums of squares."""
         if self.target_relres is None:
             return True, float("nan")
-        rel = (col_norms(R64[:, : self.C]) / rhs_norm).max().item()
+        rel = max((ss[c] ** 0.5) / rhs_norm[c] if rhs_norm[c] > 0 else ss[c] ** 0.5 for c in range(self.C))
         return rel <= self.target_relres, rel
 
-    def _refine(self, sw, s64, Z64, rhs64, ops, st, amg_box, rounds, rhs_norm, R64=None):
+    def _refine(self, sw, s64, Z64, rhs64, ops, st, amg_box, rounds, rhs_norm, R64=None, stats=None):
         """fp64 certification and refinement (dynlp/solvers.py:322-337): R64 = rhs - A Z64; if the
         certificate (or the relative residual) falls short, solve A D = R64 / scale in the working
-        precision and add D * scale. Returns (Z64, R64, hmax, bound, relres)."""
+        precision and add D * scale. `stats` (residual_stats of R64) may come with R64. Returns
+        (Z64, R64, hmax, bound, relres)."""
         C = self.C
         hmax, bound, rel = self.hmax, float("inf"), float("nan")
         dev = Z64.device
@@ -419,10 +453,12 @@ class DynLPPlus(Solver):
             if R64 is None:
                 R64 = residual(s64, Z64, rhs64)
                 st.edges += s64.nnz
-            rc = rho_cols(s64, R64).cpu().tolist()
-            h_est = float(kernels.colreduce(3, Z64[:, C:]).item())
+                stats = None
+            if stats is None:
+                stats = residual_stats(s64, R64, H=Z64[:, C:])
+            rc, ss, _, h_est = stats
             hmax, bound = self._bound(rc, h_est)
-            ok_rel, rel = self._relres_ok(R64, rhs_norm)
+            ok_rel, rel = self._relres_ok(ss, rhs_norm)
             if bound <= self.tol and ok_rel:
                 break
             scale = [r if r > 0 else 1.0 for r in rc]
@@ -433,26 +469,26 @@ class DynLPPlus(Solver):
             if self.target_relres is not None:
                 # the correction must bring the fp64 residual of every F column under the target, or
                 # as far as the working precision resolves in one round (the next round continues)
-                rnR = col_norms(R64[:, :C]).cpu().tolist()
+                rnR = [ss[c] ** 0.5 for c in range(C)]
                 fl = 3e-6 if self.dtype == torch.float32 else 1e-13
-                allowed = [max(0.5 * self.target_relres * float(rhs_norm[c]), fl * rnR[c], 1e-300) / scale[c]
-                           for c in range(C)]
+                allowed = [max(self.refine_share * self.target_relres * float(rhs_norm[c]), fl * rnR[c], 1e-300) /
+                           scale[c] for c in range(C)]
                 kw = dict(target_relres=1.0, rhs_norm=allowed + [1e300])
             Rs = _scratch("ref_Rs", Z64.shape[0], C + 1, self.dtype, dev)
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs), ld(Rs),
                       code(Rs), stream())
             D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)
             D.zero_()
-            D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, **kw)
+            D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, zero_start=True, **kw)
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(D), ld(D), code(D), ptr(sc), 1, ptr(Z64), ld(Z64),
                       code(Z64), stream())
-            R64 = None
+            R64, stats = None, None
         if R64 is None:
             R64 = residual(s64, Z64, rhs64)
             st.edges += s64.nnz
-            rc = rho_cols(s64, R64).cpu().tolist()
-            hmax, bound = self._bound(rc, float(kernels.colreduce(3, Z64[:, C:]).item()))
-            _, rel = self._relres_ok(R64, rhs_norm)
+            rc, ss, _, h_est = residual_stats(s64, R64, H=Z64[:, C:])
+            hmax, bound = self._bound(rc, h_est)
+            _, rel = self._relres_ok(ss, rhs_norm)
         return Z64, R64, hmax, bound, rel
 
     def _rhs_h(self, sys):
@@ -485,10 +521,10 @@ class DynLPPlus(Solver):
             self.hmax = hmax = hmax or 1.0
             eps = [max(tol / (1.25 * hmax), self._floor())] * C + [max(self.eps_h, self._floor(hmax))]
             rhs64 = self._rhs_h(s64)
-            rn = col_norms(rhs64[:, :C]) if self.target_relres is not None else None
+            rn = col_norms(rhs64[:, :C]).cpu().tolist() if self.target_relres is not None else None
             kw = {}
             if self.target_relres is not None:
-                kw = dict(target_relres=self.target_relres, rhs_norm=rn.cpu().tolist() + [1e300])
+                kw = dict(target_relres=self.target_relres, rhs_norm=rn + [1e300])
             Z = self._run(sw, Z, rhs, eps, ops, st, amg_box, **kw)
             Z64 = padded_empty(n, C + 1, F64, dev)
             Z64.copy_(Z)
@@ -557,7 +593,6 @@ class IncrementalLP(DynLPPlus):
         sw = sys.astype(self.dtype)
         with Timer() as tm:
             rhs64 = self._rhs_h(s64)
-            rn = col_norms(rhs64[:, :C]) if self.target_relres is not None else None
             if self.Z is None:
                 inner = DynLPPlus.solve(self, sys)
                 st.iters, st.edges, st.setup_ms, st.path = inner.iters, inner.edges, inner.setup_ms, "inc-" + inner.path
@@ -575,30 +610,36 @@ class IncrementalLP(DynLPPlus):
                     self._full_residual(s64, st)
                 amg_box = [None]
                 ops = FrontierOps(sw.W, C + 1, self.group)
-                rc = rho_cols(s64, self.R).cpu().tolist()
-                h_est = float(kernels.colreduce(3, self.Z[:, C:]).item())
+                # one pass: rho_cols, ||R_c||^2, ||rhs_c||^2 and max h
+                stats = residual_stats(s64, self.R, rhs=rhs64 if self.target_relres is not None else None,
+                                       H=self.Z[:, C:])
+                rc, ss, bb, h_est = stats
+                rn = [b ** 0.5 for b in bb[:C]] if bb is not None else None
                 hmax, bound = self._bound(rc, h_est)
-                ok_rel, rel = self._relres_ok(self.R, rn)
+                ok_rel, rel = self._relres_ok(ss, rn)
                 st.path = "inc-none"
                 if not (bound <= tol and ok_rel):
-                    eps = [tol / (1.25 * (self.hmax or 1.0))] * C + [self.eps_h]
-                    eps_d = torch.as_tensor(eps, dtype=F64, device=self.Z.device)
-                    nviol = int(kernels.flatnonzero(kernels.violating(self.R, s64.diag, eps_d)).numel())
-                    small = nviol / max(s64.n_solved, 1) <= self.push_frac and self.method in ("auto", "push")
-                    if small and self.target_relres is None:
+                    small = False
+                    if self.target_relres is None and self.method in ("auto", "push"):
+                        eps = [tol / (1.25 * (self.hmax or 1.0))] * C + [self.eps_h]
+                        eps_d = torch.as_tensor(eps, dtype=F64, device=self.Z.device)
+                        nviol = int(kernels.violating(self.R, s64.diag, eps_d).sum().item())
+                        small = nviol / max(s64.n_solved, 1) <= self.push_frac
+                    if small:
                         st.path = "inc-push"
                         for _ in range(4):
                             ok = self._push(s64, eps, st)
-                            hmax, bound = self._bound(rho_cols(s64, self.R).cpu().tolist(),
-                                                      float(kernels.colreduce(3, self.Z[:, C:]).item()))
+                            rc2, _, _, h2 = residual_stats(s64, self.R, H=self.Z[:, C:])
+                            hmax, bound = self._bound(rc2, h2)
                             if ok and bound <= tol:
                                 break
                             eps = [tol / (1.25 * hmax)] * C + [self.eps_h]
                         rel = float("nan")
-                    if not (bound <= tol and (small and self.target_relres is None)):
+                        stats = None
+                    if not (bound <= tol and small):
                         st.path = "inc-" + ("pcg" if self.method in ("auto", "pcg", "push") else self.method)
                         self.Z, self.R, hmax, bound, rel = self._refine(sw, s64, self.Z, rhs64, ops, st, amg_box, 10,
-                                                                        rn, R64=self.R)
+                                                                        rn, R64=self.R, stats=stats)
                 st.cert, st.hmax, self.hmax, st.relres = bound, hmax, hmax, rel
             self.F, self.H = self.Z[:, :C], self.Z[:, C:]
         st.ms = tm.ms

@@ -138,7 +138,7 @@ class ResidentGraph:
     """Slack-padded rows on the device. Row r owns slots [rbeg[r], rcap[r]); [rbeg[r], rend[r]) are
     stored entries. `aw` = edge weights (0 = deleted), `data` = the solver operator W_UU."""
 
-    def __init__(self, A: CSR, slack_frac=0.25, slack_min=4):
+    def __init__(self, A: CSR, slack_frac=0.25, slack_min=8):
         self._build_from(A.indptr, A.indices, A.data.to(torch.float32), A.shape[0], slack_frac, slack_min)
 
     def _build_from(self, indptr, indices, aw, n, slack_frac, slack_min):
@@ -196,7 +196,7 @@ class ResidentGraph:
         del rbeg_l
         w_live = self.data[: slots.numel()][live]
         self._build_from(indptr, self.indices[: slots.numel()][live], self.aw[: slots.numel()][live], n,
-                         self.slack_frac * grow + 0.25, self.slack_min * 2)
+                         self.slack_frac * grow + 0.25, max(self.slack_min * 2, 4))
         slots = self.slot_rows()
         j = torch.arange(slots.numel(), device=slots.device)
         live_new = j < self.rend.long()[slots]
@@ -231,7 +231,7 @@ class EdgeStream:
     equation changed and `moved` the rows that entered or left U.
     """
 
-    def __init__(self, ds: Dataset, labeled, *, eta_rel=0.0, dtype="float32", with_h=True, slack_frac=0.25,
+    def __init__(self, ds: Dataset, labeled, *, eta_rel=0.0, dtype="float32", with_h=True, slack_frac=0.25, slack_min=8,
                  active=None):
         A, K = ds.A, ds.K
         self.ds, self.K, self.dtype = ds, K, to_dtype(dtype)
@@ -241,7 +241,7 @@ class EdgeStream:
         n = A.shape[0]
         dev = A.indices.device
         self.n, self.dev = n, dev
-        self.G = ResidentGraph(A, slack_frac=slack_frac)
+        self.G = ResidentGraph(A, slack_frac=slack_frac, slack_min=slack_min)
         labeled = labeled.to(torch.bool)
         active = torch.ones(n, dtype=torch.bool, device=dev) if active is None else active.to(torch.bool)
         self.labeled = (labeled & active).to(torch.uint8)
@@ -255,6 +255,7 @@ class EdgeStream:
         self.umask = torch.zeros(n, dtype=torch.uint8, device=dev)
         self.in_t = torch.zeros(n, dtype=torch.uint8, device=dev)
         self.changed = torch.zeros(n, dtype=torch.uint8, device=dev)
+        self._squeeze = torch.zeros(n, dtype=torch.uint8, device=dev)  # rows to squeeze after deletions
         self._stat = torch.zeros(8, dtype=torch.int32, device=dev)
         self.counters = {"rebuilds": 0, "ground_changes": 0, "applied": 0, "ground_sweeps": 0, "ground_fallbacks": 0}
         self._ground()
@@ -328,7 +329,7 @@ class EdgeStream:
         if nd:
             _lib.call("dlp_graph_delete", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(du),
                       ptr(dv), nd, ptr(self.umask), ptr(self.labeled), ptr(self.y), self.K, ptr(self.rowsum),
-                      ptr(self.B), ptr(self.changed), ptr(st[2:3]), ptr(st[0:1]), s)
+                      ptr(self.B), ptr(self.changed), ptr(st[2:3]), ptr(st[0:1]), ptr(self._squeeze), s)
         if ni:
             for attempt in range(4):
                 ws = workspace("insert").get(_lib.lib().dlp_graph_insert_workspace_bytes(ni))

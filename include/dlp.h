@@ -188,12 +188,23 @@ int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_
                    dlp_stream_t stream);
 
 
+/* One pass of the certification check (dynlp/solvers.py:295-301, :322-337) over an n x C residual
+ * R (the last column the h column's): out[c] = max_u |R_uc| / diag_u (rho_cols), out[C + c] =
+ * sum_u R_uc^2, out[2C + c] = sum_u rhs_uc^2 (skipped when rhs is NULL), out[3C] = max_u |H_u| (H: one
+ * column, stride ldh; skipped when NULL). All in fp64 with a fixed reduction order. dtype of R, rhs,
+ * H and diag: f32/f64. Workspace: dlp_residual_stats_workspace_bytes(C); out: device double[3C+1]. */
+size_t dlp_residual_stats_workspace_bytes(int32_t C);
+int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const void *rhs, int64_t ldrhs,
+                       const void *diag, const void *H, int64_t ldh, int dtype, double *out, void *ws,
+                       size_t ws_bytes, dlp_stream_t stream);
+
 /* ---- (d) fused block PCG, Jacobi preconditioner --------------------------------------------
  * Replaces solvers.pcg with jacobi_M (dynlp/solvers.py:62-97): one CG per column of
  * (diag - W) Z = rhs, starting from the Z given. Per iteration three kernels (SpMM + pAp, residual
  * update + rz/norms/violation, direction update); all inner products and norms in fp64, reduced
  * in a fixed order. Stop rule `mode`: bit 0 = the reference's max_uc |R_uc|/(eps_c diag_u) <= 1,
- * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold). A proposed
+ * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold); bit 2 = the
+ * caller guarantees Z == 0 on entry, so the initial residual is rhs itself (copied, no SpMM). A proposed
  * stop is confirmed on the true residual rhs - A Z (solvers.py:85-89); `patience` iterations
  * without a 10% improvement stop the solve as the reference's stall rule does (:90-92).
  * eps and rhs_norm are HOST arrays of C doubles (rhs_norm may be NULL when bit 1 is unused).
@@ -219,7 +230,8 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
  * No reference counterpart for edge updates (the reference streams vertices); closest are
  * IncrementalStream._toggle / _label_update (dynlp/stream.py:206-235). Row r owns slots
  * [rbeg[r], rcap[r]) of col/aw/w, of which [rbeg[r], rend[r]) are stored entries. aw = graph edge
- * weights (0 = deleted: a tombstone, revived by a later insertion of the edge); w = the solver
+ * weights (0 = deleted: a tombstone, revived by a later insertion of the edge unless its row was
+ * squeezed); w = the solver
  * operator W_UU (aw masked to 0 unless both ends are in U = umask). Each applied change updates
  * rowsum[u] = sum_v w(u,v) and B[u, y_l] = sum of aw(u,l) over labelled l (both fp64, B n x K)
  * and flags changed[u] for every solved row whose equation changed. Deletions (du, dv) and
@@ -228,11 +240,13 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
  * one edge the largest batch index wins. *err (device int, caller-zeroed) reports endpoints out of
  * range; *overflow = 1 when a row ran out of slack (the edges that did not fit are not applied
  * and the graph stays consistent: rebuild with more slack and run the insertions again).
- * *n_applied (device int, may be NULL) counts applied updates. */
-int dlp_graph_delete(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, float *aw, float *w,
+ * *n_applied (device int, may be NULL) counts applied updates. With squeeze (n bytes, zero on
+ * entry and on return; may be NULL) the rows that lost entries drop them (survivors keep their order,
+ * rend shrinks), so their slots serve later insertions instead of staying as tombstones. */
+int dlp_graph_delete(int32_t n, const int32_t *rbeg, int32_t *rend, int32_t *col, float *aw, float *w,
                      const int32_t *du, const int32_t *dv, int32_t nd, const uint8_t *umask, const uint8_t *labeled,
                      const int32_t *y, int32_t K, double *rowsum, double *B, uint8_t *changed, int32_t *n_applied,
-                     int32_t *err, dlp_stream_t stream);
+                     int32_t *err, uint8_t *squeeze, dlp_stream_t stream);
 size_t dlp_graph_insert_workspace_bytes(int32_t ni);
 int dlp_graph_insert(int32_t n, const int32_t *rbeg, int32_t *rend, const int32_t *rcap, int32_t *col, float *aw,
                      float *w, const int32_t *iu, const int32_t *iv, const float *iw, int32_t ni,

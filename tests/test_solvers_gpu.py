@@ -72,6 +72,46 @@ def test_fused_pcg_fp32_and_relres_target():
     assert rel <= 1e-5 * 1.01 and st.iters < 200, (rel, st.iters)
 
 
+@pytest.mark.parametrize("graph", [True, False])
+def test_fused_pcg_zero_start_is_the_same_solve(graph):
+    """Mode bit 2 (Z == 0 on entry: R = rhs, no SpMM) gives the reference's iteration counts and
+    iterate, exactly as the plain start from Z = 0 does."""
+    g, A, S = golden_system()
+    for tag in ("pcg_loose", "pcg_tight"):
+        out = []
+        for zs in (False, True):
+            Z = torch.zeros((A.shape[0], 3), dtype=torch.float64, device="cuda")
+            st = solvers.Stats()
+            solvers.pcg(S, Z, S.rhs, g[f"{tag}_eps"].tolist(), solvers.jacobi_M(S), 10_000, st, use_graph=graph,
+                        zero_start=zs)
+            assert st.iters == int(g[f"{tag}_iters"]), (tag, zs, st.iters)
+            out.append(Z.cpu().numpy())
+        np.testing.assert_allclose(out[1], out[0], rtol=1e-13, atol=1e-15)
+        np.testing.assert_allclose(out[1], g[f"{tag}_Z"], rtol=1e-8, atol=1e-11)
+
+
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+@pytest.mark.parametrize("n,C", [(1, 1), (1000, 3), (300_000, 9), (50_000, 33)])
+def test_residual_stats_match_torch(dt, n, C):
+    """dlp_residual_stats: rho_cols, column sums of squares of R and rhs, max |h| in one pass."""
+    gen = torch.Generator(device="cuda").manual_seed(n + C)
+    ldr = C + (1 if dt == torch.float64 and C % 2 else 0)
+    R = torch.randn((n, ldr), generator=gen, device="cuda", dtype=torch.float64).to(dt)[:, :C]
+    rhs = torch.randn((n, C), generator=gen, device="cuda", dtype=torch.float64).to(dt)
+    diag = (torch.rand(n, generator=gen, device="cuda", dtype=torch.float64) + 0.5).to(dt)
+    Z = torch.randn((n, C + 2), generator=gen, device="cuda", dtype=torch.float64).to(dt)
+    S = stream.System(t=0, U=torch.arange(n, device="cuda"), W=None, s=diag, diag=diag, B=rhs, rhs=rhs, prior=None,
+                      is_new=None, seed=None, comps={}, K=C, C=C, eta=0.0, n_inserted=0, n_deleted=0, n_active=n)
+    rc, ss, bb, hm = solvers.residual_stats(S, R, rhs=rhs, H=Z[:, C:C + 1])
+    R64, d64 = R.double(), diag.double()
+    np.testing.assert_allclose(rc, (R64.abs() / d64[:, None]).max(0).values.cpu().numpy(), rtol=1e-15)
+    np.testing.assert_allclose(ss, (R64 ** 2).sum(0).cpu().numpy(), rtol=1e-12)
+    np.testing.assert_allclose(bb, (rhs.double() ** 2).sum(0).cpu().numpy(), rtol=1e-12)
+    assert hm == float(Z[:, C].double().abs().max())
+    rc2, ss2, bb2, hm2 = solvers.residual_stats(S, R)
+    assert rc2 == rc and ss2 == ss and bb2 is None and hm2 is None
+
+
 def test_push_rounds_match_reference():
     g, A, S = golden_system()
     Z, R = T(g["push_Z0"]), T(g["push_R0"])
@@ -153,7 +193,7 @@ def test_edge_stream_matches_rebuilt_system(weights):
     n, K = 4000, 3
     ds = graphs.planted_partition(n, K, 3.0, 1.0, weights=weights, seed=2)  # sparse: splits and regrounding
     lab = graphs.label_mask(n, 0.01, seed=2)
-    es = stream.EdgeStream(ds, lab, slack_frac=0.0)  # no slack: forces repacking
+    es = stream.EdgeStream(ds, lab, slack_frac=0.0, slack_min=0)  # no slack: forces repacking
     up = graphs.EdgeUpdates(ds.A, seed=3, weights=weights)
     A_sc = ds.A.to_scipy().astype(np.float64)
     y, labn = ds.y.cpu().numpy(), lab.cpu().numpy()
