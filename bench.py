@@ -74,29 +74,51 @@ def config(a):
 # clocks during the timed region
 # ---------------------------------------------------------------------------------------------
 class Clocks:
+    """nvidia-smi sampling every 20 ms on a reader thread; `wait_first` blocks (a few seconds at
+    most) until the first sample is in, so the timed region is covered from its start."""
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.p = None
+        import threading
+        self.p, self.lines, self.first = None, [], threading.Event()
+        self.t0 = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "20"], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.p = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.p.stdout:
+            if line.strip():
+                self.lines.append((time.perf_counter(), line.strip()))
+                self.first.set()
+
+    def wait_first(self, timeout=10.0):
+        if self.p is not None:
+            self.first.wait(timeout)
+        self.t0 = time.perf_counter()
 
     def stop(self):
         if self.p is None:
             return None
+        t1 = time.perf_counter()
         self.p.terminate()
         try:
-            out, _ = self.p.communicate(timeout=5)
+            self.p.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.p.kill()
-            out, _ = self.p.communicate()
-        rows = [r.split(", ") for r in out.strip().splitlines() if r.strip()]
+        self.th.join(timeout=5)
+        # samples taken inside the timed region (plus the last one before it, for short regions)
+        inside = [ln for ts, ln in self.lines if self.t0 is None or self.t0 <= ts <= t1 + 0.05]
+        before = [ln for ts, ln in self.lines if self.t0 is not None and ts < self.t0][-1:]
+        rows = [r.split(", ") for r in (before + inside)]
         rows = [r for r in rows if len(r) >= 8]
         if not rows:
             return None
@@ -104,7 +126,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][1]),
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "samples_inside_timed_region": len(inside)}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -221,6 +243,44 @@ def spmm_roofline(es, C, peaks):
                     "gathered matrix (n x ld x 4 B) fits in L2"}
 
 
+def pcg_iteration_bytes(n, nnz, C, s=4):
+    """Algorithmic bytes of one fused PCG iteration on an n-row operator with nnz entries and C
+    columns of s-byte values: the apply (row ranges, the gather model nnz (4 + s_w + C s), diag,
+    own row of P, AP written), the residual update (R read and written, AP read, diag) and the
+    direction update (P and Z read and written, R read, diag)."""
+    apply = 8 * n + nnz * (4 + 4 + C * s) + n * s + n * C * s + n * C * s
+    update = 3 * n * C * s + n * s
+    direction = 5 * n * C * s + n * s
+    return apply + update + direction
+
+
+def pcg_roofline(events, nnz, peaks, traffic_file):
+    """The fused PCG iteration (k_pcg_apply + k_pcg_update + k_pcg_dir), timed live: CUDA events
+    around every dlp_pcg call of the timed steps (on the launching stream); time per iteration =
+    the calls' total device time / their iterations (so it also carries each call's start, stop
+    checks and recheck, a conservative figure)."""
+    ms = sum(s.elapsed_time(e) for s, e, _, _, _ in events)
+    iters = sum(it for _, _, it, _, _ in events)
+    if not iters:
+        return None
+    n, C = events[0][3], events[0][4]
+    algo = pcg_iteration_bytes(n, nnz, C)
+    t = ms / iters
+    achieved = algo / (t * 1e-3) / 1e9
+    peak = peaks.get("hbm_gbs") or 6650.0
+    traffic, tsrc = None, None
+    if os.path.exists(traffic_file):
+        tr = json.load(open(traffic_file))
+        if tr.get("n") == n and tr.get("C") == C:
+            traffic, tsrc = tr.get("dram_bytes_per_iteration"), tr.get("source")
+    return {"bound": "hbm", "kernel": "fused PCG iteration: k_pcg_apply + k_pcg_update + k_pcg_dir "
+                                      "(fp32, C=%d, compact CSR of W_UU, nnz=%d)" % (C, nnz),
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback",
+            "traffic": traffic, "traffic_source": tsrc, "algorithmic_bytes_per_iteration": int(algo),
+            "ms_per_iteration": t, "iterations_timed": int(iters), "pcg_calls": len(events)}
+
+
 def ours(a):
     import torch
     import torch.distributed as dist
@@ -277,7 +337,10 @@ def ours(a):
     if world > 1:
         dist.barrier()
     clocks = Clocks(torch.cuda.current_device()) if not a.no_clocks else None
+    if clocks is not None:
+        clocks.wait_first()
     launches0 = _lib.lib().dlp_launch_count()
+    solvers.PCG_EVENTS = []  # CUDA events around the fused PCG calls of the timed steps
     torch.cuda.nvtx.range_push("timed")  # lets a profiler filter the timed steps (--nvtx-include timed/)
     times, relres, paths, iters, events = [], [], [], [], {}
     for k, b in enumerate(dev_batches):
@@ -298,8 +361,8 @@ def ours(a):
             events[k] = ev
     launches = _lib.lib().dlp_launch_count() - launches0
     torch.cuda.nvtx.range_pop()
-    clk = clocks.stop() if clocks else None
-    # end to end: host arrays in, host result out
+    pcg_events, solvers.PCG_EVENTS = solvers.PCG_EVENTS, None
+    # end to end: host arrays in, host result out (the clock sampling covers this region too)
     e2e_times = []
     h2d = sum(v.numel() * v.element_size() for v in host_batches[0].values()) if host_batches else 0
     for b in host_batches:
@@ -312,6 +375,7 @@ def ours(a):
         e.synchronize()
         e2e_times.append(s.elapsed_time(e))
         relres.append(float(res[0]))
+    clk = clocks.stop() if clocks else None
     total = torch.tensor([sum(times), sum(e2e_times)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(total, op=dist.ReduceOp.MAX)
@@ -319,7 +383,12 @@ def ours(a):
     t_dev, t_e2e = float(total[0]), float(total[1])
     value = world * a.batch * len(times) / (t_dev * 1e-3)
     e2e = world * a.batch * len(e2e_times) / (t_e2e * 1e-3)
-    roof = spmm_roofline(es, a.k + 1, peaks) if rank == 0 else None
+    roof = None
+    if rank == 0:
+        roof = pcg_roofline(pcg_events, es.solver_csr().nnz, peaks,
+                            os.path.join(ROOT, "profiles", "pcg_iteration_traffic.json"))
+        if roof is not None:
+            roof["spmm_alone"] = spmm_roofline(es, a.k + 1, peaks)
     cpu = None
     if rank == 0 and not a.no_cpu_baseline and world == 1:
         v, done, tw = cpu_batches(a, A0, ds.y.cpu().numpy(), lab.cpu().numpy(), Z0, cpu_sample, a.cpu_budget_s)

@@ -140,6 +140,11 @@ def bf16_weights(W):
     return wb
 
 
+# Optional record of fused-PCG calls: when a list, every dlp_pcg call appends (start event, end
+# event, iterations, n, C) recorded on the launching stream (a profiler hook; None = off).
+PCG_EVENTS = None
+
+
 def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400, *, target_relres=None,
         rhs_norm=None, check_every=8, use_graph=True, lowp=False, zero_start=False):
     """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
@@ -181,11 +186,18 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
             raise TypeError("the BF16 sweeps run inside the fp32 working precision")
         w_lo = bf16_weights(W)
         P_lo = _scratch("pcg_Plo", n, C, torch.bfloat16, dev, padded=True)
+    ev = None
+    if PCG_EVENTS is not None:
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ev[0].record()
     _lib.call("dlp_pcg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C, ptr(diag),
               ptr(rhs), ld(rhs), ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), code(Z), eps_h, rn,
               float(target_relres or 0.0), mode, int(max_iter), int(patience), int(check_every), int(bool(use_graph)),
               W.nnz / max(n, 1), ptr(ws), ws.numel(), ct.byref(it), ct.byref(viol), ct.byref(rel), ct.byref(status),
               stream(), ptr(w_lo), ptr(P_lo), ld(P_lo) if P_lo is not None else 0)
+    if ev is not None:
+        ev[1].record()
+        PCG_EVENTS.append((ev[0], ev[1], it.value, n, C))
     st.iters += it.value
     st.edges += (it.value + 2) * W.nnz + work_M * it.value
     st.relres = rel.value
