@@ -51,6 +51,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_graph_delete": ("ipppppppipppippppppp", ct.c_int),
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
+    "dlp_label_update": ("pidpppppipppp", ct.c_int),
+    "dlp_new_dissim": ("pipppidpp", ct.c_int),
     "dlp_graph_toggle": ("ppppppippppp", ct.c_int),
     "dlp_graph_to_csr_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_to_csr": ("ippppppppzp", ct.c_int),
@@ -66,6 +68,9 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_amg_members": ("iippppzp", ct.c_int),
     "dlp_amg_coarse_plan": ("ipppppzp", ct.c_int),
     "dlp_amg_coarsen": ("ipppppppppqppppppzp", ct.c_int),
+    "dlp_amg_coarse_keys": ("ippppippp", ct.c_int),
+    "dlp_amg_coarse_reduce_workspace_bytes": ("qi", ct.c_size_t),
+    "dlp_amg_coarse_reduce": ("qppipppppppppzp", ct.c_int),
     "dlp_amg_restrict": ("iipppqpqip", ct.c_int),
     "dlp_amg_prolong_add": ("iippqpqip", ct.c_int),
     "dlp_amg_scale_rows": ("iidpqppqip", ct.c_int),

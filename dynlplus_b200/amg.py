@@ -58,27 +58,31 @@ def members(agg, nc):
 
 
 def coarsen(W: CSR, s, agg, nc, off=None, mem=None):
-    """(W_c, s_c) of the aggregation (dynlp/amg.py:67-74), sorted CSR rows, fp64 sums."""
+    """(W_c, s_c) of the aggregation (dynlp/amg.py:67-74): sorted CSR rows, fp64 sums in the fine
+    CSR order. Every fine entry gets the key (aggregate of its row, aggregate of its column); a
+    stable sort by key brings each coarse entry's contributions together in their original order
+    and one kernel sums the runs (the reference's coalesce)."""
     dev = W.indices.device
-    if off is None:
+    n, m = W.shape[0], int(W.indices.numel())
+    if s is not None and off is None:
         off, mem = members(agg, nc)
-    ws = workspace("amg_members").get(_lib.lib().dlp_amg_members_workspace_bytes(nc))
-    toff = torch.empty(nc + 1, dtype=torch.int32, device=dev)
-    _lib.call("dlp_amg_coarse_plan", nc, ptr(off), ptr(mem), ptr(W.indptr), ptr(toff), ptr(ws), ws.numel(), stream())
-    slots = int(toff[nc].item())
-    tkey = torch.empty(max(slots, 1), dtype=torch.int32, device=dev)
-    tval = torch.empty(max(slots, 1), dtype=torch.float64, device=dev)
-    sc = torch.empty(max(nc, 1), dtype=torch.float64, device=dev) if s is not None else None
+    key = torch.empty(max(m, 1), dtype=torch.int64, device=dev)
+    val = torch.empty(max(m, 1), dtype=torch.float64, device=dev)
+    _lib.call("dlp_amg_coarse_keys", n, ptr(W.indptr), ptr(W.indices), ptr(W.data.float().contiguous()),
+              ptr(agg.to(torch.int32).contiguous()), nc, ptr(key), ptr(val), stream())
+    key, order = torch.sort(key[:m], stable=True)
+    val = val[:m][order]
     indptr_c = torch.empty(nc + 1, dtype=torch.int32, device=dev)
-    cap = max(slots // 2, 1)
-    col_c = torch.empty(cap, dtype=torch.int32, device=dev)
-    w_c = torch.empty(cap, dtype=torch.float32, device=dev)
-    _lib.call("dlp_amg_coarsen", nc, ptr(off), ptr(mem), ptr(W.indptr), ptr(W.indices),
-              ptr(W.data.float().contiguous()), ptr(agg), ptr(toff), ptr(tkey), ptr(tval), slots,
+    col_c = torch.empty(max(m, 1), dtype=torch.int32, device=dev)
+    w_c = torch.empty(max(m, 1), dtype=torch.float32, device=dev)
+    nnz = torch.empty(1, dtype=torch.int32, device=dev)
+    sc = torch.empty(max(nc, 1), dtype=torch.float64, device=dev) if s is not None else None
+    ws = workspace("amg_coarse").get(_lib.lib().dlp_amg_coarse_reduce_workspace_bytes(m, nc))
+    _lib.call("dlp_amg_coarse_reduce", m, ptr(key), ptr(val), nc, ptr(off), ptr(mem),
               ptr(s.to(torch.float64).contiguous()) if s is not None else None, ptr(sc), ptr(indptr_c), ptr(col_c),
-              ptr(w_c), ptr(ws), ws.numel(), stream())
-    nnz = int(indptr_c[nc].item())
-    Wc = CSR(w_c[:nnz], col_c[:nnz], indptr_c, (nc, nc))
+              ptr(w_c), ptr(nnz), ptr(ws), ws.numel(), stream())
+    k = int(nnz.item())
+    Wc = CSR(w_c[:k], col_c[:k], indptr_c, (nc, nc))
     return Wc, (sc[:nc] if sc is not None else None)
 
 

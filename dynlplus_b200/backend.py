@@ -59,7 +59,9 @@ def stream():
 
 
 def sync():
-    torch.cuda.synchronize()
+    """Wait for the current stream (not the whole device: another thread may be capturing a CUDA
+    graph on its own stream, and a device-wide synchronisation would invalidate that capture)."""
+    torch.cuda.current_stream().synchronize()
 
 
 def mem_used_gb() -> float:
@@ -67,7 +69,8 @@ def mem_used_gb() -> float:
 
 
 class Timer:
-    """Wall-clock timer that synchronizes the device on enter and exit (dynlp/backend.py:43-56)."""
+    """Wall-clock timer that synchronizes the current stream on enter and exit (dynlp/backend.py:43-56
+    synchronizes the device; per-stream keeps concurrent workers independent)."""
 
     def __init__(self):
         self.ms = 0.0

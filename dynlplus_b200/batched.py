@@ -91,11 +91,11 @@ class BatchedSystems:
             W = self.csr()
             Y = torch.empty((self.N, self.Ch), dtype=self.dtype, device=self.dev)
             kernels.spmm_axpy(W, X, a=self.diag, b=-1.0, out=Y, group=g)
-            torch.cuda.synchronize()
+            torch.cuda.current_stream().synchronize()
             t = time.perf_counter()
             for _ in range(reps):
                 kernels.spmm_axpy(W, X, a=self.diag, b=-1.0, out=Y, group=g)
-            torch.cuda.synchronize()
+            torch.cuda.current_stream().synchronize()
             dt = (time.perf_counter() - t) / reps
             if dt < best:
                 best, arg = dt, (g, tr)

@@ -83,3 +83,68 @@ def ground_reach(G, vmask, sink, umask, in_t, w=None):
         raise ValueError("ground_reach: entry column outside [0, n)")
     return int(cnt.item()), int(sweeps.value)
 
+
+
+# ---------------------------------------------------------------------------------------------
+# adaptive components of new vertices (dynlp/cc.py:26-83)
+# ---------------------------------------------------------------------------------------------
+def _lightest(nc, cu, cv, de):
+    """Per component with an outgoing edge: (component, the other side, weight) of its lightest one,
+    ties to the smallest other side (dynlp/cc.py:26-34). min-reductions: order-independent."""
+    dev = cu.device
+    best = torch.full((nc,), float("inf"), dtype=torch.float32, device=dev)
+    best.scatter_reduce_(0, cu, de, "amin")
+    nb = torch.full((nc,), nc, dtype=torch.int64, device=dev)
+    sel = de <= best[cu]
+    nb.scatter_reduce_(0, cu[sel], cv[sel], "amin")
+    c = torch.nonzero(nb < nc, as_tuple=False).flatten()
+    return c, nb[c], best[c]
+
+
+def fh_components(m, rows, cols, d, k, ground=None):
+    """Felzenszwalb-Huttenlocher merging in Boruvka rounds (dynlp/cc.py:37-73): each round every
+    component takes its lightest outgoing edge and merges across it when d(e) <= min over both
+    sides of Int(C) + k/|C| (Int = largest internal dissimilarity, fp32 as the reference keeps it);
+    with `ground`, components holding none then join their lightest neighbour until every one has
+    some. The merges of a round are one call of the component kernel (rank labels)."""
+    dev = rows.device
+    lab = torch.arange(m, dtype=torch.int64, device=dev)
+    Int = torch.zeros(m, dtype=torch.float32, device=dev)
+    size = torch.ones(m, dtype=torch.float32, device=dev)
+    rows, cols, d = rows.long(), cols.long(), d.to(torch.float32)
+    g_v = ground.to(torch.float32) if ground is not None else None
+    nc, fh = m, True
+    while rows.numel():
+        cu, cv = lab[rows], lab[cols]
+        ext = cu != cv
+        if not fh:
+            g = torch.zeros(nc, dtype=torch.float32, device=dev).index_add_(0, lab, g_v)
+            ext &= g[cu] == 0
+        if not bool(ext.any()):
+            break
+        c, t, dc = _lightest(nc, cu[ext], cv[ext], d[ext])
+        if fh:
+            ok = dc <= torch.minimum(Int[c] + k / size[c], Int[t] + k / size[t])
+            if not bool(ok.any()):
+                if g_v is None:
+                    break
+                fh = False
+                continue
+            c, t, dc = c[ok], t[ok], dc[ok]
+        root, nc = connected_components(nc, c.to(torch.int32), t.to(torch.int32))
+        root = root.long()
+        Int2 = torch.zeros(nc, dtype=torch.float32, device=dev).scatter_reduce_(0, root, Int, "amax")
+        Int2.scatter_reduce_(0, root[c], dc, "amax")
+        size2 = torch.zeros(nc, dtype=torch.float32, device=dev).index_add_(0, root, size)
+        lab, Int, size = root[lab], Int2, size2
+    return lab.to(torch.int32), nc
+
+
+def adaptive_components(m, rows, cols, w, s_r, s_c, wmax, ground=None):
+    """Component-adaptive merging of the new vertices (dynlp/cc.py:76-83): dissimilarity
+    1 - w/wmax scaled by the endpoints' own mean dissimilarities, k = its mean."""
+    if m == 0:
+        return torch.zeros(0, dtype=torch.int32, device=rows.device), 0
+    d = (1 - w / wmax) / torch.sqrt(s_r * s_c)
+    k = float(d.double().mean().item()) if d.numel() else 0.0
+    return fh_components(m, rows, cols, d, k, ground)

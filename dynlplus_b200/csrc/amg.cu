@@ -10,6 +10,9 @@
 // private open-addressing table, in a fixed member order with fp64 sums: deterministic.
 // Cycle (amg.py:119-134): damped Jacobi sweeps, restriction as ordered segment sums over the
 // aggregates, prolongation by gather, and the dense fp64 inverse at the coarsest level.
+#include <algorithm>
+#include <climits>
+
 #include "common.cuh"
 
 namespace dlp {
@@ -177,6 +180,60 @@ __global__ void k_coarse_emit(int32_t nc, const int32_t *__restrict__ toff, cons
     w_c[j + 1] = x;
     ++o;
   }
+}
+
+// ---- sort-based Galerkin coarsening ------------------------------------------------------------
+// keys: entry j of row u -> agg[u] * nc + agg[col[j]] (a sentinel when both ends share an aggregate);
+// after a stable sort by key, each key's entries sit together in their CSR order, so summing a run
+// front to back reproduces the per-row accumulation order of the reference's coalesce.
+constexpr long long kNoKey = 0x7fffffffffffffffll;
+
+__global__ void k_coarse_keys(int32_t n, const int32_t *__restrict__ indptr, const int32_t *__restrict__ col,
+                              const float *__restrict__ w, const int32_t *__restrict__ agg, int32_t nc, long long *key,
+                              double *val) {
+  // 8 lanes per row
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long u = t >> 3;
+  if (u >= n) return;
+  const long long a = agg[u];
+  for (int j = indptr[u] + (int)(t & 7); j < indptr[u + 1]; j += 8) {
+    const long long b = agg[col[j]];
+    key[j] = a == b ? kNoKey : a * nc + b;
+    val[j] = (double)w[j];
+  }
+}
+
+// flag[i] = 1 where a run of equal (kept) keys starts
+__global__ void k_run_starts(long long m, const long long *__restrict__ key, int32_t *flag) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const long long k = key[i];
+  flag[i] = (k != kNoKey && (i == 0 || key[i - 1] != k)) ? 1 : 0;
+}
+
+// one thread per run: the run's sum (front to back) becomes coarse entry pos[i]; rows counted
+__global__ void k_run_emit(long long m, const long long *__restrict__ key, const double *__restrict__ val,
+                           const int32_t *__restrict__ flag, const int32_t *__restrict__ pos, int32_t nc,
+                           int32_t *col_c, float *w_c, int32_t *rowcnt) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m || !flag[i]) return;
+  const long long k = key[i];
+  double acc = val[i];
+  for (long long j = i + 1; j < m && key[j] == k; ++j) acc += val[j];
+  const int32_t a = (int32_t)(k / nc);
+  col_c[pos[i]] = (int32_t)(k - (long long)a * nc);
+  w_c[pos[i]] = (float)acc;
+  atomicAdd(rowcnt + a, 1);
+}
+
+// s_c[a] = sum of s over the members of aggregate a, in member order
+__global__ void k_member_sum(int32_t nc, const int32_t *__restrict__ off, const int32_t *__restrict__ members,
+                             const double *__restrict__ s, double *sc) {
+  const long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= nc) return;
+  double acc = 0.0;
+  for (int i = off[a]; i < off[a + 1]; ++i) acc += s[members[i]];
+  sc[a] = acc;
 }
 
 // ---- cycle kernels ------------------------------------------------------------------------------
@@ -449,6 +506,58 @@ int dlp_dense_apply(int32_t nc, int32_t C, const double *M, const void *X, int64
   else
     return DLP_ERR_DTYPE;
   return check_launch();
+}
+
+int dlp_amg_coarse_keys(int32_t n, const int32_t *indptr, const int32_t *col, const float *w, const int32_t *agg,
+                        int32_t nc, int64_t *key, double *val, dlp_stream_t stream) {
+  if (n < 0 || nc < 0 || (n > 0 && (!indptr || !col || !w || !agg || !key || !val))) return DLP_ERR_INVALID;
+  if (n == 0) return DLP_OK;
+  k_coarse_keys<<<g1((long long)n * 8), kAT, 0, (cudaStream_t)stream>>>(n, indptr, col, w, agg, nc,
+                                                                        (long long *)key, val);
+  return check_launch();
+}
+
+size_t dlp_amg_coarse_reduce_workspace_bytes(int64_t m, int32_t nc) {
+  const size_t a = (((size_t)(m > 0 ? m : 1) * 4 + 4 + 255) / 256 * 256) * 2;  // flags, positions (m + 1)
+  const size_t b = (((size_t)(nc > 0 ? nc : 1) * 4 + 255) / 256 * 256);          // row counts
+  return a + b + compact_ws_bytes((int32_t)std::min<int64_t>(std::max<int64_t>(m, nc), INT32_MAX - 1));
+}
+
+int dlp_amg_coarse_reduce(int64_t m, const int64_t *key, const double *val, int32_t nc, const int32_t *off,
+                          const int32_t *members, const double *s_fine, double *s_coarse, int32_t *indptr_c,
+                          int32_t *col_c, float *w_c, int32_t *nnz_c, void *ws, size_t ws_bytes,
+                          dlp_stream_t stream) {
+  if (m < 0 || m >= INT32_MAX || nc < 0 || !indptr_c || !nnz_c || (m > 0 && (!key || !val || !col_c || !w_c)))
+    return DLP_ERR_INVALID;
+  if (s_coarse && (!s_fine || !off || !members)) return DLP_ERR_INVALID;
+  if (!ws || ws_bytes < dlp_amg_coarse_reduce_workspace_bytes(m, nc)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  char *p = (char *)ws;
+  const size_t fb = ((size_t)(m > 0 ? m : 1) * 4 + 4 + 255) / 256 * 256;  // m + 1 ints: the scan writes pos[m]
+  int32_t *flag = (int32_t *)p;
+  int32_t *pos = (int32_t *)(p + fb);
+  int32_t *rowcnt = (int32_t *)(p + 2 * fb);
+  void *scan_ws = p + 2 * fb + (((size_t)(nc > 0 ? nc : 1) * 4 + 255) / 256 * 256);
+  const size_t scan_bytes = ws_bytes - (size_t)((char *)scan_ws - p);
+  if (nc > 0) DLP_CUDA(cudaMemsetAsync(rowcnt, 0, sizeof(int32_t) * (size_t)nc, s));
+  int launches = 0;
+  if (m > 0) {
+    k_run_starts<<<g1(m), kAT, 0, s>>>(m, (const long long *)key, flag);
+    launches += 1;
+  }
+  // pos = exclusive scan of the run starts; pos[m] = number of coarse entries
+  DLP_TRY(exclusive_scan_i32(flag, (int32_t)m, pos, scan_ws, scan_bytes, s));
+  if (m > 0) {
+    k_run_emit<<<g1(m), kAT, 0, s>>>(m, (const long long *)key, val, flag, pos, nc, col_c, w_c, rowcnt);
+    launches += 1;
+  }
+  DLP_TRY(exclusive_scan_i32(rowcnt, nc, indptr_c, scan_ws, scan_bytes, s));
+  DLP_CUDA(cudaMemcpyAsync(nnz_c, indptr_c + nc, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+  if (s_coarse && nc > 0) {
+    k_member_sum<<<g1(nc), kAT, 0, s>>>(nc, off, members, s_fine, s_coarse);
+    launches += 1;
+  }
+  return check_launch(launches);
 }
 
 }  // extern "C"

@@ -469,12 +469,12 @@ static int b_phase(int phase, const BProblem &q, const BTiles &tl, const BCtl &c
 }
 
 static std::mutex g_b_mu;
-static std::unordered_map<std::string, cudaGraphExec_t> g_b_graphs;
+static std::unordered_map<std::string, GraphRef> g_b_graphs;
 static cudaStream_t g_b_capture[64];
 
 template <typename TS>
 static int b_chunk_graph(const BProblem &q, const BTiles &tl, const BCtl &c, const BParams &bp, int k,
-                         cudaGraphExec_t *out) {
+                         GraphRef *out) {
   int dev = 0;
   DLP_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return DLP_ERR_INVALID;
@@ -512,12 +512,11 @@ static int b_chunk_graph(const BProblem &q, const BTiles &tl, const BCtl &c, con
     set_cuda_error(e2);
     return DLP_ERR_CUDA;
   }
-  if (g_b_graphs.size() >= 16) {
-    for (auto &kv : g_b_graphs) cudaGraphExecDestroy(kv.second);
-    g_b_graphs.clear();
-  }
-  g_b_graphs.emplace(key, ex);
-  *out = ex;
+  auto ref = std::make_shared<GraphExec>();
+  ref->ex = ex;
+  if (g_b_graphs.size() >= 16) g_b_graphs.clear();  // bounded cache; holders keep their graphs alive
+  g_b_graphs.emplace(key, ref);
+  *out = ref;
   return DLP_OK;
 }
 
@@ -525,8 +524,9 @@ template <typename TS>
 static int b_solve(const BProblem &q, const BTiles &tl, const BCtl &c, const BParams &bp, int k, int use_graph,
                    cudaStream_t s) {
   DLP_TRY(b_phase<TS>(2, q, tl, c, bp, s));
-  cudaGraphExec_t ex = nullptr;
-  if (use_graph) DLP_TRY(b_chunk_graph<TS>(q, tl, c, bp, k, &ex));
+  GraphRef gref;
+  if (use_graph) DLP_TRY(b_chunk_graph<TS>(q, tl, c, bp, k, &gref));
+  cudaGraphExec_t ex = gref ? gref->ex : nullptr;
   int32_t counts[2] = {0, 0};
   for (int guard = 0; guard < (1 << 30); ++guard) {
     k_b_select<<<1, 1024, 0, s>>>(tl.ninst, 0, c);

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
+
 #include "dlp.h"
 
 namespace dlp {
@@ -31,6 +33,20 @@ void note_launches(unsigned long long k);  // kernels launched outside check_lau
       return DLP_ERR_CUDA;                     \
     }                                          \
   } while (0)
+
+// An instantiated CUDA graph shared between a cache and the solves replaying it: the cache may
+// drop its reference (eviction) while another thread's solve still replays the graph; the graph is
+// destroyed when the last holder lets go.
+struct GraphExec {
+  cudaGraphExec_t ex = nullptr;
+  GraphExec() = default;
+  GraphExec(const GraphExec &) = delete;
+  GraphExec &operator=(const GraphExec &) = delete;
+  ~GraphExec() {
+    if (ex) cudaGraphExecDestroy(ex);
+  }
+};
+using GraphRef = std::shared_ptr<GraphExec>;
 
 inline size_t dtype_size(int dt) { return dt == DLP_F64 ? 8 : dt == DLP_F32 ? 4 : dt == DLP_BF16 ? 2 : 0; }
 

@@ -325,6 +325,50 @@ static uint32_t table_size(int32_t ni) {
   return s;
 }
 
+// Labelled vertices entering (sign +1) or leaving (sign -1) the active set: every live neighbour v of
+// l gets B[v, y[l]] += sign * aw(l, v), and is flagged changed when it is solved
+// (dynlp/stream.py:230-235). One group of 8 lanes per labelled vertex.
+__global__ void __launch_bounds__(kGThreads)
+    k_label_update(const int32_t *__restrict__ L, int32_t nl, double sign, const int32_t *__restrict__ rbeg,
+                   const int32_t *__restrict__ rend, const int32_t *__restrict__ col, const float *__restrict__ aw,
+                   const int32_t *__restrict__ y, int32_t K, double *B, const uint8_t *__restrict__ umask,
+                   uint8_t *changed) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long g = t >> 3;
+  const int l8 = (int)(t & 7);
+  if (g >= nl) return;
+  const int32_t l = L[g];
+  const int32_t c = y[l];
+  for (int j = rbeg[l] + l8; j < rend[l]; j += 8) {
+    const float a = aw[j];
+    if (a == 0.0f) continue;
+    const int32_t v = col[j];
+    atomicAdd(B + (long long)v * K + c, sign * (double)a);
+    if (changed && umask[v]) changed[v] = 1;
+  }
+}
+
+// Per new vertex (DynLP step 1, dynlp/stream.py:72-76): its mean dissimilarity over its live
+// entries, s = (sum over w > 0 of (1 - w / wmax), each term rounded to fp32, summed in fp32 in
+// row order) / max(count, 1) + 1e-6. The terms are formed in the weights' precision first, as
+// the reference's vectorised expression does; one thread per row keeps the row order.
+template <typename TW>
+__global__ void k_new_dissim(const int32_t *__restrict__ rows, int32_t m, const int32_t *__restrict__ rbeg,
+                             const int32_t *__restrict__ rend, const TW *__restrict__ w, double wmax, float *s) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int32_t r = rows[i];
+  const TW wm = (TW)wmax;
+  float acc = 0.0f, cnt = 0.0f;
+  for (int j = rbeg[r]; j < rend[r]; ++j) {
+    const TW x = w[j];
+    if (!(x > (TW)0)) continue;
+    acc = __fadd_rn(acc, (float)((TW)1 - x / wm));
+    cnt = __fadd_rn(cnt, 1.0f);
+  }
+  s[i] = __fadd_rn(__fdiv_rn(acc, fmaxf(cnt, 1.0f)), 1e-6f);
+}
+
 }  // namespace dlp
 
 using namespace dlp;
@@ -435,6 +479,32 @@ int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t
   if (nr == 0) return DLP_OK;
   if (!rows || !umask || !prior || !Z) return DLP_ERR_INVALID;
   k_park<<<grid1(nr), kGThreads, 0, (cudaStream_t)stream>>>(rows, nr, umask, C, with_h, prior, h0, Z, ldz, R, ldr);
+  return check_launch();
+}
+
+int dlp_label_update(const int32_t *L, int32_t nl, double sign, const int32_t *rbeg, const int32_t *rend,
+                     const int32_t *col, const float *aw, const int32_t *y, int32_t K, double *B, const uint8_t *umask,
+                     uint8_t *changed, dlp_stream_t stream) {
+  if (nl < 0 || K <= 0) return DLP_ERR_INVALID;
+  if (nl == 0) return DLP_OK;
+  if (!L || !rbeg || !rend || !col || !aw || !y || !B || (changed && !umask)) return DLP_ERR_INVALID;
+  k_label_update<<<grid1((long long)nl * 8), kGThreads, 0, (cudaStream_t)stream>>>(L, nl, sign, rbeg, rend, col, aw,
+                                                                                   y, K, B, umask, changed);
+  return check_launch();
+}
+
+int dlp_new_dissim(const int32_t *rows, int32_t m, const int32_t *rbeg, const int32_t *rend, const void *w,
+                   int w_dtype, double wmax, float *s, dlp_stream_t stream) {
+  if (m < 0 || !(wmax > 0.0)) return DLP_ERR_INVALID;
+  if (m == 0) return DLP_OK;
+  if (!rows || !rbeg || !rend || !w || !s) return DLP_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (w_dtype == DLP_F32)
+    k_new_dissim<float><<<grid1(m), kGThreads, 0, st>>>(rows, m, rbeg, rend, (const float *)w, wmax, s);
+  else if (w_dtype == DLP_F64)
+    k_new_dissim<double><<<grid1(m), kGThreads, 0, st>>>(rows, m, rbeg, rend, (const double *)w, wmax, s);
+  else
+    return DLP_ERR_DTYPE;
   return check_launch();
 }
 

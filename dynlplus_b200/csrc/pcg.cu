@@ -604,10 +604,10 @@ struct GraphKeyHash {
 };
 
 static std::mutex g_graph_mu;
-static std::unordered_map<GraphKey, cudaGraphExec_t, GraphKeyHash> g_graphs;
+static std::unordered_map<GraphKey, GraphRef, GraphKeyHash> g_graphs;
 static cudaStream_t g_capture_stream[64];
 
-static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, cudaGraphExec_t *out) {
+static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, GraphRef *out) {
   int dev = 0;
   DLP_CUDA(cudaGetDevice(&dev));
   // the mean degree enters the kernels only through the gather layout it selects: key on that, so
@@ -653,12 +653,11 @@ static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, cudaGra
     set_cuda_error(e);
     return DLP_ERR_CUDA;
   }
-  if (g_graphs.size() >= 32) {  // bounded cache
-    for (auto &kv : g_graphs) cudaGraphExecDestroy(kv.second);
-    g_graphs.clear();
-  }
-  g_graphs.emplace(key, ex);
-  *out = ex;
+  auto ref = std::make_shared<GraphExec>();
+  ref->ex = ex;
+  if (g_graphs.size() >= 32) g_graphs.clear();  // bounded cache; holders keep their graphs alive
+  g_graphs.emplace(key, ref);
+  *out = ref;
   return DLP_OK;
 }
 
@@ -726,8 +725,9 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   DLP_TRY(update_phase(2, q, B, s));
   DLP_TRY(dir_phase(2, q, B, s));
   const int k = check_every > 0 ? check_every : 8;
-  cudaGraphExec_t ex = nullptr;
-  if (use_graph) DLP_TRY(get_chunk_graph(q, B, k, &ex));
+  GraphRef gref;
+  if (use_graph) DLP_TRY(get_chunk_graph(q, B, k, &gref));
+  cudaGraphExec_t ex = gref ? gref->ex : nullptr;
   PcgCtl cur{};
   DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
   DLP_CUDA(cudaStreamSynchronize(s));

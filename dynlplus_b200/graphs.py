@@ -45,7 +45,7 @@ def _t(x, dev, dtype=None):
 
 
 def coalesce(rows, cols, vals, n, dtype, device=None) -> CSR:
-    """Canonical CSR: duplicates summed, self-loops dropped (dynlp/graphs.py:92-100)."""
+    """Canonical CSR: duplicates summed, self-loops dropped (dynlp/graphs.py:36-44)."""
     dev = _dev(device) if not torch.is_tensor(rows) else rows.device
     r, c = _t(rows, dev, torch.int64), _t(cols, dev, torch.int64)
     v = _t(vals, dev, torch.float64).to(to_dtype(dtype))  # duplicates summed in the target precision
@@ -61,7 +61,7 @@ def coalesce(rows, cols, vals, n, dtype, device=None) -> CSR:
 
 
 def symmetric_from_pairs(u, v, w, n, dtype, device=None) -> CSR:
-    """dynlp/graphs.py:103-104."""
+    """dynlp/graphs.py:47-48."""
     dev = _dev(device) if not torch.is_tensor(u) else u.device
     u, v, w = _t(u, dev, torch.int64), _t(v, dev, torch.int64), _t(w, dev, torch.float64)
     return coalesce(torch.cat([u, v]), torch.cat([v, u]), torch.cat([w, w]), n, dtype, dev)
@@ -85,17 +85,17 @@ def symmetric_set(u, v, w, n, dtype, device=None) -> CSR:
 
 
 def expand_counts(counts, nseg):
-    """Segment id of each element given per-segment counts (dynlp/graphs.py:107-115)."""
+    """Segment id of each element given per-segment counts (dynlp/graphs.py:51-57)."""
     return torch.repeat_interleave(torch.arange(nseg, dtype=torch.int32, device=counts.device), counts.long())
 
 
 def csr_rows(A) -> torch.Tensor:
-    """Row index of every stored entry of a CSR matrix (dynlp/graphs.py:118-120)."""
+    """Row index of every stored entry of a CSR matrix (dynlp/graphs.py:62-64)."""
     return expand_counts(torch.diff(A.indptr), A.shape[0])
 
 
 def row_positions(indptr, rows):
-    """Positions of all stored entries in the given rows, and each one's segment (graphs.py:123-131)."""
+    """Positions of all stored entries in the given rows, and each one's segment (graphs.py:67-75)."""
     rows = rows.long()
     counts = (indptr[rows + 1] - indptr[rows]).long()
     seg = expand_counts(counts, int(rows.numel()))
@@ -114,7 +114,7 @@ def _rng(seed):
 
 
 def sbm(n, K=2, deg=10.0, p_in=0.85, seed=0, dtype="float32", device=None) -> Dataset:
-    """Planted partition (dynlp/graphs.py:156-168)."""
+    """Planted partition (dynlp/graphs.py:100-112)."""
     rs, perm = _rng(seed)
     y = rs.randint(0, K, size=n).astype(np.int32)
     members, sizes = np.argsort(y).astype(np.int64), np.bincount(y, minlength=K).astype(np.int64)
@@ -131,7 +131,7 @@ def sbm(n, K=2, deg=10.0, p_in=0.85, seed=0, dtype="float32", device=None) -> Da
 
 
 def erdos_renyi(n, K=2, deg=5.0, seed=0, dtype="float32", device=None) -> Dataset:
-    """dynlp/graphs.py:171-177."""
+    """dynlp/graphs.py:115-121."""
     rs, perm = _rng(seed)
     m = int(n * deg / 2)
     u, v = rs.randint(0, n, size=m).astype(np.int64), rs.randint(0, n, size=m).astype(np.int64)
@@ -239,7 +239,7 @@ class EdgeUpdates:
 
 
 def load(spec: str, *, n=100_000, K=2, deg=10.0, p_in=0.85, seed=0, dtype="float32", device=None) -> Dataset:
-    """dynlp/graphs.py:263-270 for the synthetic families (the IMDB/synth kNN sets are out of scope)."""
+    """dynlp/graphs.py:207-214 for the synthetic families (the IMDB/synth kNN sets are out of scope)."""
     if spec == "sbm":
         return sbm(n, K, deg, p_in, seed, dtype, device)
     if spec == "er":

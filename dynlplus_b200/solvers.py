@@ -308,6 +308,58 @@ def push(sys: System, Z, R, eps, ops: FrontierOps, st: Stats, budget_edges=None,
     return Z, R, cand.numel() == 0
 
 
+def _comp_avg(lab, nc, S_rows, T_rows, fallback):
+    """Per component of the new vertices: sum of S over sum of T (T = 0: fallback)
+    (dynlp/solvers.py:128-135)."""
+    lab = lab.long()
+    S = torch.zeros((nc,) + tuple(S_rows.shape[1:]), dtype=S_rows.dtype, device=S_rows.device).index_add_(0, lab, S_rows)
+    T = torch.zeros(nc, dtype=S_rows.dtype, device=S_rows.device).index_add_(0, lab, T_rows.to(S_rows.dtype))
+    ok = T > 0
+    Tn = torch.where(ok, T, torch.ones_like(T))
+    fb = torch.as_tensor(fallback, dtype=S_rows.dtype, device=S_rows.device)
+    if S.dim() == 2:
+        return torch.where(ok[:, None], S / Tn[:, None], fb)
+    return torch.where(ok, S / Tn, fb)
+
+
+def _rows_spmm(sys: System, rows, Y):
+    """W[rows] @ Y (rows of the system's operator, compact output)."""
+    return kernels.spmm_axpy(sys.W, Y.contiguous(), rows=rows.to(torch.int32).contiguous(), compact=True)
+
+
+def supernode_init(sys: System, X, known=None, cols=None, comp="tau"):
+    """Initialise the new rows per component of the new vertices (DynLP's supernodes,
+    dynlp/solvers.py:138-153): with known=None the share of the component's weight to each
+    labelled class (DynLP's rule); with a known mask the weighted average over labelled and known
+    neighbours. Writes X[new, cols] in place and returns X."""
+    new = torch.nonzero(sys.is_new, as_tuple=False).flatten()
+    if not new.numel() or comp not in sys.comps:
+        return X
+    cols = slice(0, sys.C) if cols is None else cols
+    B = sys.B.to(X.dtype)
+    s_, t = sys.label_cols(B)[new], B[new].sum(dim=1)
+    if known is not None:
+        kf = known.to(X.dtype)
+        s_ = s_ + _rows_spmm(sys, new, X[:, cols] * kf[:, None])
+        t = t + _rows_spmm(sys, new, kf[:, None])[:, 0]
+    lab, nc = sys.comps[comp]
+    X[new, cols] = _comp_avg(lab, nc, s_, t, sys.prior.to(X.dtype)[None, :])[lab.long()]
+    return X
+
+
+def init_h(sys: System, H, known, fallback, comp="fh"):
+    """New rows: h = 1 + the component's weighted average h over known neighbours, labelled ones
+    counting with h = 0 (dynlp/solvers.py:156-163). Writes H[new, 0] in place and returns H."""
+    new = torch.nonzero(sys.is_new, as_tuple=False).flatten()
+    if new.numel() and comp in sys.comps:
+        kf = known.to(H.dtype)
+        lab, nc = sys.comps[comp]
+        a = _rows_spmm(sys, new, (H[:, 0] * kf)[:, None])[:, 0]
+        b = sys.B.to(H.dtype)[new].sum(dim=1) + _rows_spmm(sys, new, kf[:, None])[:, 0]
+        H[new, 0] = (_comp_avg(lab, nc, a, b, fallback - 1) + 1)[lab.long()]
+    return H
+
+
 def predict(F, K):
     """dynlp/solvers.py:166-167."""
     return (F[:, 0] > 0.5).to(torch.int32) if K == 2 else F.argmax(dim=1).to(torch.int32)
@@ -336,9 +388,9 @@ class Solver:
 
 class DynLP(Solver):
     """DynLP's frontier Jacobi (Algorithm 2, dynlp/solvers.py:213-241) on the frontier kernels: the
-    frontier starts at the seed rows; each round updates the rows that changed by more than delta
-    and the next frontier is their neighbourhood. (The paper's tau-component initialisation of new
-    vertices is not run: new rows start at the prior.)"""
+    new rows start at their component's label share (supernode_init, the paper's tau components or
+    the adaptive ones with comp="fh"), the frontier starts at the seed rows; each round updates
+    the rows that changed by more than delta and the next frontier is their neighbourhood."""
 
     def __init__(self, n_total, K, dtype="float32", delta=1e-4, group="auto", comp="tau", max_iter=10**7):
         super().__init__(n_total, K, dtype)
@@ -348,7 +400,7 @@ class DynLP(Solver):
     def solve(self, sys, record=None):
         st, sys = Stats(path="frontier-jacobi"), sys.astype(self.dtype)
         with Timer() as tm:
-            X = self._warm(sys).contiguous()
+            X = supernode_init(sys, self._warm(sys).contiguous(), comp=self.comp)
             ops = FrontierOps(sys.W, self.C, self.group)
             n = X.shape[0]
             frontier = kernels.flatnonzero(sys.seed.to(torch.uint8))
@@ -516,8 +568,9 @@ class DynLPPlus(Solver):
             n = sys.n_u
             if self.H is None:
                 self.H = torch.zeros((self.n_total, 1), dtype=self.store_dtype, device=dev)
-            X = self._warm(sw)
-            Hc = self.H[sw.U].to(self.dtype)
+            known = ~sw.is_new
+            X = supernode_init(sw, self._warm(sw), known, comp="fh")
+            Hc = init_h(sw, self.H[sw.U].to(self.dtype), known, self.hmax or 1.0)
             Z = padded_empty(n, C + 1, self.dtype, dev)
             Z[:, :C] = X
             Z[:, C:] = Hc
@@ -613,6 +666,10 @@ class IncrementalLP(DynLPPlus):
                 self.since_full = 0
             else:
                 self._park(s64, sys.moved)
+                if s64.comps:  # vertex arrivals: new rows start at their component's average
+                    known = s64.solved & ~s64.is_new
+                    supernode_init(s64, self.Z[:, :C], known, comp="fh")
+                    init_h(s64, self.Z[:, C:], known, self.hmax or 1.0)
                 Q = sys.changed
                 if Q is not None and Q.numel():
                     residual(s64, self.Z, rhs64, out=self.R, rows=Q)

@@ -83,13 +83,50 @@ def _onehot_labels(y, lab_mask, K, dev):
     return X
 
 
-def build_system(ds: Dataset, active, labeled, *, eta=0.0, dtype="float32", t=0, prev_U=None, ins=0, dele=0):
+def _range_positions(beg, end):
+    """Slot positions of the ranges [beg[i], end[i]) and each one's range index, in range order."""
+    counts = (end.long() - beg.long()).clamp(min=0)
+    seg = torch.repeat_interleave(torch.arange(beg.numel(), device=beg.device), counts)
+    if not seg.numel():
+        return torch.zeros(0, dtype=torch.int64, device=beg.device), seg
+    excl = torch.cumsum(counts, 0) - counts
+    return beg.long()[seg] + (torch.arange(seg.numel(), device=beg.device) - excl[seg]), seg
+
+
+def new_components(rows, rbeg, rend, col, w, nl, tau, wmax, ground):
+    """DynLP step 1 for the m = len(rows) new vertices (dynlp/stream.py:67-81), on the device:
+    each one's mean dissimilarity s over its live entries (`dlp_new_dissim`, row order), then the
+    components over edges heavier than tau between new vertices ("tau", the paper's) and the
+    adaptive FH components on 1 - w/wmax scaled by sqrt(s_u s_v) ("fh"). `nl` maps a column id to
+    its new-vertex index (-1: not new); `ground` is each new vertex's label weight."""
+    m = int(rows.numel())
+    dev = rows.device
+    if m == 0:
+        z = torch.zeros(0, dtype=torch.int32, device=dev)
+        return {"tau": (z, 0), "fh": (z, 0)}
+    rows = rows.to(torch.int32).contiguous()
+    s = torch.empty(m, dtype=torch.float32, device=dev)
+    _lib.call("dlp_new_dissim", ptr(rows), m, ptr(rbeg), ptr(rend), ptr(w), code(w), float(wmax), ptr(s), stream())
+    pos, seg = _range_positions(rbeg[rows.long()], rend[rows.long()])
+    wv = w[pos]
+    c = nl[col[pos].long()]
+    e = (wv > 0) & (c >= 0)
+    r, c, we = seg[e], c[e].long(), wv[e]
+    heavy = we > tau
+    tau_c = cc.connected_components(m, r[heavy].to(torch.int32), c[heavy].to(torch.int32))
+    fh_c = cc.adaptive_components(m, r, c, we, s[r], s[c], wmax, ground.to(torch.float32))
+    return {"tau": tau_c, "fh": fh_c}
+
+
+def build_system(ds: Dataset, active, labeled, *, eta=0.0, dtype="float32", t=0, prev_U=None, ins=0, dele=0,
+                 ins_ids=None, del_ids=None, tau=None, wmax=None):
     """The grounded system of one batch (Stream._build, dynlp/stream.py:142-177), on the device.
 
     U = active unlabelled vertices whose component (within the active unlabelled subgraph) holds
     label weight; W = A[U, U] in CSR order; B = A @ onehot(y_L); s = sum(B) + eta; diag = s +
-    rowsum(W); rhs = B (class 1 when K == 2) + eta * prior. The new-vertex components and DynLP's
-    seed set are not built (they serve the vertex-arrival warm start)."""
+    rowsum(W); rhs = B (class 1 when K == 2) + eta * prior. With the batch's inserted / deleted
+    vertex ids, DynLP's seed is the new rows plus the neighbours of those vertices; with tau and
+    wmax the new vertices' components (tau and FH) are built too (dynlp/stream.py:170-175)."""
     A, K = ds.A, ds.K
     dev = A.indices.device
     n = A.shape[0]
@@ -122,8 +159,25 @@ def build_system(ds: Dataset, active, labeled, *, eta=0.0, dtype="float32", t=0,
     prior = torch.full((1 if K == 2 else K,), 0.5 if K == 2 else 1.0 / K, dtype=torch.float64, device=dev)
     rhs = (Bm[:, 1:2] if K == 2 else Bm) + eta * prior[None, :]
     is_new = torch.ones(n_u, dtype=torch.bool, device=dev) if prev_U is None else ~prev_U[U]
+    seed = is_new.clone()
+    if ins_ids is not None or del_ids is not None:
+        touch = torch.zeros((n, 1), dtype=torch.float64, device=dev)
+        for ids in (ins_ids, del_ids):
+            if ids is not None and ids.numel():
+                touch[ids.long(), 0] = 1.0
+        seed |= kernels.spmm_axpy(A, touch)[U, 0] > 0
+        ins, dele = (int(ins_ids.numel()) if ins_ids is not None else ins), \
+            (int(del_ids.numel()) if del_ids is not None else dele)
+    comps = {}
+    if tau is not None:
+        new = torch.nonzero(is_new, as_tuple=False).flatten()
+        nl = torch.full((n_u,), -1, dtype=torch.int64, device=dev)
+        nl[new] = torch.arange(new.numel(), device=dev)
+        Wd = W.data.to(dt)
+        comps = new_components(new, W.indptr[:-1], W.indptr[1:], W.indices, Wd, nl, tau, wmax,
+                               Bm[new].to(dt).sum(dim=1))
     sysd = dict(t=t, U=U, W=W, s=s.to(dt), diag=diag.to(dt), B=Bm.to(dt), rhs=rhs.to(dt).contiguous(),
-                prior=prior.to(dt), is_new=is_new, seed=is_new.clone(), comps={}, K=K, C=1 if K == 2 else K, eta=eta,
+                prior=prior.to(dt), is_new=is_new, seed=seed, comps=comps, K=K, C=1 if K == 2 else K, eta=eta,
                 n_inserted=ins, n_deleted=dele, n_active=int(active.sum().item()), n_ungrounded=n_ungrounded)
     sysd["rhs_h"] = torch.cat([sysd["rhs"], sysd["diag"][:, None]], dim=1).contiguous()
     S = System(**sysd)
@@ -244,6 +298,7 @@ class EdgeStream:
         self.G = ResidentGraph(A, slack_frac=slack_frac, slack_min=slack_min)
         labeled = labeled.to(torch.bool)
         active = torch.ones(n, dtype=torch.bool, device=dev) if active is None else active.to(torch.bool)
+        self.active, self.labeled_all = active.clone(), labeled.clone()
         self.labeled = (labeled & active).to(torch.uint8)
         self.vmask = (active & ~labeled).to(torch.uint8)
         self.y = ds.y.to(torch.int32).contiguous()
@@ -314,6 +369,7 @@ class EdgeStream:
     def apply_edges(self, ins_u=None, ins_v=None, ins_w=None, del_u=None, del_v=None) -> System:
         """Apply one edge batch (deletions, then insertions) and return the updated system."""
         G, n = self.G, self.n
+        self._vertex_batch = None
         for name, x in (("ins_u", ins_u), ("ins_v", ins_v), ("del_u", del_u), ("del_v", del_v)):
             if x is not None and not torch.is_tensor(x) and len(x) and (np.min(x) < 0 or np.max(x) >= n):
                 raise ValueError(f"edge batch rejected: {name} has vertex ids outside [0, {n})")
@@ -362,6 +418,63 @@ class EdgeStream:
         self.counters["applied"] += int(st[2].item()) + int(st[3].item())
         return self.system
 
+    def apply_vertices(self, ins, dele, tau=None, wmax=None) -> System:
+        """One vertex-arrival batch (IncrementalStream.batches, dynlp/stream.py:300-346): the
+        vertices `dele` leave the active set, then `ins` join it (labelled ones move their label
+        weight onto their neighbours' B rows, dynlp/stream.py:230-235); the grounded set is
+        re-checked, membership changes toggle the solver weights (:206-228) and every changed
+        row's equation is rebuilt. The system carries the new rows (in U now, not at the previous
+        batch), DynLP's seed (new rows and the neighbours of the batch's vertices, within U) and,
+        with tau / wmax, the new vertices' components over the masked weights (:336-339)."""
+        G, n, dev, s = self.G, self.n, self.dev, stream()
+        ins = ins.to(device=dev, dtype=torch.int64)
+        dele = dele.to(device=dev, dtype=torch.int64)
+        prev_u = self.umask.bool().clone()
+        self._vertex_batch = None
+        self.changed.zero_()
+        lab_all = self.labeled_all
+        for ids, on in ((dele, False), (ins, True)):
+            if not ids.numel():
+                continue
+            self.active[ids] = on
+            L = ids[lab_all[ids]].to(torch.int32).contiguous()
+            V = ids[~lab_all[ids]]
+            self.vmask[V] = 1 if on else 0
+            if L.numel():
+                self.labeled[L.long()] = 1 if on else 0
+                _lib.call("dlp_label_update", ptr(L), int(L.numel()), 1.0 if on else -1.0, ptr(G.rbeg), ptr(G.rend),
+                          ptr(G.indices), ptr(G.aw), ptr(self.y), self.K, ptr(self.B), ptr(self.umask),
+                          ptr(self.changed), s)
+        nmoved = self._ground()
+        moved = torch.zeros(0, dtype=torch.int32, device=dev)
+        if nmoved:
+            moved = kernels.flatnonzero(self.in_t)
+            _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(moved),
+                      int(moved.numel()), ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), s)
+            self.counters["ground_changes"] += nmoved
+        Q = kernels.flatnonzero(self.changed)
+        self._system_rows(Q, int(Q.numel()))
+        self.t += 1
+        self.last_changed, self.last_moved = Q, moved
+        self.n_ins, self.n_del = int(ins.numel()), int(dele.numel())
+        um = self.umask.bool()
+        is_new = um & ~prev_u
+        mark = torch.zeros(n, dtype=torch.uint8, device=dev)
+        touched = torch.cat([ins, dele]).to(torch.int32).contiguous()
+        if touched.numel():
+            _lib.call("dlp_mark_neighbors", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(touched),
+                      int(touched.numel()), ptr(mark), s)
+        seed = (mark.bool() | is_new) & um
+        comps = {}
+        if tau is not None:
+            new = torch.nonzero(is_new, as_tuple=False).flatten()
+            nl = torch.full((n,), -1, dtype=torch.int64, device=dev)
+            nl[new] = torch.arange(new.numel(), device=dev)
+            wd = G.data if self.dtype == torch.float32 else G.data.to(self.dtype)
+            comps = new_components(new, G.rbeg, G.rend, G.indices, wd, nl, tau, wmax, self.B[new].sum(dim=1))
+        self._vertex_batch = {"is_new": is_new, "seed": seed, "comps": comps}
+        return self.system
+
     def solver_csr(self) -> CSR:
         """Compact CSR of W_UU (live solver entries only) for the current batch (cached)."""
         if getattr(self, "_csr_t", None) == (self.t, id(self.G.indices)):
@@ -387,8 +500,11 @@ class EdgeStream:
         n, C, dev = self.n, self.C, self.dev
         um = self.umask.bool()
         s64 = self.diag64 - self.rowsum
-        common = dict(t=self.t, U=torch.arange(n, device=dev), W=self.solver_csr(), is_new=torch.zeros(n, dtype=torch.bool,
-                      device=dev), seed=self.changed.bool(), comps={}, K=self.K, C=C, eta=self.eta,
+        vx = getattr(self, "_vertex_batch", None)
+        common = dict(t=self.t, U=torch.arange(n, device=dev), W=self.solver_csr(),
+                      is_new=vx["is_new"] if vx else torch.zeros(n, dtype=torch.bool, device=dev),
+                      seed=vx["seed"] if vx else self.changed.bool(), comps=vx["comps"] if vx else {}, K=self.K, C=C,
+                      eta=self.eta,
                       n_inserted=self.n_ins, n_deleted=self.n_del, n_active=int(self.vmask.sum().item() +
                                                                                self.labeled.sum().item()),
                       n_ungrounded=int((self.vmask.bool() & ~um).sum().item()), solved=um,
@@ -401,3 +517,109 @@ class EdgeStream:
         S._conv[torch.float64] = System(s=s64, diag=self.diag64, B=self.B, rhs=self.rhs64[:, :C], prior=self.prior64,
                                         rhs_h=self.rhs64[:, :ch], **common)
         return S
+
+
+# ---------------------------------------------------------------------------------------------
+# the vertex-arrival stream (dynlp/stream.py:84-177) and its resident form (:180-346)
+# ---------------------------------------------------------------------------------------------
+class Stream:
+    """Reveals a dataset in batches (dynlp/stream.py:84-128): an initial snapshot, then batches of
+    new vertices, with a label_frac share of all vertices carrying ground truth, and deletions of
+    del_frac x batch-size random active unlabelled vertices. The whole schedule is drawn up front
+    on the host with a NumPy RandomState(seed + 7), the same draws in the same order as the
+    reference, so a run reproduces the reference's schedule on NumPy exactly. `batches()` yields
+    the grounded system of every batch (Stream._build) built on the device."""
+
+    def __init__(self, ds: Dataset, *, label_frac=0.01, init_frac=0.1, n_batches=10, del_frac=0.1, eta_rel=0.0,
+                 seed=0, dtype="float32"):
+        self.ds, self.dtype, self.del_frac = ds, dtype, del_frac
+        n, K = ds.n, ds.K
+        dev = ds.A.indices.device
+        y = ds.y.cpu().numpy()
+        rs = np.random.RandomState(seed + 7)
+        cand = np.flatnonzero(y >= 0)
+        lab = np.zeros(n, dtype=bool)
+        lab[cand[rs.permutation(cand.shape[0])[: max(K, int(label_frac * n))]]] = True
+        order = ds.order.cpu().numpy().astype(np.int64).copy()
+        n0 = max(int(init_frac * n), 2 * K)
+        pos = np.empty(n, dtype=np.int64)
+        pos[order] = np.arange(n)
+        for c in range(K):  # the initial snapshot needs a labelled vertex of every class
+            lc = np.flatnonzero(lab & (y == c))
+            if not lc.shape[0]:
+                lc = np.flatnonzero(y == c)[:1]
+                lab[lc] = True
+            if lc.shape[0] and int(pos[lc].min()) >= n0:
+                free = np.flatnonzero(~lab[order[:n0]])
+                v, j = int(lc[0]), int(free[int(rs.randint(0, free.shape[0]))])
+                a, pv = int(order[j]), int(pos[v])
+                order[j], order[pv], pos[v], pos[a] = v, a, j, pv
+        self.n0 = n0
+        self.labeled = torch.as_tensor(lab, device=dev)
+        self.order = torch.as_tensor(order, device=dev)
+        chunks = np.array_split(order[n0:], n_batches) if n_batches > 0 else []
+        data = ds.A.data.cpu().numpy()
+        # the component threshold and scale, as the reference takes them (NumPy reductions)
+        self.tau, self.wmax = float(data.mean()), float(data.max())
+        self.eta = float(eta_rel * data.sum() / n)
+        self.prior = torch.full((1 if K == 2 else K,), 0.5 if K == 2 else 1.0 / K, dtype=to_dtype(dtype), device=dev)
+        active = np.zeros(n, dtype=bool)
+        sched = []
+        for t in range(1 + len(chunks)):
+            ins, dele = (order[:n0] if t == 0 else chunks[t - 1]), np.zeros(0, dtype=np.int64)
+            if t:
+                pool = np.flatnonzero(active & ~lab)
+                nd = min(int(del_frac * ins.shape[0]), max(pool.shape[0] - 1, 0))
+                if nd > 0:
+                    dele = pool[rs.permutation(pool.shape[0])[:nd]]
+            active[ins], active[dele] = True, False
+            sched.append((torch.as_tensor(ins.astype(np.int64), device=dev),
+                          torch.as_tensor(dele.astype(np.int64), device=dev)))
+        self.schedule = sched
+
+    def __len__(self):
+        return len(self.schedule)
+
+    def batches(self):
+        n, dev = self.ds.n, self.ds.A.indices.device
+        active = torch.zeros(n, dtype=torch.bool, device=dev)
+        prev_u = torch.zeros(n, dtype=torch.bool, device=dev)
+        for t, (ins, dele) in enumerate(self.schedule):
+            active[ins] = True
+            active[dele] = False
+            S = self._build(t, active, prev_u, ins, dele)
+            prev_u = torch.zeros(n, dtype=torch.bool, device=dev)
+            prev_u[S.U] = True
+            yield S
+
+    def _build(self, t, active, prev_u, ins, dele) -> System:
+        return build_system(self.ds, active, self.labeled, eta=self.eta, dtype=self.dtype, t=t, prev_U=prev_u,
+                            ins_ids=ins, del_ids=dele, tau=self.tau, wmax=self.wmax)
+
+
+class IncrementalStream(Stream):
+    """The same stream with the batch system resident and updated in place (dynlp/stream.py:180-346):
+    global vertex ids, inert rows outside U, solver weights masked in place, label weights moved
+    by the batch's labelled vertices, and the grounded set re-checked on the device (by
+    reachability from the labelled vertices, which gives the reference's ball-check-or-CC result).
+    Systems are live until the next batch. `ball_hops` is accepted for the reference's signature;
+    the reachability check needs no ball."""
+
+    def __init__(self, ds: Dataset, *, ball_hops=3, slack_frac=0.25, **kw):
+        super().__init__(ds, **kw)
+        self.ball_hops = ball_hops
+        self.slack_frac = slack_frac
+        self.counters = {"ground_sweeps": 0, "ground_fallbacks": 0}
+        self.resident = None
+
+    def batches(self):
+        n, dev = self.ds.n, self.ds.A.indices.device
+        es = EdgeStream(self.ds, self.labeled, eta_rel=0.0, dtype=self.dtype, slack_frac=self.slack_frac,
+                        active=torch.zeros(n, dtype=torch.bool, device=dev))
+        es.eta = self.eta
+        self.resident = es
+        for ins, dele in self.schedule:
+            S = es.apply_vertices(ins, dele, tau=self.tau, wmax=self.wmax)
+            self.counters.update(ground_sweeps=es.counters["ground_sweeps"],
+                                 ground_fallbacks=es.counters["ground_fallbacks"])
+            yield S

@@ -297,6 +297,19 @@ int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t
 int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
                    void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream);
 
+/* Labelled vertices L entering (sign = +1) or leaving (sign = -1) the active set
+ * (IncrementalStream._label_update, dynlp/stream.py:230-235): B[v, y[l]] += sign * aw(l, v) for every
+ * live entry (l, v); changed[v] = 1 where umask[v] (changed may be NULL). */
+int dlp_label_update(const int32_t *L, int32_t nl, double sign, const int32_t *rbeg, const int32_t *rend,
+                     const int32_t *col, const float *aw, const int32_t *y, int32_t K, double *B, const uint8_t *umask,
+                     uint8_t *changed, dlp_stream_t stream);
+
+/* DynLP step 1's per-vertex scale for the m new vertices rows[0..m) (new_components,
+ * dynlp/stream.py:72-76): s[i] = fp32 row-order sum over live entries (w > 0) of fp32(1 - w/wmax),
+ * divided by max(count, 1), plus 1e-6. w: f32 or f64 (the term is formed in that precision). */
+int dlp_new_dissim(const int32_t *rows, int32_t m, const int32_t *rbeg, const int32_t *rend, const void *w,
+                   int w_dtype, double wmax, float *s, dlp_stream_t stream);
+
 /* After dlp_cc_graph with the labelled vertices as sink: umask[v] = vmask[v] && parent[v] ==
  * parent[n] (the grounded vertices, dynlp/stream.py:150-159, :275-280); in_t[v] = 1 where membership
  * changed; *count (device int, caller-zeroed) += number of changes. */
@@ -344,7 +357,23 @@ int dlp_amg_coarsen(int32_t nc, const int32_t *off, const int32_t *members, cons
                     const float *w, const int32_t *agg, const int32_t *toff, int32_t *tkey, double *tval,
                     int64_t total_slots, const double *s_fine, double *s_coarse, int32_t *indptr_c, int32_t *col_c,
                     float *w_c, void *ws, size_t ws_bytes, dlp_stream_t stream);
-/* V-cycle pieces (amg.py:460-480 region, Level.apply / _smooth / _cycle):
+/* Sort-based Galerkin coarsening (the coalesce of dynlp/amg.py:67-74), in two calls around a stable
+ * sort by key the caller runs: dlp_amg_coarse_keys writes, for each of the fine operator's stored
+ * entries j (rows u < n), key[j] = agg[u] * nc + agg[col[j]] and val[j] = w[j], or key[j] = INT64_MAX
+ * when both ends share an aggregate; after the stable sort (keys with their values),
+ * dlp_amg_coarse_reduce sums each run of equal keys front to back in fp64 (the fine CSR order) into
+ * the sorted coarse CSR (indptr_c[nc+1], col_c, w_c in fp32, *nnz_c device int), and with s_coarse,
+ * s_c[a] = the fine grounding summed over the members of a in member order. m < 2^31 entries.
+ * Workspace: dlp_amg_coarse_reduce_workspace_bytes(m, nc). */
+int dlp_amg_coarse_keys(int32_t n, const int32_t *indptr, const int32_t *col, const float *w, const int32_t *agg,
+                        int32_t nc, int64_t *key, double *val, dlp_stream_t stream);
+size_t dlp_amg_coarse_reduce_workspace_bytes(int64_t m, int32_t nc);
+int dlp_amg_coarse_reduce(int64_t m, const int64_t *key, const double *val, int32_t nc, const int32_t *off,
+                          const int32_t *members, const double *s_fine, double *s_coarse, int32_t *indptr_c,
+                          int32_t *col_c, float *w_c, int32_t *nnz_c, void *ws, size_t ws_bytes,
+                          dlp_stream_t stream);
+
+/* V-cycle pieces (amg.py:28-31 Level.apply, :114-131 _smooth / _cycle):
  * restrict Rc[a,:] = sum over members of R (ordered); prolong X[u,:] += Xc[agg[u],:];
  * scale_rows X = omega R / diag; jacobi_sweep Y = X + omega ((RHS + W X) / diag - X);
  * dense_apply Y = M X with M a row-major fp64 nc x nc matrix (the coarsest-level inverse). */

@@ -14,7 +14,7 @@ import scipy.sparse.csgraph as csg
 # graphs (dynlp/graphs.py)
 # ---------------------------------------------------------------------------------------------
 def coalesce(rows, cols, vals, n, dtype):
-    """Canonical CSR: duplicates summed, self-loops dropped (dynlp/graphs.py:92-100)."""
+    """Canonical CSR: duplicates summed, self-loops dropped (dynlp/graphs.py:36-44)."""
     keep = rows != cols
     coo = ssp.coo_matrix((np.asarray(vals)[keep].astype(dtype),
                           (np.asarray(rows)[keep].astype(np.int32), np.asarray(cols)[keep].astype(np.int32))),
@@ -26,12 +26,12 @@ def coalesce(rows, cols, vals, n, dtype):
 
 
 def symmetric_from_pairs(u, v, w, n, dtype):
-    """dynlp/graphs.py:103-104."""
+    """dynlp/graphs.py:47-48."""
     return coalesce(np.concatenate([u, v]), np.concatenate([v, u]), np.concatenate([w, w]), n, dtype)
 
 
 def csr_rows(A):
-    """Row index of every stored entry (dynlp/graphs.py:118-120)."""
+    """Row index of every stored entry (dynlp/graphs.py:62-64)."""
     return np.repeat(np.arange(A.shape[0], dtype=np.int32), np.diff(A.indptr))
 
 
@@ -417,3 +417,191 @@ class AMGOracle:
 
     def __call__(self, R):
         return self._cycle(0, R)
+
+
+# ---------------------------------------------------------------------------------------------
+# vertex-arrival streams and new-vertex warm starts (dynlp/stream.py:61-177, dynlp/cc.py:26-83,
+# dynlp/solvers.py:128-163)
+# ---------------------------------------------------------------------------------------------
+def stream_schedule(y, K, order, label_frac=0.01, init_frac=0.1, n_batches=10, del_frac=0.1, seed=0):
+    """The reference Stream's up-front draws (dynlp/stream.py:89-128) on a NumPy RandomState:
+    the labelled set, the arrival order (one labelled vertex of every class moved into the initial
+    snapshot), the initial size n0 and the (inserted, deleted) vertex lists of every batch."""
+    y = np.asarray(y)
+    n = y.shape[0]
+    rs = np.random.RandomState(seed + 7)
+    cand = np.flatnonzero(y >= 0)
+    labeled = np.zeros(n, dtype=bool)
+    labeled[cand[rs.permutation(cand.shape[0])[: max(K, int(label_frac * n))]]] = True
+    order = np.array(order, dtype=np.int64, copy=True)
+    n0 = max(int(init_frac * n), 2 * K)
+    pos = np.empty(n, dtype=np.int64)
+    pos[order] = np.arange(n)
+    for c in range(K):
+        lc = np.flatnonzero(labeled & (y == c))
+        if lc.shape[0] == 0:
+            lc = np.flatnonzero(y == c)[:1]
+            labeled[lc] = True
+        if lc.shape[0] and int(pos[lc].min()) >= n0:
+            free = np.flatnonzero(~labeled[order[:n0]])
+            v, j = int(lc[0]), int(free[int(rs.randint(0, free.shape[0]))])
+            a, pv = int(order[j]), int(pos[v])
+            order[j], order[pv], pos[v], pos[a] = v, a, j, pv
+    chunks = np.array_split(order[n0:], n_batches) if n_batches > 0 else []
+    active = np.zeros(n, dtype=bool)
+    sched = []
+    for t in range(1 + len(chunks)):
+        ins = order[:n0] if t == 0 else chunks[t - 1]
+        dele = np.zeros(0, dtype=np.int64)
+        if t:
+            pool = np.flatnonzero(active & ~labeled)
+            nd = min(int(del_frac * ins.shape[0]), max(pool.shape[0] - 1, 0))
+            if nd > 0:
+                dele = pool[rs.permutation(pool.shape[0])[:nd]]
+        active[ins] = True
+        active[dele] = False
+        sched.append((np.asarray(ins, np.int64), np.asarray(dele, np.int64)))
+    return labeled, order, n0, sched
+
+
+def _lightest_edge(nc, cu, cv, de):
+    """Per component with an outgoing edge: the lightest one (ties: smallest other side)
+    (dynlp/cc.py:26-34)."""
+    best = np.full(nc, np.inf, dtype=np.float32)
+    np.minimum.at(best, cu, de)
+    nb = np.full(nc, nc, dtype=np.int32)
+    sel = de <= best[cu]
+    np.minimum.at(nb, cu[sel], cv[sel])
+    c = np.flatnonzero(nb < nc).astype(np.int32)
+    return c, nb[c], best[c]
+
+
+def fh_components(m, rows, cols, d, k, ground=None):
+    """Felzenszwalb-Huttenlocher merging in Boruvka rounds (dynlp/cc.py:37-73): every component
+    takes its lightest outgoing edge and merges across it when d <= min over both sides of
+    Int(C) + k / |C|; then, with `ground`, components without ground join their lightest
+    neighbour until none is left."""
+    lab = np.arange(m, dtype=np.int32)
+    Int = np.zeros(m, dtype=np.float32)
+    size = np.ones(m, dtype=np.float32)
+    rows, cols, d = np.asarray(rows, np.int32), np.asarray(cols, np.int32), np.asarray(d, np.float32)
+    nc, fh = m, True
+    while rows.shape[0]:
+        cu, cv = lab[rows], lab[cols]
+        ext = cu != cv
+        if not fh:
+            g = np.zeros(nc, dtype=np.float32)
+            np.add.at(g, lab, ground)
+            ext &= g[cu] == 0
+        if not ext.any():
+            break
+        c, t, dc = _lightest_edge(nc, cu[ext], cv[ext], d[ext])
+        if fh:
+            ok = dc <= np.minimum(Int[c] + k / size[c], Int[t] + k / size[t])
+            if not ok.any():
+                if ground is None:
+                    break
+                fh = False
+                continue
+            c, t, dc = c[ok], t[ok], dc[ok]
+        root, nc = connected_components(nc, c, t)
+        Int2 = np.zeros(nc, dtype=np.float32)
+        size2 = np.zeros(nc, dtype=np.float32)
+        np.maximum.at(Int2, root, Int)
+        np.maximum.at(Int2, root[c], dc)
+        np.add.at(size2, root, size)
+        lab, Int, size = root[lab], Int2, size2
+    return lab, nc
+
+
+def new_components(m, lr, lc, w, tau, wmax, ground):
+    """DynLP step 1 for the m new vertices (dynlp/stream.py:67-81): components over edges
+    heavier than tau among new vertices, and the adaptive (FH) ones on dissimilarities 1 - w/wmax
+    scaled by each endpoint's mean dissimilarity (dynlp/cc.py:76-83)."""
+    w = np.asarray(w)
+    on = w > 0
+    s = np.zeros(m, dtype=np.float32)
+    cnt = np.zeros(m, dtype=np.float32)
+    np.add.at(s, lr, np.where(on, 1 - w / wmax, 0).astype(np.float32))
+    np.add.at(cnt, lr, on.astype(np.float32))
+    s = s / np.maximum(cnt, 1) + 1e-6
+    e = on & (lc >= 0)
+    r, c, we = lr[e], lc[e], w[e]
+    heavy = we > tau
+    out = {"tau": connected_components(m, r[heavy], c[heavy])}
+    if m == 0:
+        out["fh"] = (np.zeros(0, dtype=np.int32), 0)
+    else:
+        d = (1 - we / wmax) / np.sqrt(s[r] * s[c])
+        out["fh"] = fh_components(m, r, c, d, float(d.mean()) if d.shape[0] else 0.0,
+                                  np.asarray(ground).astype(np.float32))
+    return out
+
+
+def stream_system(A, y, K, active, labeled, prevU, ins, dele, tau, wmax, eta=0.0, dtype=np.float64):
+    """Stream._build (dynlp/stream.py:142-177): the grounded system plus the new rows (not in U at
+    the previous batch), DynLP's seed (new rows and neighbours of inserted/deleted vertices) and
+    the new vertices' components."""
+    S = build_system(A, y, K, active, labeled, eta=eta, dtype=dtype)
+    U, W, Bm = S["U"], S["W"], S["B"]
+    n, n_u = A.shape[0], U.shape[0]
+    is_new = ~prevU[U]
+    touch = np.zeros(n, dtype=dtype)
+    touch[ins], touch[dele] = 1, 1
+    seed = is_new | ((A.astype(dtype) @ touch)[U] > 0)
+    new = np.flatnonzero(is_new)
+    nl = np.full(n_u, -1, dtype=np.int32)
+    nl[new] = np.arange(new.shape[0], dtype=np.int32)
+    rW = csr_rows(W)
+    on = is_new[rW]
+    S.update(is_new=is_new, seed=seed,
+             comps=new_components(int(is_new.sum()), nl[rW[on]], nl[W.indices[on]], W.data[on], tau, wmax,
+                                  Bm[is_new].sum(axis=1)))
+    return S
+
+
+def _comp_avg(lab, nc, S_rows, T_rows, fallback):
+    """Per component of the new vertices: sum S / sum T (T = 0: fallback) (dynlp/solvers.py:128-135)."""
+    S = np.zeros((nc,) + S_rows.shape[1:], dtype=S_rows.dtype)
+    T = np.zeros(nc, dtype=S_rows.dtype)
+    np.add.at(S, lab, S_rows)
+    np.add.at(T, lab, T_rows)
+    ok = T > 0
+    Tn = np.where(ok, T, 1)
+    if S.ndim == 2:
+        return np.where(ok[:, None], S / Tn[:, None], fallback)
+    return np.where(ok, S / Tn, fallback)
+
+
+def supernode_init(W, B, K, prior, is_new, comps, X, known=None, comp="tau"):
+    """New rows start at their component's average (dynlp/solvers.py:138-153): the share of the
+    component's weight to each labelled class (known=None, DynLP's rule), or with `known` the
+    weighted average over labelled and known neighbours."""
+    new = np.flatnonzero(is_new)
+    if new.shape[0] == 0:
+        return X
+    Bc = B[:, 1:2] if K == 2 else B
+    s_, t = Bc[new], B[new].sum(axis=1)
+    if known is not None:
+        kf = known.astype(X.dtype)
+        Wn = W[new]
+        s_ = s_ + Wn @ (X * kf[:, None])
+        t = t + Wn @ kf
+    lab, nc = comps[comp]
+    X = X.copy()
+    X[new] = _comp_avg(lab, nc, s_, t, prior[None, :])[lab]
+    return X
+
+
+def init_h(W, B, is_new, comps, H, known, fallback, comp="fh"):
+    """New rows: h = 1 + the component's weighted average h of known neighbours (labelled ones
+    count with h = 0) (dynlp/solvers.py:156-163)."""
+    new = np.flatnonzero(is_new)
+    H = H.copy()
+    if new.shape[0]:
+        kf = known.astype(H.dtype)
+        Wn = W[new]
+        lab, nc = comps[comp]
+        hc = _comp_avg(lab, nc, Wn @ (H[:, 0] * kf), B[new].sum(axis=1) + Wn @ kf, fallback - 1) + 1
+        H[new, 0] = hc[lab]
+    return H

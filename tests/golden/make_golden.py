@@ -177,6 +177,60 @@ def gen_amg(dl):
     save("amg.npz", **out)
 
 
+def gen_stream(dl):
+    """The vertex-arrival streams (dynlp/stream.py:84-346): the schedule drawn up front, every
+    batch's system from Stream._build (U, is_new, seed, the new vertices' tau and FH components)
+    and from IncrementalStream (solved/changed rows, global-index diag and rhs), and the warm
+    starts supernode_init / init_h (dynlp/solvers.py:128-163) on those systems."""
+    from dynlp import graphs, solvers
+    from dynlp.stream import IncrementalStream, Stream
+    out = {}
+    ds = graphs.sbm(2000, K=3, deg=8, seed=3, dtype="float64")
+    kw = dict(init_frac=0.2, n_batches=4, label_frac=0.02, del_frac=0.1, seed=1, dtype="float64")
+    st = Stream(ds, **kw)
+    out.update(csr_parts("A", ds.A))
+    out.update({"y": np.asarray(ds.y, np.int32), "K": np.int64(ds.K), "order_in": np.asarray(ds.order, np.int64),
+                "order": np.asarray(st.order, np.int64), "labeled": np.asarray(st.labeled), "n0": np.int64(st.n0),
+                "tau": np.float64(st.tau), "wmax": np.float64(st.wmax), "eta": np.float64(st.eta),
+                "nbatches": np.int64(len(st.schedule))})
+    for t, (ins, dele) in enumerate(st.schedule):
+        out[f"t{t}_ins"], out[f"t{t}_del"] = np.asarray(ins, np.int64), np.asarray(dele, np.int64)
+    rs = np.random.RandomState(9)
+    for t, s in enumerate(st.batches()):
+        p = f"s{t}"
+        out.update({f"{p}_U": np.asarray(s.U, np.int64), f"{p}_is_new": np.asarray(s.is_new),
+                    f"{p}_seed": np.asarray(s.seed), f"{p}_diag": s.diag, f"{p}_rhs": s.rhs,
+                    f"{p}_n_ungrounded": np.int64(s.n_ungrounded)})
+        for name in ("tau", "fh"):
+            lab, nc = s.comps[name]
+            out[f"{p}_{name}"], out[f"{p}_{name}_nc"] = np.asarray(lab, np.int32), np.int64(nc)
+        # warm starts on this system: DynLP's rule (known=None) and DynLP+'s (known = old rows)
+        X = rs.random_sample((s.n_u, s.C))
+        H = 1.0 + rs.random_sample((s.n_u, 1))
+        out[f"{p}_X"], out[f"{p}_H"] = X, H
+        out[f"{p}_sn_tau"] = solvers.supernode_init(s, X.copy(), comp="tau")
+        known = ~np.asarray(s.is_new)
+        out[f"{p}_sn_fh"] = solvers.supernode_init(s, X.copy(), known, comp="fh")
+        out[f"{p}_ih"] = solvers.init_h(s, H.copy(), known, 7.0)
+    # the resident form on the same graph with float32 weights (the resident graph keeps fp32 edge
+    # weights; its fp64 system is built from them, as the reference's W64 is from a float32 A)
+    ds32 = graphs.sbm(2000, K=3, deg=8, seed=3, dtype="float32")
+    out.update(csr_parts("A32", ds32.A))
+    out.update({"tau32": np.float64(float(ds32.A.data.mean())), "wmax32": np.float64(float(ds32.A.data.max()))})
+    ist = IncrementalStream(ds32, ball_hops=3, **{**kw, "dtype": "float32"})
+    for t, s in enumerate(ist.batches()):
+        p = f"i{t}"
+        out.update({f"{p}_solved": np.asarray(s.solved), f"{p}_changed": np.asarray(s.changed, np.int64),
+                    f"{p}_is_new": np.asarray(s.is_new), f"{p}_seed": np.asarray(s.seed),
+                    f"{p}_diag": np.asarray(s.astype("float64").diag), f"{p}_rhs": np.asarray(s.astype("float64").rhs),
+                    f"{p}_n_ungrounded": np.int64(s.n_ungrounded)})
+        for name in ("tau", "fh"):
+            lab, nc = s.comps[name]
+            out[f"{p}_{name}"], out[f"{p}_{name}_nc"] = np.asarray(lab, np.int32), np.int64(nc)
+    out["inc_counters"] = np.asarray([ist.counters["ball_checks"], ist.counters["full_ground"]], np.int64)
+    save("stream.npz", **out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", default="/root/reference")
@@ -184,7 +238,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     import cupy_shim
     dl = cupy_shim.install(a.reference)
-    gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg}
+    gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg,
+            "stream": gen_stream}
     for name, fn in gens.items():
         if not a.only or name in a.only.split(","):
             fn(dl)

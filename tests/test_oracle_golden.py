@@ -107,3 +107,55 @@ def test_amg_matches_reference():
     for i, L in enumerate(amg.levels):
         np.testing.assert_array_equal(L["agg"], g[f"L{i}_agg"])
     np.testing.assert_allclose(amg(g["R"].astype(np.float64)), g["MR"], rtol=1e-4, atol=1e-5 * abs(g["MR"]).max())
+
+
+def _stream_fixture():
+    g = load_golden("stream.npz")
+    A = golden_csr(g, "A")
+    return g, A, g["y"], int(g["K"])
+
+
+def test_stream_schedule_matches_reference():
+    g, A, y, K = _stream_fixture()
+    lab, order, n0, sched = O.stream_schedule(y, K, g["order_in"], label_frac=0.02, init_frac=0.2, n_batches=4,
+                                              del_frac=0.1, seed=1)
+    np.testing.assert_array_equal(lab, g["labeled"])
+    np.testing.assert_array_equal(order, g["order"])
+    assert n0 == int(g["n0"]) and len(sched) == int(g["nbatches"])
+    for t, (ins, dele) in enumerate(sched):
+        np.testing.assert_array_equal(ins, g[f"t{t}_ins"])
+        np.testing.assert_array_equal(dele, g[f"t{t}_del"])
+    assert float(A.data.mean()) == float(g["tau"]) and float(A.data.max()) == float(g["wmax"])
+
+
+def test_stream_systems_and_warm_starts_match_reference():
+    """Every batch of Stream._build: U, the new rows, DynLP's seed, the tau and FH components of
+    the new vertices (exact), and the warm starts supernode_init / init_h (dynlp/solvers.py:128-163)."""
+    g, A, y, K = _stream_fixture()
+    n = A.shape[0]
+    labeled = g["labeled"]
+    active, prevU = np.zeros(n, bool), np.zeros(n, bool)
+    for t in range(int(g["nbatches"])):
+        ins, dele = g[f"t{t}_ins"], g[f"t{t}_del"]
+        active[ins], active[dele] = True, False
+        S = O.stream_system(A, y, K, active, labeled, prevU, ins, dele, float(g["tau"]), float(g["wmax"]))
+        p = f"s{t}"
+        np.testing.assert_array_equal(S["U"], g[f"{p}_U"])
+        np.testing.assert_array_equal(S["is_new"], g[f"{p}_is_new"])
+        np.testing.assert_array_equal(S["seed"], g[f"{p}_seed"])
+        for name in ("tau", "fh"):
+            lab, nc = S["comps"][name]
+            np.testing.assert_array_equal(lab, g[f"{p}_{name}"], err_msg=f"{p} {name}")
+            assert nc == int(g[f"{p}_{name}_nc"])
+        np.testing.assert_allclose(S["diag"], g[f"{p}_diag"], rtol=1e-13)
+        np.testing.assert_allclose(S["rhs"], g[f"{p}_rhs"], rtol=1e-13, atol=1e-15)
+        prior = np.full(K, 1.0 / K)
+        X0 = O.supernode_init(S["W"], S["B"], K, prior, S["is_new"], S["comps"], g[f"{p}_X"], comp="tau")
+        np.testing.assert_allclose(X0, g[f"{p}_sn_tau"], rtol=1e-13)
+        known = ~S["is_new"]
+        X1 = O.supernode_init(S["W"], S["B"], K, prior, S["is_new"], S["comps"], g[f"{p}_X"], known, comp="fh")
+        np.testing.assert_allclose(X1, g[f"{p}_sn_fh"], rtol=1e-13)
+        H1 = O.init_h(S["W"], S["B"], S["is_new"], S["comps"], g[f"{p}_H"], known, 7.0)
+        np.testing.assert_allclose(H1, g[f"{p}_ih"], rtol=1e-13)
+        prevU = np.zeros(n, bool)
+        prevU[S["U"]] = True
