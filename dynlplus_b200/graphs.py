@@ -238,10 +238,44 @@ class EdgeUpdates:
                     del_u=(dk // n).astype(np.int32), del_v=(dk % n).astype(np.int32))
 
 
+def from_npz(path, dtype="float32", seed=0, name=None, device=None) -> Dataset:
+    """An edge list on disk (dynlp/graphs.py:176-184): arrays src, dst, y and optional w (default 1)
+    and order (default a RandomState(seed + 1) permutation, the reference's draw); the graph is the
+    symmetric coalesced CSR of the pairs (duplicates summed, self-loops dropped), K = max(y) + 1."""
+    import os
+    z = np.load(path)
+    keys = set(z.files)
+    y = np.asarray(z["y"]).astype(np.int32)
+    n = int(y.shape[0])
+    src, dst = np.asarray(z["src"]).astype(np.int64), np.asarray(z["dst"]).astype(np.int64)
+    w = np.asarray(z["w"]) if "w" in keys else np.ones(src.shape[0])
+    order = np.asarray(z["order"]).astype(np.int64) if "order" in keys else np.random.RandomState(seed + 1).permutation(n)
+    dev = _dev(device)
+    A = symmetric_from_pairs(src, dst, w, n, dtype, dev)
+    return Dataset(name or os.path.basename(path), A, _t(y, dev), int(y.max()) + 1 if n else 0, _t(order, dev))
+
+
+def save_npz(ds: Dataset, path, with_order=True):
+    """The edge-list format of `from_npz` (the reference's graph cache, dynlp/graphs.py:201-203): the
+    upper triangle of A as src < dst with weights w, the labels y and (optionally) the order."""
+    A = ds.A
+    rows = csr_rows(A).long()
+    up = rows < A.indices.long()
+    arrays = dict(src=rows[up].cpu().numpy(), dst=A.indices.long()[up].cpu().numpy(),
+                  w=A.data[up].cpu().numpy(), y=ds.y.cpu().numpy().astype(np.int32))
+    if with_order:
+        arrays["order"] = ds.order.cpu().numpy().astype(np.int64)
+    np.savez(path, **arrays)
+    return path
+
+
 def load(spec: str, *, n=100_000, K=2, deg=10.0, p_in=0.85, seed=0, dtype="float32", device=None) -> Dataset:
-    """dynlp/graphs.py:207-214 for the synthetic families (the IMDB/synth kNN sets are out of scope)."""
+    """dynlp/graphs.py:207-214: the synthetic families and edge lists on disk (`*.npz`); the IMDB /
+    synth kNN sets (downloads and a kNN build) are out of scope."""
     if spec == "sbm":
         return sbm(n, K, deg, p_in, seed, dtype, device)
     if spec == "er":
         return erdos_renyi(n, K, deg, seed, dtype, device)
-    raise ValueError(f"unknown dataset {spec!r} (synthetic sbm / er only)")
+    if spec.endswith(".npz"):
+        return from_npz(spec, dtype, seed, device=device)
+    raise ValueError(f"unknown dataset {spec!r} (sbm, er or an edge-list .npz)")

@@ -386,6 +386,35 @@ class Solver:
         return self.F[sys.U]
 
 
+class ItLP(Solver):
+    """Plain Jacobi label propagation from the prior (dynlp/solvers.py:188-210): X = (rhs + W X) /
+    diag over all rows until no entry moves by more than delta, one frontier-Jacobi launch over
+    every row per sweep (its change flags are the stop test)."""
+    name = "itlp"
+
+    def __init__(self, n_total, K, dtype="float32", delta=1e-4, max_iter=200_000):
+        super().__init__(n_total, K, dtype)
+        self.delta, self.max_iter = delta, max_iter
+
+    def solve(self, sys):
+        st, sys = Stats(path="jacobi"), sys.astype(self.dtype)
+        with Timer() as tm:
+            X = self._warm(sys).contiguous()
+            X[:] = sys.prior
+            n = X.shape[0]
+            if n:
+                ops = FrontierOps(sys.W, self.C)
+                rows = torch.arange(n, dtype=torch.int32, device=X.device)
+                for _ in range(self.max_iter):
+                    Y, ch = ops.jacobi(rows, X, sys.rhs, sys.diag, self.delta)
+                    X, st.iters, st.edges = Y, st.iters + 1, st.edges + sys.nnz
+                    if not bool(ch.any()):
+                        break
+            self._store(sys, X)
+        st.ms = tm.ms
+        return st
+
+
 class DynLP(Solver):
     """DynLP's frontier Jacobi (Algorithm 2, dynlp/solvers.py:213-241) on the frontier kernels: the
     new rows start at their component's label share (supernode_init, the paper's tau components or
@@ -729,6 +758,8 @@ class Reference:
 def make(name, n_total, K, *, dtype, delta, tol, group, max_iter=None):
     """dynlp/solvers.py:448-458."""
     kw = {} if max_iter is None else {"max_iter": max_iter}
+    if name == "itlp":
+        return ItLP(n_total, K, dtype, delta, **kw)
     if name in ("dynlp", "dynlp-fh"):
         return DynLP(n_total, K, dtype, delta, group, comp="fh" if name == "dynlp-fh" else "tau", **kw)
     if name == "dynlp+inc":
@@ -738,4 +769,4 @@ def make(name, n_total, K, *, dtype, delta, tol, group, max_iter=None):
     raise ValueError(f"unknown solver {name!r}")
 
 
-SOLVERS = ["dynlp", "dynlp-fh", "dynlp+pcg", "dynlp+amg", "dynlp+auto", "dynlp+inc"]
+SOLVERS = ["itlp", "dynlp", "dynlp-fh", "dynlp+pcg", "dynlp+amg", "dynlp+auto", "dynlp+inc"]

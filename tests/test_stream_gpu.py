@@ -126,3 +126,25 @@ def test_solvers_on_vertex_stream_are_close_to_direct(name):
             assert err < 1e-3, err
         else:
             assert err <= max(1.05 * stt.cert, 1e-9), (err, stt.cert)
+
+
+@pytest.mark.parametrize("incremental", [False, True])
+def test_streaming_benchmark_rows(tmp_path, incremental):
+    """The reference's streaming benchmark (dynlp/bench.py) on a small SBM stream: one CSV row per
+    batch and solver with the reference's columns; certified solvers within their bound of F*."""
+    import csv
+    from dynlplus_b200 import bench as sb
+    out = str(tmp_path / "run.csv")
+    names = "itlp,dynlp,dynlp-fh,dynlp+pcg,dynlp+auto" + (",dynlp+inc" if incremental else "")
+    argv = ["--dataset", "sbm", "--n", "6000", "--classes", "3", "--deg", "8", "--batches", "3", "--init-frac", "0.4",
+            "--label-frac", "0.02", "--solvers", names, "--out", out, "--no-warmup"] + (["--incremental"] if incremental
+                                                                                        else [])
+    rows = sb.main(argv)
+    assert len(rows) == 4 * len(names.split(","))
+    with open(out) as fh:
+        r = list(csv.DictReader(fh))
+    assert list(r[0].keys()) == sb.FIELDS and len(r) == len(rows)
+    for row in rows:
+        if row["solver"].startswith("dynlp+"):
+            assert row["err_max"] <= max(1.05 * row["cert_self"], 1e-9), row
+        assert 0.0 <= row["acc_true"] <= 1.0
