@@ -76,25 +76,36 @@ class AdmissionError(RuntimeError):
 
 class Server:
     def __init__(self, ds, labeled, *, dtype="float32", target_relres=1e-6, tol=1e-3, hbm_budget_bytes=None,
-                 max_fresh_batch=64, fresh_dtype=torch.float64):
+                 max_fresh_batch=64, fresh_dtype=torch.float64, mode="continuous", lowp=False):
+        """mode="continuous": the loop described above. mode="sequential": the plain path it is
+        measured against -- one worker, requests served one at a time in arrival order, every update
+        solved on its own and every fresh solve launched alone. lowp: BF16 gathers in the update
+        solves' working-precision sweeps (fp64 refinement keeps the target)."""
+        if mode not in ("continuous", "sequential"):
+            raise ValueError(f"unknown serving mode {mode!r}")
+        self.mode = mode
         self.target = target_relres
         self.K = ds.K
         self.fresh_dtype = fresh_dtype
         self.es = stream.EdgeStream(ds, labeled, dtype=dtype)
         self.solver = solvers.IncrementalLP(ds.n, ds.K, dtype, tol=tol, method="pcg", target_relres=target_relres,
-                                            full_every=16)
+                                            full_every=16, lowp=lowp)
         self.solver.solve(self.es.system)
         self.labels = self._snapshot()
         self.version = 0
         free, total = torch.cuda.mem_get_info()
         self.budget = int(hbm_budget_bytes if hbm_budget_bytes is not None else 0.5 * free)
-        self.max_fresh_batch = max_fresh_batch
+        self.max_fresh_batch = max_fresh_batch if mode == "continuous" else 1
         self._q = {"update": queue.Queue(), "query": queue.Queue(), "fresh": queue.Queue()}
+        if mode == "sequential":  # one queue for every kind: arrival order, one request at a time
+            one = queue.Queue()
+            self._q = {k: one for k in self._q}
         self._streams = {k: torch.cuda.Stream() for k in self._q}
         self._stop = threading.Event()
         self._lock = threading.Lock()
         self.done: list[_Item] = []
-        self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in self._q]
+        kinds = list(self._q) if mode == "continuous" else ["all"]
+        self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in kinds]
         self._dev = torch.cuda.current_device()
         for t in self._threads:
             t.start()
@@ -114,7 +125,7 @@ class Server:
 
     def close(self):
         self._stop.set()
-        for q in self._q.values():
+        for q in {id(q): q for q in self._q.values()}.values():
             q.put(None)
         for t in self._threads:
             t.join(timeout=60)
@@ -145,6 +156,8 @@ class Server:
 
     def _drain(self, kind, first, limit=None):
         items = [first]
+        if self.mode == "sequential":
+            return items
         q = self._q[kind]
         while limit is None or len(items) < limit:
             try:
@@ -159,13 +172,14 @@ class Server:
 
     def _worker(self, kind):
         torch.cuda.set_device(self._dev)
-        with torch.cuda.stream(self._streams[kind]):
+        q = self._q["update"] if kind == "all" else self._q[kind]
+        with torch.cuda.stream(self._streams["update" if kind == "all" else kind]):
             while not self._stop.is_set():
-                first = self._q[kind].get()
+                first = q.get()
                 if first is None:
                     break
                 try:
-                    getattr(self, "_do_" + kind)(first)
+                    getattr(self, "_do_" + first.kind)(first)
                 except BaseException as e:  # a failing batch fails its requests, not the server
                     self._finish([first], [e])
 

@@ -563,7 +563,8 @@ class DynLPPlus(Solver):
                 # the correction must bring the fp64 residual of every F column under the target, or
                 # as far as the working precision resolves in one round (the next round continues)
                 rnR = [ss[c] ** 0.5 for c in range(C)]
-                fl = 3e-6 if self.dtype == torch.float32 else 1e-13
+                # what one round can resolve: bf16 gathers ~2e-3, fp32 sweeps ~3e-6, fp64 ~1e-13
+                fl = (2e-3 if self.lowp else 3e-6) if self.dtype == torch.float32 else 1e-13
                 allowed = [max(self.refine_share * self.target_relres * float(rhs_norm[c]), fl * rnR[c], 1e-300) /
                            scale[c] for c in range(C)]
                 kw = dict(target_relres=1.0, rhs_norm=allowed + [1e300])

@@ -21,7 +21,10 @@ def _alone_fresh(req):
     return Fs[0]
 
 
-def test_results_alone_equal_results_in_the_mix():
+@pytest.mark.parametrize("mode,lowp", [("continuous", False), ("sequential", False), ("continuous", True)])
+def test_results_alone_equal_results_in_the_mix(mode, lowp):
+    """The continuous loop (FP32 and BF16 sweeps) and the one-at-a-time baseline give the results of
+    each request served alone."""
     n, K = 20_000, 4
     ds = graphs.er_graph(n, 10, K, seed=7)
     lab = graphs.label_mask(n, 0.01, seed=7)
@@ -29,7 +32,7 @@ def test_results_alone_equal_results_in_the_mix():
     batches = [up.next(int(s)) for s in (50, 400, 10, 1200, 300)]
     fresh = [_fresh(i) for i in range(5)]
 
-    srv = serve.Server(ds, lab, target_relres=1e-6)
+    srv = serve.Server(ds, lab, target_relres=1e-6, mode=mode, lowp=lowp)
     futs = []
     for i, b in enumerate(batches):  # interleave updates, fresh solves and queries
         futs.append(srv.submit(serve.EdgeUpdate(b["ins_u"], b["ins_v"], b["ins_w"], b["del_u"], b["del_v"])))
