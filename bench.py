@@ -106,6 +106,10 @@ class Clocks:
             self.first.wait(timeout)
         self.t0 = time.perf_counter()
 
+    def mark(self):
+        """The timed region starts now (samples before it are not summarised)."""
+        self.t0 = time.perf_counter()
+
     def stop(self):
         if self.p is None:
             return None
@@ -329,17 +333,21 @@ def ours(a):
             return st, res
         return st, None
 
+    dev_batches = [to_dev(b) for b in batches[a.warmup: a.warmup + a.steps]]
+    host_batches = [to_pinned(b) for b in batches[a.warmup + a.steps:]]
+    # the clock sampler starts before the warm-up, so the timed steps follow the last warm-up step
+    # directly (an idle gap before them would let the clocks drop)
+    clocks = Clocks(torch.cuda.current_device()) if not a.no_clocks else None
+    if clocks is not None:
+        clocks.wait_first()
     # warm-up (not timed)
     for b in batches[: a.warmup]:
         step(to_dev(b))
     torch.cuda.synchronize()
-    dev_batches = [to_dev(b) for b in batches[a.warmup: a.warmup + a.steps]]
-    host_batches = [to_pinned(b) for b in batches[a.warmup + a.steps:]]
     if world > 1:
         dist.barrier()
-    clocks = Clocks(torch.cuda.current_device()) if not a.no_clocks else None
     if clocks is not None:
-        clocks.wait_first()
+        clocks.mark()
     launches0 = _lib.lib().dlp_launch_count()
     solvers.PCG_EVENTS = []  # CUDA events around the fused PCG calls of the timed steps
     torch.cuda.nvtx.range_push("timed")  # lets a profiler filter the timed steps (--nvtx-include timed/)

@@ -71,17 +71,18 @@ def ground_reach(G, vmask, sink, umask, in_t, w=None):
     import ctypes as ct
     n = G.shape[0]
     dev = G.indices.device
-    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
-    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    ce = torch.zeros(2, dtype=torch.int32, device=dev)  # [changes, error]: read back together
+    cnt, err = ce[0:1], ce[1:2]
     sweeps = ct.c_int32(0)
     ws = workspace("ground_reach").get(_lib.lib().dlp_ground_reach_workspace_bytes(n))
     rbeg, rend = (G.rbeg, G.rend) if hasattr(G, "rbeg") else (G.indptr[:-1], G.indptr[1:])
     _lib.call("dlp_ground_reach", n, ptr(rbeg), ptr(rend), ptr(G.indices), ptr(w), code(w) if w is not None else 0,
               ptr(vmask), ptr(sink), ptr(umask), ptr(in_t), ptr(cnt), ptr(err), ct.addressof(sweeps), ptr(ws),
               ws.numel(), stream())
-    if int(err.item()):
+    changes, bad = ce.tolist()
+    if bad:
         raise ValueError("ground_reach: entry column outside [0, n)")
-    return int(cnt.item()), int(sweeps.value)
+    return changes, int(sweeps.value)
 
 
 

@@ -729,9 +729,13 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   if (use_graph) DLP_TRY(get_chunk_graph(q, B, k, &gref));
   cudaGraphExec_t ex = gref ? gref->ex : nullptr;
   PcgCtl cur{};
-  DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
-  DLP_CUDA(cudaStreamSynchronize(s));
-  if (max_iter <= 0 && cur.done == 0) cur.done = 3;
+  if (max_iter <= 0) {
+    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    DLP_CUDA(cudaStreamSynchronize(s));
+    if (cur.done == 0) cur.done = 3;
+  }
+  // otherwise the first chunk goes out without a round trip: when the start already meets the
+  // stop rule, its kernels see ctl->done and return at once
   while ((cur.done == 0 || cur.done == 1) && !cur.bad) {
     if (cur.done == 0) {
       if (ex) {

@@ -110,8 +110,14 @@ def residual_stats(sys: System, R, rhs=None, H=None):
                   ptr(sys.diag.to(dt)), ptr(H), ld(H) if H is not None else 1, code(R), ptr(out), ptr(ws), ws.numel(),
                   stream())
     v = out.cpu().tolist()
-    return (v[:C], v[C:2 * C], v[2 * C:3 * C] if rhs is not None else None,
-            v[3 * C] if H is not None else None)
+    res = _Stats((v[:C], v[C:2 * C], v[2 * C:3 * C] if rhs is not None else None, v[3 * C] if H is not None else None))
+    res.dev = out  # the device copy: the refinement scales from it without an upload
+    return res
+
+
+class _Stats(tuple):
+    """residual_stats' result: (rho_cols, sums of R^2, sums of rhs^2, max |h|) with `.dev`, the
+    device array they were read from."""
 
 
 class JacobiM:
@@ -555,7 +561,11 @@ class DynLPPlus(Solver):
             if bound <= self.tol and ok_rel:
                 break
             scale = [r if r > 0 else 1.0 for r in rc]
-            sc = torch.tensor(scale, dtype=F64, device=dev)
+            dv = getattr(stats, "dev", None)
+            if dv is not None and dv.device == dev and dv.numel() >= C + 1:
+                sc = torch.where(dv[: C + 1] > 0, dv[: C + 1], torch.ones_like(dv[: C + 1]))  # = scale, on device
+            else:
+                sc = torch.tensor(scale, dtype=F64, device=dev)
             eps_c = [min(max(e / s, self._floor(h_est)), 1.0) for e, s in
                      zip([self.tol / (1.25 * hmax)] * C + [self.eps_h], scale)]
             kw = {}

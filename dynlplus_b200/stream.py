@@ -394,14 +394,17 @@ class EdgeStream:
                           ptr(G.data), ptr(iu), ptr(iv), ptr(iw), ni, ptr(self.umask), ptr(self.labeled), ptr(self.y),
                           self.K, ptr(self.rowsum), ptr(self.B), ptr(self.changed), ptr(st[1:2]), ptr(st[3:4]),
                           ptr(st[0:1]), ptr(ws), ws.numel(), s)
-                if int(st[1].item()) == 0:
+                flags = st[0:4].tolist()  # [error, overflow, deleted, inserted]: one read-back
+                if flags[1] == 0:
                     break
                 G.rebuild()  # a row ran out of slack: repack with more and apply the batch again
                 self.counters["rebuilds"] += 1
             else:
                 raise RuntimeError("edge insertion kept overflowing after repacking")
-        if int(st[0].item()):
-            raise ValueError(f"edge batch rejected: {_lib.STATUS.get(int(st[0].item()))} (vertex id out of range?)")
+        else:
+            flags = st[0:4].tolist()
+        if flags[0]:
+            raise ValueError(f"edge batch rejected: {_lib.STATUS.get(flags[0])} (vertex id out of range?)")
         # grounding: components of the unlabelled subgraph with the labelled vertices as a sink
         nmoved = self._ground()
         moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
@@ -415,7 +418,9 @@ class EdgeStream:
         self.t += 1
         self.last_changed, self.last_moved = Q, moved
         self.n_ins, self.n_del = ni, nd
-        self.counters["applied"] += int(st[2].item()) + int(st[3].item())
+        self.counters["applied"] += flags[2] + flags[3]
+        if nmoved:
+            self._counts = None
         return self.system
 
     def apply_vertices(self, ins, dele, tau=None, wmax=None) -> System:
@@ -473,6 +478,7 @@ class EdgeStream:
             wd = G.data if self.dtype == torch.float32 else G.data.to(self.dtype)
             comps = new_components(new, G.rbeg, G.rend, G.indices, wd, nl, tau, wmax, self.B[new].sum(dim=1))
         self._vertex_batch = {"is_new": is_new, "seed": seed, "comps": comps}
+        self._counts = None
         return self.system
 
     def solver_csr(self) -> CSR:
@@ -499,15 +505,21 @@ class EdgeStream:
         """Global-index system of the current batch (arrays live until the next batch)."""
         n, C, dev = self.n, self.C, self.dev
         um = self.umask.bool()
-        s64 = self.diag64 - self.rowsum
+        if getattr(self, "_s64", None) is None:
+            self._s64 = torch.empty(n, dtype=torch.float64, device=dev)
+            self._ids = torch.arange(n, device=dev)
+        s64 = torch.sub(self.diag64, self.rowsum, out=self._s64)
+        # active and ungrounded counts change only with vertex batches or membership changes
+        if getattr(self, "_counts", None) is None:
+            self._counts = torch.stack([self.vmask.sum() + self.labeled.sum(), (self.vmask.bool() & ~um).sum()]).tolist()
+        n_active, n_ungrounded = self._counts
         vx = getattr(self, "_vertex_batch", None)
-        common = dict(t=self.t, U=torch.arange(n, device=dev), W=self.solver_csr(),
+        common = dict(t=self.t, U=self._ids, W=self.solver_csr(),
                       is_new=vx["is_new"] if vx else torch.zeros(n, dtype=torch.bool, device=dev),
                       seed=vx["seed"] if vx else self.changed.bool(), comps=vx["comps"] if vx else {}, K=self.K, C=C,
                       eta=self.eta,
-                      n_inserted=self.n_ins, n_deleted=self.n_del, n_active=int(self.vmask.sum().item() +
-                                                                               self.labeled.sum().item()),
-                      n_ungrounded=int((self.vmask.bool() & ~um).sum().item()), solved=um,
+                      n_inserted=self.n_ins, n_deleted=self.n_del, n_active=int(n_active),
+                      n_ungrounded=int(n_ungrounded), solved=um,
                       changed=self.last_changed, moved=self.last_moved)
         ch = C + (1 if self.with_h else 0)
         S = System(s=s64.to(self.dtype), diag=self.diag32 if self.dtype == torch.float32 else self.diag64.to(self.dtype),
