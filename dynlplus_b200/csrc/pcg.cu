@@ -31,9 +31,11 @@ struct PcgCtl {
   double best, viol, relres, target;
 };
 
+// Per-block partials are stored output-major: output o of block b at part[o * nbmax + b].
 struct PcgBufs {
   PcgCtl *ctl;
-  double *alpha, *beta, *rz, *eps, *rhsn, *epsinv, *part1, *part2, *partv;
+  double *alpha, *beta, *rz, *eps, *rhsn, *epsinv, *part1, *part2;
+  int nbmax;
 };
 
 constexpr int kUpdBlocksPerSM = 8;
@@ -47,9 +49,8 @@ static size_t pcg_ws_bytes(int C) {
   const size_t nb = (size_t)std::max(upd_blocks(), apply_blocks());
   size_t b = align256(sizeof(PcgCtl));
   b += 6 * align256(sizeof(double) * C);
-  b += align256(sizeof(double) * nb * C);      // part1
-  b += align256(sizeof(double) * nb * C * 2);  // part2 (rz, ss)
-  b += align256(sizeof(double) * nb);          // partv
+  b += align256(sizeof(double) * nb * C);            // part1 (pAp)
+  b += align256(sizeof(double) * nb * (2 * C + 1));  // part2 (rz, ss, violation)
   return b;
 }
 
@@ -67,8 +68,7 @@ static PcgBufs carve(void *ws, int C) {
   B.part1 = (double *)p;
   p += align256(sizeof(double) * nb * C);
   B.part2 = (double *)p;
-  p += align256(sizeof(double) * nb * C * 2);
-  B.partv = (double *)p;
+  B.nbmax = (int)nb;
   return B;
 }
 
@@ -84,6 +84,62 @@ __device__ __forceinline__ bool last_block(uint32_t *counter) {
   __syncthreads();
   if (is_last) __threadfence();
   return is_last;
+}
+
+// Deterministic reduction of per-block partials by every thread of the calling (last) block:
+// output o < NO is the sum (o < nsum) or the max (of non-negative values) of part[o * stride + b]
+// over b < nb. Thread t takes b = t, t + NT, ... in ascending order, kRows rows of kOut outputs
+// loaded together (kRows trades registers for loads in flight); then a fixed xor tree over the warp
+// and a fixed-order pass over the warps, after which emit(o, value) runs on one thread per output.
+// The order depends only on nb.
+template <int NT, int kRows, class Emit>
+__device__ __forceinline__ void block_partials_reduce(const double *part, long long stride, int nb, int NO, int nsum,
+                                                      Emit emit) {
+  constexpr int kOut = 4, kChunk = 64, NW = NT / 32;
+  __shared__ double s_w[NW][kChunk];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int c0 = 0; c0 < NO; c0 += kChunk) {
+    const int nc = min(kChunk, NO - c0);
+    for (int o0 = 0; o0 < nc; o0 += kOut) {
+      double v[kOut];
+#pragma unroll
+      for (int k = 0; k < kOut; ++k) v[k] = 0.0;
+      for (int b0 = tid; b0 < nb; b0 += kRows * NT) {
+        double x[kRows][kOut];
+#pragma unroll
+        for (int j = 0; j < kRows; ++j)
+#pragma unroll
+          for (int k = 0; k < kOut; ++k) {
+            const int b = b0 + j * NT;
+            x[j][k] = (b < nb && o0 + k < nc) ? __ldcg(part + (long long)(c0 + o0 + k) * stride + b) : 0.0;
+          }
+#pragma unroll
+        for (int j = 0; j < kRows; ++j)
+#pragma unroll
+          for (int k = 0; k < kOut; ++k) v[k] = c0 + o0 + k < nsum ? v[k] + x[j][k] : fmax(v[k], x[j][k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kOut; ++k) {
+        const bool sum = c0 + o0 + k < nsum;
+        double x = v[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const double y = __shfl_xor_sync(0xffffffffu, x, off);
+          x = sum ? x + y : fmax(x, y);
+        }
+        if (lane == 0 && o0 + k < nc) s_w[wid][o0 + k] = x;
+      }
+    }
+    __syncthreads();
+    for (int o = tid; o < nc; o += NT) {
+      const bool sum = c0 + o < nsum;
+      double x = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) x = sum ? x + s_w[w][o] : fmax(x, s_w[w][o]);
+      emit(c0 + o, x);
+    }
+    __syncthreads();
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -187,17 +243,14 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
   for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
     double s = 0.0;
     for (int w = 0; w < kThreads / 32; ++w) s += sm[w][c];
-    p.B.part1[(long long)blockIdx.x * p.C + c] = s;
+    p.B.part1[(long long)c * p.B.nbmax + blockIdx.x] = s;
   }
   if (last_block(&ctl->cnt1)) {
-    // one warp per column: lane-strided loads over the block partials, fixed-order tree
-    for (int c = wid; c < p.C; c += kThreads / 32) {
-      const double s = warp_strided_reduce(p.B.part1 + c, p.C, (int)gridDim.x, false);
-      if (lane == 0) {
-        const double al = s > 0.0 ? p.B.rz[c] / s : 0.0;
-        p.B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
-      }
-    }
+    const PcgBufs &B = p.B;
+    block_partials_reduce<kThreads, 2>(B.part1, B.nbmax, (int)gridDim.x, p.C, p.C, [&](int c, double s) {
+      const double al = s > 0.0 ? B.rz[c] / s : 0.0;
+      B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
+    });
     if (threadIdx.x == 0) ctl->cnt1 = 0;
   }
 }
@@ -210,6 +263,13 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
 // ------------------------------------------------------------------------------------------------
 constexpr int kSweepUnroll = 4;
 constexpr int kSweepThreads = 256;
+
+// fp32 sweeps fit in 64 registers without spilling (4 resident blocks per SM); fp64 ones keep the
+// compiler's choice.
+template <typename T>
+constexpr int sweep_min_blocks() {
+  return sizeof(T) == 4 ? 4 : 1;
+}
 
 struct SweepIdx {
   long long r0, RS;
@@ -248,7 +308,7 @@ __device__ __forceinline__ double block_column_sum(const double *v, int c, int64
 // A non-finite residual entry stops the solve with status 4 (breakdown) instead of letting the
 // max-reductions (which skip NaN) read it as convergence.
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t n, int32_t C, T *__restrict__ R,
+__global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_update(int phase, int32_t n, int32_t C, T *__restrict__ R,
                                                               int64_t ldr, const T *__restrict__ AP, int64_t ldap,
                                                               const T *__restrict__ diag, PcgBufs B) {
   PcgCtl *ctl = B.ctl;
@@ -261,15 +321,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t
     const int c = ix.c;
     const T al = phase == 0 ? (T)B.alpha[c] : T(0);
     const double einv = B.epsinv[c];
+    // element offsets advance by addition (no 64-bit multiply per element)
+    const long long rstep = ix.RS * ldr, astep = ix.RS * ldap;
+    long long offr = ix.r0 * ldr + c, offa = ix.r0 * ldap + c;
     for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
       T rv[kSweepUnroll], ap[kSweepUnroll], dv[kSweepUnroll];
 #pragma unroll
       for (int u = 0; u < kSweepUnroll; ++u) {
         const long long rr = r + u * ix.RS;
         const bool ok = rr < n;
-        rv[u] = ok ? R[rr * ldr + c] : T(0);
+        rv[u] = ok ? R[offr + u * rstep] : T(0);
         dv[u] = ok ? diag[rr] : T(1);
-        ap[u] = (ok && phase == 0) ? AP[rr * ldap + c] : T(0);
+        ap[u] = (ok && phase == 0) ? AP[offa + u * astep] : T(0);
       }
 #pragma unroll
       for (int u = 0; u < kSweepUnroll; ++u) {
@@ -277,16 +340,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t
         if (rr < n) {
           if (phase == 0) {
             rv[u] = rv[u] - al * ap[u];
-            R[rr * ldr + c] = rv[u];
+            R[offr + u * rstep] = rv[u];
           }
           const double r64 = (double)rv[u];
-          const double dinv = 1.0 / (double)dv[u];
+          const double dinv = __drcp_rn((double)dv[u]);  // correctly rounded: the value of 1.0 / d
           bad |= !isfinite(r64);
           rz += r64 * r64 * dinv;
           ss += r64 * r64;
           vmax = fmax(vmax, fabs(r64) * dinv * einv);
         }
       }
+      offr += kSweepUnroll * rstep;
+      offa += kSweepUnroll * astep;
     }
   }
   if (bad) ctl->bad = 1;
@@ -301,23 +366,25 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t
     const double a = block_column_sum(s_rz, c, ldr);
     const double b = block_column_sum(s_ss, c, ldr);
     if (lane == 0) {
-      B.part2[((long long)blockIdx.x * C + c) * 2 + 0] = a;
-      B.part2[((long long)blockIdx.x * C + c) * 2 + 1] = b;
+      B.part2[(long long)c * B.nbmax + blockIdx.x] = a;
+      B.part2[(long long)(C + c) * B.nbmax + blockIdx.x] = b;
     }
   }
   if (tid == 0) {
     double v = 0.0;
     for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
-    B.partv[blockIdx.x] = v;
+    B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
   }
   if (last_block(&ctl->cnt2)) {
+    // outputs: rz_c (c < C), ss_c (C + c), violation (2C)
+    __shared__ double s_out[2 * 256 + 1];
+    block_partials_reduce<kSweepThreads, 2>(B.part2, B.nbmax, (int)gridDim.x, 2 * C + 1, 2 * C,
+                                            [&](int o, double v) { s_out[o] = v; });
     __shared__ double s_rel;
     if (tid == 0) s_rel = 0.0;
     __syncthreads();
-    for (int c = wid; c < C; c += kSweepThreads / 32) {
-      const double a = warp_strided_reduce(B.part2 + (long long)c * 2 + 0, (long long)C * 2, (int)gridDim.x, false);
-      const double b = warp_strided_reduce(B.part2 + (long long)c * 2 + 1, (long long)C * 2, (int)gridDim.x, false);
-      if (lane != 0) continue;
+    for (int c = tid; c < C; c += kSweepThreads) {
+      const double a = s_out[c], b = s_out[C + c];
       const double rzo = B.rz[c];
       const double be = (phase != 2 && rzo > 0.0) ? a / rzo : 0.0;
       B.beta[c] = isfinite(be) && fabs(be) < 1e30 ? be : 0.0;
@@ -327,12 +394,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t
       atomicMax((unsigned long long *)&s_rel, __double_as_longlong(rel));
     }
     __syncthreads();
-    __shared__ double s_vmax;
-    if (wid == 0) {
-      const double v = warp_strided_reduce(B.partv, 1, (int)gridDim.x, true);
-      if (lane == 0) s_vmax = v;
-    }
-    __syncthreads();
+    const double s_vmax = s_out[2 * C];
     if (tid == 0) {
       const double v = s_vmax;
       const double rel = s_rel;
@@ -372,7 +434,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_update(int phase, int32_t
 //   mode 0: both (skipping the P update when a stop was proposed)   mode 1: P update only
 //   mode 2: P = R/diag
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z,
+__global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z,
                                                            int64_t ldz, T *__restrict__ P, int64_t ldp,
                                                            const T *__restrict__ R, int64_t ldr,
                                                            const T *__restrict__ diag, PcgBufs B, bf16 *P_lo,
@@ -385,34 +447,65 @@ __global__ void __launch_bounds__(kSweepThreads) k_pcg_dir(int mode, int32_t n, 
   const int c = ix.c;
   const T al = mode == 0 ? (T)B.alpha[c] : T(0);
   const T be = mode == 2 ? T(0) : (T)B.beta[c];
+  const long long zstep = ix.RS * ldz, pstep = ix.RS * ldp, rstep = ix.RS * ldr;
+  long long offz = ix.r0 * ldz + c, offp = ix.r0 * ldp + c, offr = ix.r0 * ldr + c;
   for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
-    T pv[kSweepUnroll], rv[kSweepUnroll], dv[kSweepUnroll];
+    // every load of the batch is issued before any store (Z included)
+    T pv[kSweepUnroll], rv[kSweepUnroll], dv[kSweepUnroll], zv[kSweepUnroll];
 #pragma unroll
     for (int u = 0; u < kSweepUnroll; ++u) {
       const long long rr = r + u * ix.RS;
       const bool ok = rr < n;
-      pv[u] = ok ? P[rr * ldp + c] : T(0);
-      rv[u] = (ok && upd_p) ? R[rr * ldr + c] : T(0);
+      pv[u] = ok ? P[offp + u * pstep] : T(0);
+      zv[u] = (ok && mode == 0) ? Z[offz + u * zstep] : T(0);
+      rv[u] = (ok && upd_p) ? R[offr + u * rstep] : T(0);
       dv[u] = (ok && upd_p) ? diag[rr] : T(1);
     }
 #pragma unroll
     for (int u = 0; u < kSweepUnroll; ++u) {
       const long long rr = r + u * ix.RS;
       if (rr < n) {
-        if (mode == 0) Z[rr * ldz + c] += al * pv[u];
+        if (mode == 0) Z[offz + u * zstep] = zv[u] + al * pv[u];
         if (upd_p) {
           const T y = rv[u] / dv[u];
           const T pn = mode == 2 ? y : y + be * pv[u];
-          P[rr * ldp + c] = pn;
+          P[offp + u * pstep] = pn;
           if (P_lo) P_lo[rr * ld_lo + c] = cvt<bf16>(pn);
         }
       }
     }
+    offz += kSweepUnroll * zstep;
+    offp += kSweepUnroll * pstep;
+    offr += kSweepUnroll * rstep;
   }
 }
 
-// The sweeps need ld <= threads in the grid (at least one row per pass); dlp_pcg checks it.
-static int sweep_blocks(int64_t) { return upd_blocks(); }
+// Blocks per SM of a grid-stride kernel that are resident at once: its grid is that many blocks per
+// SM (one wave), since a second, partial wave leaves most SMs idle while it drains. Computed once
+// per kernel instantiation from the occupancy calculator (first called before any stream capture),
+// capped at the kUpdBlocksPerSM blocks per SM the partial-sum buffers hold.
+template <class K>
+static int resident_per_sm(K *kernel, int threads) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess || per < 1) {
+    (void)cudaGetLastError();
+    per = 1;
+  }
+  return std::min(per, kUpdBlocksPerSM);
+}
+
+// The sweeps need ld <= threads in the grid (at least one row per pass): with one block per SM at
+// least, dlp_pcg's check ld <= sm_count() * kSweepThreads covers every grid below.
+template <typename TS>
+static int update_grid() {
+  static const int per = resident_per_sm(k_pcg_update<TS>, kSweepThreads);
+  return sm_count() * per;
+}
+template <typename TS>
+static int dir_grid() {
+  static const int per = resident_per_sm(k_pcg_dir<TS>, kSweepThreads);
+  return sm_count() * per;
+}
 
 // ------------------------------------------------------------------------------------------------
 // Certification statistics in one sweep: per column max |R|/diag and sum R^2 (and sum rhs^2), plus
@@ -519,7 +612,7 @@ struct PcgProblem {
 };
 
 template <class T>
-static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, bool launch = true) {
   Layout L;
   const bool lo = sizeof(typename T::TX) == 2;
   const void *X = lo ? q.P_lo : q.P;
@@ -528,16 +621,22 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   ApplyArgs<T> a{q.rbeg, q.rend, q.col, (const typename T::TW *)(lo ? q.w_lo : q.w), q.n, q.C,
                  (const typename T::TX *)X, ldx, (const typename T::TV *)q.diag, (typename T::TY *)q.AP, q.ldap, B,
                  L.G, L.LV, L.NV, lo ? (const typename T::TV *)q.P : nullptr, q.ldp};
-  const int grid = apply_blocks();
   constexpr int VWV = 16 / sizeof(typename T::TX);
-#define DLP_APPLY_CASE(VW_)                                                           \
-  switch (L.VPL) {                                                                    \
-    case 1: k_pcg_apply<T, VW_, 1><<<grid, kThreads, 0, s>>>(a); break;              \
-    case 2: k_pcg_apply<T, VW_, 2><<<grid, kThreads, 0, s>>>(a); break;              \
-    case 3: k_pcg_apply<T, VW_, 3><<<grid, kThreads, 0, s>>>(a); break;              \
-    case 4: k_pcg_apply<T, VW_, 4><<<grid, kThreads, 0, s>>>(a); break;              \
-    case 8: k_pcg_apply<T, VW_, 8><<<grid, kThreads, 0, s>>>(a); break;              \
-    default: return DLP_ERR_INVALID;                                                  \
+  // launch == false only fills the one-wave grid cache (outside stream capture)
+#define DLP_APPLY_ONE(VW_, VPL_)                                                        \
+  case VPL_: {                                                                          \
+    static const int per = resident_per_sm(k_pcg_apply<T, VW_, VPL_>, kThreads);       \
+    if (launch) k_pcg_apply<T, VW_, VPL_><<<sm_count() * per, kThreads, 0, s>>>(a);     \
+    break;                                                                              \
+  }
+#define DLP_APPLY_CASE(VW_)                                                             \
+  switch (L.VPL) {                                                                      \
+    DLP_APPLY_ONE(VW_, 1)                                                               \
+    DLP_APPLY_ONE(VW_, 2)                                                               \
+    DLP_APPLY_ONE(VW_, 3)                                                               \
+    DLP_APPLY_ONE(VW_, 4)                                                               \
+    DLP_APPLY_ONE(VW_, 8)                                                               \
+    default: return DLP_ERR_INVALID;                                                    \
   }
   if (L.VW == 1) {
     DLP_APPLY_CASE(1)
@@ -545,19 +644,20 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
     DLP_APPLY_CASE(VWV)
   }
 #undef DLP_APPLY_CASE
-  return check_launch();
+#undef DLP_APPLY_ONE
+  return launch ? check_launch() : DLP_OK;
 }
 
 template <typename TS>
 static int launch_update(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
-  k_pcg_update<TS><<<sweep_blocks(q.ldr), kSweepThreads, 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, (const TS *)q.AP,
+  k_pcg_update<TS><<<update_grid<TS>(), kSweepThreads, 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, (const TS *)q.AP,
                                                             q.ldap, (const TS *)q.diag, B);
   return check_launch();
 }
 
 template <typename TS>
 static int launch_dir(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
-  k_pcg_dir<TS><<<sweep_blocks(q.ldr), kSweepThreads, 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
+  k_pcg_dir<TS><<<dir_grid<TS>(), kSweepThreads, 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
                                                          (const TS *)q.R, q.ldr, (const TS *)q.diag, B,
                                                          (bf16 *)q.P_lo, q.ld_lo);
   return check_launch();
@@ -574,6 +674,18 @@ static int iteration(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   else DLP_TRY(launch_apply<T_W32X64>(q, B, s));
   DLP_TRY(launch_update<double>(0, q, B, s));
   return launch_dir<double>(0, q, B, s);
+}
+
+// Fills the one-wave grid caches of the kernels iteration() launches, without launching.
+static int prime_grids(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  if (q.dtype == DLP_F32) {
+    (void)update_grid<float>();
+    (void)dir_grid<float>();
+    return q.w_lo ? launch_apply<T_BF16F>(q, B, s, false) : launch_apply<T_F32>(q, B, s, false);
+  }
+  (void)update_grid<double>();
+  (void)dir_grid<double>();
+  return q.w_dtype == DLP_F64 ? launch_apply<T_F64>(q, B, s, false) : launch_apply<T_W32X64>(q, B, s, false);
 }
 
 static int true_residual(const PcgProblem &q, cudaStream_t s) {
@@ -633,6 +745,7 @@ static int get_chunk_graph(const PcgProblem &q, const PcgBufs &B, int k, GraphRe
   if (dev < 0 || dev >= 64) return DLP_ERR_INVALID;
   if (!g_capture_stream[dev]) DLP_CUDA(cudaStreamCreateWithFlags(&g_capture_stream[dev], cudaStreamNonBlocking));
   cudaStream_t cs = g_capture_stream[dev];
+  DLP_TRY(prime_grids(q, B, cs));  // occupancy queries stay out of the capture
   DLP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   int st = DLP_OK;
   for (int i = 0; i < k && st == DLP_OK; ++i) st = iteration(q, B, cs);
@@ -677,7 +790,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
             double *relres_out, int32_t *status_out, dlp_stream_t stream, const void *w_lo, void *P_lo,
             int64_t ld_lo) {
   if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
-  if (ldr > (int64_t)upd_blocks() * kSweepThreads) return DLP_ERR_INVALID;
+  if (ldr > (int64_t)sm_count() * kSweepThreads) return DLP_ERR_INVALID;
   if ((w_lo || P_lo) && (!w_lo || !P_lo || ld_lo < C || dtype != DLP_F32)) return DLP_ERR_INVALID;
   if ((mode & 3) == 0 || mode > 7 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
@@ -771,11 +884,13 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
                        const void *diag, const void *H, int64_t ldh, int dtype, double *out, void *ws,
                        size_t ws_bytes, dlp_stream_t stream) {
   if (n < 0 || C <= 0 || ldr < C || (rhs && ldrhs < C) || !out || (n > 0 && (!R || !diag))) return DLP_ERR_INVALID;
-  if (ldr > (int64_t)upd_blocks() * kSweepThreads) return DLP_ERR_INVALID;
+  if (ldr > (int64_t)sm_count() * kSweepThreads) return DLP_ERR_INVALID;
   if (dtype != DLP_F32 && dtype != DLP_F64) return DLP_ERR_DTYPE;
   if (!ws || ws_bytes < dlp_residual_stats_workspace_bytes(C)) return DLP_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;
-  const int nb = upd_blocks();
+  static const int per32 = resident_per_sm(k_resid_stats<float>, kSweepThreads);
+  static const int per64 = resident_per_sm(k_resid_stats<double>, kSweepThreads);
+  const int nb = sm_count() * (dtype == DLP_F32 ? per32 : per64);  // one wave, <= upd_blocks()
   double *part = (double *)ws;
   if (dtype == DLP_F32)
     k_resid_stats<float><<<nb, kSweepThreads, 0, s>>>(n, C, (const float *)R, ldr, (const float *)rhs, ldrhs,
