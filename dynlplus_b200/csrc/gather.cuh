@@ -2,6 +2,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -77,15 +78,42 @@ constexpr int gather_batch_lean() {
   return VPL * VW * (int)(sizeof(TA) / 4) <= 8 ? 4 : VPL * VW * (int)(sizeof(TA) / 4) <= 16 ? 2 : 1;
 }
 
+// One 12-float row (three 16-byte vectors) at a 16-byte aligned address, in two loads: the row's
+// 32-byte aligned half goes through one 256-bit load (sm_100 ld.global.v8) and the other 16 bytes
+// through one 128-bit load. Same 48 bytes and the same two 32-byte sectors as three 128-bit loads,
+// with one load instruction fewer per gathered row. The values stay in load order: raw[0..1] hold
+// the 256-bit half and raw[2] the 128-bit part; with hi (the row starts 16 bytes into a 32-byte
+// sector) columns 0-3 are raw[2], 4-11 raw[0..1], else columns 0-7 are raw[0..1], 8-11 raw[2].
+__device__ __forceinline__ bool load_row12(const float *__restrict__ xr, float (&raw)[3][4]) {
+  const bool hi = ((uintptr_t)xr & 16u) != 0;
+  const float *p8 = xr + (hi ? 4 : 0);
+  const float *p4 = xr + (hi ? 0 : 8);
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(raw[0][0]), "=f"(raw[0][1]), "=f"(raw[0][2]), "=f"(raw[0][3]), "=f"(raw[1][0]), "=f"(raw[1][1]),
+        "=f"(raw[1][2]), "=f"(raw[1][3])
+      : "l"(p8));
+  const float4 f = __ldg(reinterpret_cast<const float4 *>(p4));
+  raw[2][0] = f.x;
+  raw[2][1] = f.y;
+  raw[2][2] = f.z;
+  raw[2][3] = f.w;
+  return hi;
+}
+
 // Sum over the stored entries of one row of w_j * X[col_j, :] for the lane's vectors, reduced
 // over the group's edge slots (every lane of the warp must call this: it shuffles). Each lane
 // takes its entries in batches of U: the U column indices and weights are loaded first, then the
 // U neighbour rows, then the U multiply-adds, so U row gathers are in flight per lane instead of
 // one. The per-lane accumulation order (entries beg+es, beg+es+ES, ...) is that of a plain loop.
-template <typename TW, typename TX, typename TA, int VW, int VPL, int U = gather_batch_wide<TA, VW, VPL>()>
+// ROW12 = true takes the two-load path of load_row12: fp32 rows of three 16-byte vectors (VW 4,
+// VPL 3) held whole by one lane (the caller guarantees LV == 1, NV == 3); false the per-vector loads.
+template <typename TW, typename TX, typename TA, int VW, int VPL, int U = gather_batch_wide<TA, VW, VPL>(),
+          bool ROW12 = false>
 __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, const TW *__restrict__ w,
                                            const TX *__restrict__ X, int64_t ldx, int beg, int end, int es,
                                            int ES, int cl, int LV, int NV, int G, TA (&acc)[VPL][VW]) {
+  static_assert(!ROW12 || (std::is_same<TX, float>::value && std::is_same<TA, float>::value && VW == 4 && VPL == 3),
+                "the two-load path gathers fp32 rows of three 16-byte vectors");
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
@@ -100,26 +128,49 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
       wv[u] = j < end ? cvt<TA>(ld_stream(w + j)) : TA(0);
     }
     TA t[U][VPL][VW];
+    bool hi[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const TX *xr = X + (long long)(v[u] < 0 ? 0 : v[u]) * ldx;
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        const int vi = cl + k * LV;
-        if (v[u] >= 0 && vi < NV) {
-          load_vec<TX, VW, TA>(xr + (long long)vi * VW, t[u][k]);
+      hi[u] = false;
+      if constexpr (ROW12) {
+        if (v[u] >= 0) {
+          hi[u] = load_row12(xr, t[u]);
         } else {
 #pragma unroll
-          for (int i = 0; i < VW; ++i) t[u][k][i] = TA(0);
+          for (int k = 0; k < VPL; ++k)
+#pragma unroll
+            for (int i = 0; i < VW; ++i) t[u][k][i] = TA(0);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < VPL; ++k) {
+          const int vi = cl + k * LV;
+          if (v[u] >= 0 && vi < NV) {
+            load_vec<TX, VW, TA>(xr + (long long)vi * VW, t[u][k]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < VW; ++i) t[u][k][i] = TA(0);
+          }
         }
       }
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+    for (int u = 0; u < U; ++u) {
+      if constexpr (ROW12) {  // columns from the load order of load_row12
 #pragma unroll
-      for (int k = 0; k < VPL; ++k)
+        for (int i = 0; i < VW; ++i) {
+          acc[0][i] = fmaa(wv[u], hi[u] ? t[u][2][i] : t[u][0][i], acc[0][i]);
+          acc[1][i] = fmaa(wv[u], hi[u] ? t[u][0][i] : t[u][1][i], acc[1][i]);
+          acc[2][i] = fmaa(wv[u], hi[u] ? t[u][1][i] : t[u][2][i], acc[2][i]);
+        }
+      } else {
 #pragma unroll
-        for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv[u], t[u][k][i], acc[k][i]);
+        for (int k = 0; k < VPL; ++k)
+#pragma unroll
+          for (int i = 0; i < VW; ++i) acc[k][i] = fmaa(wv[u], t[u][k][i], acc[k][i]);
+      }
+    }
   }
   for (int off = LV; off < G; off <<= 1) {
 #pragma unroll

@@ -168,7 +168,10 @@ constexpr int apply_min_blocks() {
   return (sizeof(typename T::TA) == 4 && VPL * VW <= 12 && VPL <= 4) ? 4 : 1;
 }
 
-template <class T, int VW, int VPL>
+// ROW12 as in gather_row: fp32 12-float rows held whole by one lane, two loads per row, one row in
+// flight per lane (measured on B200 at n = 1M, degree 10, C = 9: 150 us against 166 us for two rows
+// in flight, which spill under the 64-register cap, and 160 us for per-vector loads).
+template <class T, int VW, int VPL, bool ROW12 = false>
 __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_pcg_apply(ApplyArgs<T> p) {
   using TA = typename T::TA;
   PcgCtl *ctl = p.B.ctl;
@@ -198,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, gather_batch_lean<TA, VW, VPL>()>(
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 1 : gather_batch_lean<TA, VW, VPL>()), ROW12>(
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);
@@ -638,7 +641,12 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, b
     DLP_APPLY_ONE(VW_, 8)                                                               \
     default: return DLP_ERR_INVALID;                                                    \
   }
-  if (L.VW == 1) {
+  constexpr bool row12 = std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value;
+  if (row12 && L.VW == 4 && L.VPL == 3 && L.LV == 1) {
+    // fp32 rows of 12 floats held whole by one lane: the two-load gather (load_row12)
+    static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, row12>, kThreads);
+    if (launch) k_pcg_apply<T, VWV, 3, row12><<<sm_count() * per, kThreads, 0, s>>>(a);
+  } else if (L.VW == 1) {
     DLP_APPLY_CASE(1)
   } else {
     DLP_APPLY_CASE(VWV)
