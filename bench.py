@@ -50,6 +50,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-budget-s", type=float, default=150.0, help="wall budget of the CPU reference legs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch the PCG kernels one by one instead of as a CUDA graph (for kernel profilers)")
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
     ap.add_argument("--workload", default="edge-stream",
                     choices=["edge-stream", "static", "amg", "batched", "serving"],
@@ -585,6 +587,9 @@ def wl_serving(a):
 
 def main(argv=None):
     a = parse(argv)
+    if a.no_graphs:
+        from dynlplus_b200 import solvers
+        solvers.GRAPHS = False
     if a.impl == "reference":
         return reference_arm(a)
     if a.workload != "edge-stream":

@@ -150,9 +150,14 @@ def bf16_weights(W):
 # event, iterations, n, C) recorded on the launching stream (a profiler hook; None = off).
 PCG_EVENTS = None
 
+# Default of pcg(use_graph=None): run the PCG iteration loop as a CUDA graph (True), or launch its
+# kernels one by one (False: the same kernels, for kernel-level profilers that do not follow graph
+# control flow).
+GRAPHS = True
+
 
 def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400, *, target_relres=None,
-        rhs_norm=None, check_every=8, use_graph=True, lowp=False, zero_start=False):
+        rhs_norm=None, check_every=8, use_graph=None, lowp=False, zero_start=False):
     """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
 
     Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
@@ -198,7 +203,8 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
         ev[0].record()
     _lib.call("dlp_pcg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C, ptr(diag),
               ptr(rhs), ld(rhs), ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), code(Z), eps_h, rn,
-              float(target_relres or 0.0), mode, int(max_iter), int(patience), int(check_every), int(bool(use_graph)),
+              float(target_relres or 0.0), mode, int(max_iter), int(patience), int(check_every),
+              int(bool(GRAPHS if use_graph is None else use_graph)),
               W.nnz / max(n, 1), ptr(ws), ws.numel(), ct.byref(it), ct.byref(viol), ct.byref(rel), ct.byref(status),
               stream(), ptr(w_lo), ptr(P_lo), ld(P_lo) if P_lo is not None else 0)
     if ev is not None:

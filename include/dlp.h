@@ -208,8 +208,12 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
  * stop is confirmed on the true residual rhs - A Z (solvers.py:85-89); `patience` iterations
  * without a 10% improvement stop the solve as the reference's stall rule does (:90-92).
  * eps and rhs_norm are HOST arrays of C doubles (rhs_norm may be NULL when bit 1 is unused).
- * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual). The chunk of
- * check_every iterations is replayed as a CUDA graph when use_graph != 0 (cached per problem).
+ * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual). With
+ * use_graph != 0 the iteration loop runs on the device as one CUDA graph with a conditional WHILE
+ * node (cached per problem; the host reads the control block once per loop and once per recheck);
+ * where conditional nodes are unavailable, chunks of check_every iterations are replayed as graphs.
+ * use_graph == 0 launches the kernels directly and reads the control block every check_every
+ * iterations.
  * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap,
  * 4 breakdown (a non-finite residual entry). eps may be NULL when bit 0 is unused.
  * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C).
