@@ -100,6 +100,25 @@ __device__ __forceinline__ bool load_row12(const float *__restrict__ xr, float (
   return hi;
 }
 
+// Store counterpart of load_row12: the 12 values v (columns 0-11) of a row at a 16-byte aligned
+// address in one 256-bit store (the 32-byte aligned half) and one 128-bit store.
+__device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {
+  const bool hi = ((uintptr_t)yr & 16u) != 0;
+  float *p8 = yr + (hi ? 4 : 0);
+  float *p4 = yr + (hi ? 0 : 8);
+  float e[8], g[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    e[i] = hi ? v[1][i] : v[0][i];
+    e[4 + i] = hi ? v[2][i] : v[1][i];
+    g[i] = hi ? v[0][i] : v[2][i];
+  }
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p8), "f"(e[0]), "f"(e[1]), "f"(e[2]),
+               "f"(e[3]), "f"(e[4]), "f"(e[5]), "f"(e[6]), "f"(e[7])
+               : "memory");
+  *reinterpret_cast<float4 *>(p4) = make_float4(g[0], g[1], g[2], g[3]);
+}
+
 // Sum over the stored entries of one row of w_j * X[col_j, :] for the lane's vectors, reduced
 // over the group's edge slots (every lane of the warp must call this: it shuffles). Each lane
 // takes its entries in batches of U: the U column indices and weights are loaded first, then the

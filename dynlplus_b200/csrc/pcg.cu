@@ -165,6 +165,7 @@ struct ApplyArgs {
   int G, LV, NV;
   const typename T::TV *Pown;  // own-row P for the diagonal term and pAp (NULL: P itself)
   int64_t ldpo;
+  int ap_row12;  // AP rows are 16-byte aligned and >= 12 wide: whole-row vector stores (two-load path)
 };
 
 // Small fp32 rows fit in 64 registers (4 blocks of 256 threads per SM); the wider or fp64 ones keep
@@ -211,18 +212,39 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);
+      if constexpr (ROW12) {
+        // the own row in two loads too (its 48 bytes are 16-byte aligned, as for every gathered row)
+        float pw[3][4];
+        const bool hi = load_row12(p.P + r * p.ldp, pw);
+        float apv[3][4];
 #pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        const int vi = cl + k * LV;
-        if (vi < NV) {
+        for (int k = 0; k < 3; ++k)
 #pragma unroll
-          for (int i = 0; i < VW; ++i) {
-            const int c = vi * VW + i;
+          for (int i = 0; i < 4; ++i) {
+            const int c = k * 4 + i;
+            const float pv = k == 0 ? (hi ? pw[2][i] : pw[0][i]) : k == 1 ? (hi ? pw[0][i] : pw[1][i])
+                                                                        : (hi ? pw[1][i] : pw[2][i]);
+            apv[k][i] = d * pv - acc[k][i];  // padding columns too when the whole row is stored
             if (c < p.C) {
-              const TA pv = p.Pown ? cvt<TA>(p.Pown[r * p.ldpo + c]) : cvt<TA>(p.P[r * p.ldp + c]);
-              const TA ap = d * pv - acc[k][i];
-              p.AP[r * p.ldap + c] = cvt<typename T::TY>(ap);
-              dot[k][i] += (double)pv * (double)ap;
+              if (!p.ap_row12) p.AP[r * p.ldap + c] = apv[k][i];
+              dot[k][i] += (double)pv * (double)apv[k][i];
+            }
+          }
+        if (p.ap_row12) store_row12(p.AP + r * p.ldap, apv);
+      } else {
+#pragma unroll
+        for (int k = 0; k < VPL; ++k) {
+          const int vi = cl + k * LV;
+          if (vi < NV) {
+#pragma unroll
+            for (int i = 0; i < VW; ++i) {
+              const int c = vi * VW + i;
+              if (c < p.C) {
+                const TA pv = p.Pown ? cvt<TA>(p.Pown[r * p.ldpo + c]) : cvt<TA>(p.P[r * p.ldp + c]);
+                const TA ap = d * pv - acc[k][i];
+                p.AP[r * p.ldap + c] = cvt<typename T::TY>(ap);
+                dot[k][i] += (double)pv * (double)ap;
+              }
             }
           }
         }
@@ -335,39 +357,46 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
   if (ix.on) {
     const int c = ix.c;
     const T al = phase == 0 ? (T)B.alpha[c] : T(0);
-    const double einv = B.epsinv[c];
     // element offsets advance by addition (no 64-bit multiply per element)
     const long long rstep = ix.RS * ldr, astep = ix.RS * ldap;
     long long offr = ix.r0 * ldr + c, offa = ix.r0 * ldap + c;
-    for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
+    double rmax = 0.0;  // max |R| / diag; the column's 1/eps scales it once at the end
+    auto element = [&](T rv, T ap, T dv, long long o) {
+      if (phase == 0) {
+        rv = rv - al * ap;
+        R[o] = rv;
+      }
+      const double r64 = (double)rv;
+      const double dinv = __drcp_rn((double)dv);  // correctly rounded: the value of 1.0 / d
+      const double r2 = r64 * r64;
+      rz += r2 * dinv;
+      ss += r2;
+      rmax = fmax(rmax, fabs(r64) * dinv);
+    };
+    long long r = ix.r0;
+    // full batches: kSweepUnroll rows in range, every load issued before any is used
+    for (; r + (kSweepUnroll - 1) * ix.RS < n; r += kSweepUnroll * ix.RS) {
       T rv[kSweepUnroll], ap[kSweepUnroll], dv[kSweepUnroll];
 #pragma unroll
       for (int u = 0; u < kSweepUnroll; ++u) {
-        const long long rr = r + u * ix.RS;
-        const bool ok = rr < n;
-        rv[u] = ok ? R[offr + u * rstep] : T(0);
-        dv[u] = ok ? diag[rr] : T(1);
-        ap[u] = (ok && phase == 0) ? AP[offa + u * astep] : T(0);
+        rv[u] = R[offr + u * rstep];
+        dv[u] = diag[r + u * ix.RS];
+        ap[u] = phase == 0 ? AP[offa + u * astep] : T(0);
       }
 #pragma unroll
-      for (int u = 0; u < kSweepUnroll; ++u) {
-        const long long rr = r + u * ix.RS;
-        if (rr < n) {
-          if (phase == 0) {
-            rv[u] = rv[u] - al * ap[u];
-            R[offr + u * rstep] = rv[u];
-          }
-          const double r64 = (double)rv[u];
-          const double dinv = __drcp_rn((double)dv[u]);  // correctly rounded: the value of 1.0 / d
-          bad |= !isfinite(r64);
-          rz += r64 * r64 * dinv;
-          ss += r64 * r64;
-          vmax = fmax(vmax, fabs(r64) * dinv * einv);
-        }
-      }
+      for (int u = 0; u < kSweepUnroll; ++u) element(rv[u], ap[u], dv[u], offr + u * rstep);
       offr += kSweepUnroll * rstep;
       offa += kSweepUnroll * astep;
     }
+    for (; r < n; r += ix.RS) {  // the last rows, one at a time
+      element(R[offr], phase == 0 ? AP[offa] : T(0), diag[r], offr);
+      offr += rstep;
+      offa += astep;
+    }
+    // a non-finite entry makes the fp64 sum of squares non-finite (fp32 squares cannot overflow it)
+    bad = !isfinite(ss);
+    // rounding is monotone, so scaling the max equals the max of the scaled ratios
+    vmax = rmax * B.epsinv[c];
   }
   if (bad) ctl->bad = 1;
   const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
@@ -637,7 +666,8 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, b
   DLP_TRY(choose_layout(q.C, sizeof(typename T::TX), X, ldx, 0, q.avg_deg, &L));
   ApplyArgs<T> a{q.rbeg, q.rend, q.col, (const typename T::TW *)(lo ? q.w_lo : q.w), q.n, q.C,
                  (const typename T::TX *)X, ldx, (const typename T::TV *)q.diag, (typename T::TY *)q.AP, q.ldap, B,
-                 L.G, L.LV, L.NV, lo ? (const typename T::TV *)q.P : nullptr, q.ldp};
+                 L.G, L.LV, L.NV, lo ? (const typename T::TV *)q.P : nullptr, q.ldp,
+                 (int)(q.ldap >= 12 && q.ldap % 4 == 0 && (uintptr_t)q.AP % 16 == 0)};
   constexpr int VWV = 16 / sizeof(typename T::TX);
   // launch == false only fills the one-wave grid cache (outside stream capture)
 #define DLP_APPLY_ONE(VW_, VPL_)                                                        \

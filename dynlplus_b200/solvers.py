@@ -177,7 +177,9 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
         raise TypeError("fp32 PCG needs fp32 weights")
     R = _scratch("pcg_R", n, C, dt, dev)
     P = _scratch("pcg_P", n, C, dt, dev, padded=True)
-    AP = _scratch("pcg_AP", n, C, dt, dev)
+    # padded like P: the apply writes whole 16-byte aligned rows (two vector stores per row for
+    # fp32 rows of 9-12 columns) instead of one scalar store per column
+    AP = _scratch("pcg_AP", n, C, dt, dev, padded=True)
     eps_h = (ct.c_double * C)(*[float(e) for e in eps]) if eps is not None else None
     mode = 1 if eps is not None else 0
     rn = None
