@@ -100,6 +100,28 @@ __device__ __forceinline__ bool load_row12(const float *__restrict__ xr, float (
   return hi;
 }
 
+// fp64 counterpart: one 10-double row (five 16-byte vectors) at a 16-byte aligned address in three
+// loads (two 256-bit, one 128-bit) instead of five 128-bit ones; the same 80 bytes and sectors. raw in
+// load order (flat f = 2 k + i): f 0-3 and 4-7 the two 256-bit loads, f 8-9 the 128-bit one. Without
+// hi the row's columns are f 0-9 in order; with hi (the row starts 16 bytes into a 32-byte sector)
+// columns 0-1 are f 8-9 and columns 2-9 are f 0-7.
+__device__ __forceinline__ bool load_row10d(const double *__restrict__ xr, double (&raw)[5][2]) {
+  const bool hi = ((uintptr_t)xr & 16u) != 0;
+  const double *pa = xr + (hi ? 2 : 0);
+  const double *pb = xr + (hi ? 6 : 4);
+  const double *pg = xr + (hi ? 0 : 8);
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(raw[0][0]), "=d"(raw[0][1]), "=d"(raw[1][0]), "=d"(raw[1][1])
+      : "l"(pa));
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(raw[2][0]), "=d"(raw[2][1]), "=d"(raw[3][0]), "=d"(raw[3][1])
+      : "l"(pb));
+  const double2 g = __ldg(reinterpret_cast<const double2 *>(pg));
+  raw[4][0] = g.x;
+  raw[4][1] = g.y;
+  return hi;
+}
+
 // Store counterpart of load_row12: the 12 values v (columns 0-11) of a row at a 16-byte aligned
 // address in one 256-bit store (the 32-byte aligned half) and one 128-bit store.
 __device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {
@@ -124,15 +146,23 @@ __device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {
 // takes its entries in batches of U: the U column indices and weights are loaded first, then the
 // U neighbour rows, then the U multiply-adds, so U row gathers are in flight per lane instead of
 // one. The per-lane accumulation order (entries beg+es, beg+es+ES, ...) is that of a plain loop.
-// ROW12 = true takes the two-load path of load_row12: fp32 rows of three 16-byte vectors (VW 4,
-// VPL 3) held whole by one lane (the caller guarantees LV == 1, NV == 3); false the per-vector loads.
+// How a lane reads a gathered row: kRowVec one 16-byte vector at a time (VPL per lane, LV lanes per
+// row); kRow12F the two loads of load_row12 (fp32 rows of three 16-byte vectors: VW 4, VPL 3) and
+// kRow10D the three loads of load_row10d (fp64 rows of five: VW 2, VPL 5), each with the whole row
+// held by one lane (the caller guarantees LV == 1).
+enum RowPath : int { kRowVec = 0, kRow12F = 1, kRow10D = 2 };
+
 template <typename TW, typename TX, typename TA, int VW, int VPL, int U = gather_batch_wide<TA, VW, VPL>(),
-          bool ROW12 = false>
+          int ROW = kRowVec>
 __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, const TW *__restrict__ w,
                                            const TX *__restrict__ X, int64_t ldx, int beg, int end, int es,
                                            int ES, int cl, int LV, int NV, int G, TA (&acc)[VPL][VW]) {
-  static_assert(!ROW12 || (std::is_same<TX, float>::value && std::is_same<TA, float>::value && VW == 4 && VPL == 3),
+  static_assert(ROW != kRow12F ||
+                    (std::is_same<TX, float>::value && std::is_same<TA, float>::value && VW == 4 && VPL == 3),
                 "the two-load path gathers fp32 rows of three 16-byte vectors");
+  static_assert(ROW != kRow10D ||
+                    (std::is_same<TX, double>::value && std::is_same<TA, double>::value && VW == 2 && VPL == 5),
+                "the three-load path gathers fp64 rows of five 16-byte vectors");
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
@@ -152,9 +182,10 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
     for (int u = 0; u < U; ++u) {
       const TX *xr = X + (long long)(v[u] < 0 ? 0 : v[u]) * ldx;
       hi[u] = false;
-      if constexpr (ROW12) {
+      if constexpr (ROW != kRowVec) {
         if (v[u] >= 0) {
-          hi[u] = load_row12(xr, t[u]);
+          if constexpr (ROW == kRow12F) hi[u] = load_row12(xr, t[u]);
+          else hi[u] = load_row10d(xr, t[u]);
         } else {
 #pragma unroll
           for (int k = 0; k < VPL; ++k)
@@ -176,12 +207,18 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      if constexpr (ROW12) {  // columns from the load order of load_row12
+      if constexpr (ROW == kRow12F) {  // columns from the load order of load_row12
 #pragma unroll
         for (int i = 0; i < VW; ++i) {
           acc[0][i] = fmaa(wv[u], hi[u] ? t[u][2][i] : t[u][0][i], acc[0][i]);
           acc[1][i] = fmaa(wv[u], hi[u] ? t[u][0][i] : t[u][1][i], acc[1][i]);
           acc[2][i] = fmaa(wv[u], hi[u] ? t[u][1][i] : t[u][2][i], acc[2][i]);
+        }
+      } else if constexpr (ROW == kRow10D) {  // columns from the load order of load_row10d
+#pragma unroll
+        for (int c = 0; c < 10; ++c) {
+          const int fh = c < 2 ? 8 + c : c - 2;
+          acc[c / 2][c % 2] = fmaa(wv[u], hi[u] ? t[u][fh / 2][fh % 2] : t[u][c / 2][c % 2], acc[c / 2][c % 2]);
         }
       } else {
 #pragma unroll

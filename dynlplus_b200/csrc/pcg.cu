@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 1 : gather_batch_lean<TA, VW, VPL>()), ROW12>(
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 1 : gather_batch_lean<TA, VW, VPL>()),
+               (ROW12 ? kRow12F : kRowVec)>(
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);

@@ -69,10 +69,10 @@ struct SpmmArgs {
   int64_t ldxo;
 };
 
-// ROW12 as in gather_row, with two rows in flight per lane (measured on B200 at n = 1M, degree 10,
-// C = 9: 133 us against 137 us for per-vector loads with four in flight and 157 us for the two-load
-// path with four).
-template <class T, int VW, int VPL, bool ROW12 = false>
+// ROW as in gather_row. kRow12F runs with two rows in flight per lane (measured on B200 at n = 1M,
+// degree 10, C = 9: 133 us against 137 us for per-vector loads with four in flight and 157 us for the
+// two-load path with four).
+template <class T, int VW, int VPL, int ROW = kRowVec>
 __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
   using TA = typename T::TA;
   using TX = typename T::TX;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, TX, TA, VW, VPL, (ROW12 ? 2 : gather_batch_wide<TA, VW, VPL>()), ROW12>(
+    gather_row<typename T::TW, TX, TA, VW, VPL, (ROW == kRow12F ? 2 : gather_batch_wide<TA, VW, VPL>()), ROW>(
         p.col, p.w, p.X, p.ldx, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
       const long long orow = p.compact ? gi : (long long)r;
@@ -124,18 +124,26 @@ static int launch_spmm_vw(const SpmmArgs<T> &a, int VPL, dlp_stream_t s) {
   const int grid = grid_for(a.n_rows, a.G);
   constexpr bool kRow12 =
       VW == 4 && std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value;
+  constexpr bool kRow10 =
+      VW == 2 && std::is_same<typename T::TX, double>::value && std::is_same<typename T::TA, double>::value;
   switch (VPL) {
     case 1: k_spmm<T, VW, 1><<<grid, kThreads, 0, (cudaStream_t)s>>>(a); break;
     case 2: k_spmm<T, VW, 2><<<grid, kThreads, 0, (cudaStream_t)s>>>(a); break;
     case 3:
       if (kRow12 && a.LV == 1) {  // fp32 12-float rows held whole by one lane: two loads per row
-        k_spmm<T, VW, 3, kRow12><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
+        k_spmm<T, VW, 3, (kRow12 ? kRow12F : kRowVec)><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
       } else {
         k_spmm<T, VW, 3><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
       }
       break;
     case 4: k_spmm<T, VW, 4><<<grid, kThreads, 0, (cudaStream_t)s>>>(a); break;
     case 8: k_spmm<T, VW, 8><<<grid, kThreads, 0, (cudaStream_t)s>>>(a); break;
+    case 5:  // fp64 10-double rows held whole by one lane (run_spmm): three loads per row
+      if constexpr (kRow10) {
+        k_spmm<T, VW, 5, kRow10D><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
+        break;
+      }
+      return DLP_ERR_INVALID;
     default: return DLP_ERR_INVALID;
   }
   return check_launch();
@@ -148,6 +156,14 @@ static int run_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col
                     int32_t group, double avg_deg, dlp_stream_t s, const void *Xo = nullptr, int64_t ldxo = 0) {
   Layout L;
   DLP_TRY(choose_layout(C, sizeof(typename T::TX), X, ldx, group, avg_deg, &L));
+  if (std::is_same<typename T::TX, double>::value && std::is_same<typename T::TA, double>::value && L.VW == 2 &&
+      L.NV == 5) {
+    // fp64 rows of five 16-byte vectors (9-10 columns): one lane holds the whole row and reads it in
+    // three loads (load_row10d); the edge slots per row stay as chosen
+    L.G /= L.LV;
+    L.LV = 1;
+    L.VPL = 5;
+  }
   SpmmArgs<T> p{rbeg, rend, col, (const typename T::TW *)w, n_rows, rows, C, (const typename T::TX *)X, ldx,
                 (const typename T::TV *)a, alpha, b, (const typename T::TV *)RHS, ldr, cr,
                 (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV, (const typename T::TV *)Xo, ldxo};
