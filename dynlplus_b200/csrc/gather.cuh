@@ -122,6 +122,34 @@ __device__ __forceinline__ bool load_row10d(const double *__restrict__ xr, doubl
   return hi;
 }
 
+// Column c (0-9) of a row read by load_row10d.
+__device__ __forceinline__ double row10_col(const double (&raw)[5][2], bool hi, int c) {
+  const int fh = c < 2 ? 8 + c : c - 2;  // c is a compile-time index at every (unrolled) call
+  return hi ? raw[fh / 2][fh % 2] : raw[c / 2][c % 2];
+}
+
+// Store counterpart of load_row10d: the 10 values v of a row at a 16-byte aligned address in two
+// 256-bit stores and one 128-bit store.
+__device__ __forceinline__ void store_row10d(double *yr, const double (&v)[10]) {
+  const bool hi = ((uintptr_t)yr & 16u) != 0;
+  double *pa = yr + (hi ? 2 : 0);
+  double *pb = yr + (hi ? 6 : 4);
+  double *pg = yr + (hi ? 0 : 8);
+  double A[4], B[4], G[2];  // selects between fixed indices keep v in registers
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    A[k] = hi ? v[2 + k] : v[k];
+    B[k] = hi ? v[6 + k] : v[4 + k];
+  }
+  G[0] = hi ? v[0] : v[8];
+  G[1] = hi ? v[1] : v[9];
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(pa), "d"(A[0]), "d"(A[1]), "d"(A[2]), "d"(A[3])
+               : "memory");
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(pb), "d"(B[0]), "d"(B[1]), "d"(B[2]), "d"(B[3])
+               : "memory");
+  *reinterpret_cast<double2 *>(pg) = make_double2(G[0], G[1]);
+}
+
 // Store counterpart of load_row12: the 12 values v (columns 0-11) of a row at a 16-byte aligned
 // address in one 256-bit store (the 32-byte aligned half) and one 128-bit store.
 __device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {

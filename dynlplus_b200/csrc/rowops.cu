@@ -67,6 +67,9 @@ struct SpmmArgs {
   int G, LV, NV;
   const typename T::TV *Xo;  // own-row values for the a-term (NULL: X itself)
   int64_t ldxo;
+  // kRow10D epilogue: the own row, the RHS row and the Y row are read / written whole (three
+  // accesses each) when their rows are 16-byte aligned and hold 10 values
+  int own10, rhs10, y10;
 };
 
 // ROW as in gather_row. kRow12F runs with two rows in flight per lane (measured on B200 at n = 1M,
@@ -94,6 +97,48 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
     TA acc[VPL][VW];
     gather_row<typename T::TW, TX, TA, VW, VPL, (ROW == kRow12F ? 2 : gather_batch_wide<TA, VW, VPL>()), ROW>(
         p.col, p.w, p.X, p.ldx, beg, end, es, ES, cl, LV, NV, G, acc);
+    if constexpr (ROW == kRow10D) {
+      if (valid && es == 0) {  // same arithmetic, in the same order, as the per-column epilogue below
+        const long long orow = p.compact ? gi : (long long)r;
+        const double av = p.a ? (double)p.alpha * (double)p.a[r] : 0.0;
+        double yv[10];  // terms added one row at a time: each row read just before its use
+#pragma unroll
+        for (int c = 0; c < 10; ++c) yv[c] = (double)p.b * acc[c / 2][c % 2];
+        if (p.a) {
+          if (p.own10) {
+            double xo[5][2];
+            const bool hx = load_row10d(p.Xo ? p.Xo + (long long)r * p.ldxo : p.X + (long long)r * p.ldx, xo);
+#pragma unroll
+            for (int c = 0; c < 10; ++c) yv[c] = fmaa(av, row10_col(xo, hx, c), yv[c]);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 10; ++c)
+              if (c < p.C)
+                yv[c] = fmaa(av, p.Xo ? p.Xo[(long long)r * p.ldxo + c] : p.X[(long long)r * p.ldx + c], yv[c]);
+          }
+        }
+        if (p.rhs) {
+          if (p.rhs10) {
+            double rh[5][2];
+            const bool hr = load_row10d(p.rhs + (long long)r * p.ldr, rh);
+#pragma unroll
+            for (int c = 0; c < 10; ++c) yv[c] += (double)p.cr * row10_col(rh, hr, c);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 10; ++c)
+              if (c < p.C) yv[c] += (double)p.cr * p.rhs[(long long)r * p.ldr + c];
+          }
+        }
+        if (p.y10) {
+          store_row10d(p.Y + orow * p.ldy, yv);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 10; ++c)
+            if (c < p.C) p.Y[orow * p.ldy + c] = yv[c];
+        }
+      }
+      continue;
+    }
     if (valid && es == 0) {
       const long long orow = p.compact ? gi : (long long)r;
       const TA av = p.a ? (TA)p.alpha * cvt<TA>(p.a[r]) : TA(0);
@@ -166,7 +211,13 @@ static int run_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col
   }
   SpmmArgs<T> p{rbeg, rend, col, (const typename T::TW *)w, n_rows, rows, C, (const typename T::TX *)X, ldx,
                 (const typename T::TV *)a, alpha, b, (const typename T::TV *)RHS, ldr, cr,
-                (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV, (const typename T::TV *)Xo, ldxo};
+                (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV, (const typename T::TV *)Xo, ldxo, 0, 0, 0};
+  if (L.VPL == 5 && L.LV == 1) {  // the kRow10D layout chosen above: whole-row epilogue where aligned
+    auto rows10 = [](const void *q, int64_t ldq) { return q && (uintptr_t)q % 16 == 0 && ldq % 2 == 0 && ldq >= 10; };
+    p.own10 = Xo ? rows10(Xo, ldxo) : 1;
+    p.rhs10 = rows10(RHS, ldr);
+    p.y10 = rows10(Y, ldy);
+  }
   constexpr int VWV = 16 / sizeof(typename T::TX);
   if (L.VW == 1) return launch_spmm_vw<T, 1>(p, L.VPL, s);
   return launch_spmm_vw<T, VWV>(p, L.VPL, s);

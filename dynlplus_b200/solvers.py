@@ -71,7 +71,10 @@ def apply_A(sys: System, X):
 
 
 def residual(sys: System, X, rhs, out=None, rows=None):
-    """rhs - A X in one fused pass (fp64 when X is fp64)."""
+    """rhs - A X in one fused pass (fp64 when X is fp64). A full residual it allocates has 16-byte
+    aligned padded rows, which the SpMM writes whole."""
+    if out is None and rows is None:
+        out = padded_empty(X.shape[0], X.shape[1], X.dtype, X.device)
     return kernels.spmm_axpy(sys.W, X, a=sys.diag.to(X.dtype), alpha=-1.0, b=1.0, rhs=rhs, out=out, rows=rows)
 
 
