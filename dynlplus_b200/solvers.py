@@ -698,7 +698,8 @@ class IncrementalLP(DynLPPlus):
     def _park(self, s64, rows):
         if rows is not None and rows.numel():
             h0 = float(self.hmax or 1.0)
-            _lib.call("dlp_park_rows", ptr(rows), int(rows.numel()), ptr(s64.solved.to(torch.uint8)), self.C, 1,
+            sol = s64.solved.view(torch.uint8) if s64.solved.dtype == torch.bool else s64.solved.to(torch.uint8)
+            _lib.call("dlp_park_rows", ptr(rows), int(rows.numel()), ptr(sol), self.C, 1,
                       ptr(s64.prior.to(F64).contiguous()), h0, ptr(self.Z), ld(self.Z), ptr(self.R), ld(self.R),
                       stream())
 

@@ -504,10 +504,11 @@ class EdgeStream:
     def system(self) -> System:
         """Global-index system of the current batch (arrays live until the next batch)."""
         n, C, dev = self.n, self.C, self.dev
-        um = self.umask.bool()
+        um = self.umask.view(torch.bool)  # 0/1 bytes: a view, no conversion kernel
         if getattr(self, "_s64", None) is None:
             self._s64 = torch.empty(n, dtype=torch.float64, device=dev)
             self._ids = torch.arange(n, device=dev)
+            self._no_new = torch.zeros(n, dtype=torch.bool, device=dev)
         s64 = torch.sub(self.diag64, self.rowsum, out=self._s64)
         # active and ungrounded counts change only with vertex batches or membership changes
         if getattr(self, "_counts", None) is None:
@@ -515,14 +516,16 @@ class EdgeStream:
         n_active, n_ungrounded = self._counts
         vx = getattr(self, "_vertex_batch", None)
         common = dict(t=self.t, U=self._ids, W=self.solver_csr(),
-                      is_new=vx["is_new"] if vx else torch.zeros(n, dtype=torch.bool, device=dev),
-                      seed=vx["seed"] if vx else self.changed.bool(), comps=vx["comps"] if vx else {}, K=self.K, C=C,
+                      is_new=vx["is_new"] if vx else self._no_new,
+                      seed=vx["seed"] if vx else self.changed.view(torch.bool), comps=vx["comps"] if vx else {}, K=self.K,
+                      C=C,
                       eta=self.eta,
                       n_inserted=self.n_ins, n_deleted=self.n_del, n_active=int(n_active),
                       n_ungrounded=int(n_ungrounded), solved=um,
                       changed=self.last_changed, moved=self.last_moved)
         ch = C + (1 if self.with_h else 0)
-        S = System(s=s64.to(self.dtype), diag=self.diag32 if self.dtype == torch.float32 else self.diag64.to(self.dtype),
+        # the grounding stays fp64 in every precision (its one reader, the AMG setup, works in fp64)
+        S = System(s=s64, diag=self.diag32 if self.dtype == torch.float32 else self.diag64.to(self.dtype),
                    B=self.B, rhs=self.rhs32[:, :C] if self.dtype == torch.float32 else self.rhs64[:, :C].to(self.dtype),
                    prior=self.prior64.to(self.dtype), rhs_h=self.rhs32[:, :ch] if self.dtype == torch.float32 else None,
                    **common)
