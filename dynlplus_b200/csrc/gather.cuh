@@ -128,26 +128,31 @@ __device__ __forceinline__ double row10_col(const double (&raw)[5][2], bool hi, 
   return hi ? raw[fh / 2][fh % 2] : raw[c / 2][c % 2];
 }
 
-// Store counterpart of load_row10d: the 10 values v of a row at a 16-byte aligned address in two
-// 256-bit stores and one 128-bit store.
+// Store counterpart of load_row10d: the values v of a row of 16-byte aligned address yr, exactly its
+// first 10 (FULL) or 9 doubles, nothing beyond. 10: two 256-bit stores and one 128-bit store. 9
+// (where the tenth slot may belong to the caller): one 256-bit, two 128-bit and one 64-bit store.
+template <bool FULL>
 __device__ __forceinline__ void store_row10d(double *yr, const double (&v)[10]) {
   const bool hi = ((uintptr_t)yr & 16u) != 0;
-  double *pa = yr + (hi ? 2 : 0);
-  double *pb = yr + (hi ? 6 : 4);
-  double *pg = yr + (hi ? 0 : 8);
-  double A[4], B[4], G[2];  // selects between fixed indices keep v in registers
+  double A[4];  // selects between fixed indices keep v in registers
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    A[k] = hi ? v[2 + k] : v[k];
-    B[k] = hi ? v[6 + k] : v[4 + k];
-  }
-  G[0] = hi ? v[0] : v[8];
-  G[1] = hi ? v[1] : v[9];
+  for (int k = 0; k < 4; ++k) A[k] = hi ? v[2 + k] : v[k];
+  double *pa = yr + (hi ? 2 : 0);
   asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(pa), "d"(A[0]), "d"(A[1]), "d"(A[2]), "d"(A[3])
                : "memory");
-  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(pb), "d"(B[0]), "d"(B[1]), "d"(B[2]), "d"(B[3])
-               : "memory");
-  *reinterpret_cast<double2 *>(pg) = make_double2(G[0], G[1]);
+  if constexpr (FULL) {  // hi: 0-1, 2-5, 6-9   else: 0-3, 4-7, 8-9
+    double B[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) B[k] = hi ? v[6 + k] : v[4 + k];
+    double *pb = yr + (hi ? 6 : 4);
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(pb), "d"(B[0]), "d"(B[1]), "d"(B[2]), "d"(B[3])
+                 : "memory");
+    *reinterpret_cast<double2 *>(yr + (hi ? 0 : 8)) = make_double2(hi ? v[0] : v[8], hi ? v[1] : v[9]);
+  } else {  // hi: 2-5, 6-7, 0-1, 8   else: 0-3, 4-5, 6-7, 8
+    *reinterpret_cast<double2 *>(yr + (hi ? 6 : 4)) = make_double2(hi ? v[6] : v[4], hi ? v[7] : v[5]);
+    *reinterpret_cast<double2 *>(yr + (hi ? 0 : 6)) = make_double2(hi ? v[0] : v[6], hi ? v[1] : v[7]);
+    yr[8] = v[8];
+  }
 }
 
 // Store counterpart of load_row12: the 12 values v (columns 0-11) of a row at a 16-byte aligned

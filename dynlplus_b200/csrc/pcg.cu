@@ -337,6 +337,8 @@ __device__ __forceinline__ double block_column_sum(const double *v, int c, int64
 // K2: residual update + reductions + stop decision
 //   phase 0: iteration (R -= alpha AP)      phase 1: recheck of a true residual
 //   phase 2: initial residual (sets best, rz)
+//   phase 3: as phase 2, the initial residual copied into R from the array passed as AP (the rhs of
+//            a zero start) in the same sweep
 // A non-finite residual entry stops the solve with status 4 (breakdown) instead of letting the
 // max-reductions (which skip NaN) read it as convergence.
 template <typename T>
@@ -366,6 +368,8 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
       if (phase == 0) {
         rv = rv - al * ap;
         R[o] = rv;
+      } else if (phase == 3) {
+        R[o] = rv;
       }
       const double r64 = (double)rv;
       const double dinv = __drcp_rn((double)dv);  // correctly rounded: the value of 1.0 / d
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
       T rv[kSweepUnroll], ap[kSweepUnroll], dv[kSweepUnroll];
 #pragma unroll
       for (int u = 0; u < kSweepUnroll; ++u) {
-        rv[u] = R[offr + u * rstep];
+        rv[u] = phase == 3 ? AP[offa + u * astep] : R[offr + u * rstep];
         dv[u] = diag[r + u * ix.RS];
         ap[u] = phase == 0 ? AP[offa + u * astep] : T(0);
       }
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
       offa += kSweepUnroll * astep;
     }
     for (; r < n; r += ix.RS) {  // the last rows, one at a time
-      element(R[offr], phase == 0 ? AP[offa] : T(0), diag[r], offr);
+      element(phase == 3 ? AP[offa] : R[offr], phase == 0 ? AP[offa] : T(0), diag[r], offr);
       offr += rstep;
       offa += astep;
     }
@@ -431,7 +435,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
     for (int c = tid; c < C; c += kSweepThreads) {
       const double a = s_out[c], b = s_out[C + c];
       const double rzo = B.rz[c];
-      const double be = (phase != 2 && rzo > 0.0) ? a / rzo : 0.0;
+      const double be = (phase < 2 && rzo > 0.0) ? a / rzo : 0.0;
       B.beta[c] = isfinite(be) && fabs(be) < 1e30 ? be : 0.0;
       B.rz[c] = a;
       const double rel = B.rhsn[c] > 0.0 ? sqrt(b) / B.rhsn[c] : sqrt(b);
@@ -450,7 +454,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
       if (ctl->mode & 2) m = fmax(m, ctl->target > 0.0 ? rel / ctl->target : rel);
       const bool conv = m <= 1.0 && !ctl->bad;
       if (phase == 0) ctl->iters += 1;
-      if (phase == 2) {
+      if (phase >= 2) {  // the initial residual
         ctl->best = m;
         ctl->stall = 0;
         ctl->done = conv ? 5 : 0;
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
 
 // K3: Z += alpha P; P = R/diag + beta P
 //   mode 0: both (skipping the P update when a stop was proposed)   mode 1: P update only
-//   mode 2: P = R/diag
+//   mode 2: P = R/diag      mode 4: P = R/diag and Z = 0 (a zero start)
 template <typename T>
 __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z,
                                                            int64_t ldz, T *__restrict__ P, int64_t ldp,
@@ -493,7 +497,8 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
   if (!ix.on) return;
   const int c = ix.c;
   const T al = mode == 0 ? (T)B.alpha[c] : T(0);
-  const T be = mode == 2 ? T(0) : (T)B.beta[c];
+  const bool init = mode == 2 || mode == 4;  // P = R/diag: the old P is not read
+  const T be = init ? T(0) : (T)B.beta[c];
   const long long zstep = ix.RS * ldz, pstep = ix.RS * ldp, rstep = ix.RS * ldr;
   long long offz = ix.r0 * ldz + c, offp = ix.r0 * ldp + c, offr = ix.r0 * ldr + c;
   for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
@@ -503,7 +508,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
     for (int u = 0; u < kSweepUnroll; ++u) {
       const long long rr = r + u * ix.RS;
       const bool ok = rr < n;
-      pv[u] = ok ? P[offp + u * pstep] : T(0);
+      pv[u] = (ok && !init) ? P[offp + u * pstep] : T(0);
       zv[u] = (ok && mode == 0) ? Z[offz + u * zstep] : T(0);
       rv[u] = (ok && upd_p) ? R[offr + u * rstep] : T(0);
       dv[u] = (ok && upd_p) ? diag[rr] : T(1);
@@ -513,9 +518,10 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
       const long long rr = r + u * ix.RS;
       if (rr < n) {
         if (mode == 0) Z[offz + u * zstep] = zv[u] + al * pv[u];
+        if (mode == 4) Z[offz + u * zstep] = T(0);
         if (upd_p) {
           const T y = rv[u] / dv[u];
-          const T pn = mode == 2 ? y : y + be * pv[u];
+          const T pn = init ? y : y + be * pv[u];
           P[offp + u * pstep] = pn;
           if (P_lo) P_lo[rr * ld_lo + c] = cvt<bf16>(pn);
         }
@@ -701,10 +707,14 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, b
   return launch ? check_launch() : DLP_OK;
 }
 
+// src (phase 3 only): the array the initial residual is copied from, in place of AP
 template <typename TS>
-static int launch_update(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
-  k_pcg_update<TS><<<update_grid<TS>(), kSweepThreads, 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, (const TS *)q.AP,
-                                                            q.ldap, (const TS *)q.diag, B);
+static int launch_update(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s,
+                         const void *src = nullptr, int64_t ldsrc = 0) {
+  const TS *ap = phase == 3 ? (const TS *)src : (const TS *)q.AP;
+  const int64_t ldap = phase == 3 ? ldsrc : q.ldap;
+  k_pcg_update<TS><<<update_grid<TS>(), kSweepThreads, 0, s>>>(phase, q.n, q.C, (TS *)q.R, q.ldr, ap, ldap,
+                                                            (const TS *)q.diag, B);
   return check_launch();
 }
 
@@ -749,6 +759,12 @@ static int true_residual(const PcgProblem &q, cudaStream_t s) {
 
 static int update_phase(int phase, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   return q.dtype == DLP_F32 ? launch_update<float>(phase, q, B, s) : launch_update<double>(phase, q, B, s);
+}
+
+// the initial phase of a zero start: R = rhs in the same sweep as the initial reductions
+static int update_from_rhs(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  return q.dtype == DLP_F32 ? launch_update<float>(3, q, B, s, q.rhs, q.ldrhs)
+                            : launch_update<double>(3, q, B, s, q.rhs, q.ldrhs);
 }
 
 static int dir_phase(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
@@ -970,16 +986,16 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
     DLP_CUDA(cudaMemsetAsync(B.rhsn, 0, sizeof(double) * C, s));
   }
   DLP_CUDA(cudaMemsetAsync(B.rz, 0, sizeof(double) * C, s));
-  // R = rhs - A Z (= rhs when Z is known to be zero); best = violation; P = R/diag; rz = R.(R/diag)
+  // R = rhs - A Z, best = violation, rz = R.(R/diag), P = R/diag; a zero start takes R = rhs in the
+  // update sweep itself and sets Z = 0 in the direction sweep (no SpMM, no separate copy)
   if (mode & 4) {
-    const size_t es = q.dtype == DLP_F32 ? 4 : 8;
-    DLP_CUDA(cudaMemcpy2DAsync(q.R, (size_t)q.ldr * es, q.rhs, (size_t)q.ldrhs * es, (size_t)q.C * es, (size_t)q.n,
-                               cudaMemcpyDeviceToDevice, s));
+    DLP_TRY(update_from_rhs(q, B, s));
+    DLP_TRY(dir_phase(4, q, B, s));
   } else {
     DLP_TRY(true_residual(q, s));
+    DLP_TRY(update_phase(2, q, B, s));
+    DLP_TRY(dir_phase(2, q, B, s));
   }
-  DLP_TRY(update_phase(2, q, B, s));
-  DLP_TRY(dir_phase(2, q, B, s));
   const int k = check_every > 0 ? check_every : 8;
   // graphs: the device-side loop, else (a driver without conditional nodes) chunks of k iterations
   GraphRef lref, gref;

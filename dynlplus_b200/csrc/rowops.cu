@@ -67,8 +67,9 @@ struct SpmmArgs {
   int G, LV, NV;
   const typename T::TV *Xo;  // own-row values for the a-term (NULL: X itself)
   int64_t ldxo;
-  // kRow10D epilogue: the own row, the RHS row and the Y row are read / written whole (three
-  // accesses each) when their rows are 16-byte aligned and hold 10 values
+  // kRow10D epilogue: the own row and the RHS row are read whole (three loads) and the Y row is
+  // written in three or four vector stores (exactly its C values) when their rows are 16-byte
+  // aligned and hold 10 values
   int own10, rhs10, y10;
 };
 
@@ -129,8 +130,9 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
               if (c < p.C) yv[c] += (double)p.cr * p.rhs[(long long)r * p.ldr + c];
           }
         }
-        if (p.y10) {
-          store_row10d(p.Y + orow * p.ldy, yv);
+        if (p.y10) {  // exactly the C = 9 or 10 columns: the caller's other columns stay untouched
+          if (p.C == 10) store_row10d<true>(p.Y + orow * p.ldy, yv);
+          else store_row10d<false>(p.Y + orow * p.ldy, yv);
         } else {
 #pragma unroll
           for (int c = 0; c < 10; ++c)

@@ -4,22 +4,48 @@
 namespace dlp {
 
 // op 0: Y = X / scale[c]   op 1: Y += X * scale[c]   op 2: Y = X * scale[c]   op 3: Y = X + Y * scale[c]
+// Thread t of the grid owns column c = t mod C of rows t/C, t/C + RS, ... (RS = threads / C): no
+// integer division per element, consecutive threads on consecutive columns of a row, and
+// kColsUnroll rows loaded before any is stored.
+constexpr int kColsUnroll = 4;
+constexpr int kColsThreads = 256;
+
 template <typename TX, typename TY>
-__global__ void k_cols_scale(int32_t n, int32_t C, const TX *__restrict__ X, int64_t ldx,
-                             const double *__restrict__ scale, int op, TY *Y, int64_t ldy) {
+__global__ void __launch_bounds__(kColsThreads) k_cols_scale(int32_t n, int32_t C, const TX *__restrict__ X,
+                                                             int64_t ldx, const double *__restrict__ scale, int op,
+                                                             TY *Y, int64_t ldy) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)n * C) return;
-  const long long r = t / C;
-  const int c = (int)(t % C);
-  const double x = (double)X[r * ldx + c];
+  const long long RS = (long long)gridDim.x * blockDim.x / C;
+  const long long r0 = t / C;
+  const int c = (int)(t - r0 * C);
+  if (r0 >= RS) return;
   const double s = scale[c];
-  if constexpr (sizeof(TY) == 2) {
-    Y[r * ldy + c] = cvt<TY>(x * s);  // the bf16 mirror: op 2 only
-  } else {
-    if (op == 0) Y[r * ldy + c] = (TY)(x / s);
-    else if (op == 1) Y[r * ldy + c] = (TY)((double)Y[r * ldy + c] + x * s);
-    else if (op == 2) Y[r * ldy + c] = (TY)(x * s);
-    else Y[r * ldy + c] = (TY)(x + (double)Y[r * ldy + c] * s);
+  const bool rd = sizeof(TY) != 2 && (op == 1 || op == 3);  // the op reads Y
+  const long long sx = RS * ldx, sy = RS * ldy;
+  long long ox = r0 * ldx + c, oy = r0 * ldy + c;
+  for (long long r = r0; r < n; r += kColsUnroll * RS) {
+    double x[kColsUnroll], y[kColsUnroll];
+#pragma unroll
+    for (int u = 0; u < kColsUnroll; ++u) {
+      const bool ok = r + u * RS < n;
+      x[u] = ok ? (double)X[ox + u * sx] : 0.0;
+      if constexpr (sizeof(TY) != 2) y[u] = (ok && rd) ? (double)Y[oy + u * sy] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kColsUnroll; ++u) {
+      if (r + u * RS >= n) continue;
+      TY *yp = Y + oy + u * sy;
+      if constexpr (sizeof(TY) == 2) {
+        *yp = cvt<TY>(x[u] * s);  // the bf16 mirror: op 2 only
+      } else {
+        if (op == 0) *yp = (TY)(x[u] / s);
+        else if (op == 1) *yp = (TY)(y[u] + x[u] * s);
+        else if (op == 2) *yp = (TY)(x[u] * s);
+        else *yp = (TY)(x[u] + y[u] * s);
+      }
+    }
+    ox += kColsUnroll * sx;
+    oy += kColsUnroll * sy;
   }
 }
 
@@ -50,18 +76,22 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
   if (n < 0 || C <= 0 || ldx < C || ldy < C || op < 0 || op > 3) return DLP_ERR_INVALID;
   if (n == 0) return DLP_OK;
   if (!X || !Y || !scale) return DLP_ERR_INVALID;
-  const int grid = ceil_div_i((long long)n * C, 256);
+  // enough threads for a row pass (>= C) and for the elements, at most 8 resident blocks per SM
+  long long blocks = ceil_div_i((long long)n * C, (long long)kColsThreads * kColsUnroll);
+  blocks = std::min(blocks, (long long)sm_count() * 8);
+  blocks = std::max(blocks, (long long)ceil_div_i((long long)C, kColsThreads));
+  const int grid = (int)blocks;
   cudaStream_t s = (cudaStream_t)stream;
   if (x_dtype == DLP_F64 && y_dtype == DLP_F32)
-    k_cols_scale<double, float><<<grid, 256, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (float *)Y, ldy);
+    k_cols_scale<double, float><<<grid, kColsThreads, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (float *)Y, ldy);
   else if (x_dtype == DLP_F32 && y_dtype == DLP_F64)
-    k_cols_scale<float, double><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (double *)Y, ldy);
+    k_cols_scale<float, double><<<grid, kColsThreads, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (double *)Y, ldy);
   else if (x_dtype == DLP_F64 && y_dtype == DLP_F64)
-    k_cols_scale<double, double><<<grid, 256, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (double *)Y, ldy);
+    k_cols_scale<double, double><<<grid, kColsThreads, 0, s>>>(n, C, (const double *)X, ldx, scale, op, (double *)Y, ldy);
   else if (x_dtype == DLP_F32 && y_dtype == DLP_F32)
-    k_cols_scale<float, float><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (float *)Y, ldy);
+    k_cols_scale<float, float><<<grid, kColsThreads, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (float *)Y, ldy);
   else if (x_dtype == DLP_F32 && y_dtype == DLP_BF16 && op == 2)
-    k_cols_scale<float, bf16><<<grid, 256, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (bf16 *)Y, ldy);
+    k_cols_scale<float, bf16><<<grid, kColsThreads, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (bf16 *)Y, ldy);
   else
     return DLP_ERR_DTYPE;
   return check_launch();

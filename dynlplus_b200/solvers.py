@@ -164,10 +164,13 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
 
     Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
-    residual ||R_c|| / rhs_norm_c <= target must hold as well (rhs_norm defaults to ||rhs_c||)."""
+    residual ||R_c|| / rhs_norm_c <= target must hold as well (rhs_norm defaults to ||rhs_c||).
+    zero_start: the solve starts from Z = 0 whatever Z holds, with rhs as the initial residual."""
     if eps is None and target_relres is None:
         raise ValueError("pcg needs eps and/or target_relres")
     if M is not None and not isinstance(M, JacobiM):
+        if zero_start:
+            Z.zero_()  # the generic loop starts from the Z it is given
         return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, lowp)
     n, C = Z.shape
     if n == 0:
@@ -507,7 +510,8 @@ class DynLPPlus(Solver):
 
     def _run(self, sys, Z, rhs, eps, ops, st, amg_box, zero_start=False, **kw):
         """auto: push when few rows violate, else PCG/AMG (dynlp/solvers.py:272-288). With
-        zero_start (Z == 0 on entry) the residual is rhs itself and is not recomputed."""
+        zero_start the solve starts from Z = 0 (Z's incoming values are ignored) and the residual is
+        rhs itself."""
         if self.method != "auto":
             st.path = self.method
             return self._global(sys, Z, rhs, eps, st, amg_box, zero_start=zero_start, **kw)
@@ -523,6 +527,7 @@ class DynLPPlus(Solver):
             st.path = "amg" if self._use_amg() else "pcg"
             return self._global(sys, Z, rhs, eps, st, amg_box, zero_start=zero_start, **kw)
         if zero_start:
+            Z.zero_()
             R = rhs.clone()  # push updates R in place
         Z, R, ok = push(sys, Z, R, eps, ops, st, self.push_budget * max(sys.nnz, 1))
         st.path = "push"
@@ -592,8 +597,7 @@ class DynLPPlus(Solver):
             Rs = _scratch("ref_Rs", Z64.shape[0], C + 1, self.dtype, dev)
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs), ld(Rs),
                       code(Rs), stream())
-            D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)
-            D.zero_()
+            D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)  # zeroed by the zero start
             D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, zero_start=True, **kw)
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(D), ld(D), code(D), ptr(sc), 1, ptr(Z64), ld(Z64),
                       code(Z64), stream())

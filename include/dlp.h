@@ -203,12 +203,15 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
  * (diag - W) Z = rhs, starting from the Z given. Per iteration three kernels (SpMM + pAp, residual
  * update + rz/norms/violation, direction update); all inner products and norms in fp64, reduced
  * in a fixed order. Stop rule `mode`: bit 0 = the reference's max_uc |R_uc|/(eps_c diag_u) <= 1,
- * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold); bit 2 = the
- * caller guarantees Z == 0 on entry, so the initial residual is rhs itself (copied, no SpMM). A proposed
+ * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold); bit 2 = a zero
+ * start: Z is set to 0 (its incoming values are ignored) and the initial residual is rhs itself (no
+ * SpMM; R is written in the first sweep). A proposed
  * stop is confirmed on the true residual rhs - A Z (solvers.py:85-89); `patience` iterations
  * without a 10% improvement stop the solve as the reference's stall rule does (:90-92).
  * eps and rhs_norm are HOST arrays of C doubles (rhs_norm may be NULL when bit 1 is unused).
- * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual). With
+ * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual; for fp32 rows of
+ * 9-12 columns with ldap >= 12 on 16-byte boundaries AP is written whole, its padding columns
+ * included). With
  * use_graph != 0 the iteration loop runs on the device as one CUDA graph with a conditional WHILE
  * node (cached per problem; the host reads the control block once per loop and once per recheck);
  * where conditional nodes are unavailable, chunks of check_every iterations are replayed as graphs.

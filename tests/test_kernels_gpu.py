@@ -90,6 +90,79 @@ def test_spmm_widths_and_fp64_residual(C):
     np.testing.assert_allclose(got32.cpu().numpy(), A @ X.astype(np.float32), rtol=2e-5, atol=2e-5)
 
 
+@pytest.mark.parametrize("C", [9, 10])
+@pytest.mark.parametrize("ld_x,ld_r,ld_y", [(10, 10, 10), (16, 0, 12), (10, 11, 0), (12, 10, 14)])
+def test_spmm_fp64_whole_rows(C, ld_x, ld_r, ld_y):
+    """fp64 rows of 9-10 values (one lane per row, three loads; the own row and the rhs row read whole
+    and the output written in vector stores where their rows are padded and 16-byte aligned; ld 0 =
+    unpadded, odd ld = unaligned rows) against numpy: full rows, a row subset in place, compact rows.
+    Columns of the output beyond C keep their values."""
+    rs = np.random.RandomState(C * 100 + ld_x + ld_r + ld_y)
+    n = 3001
+    A = O.symmetric_from_pairs(rs.randint(0, n, 30000), rs.randint(0, n, 30000), rs.rand(30000), n, np.float32)
+    W = CSR.from_scipy(A)
+    X, rhs, d = rs.rand(n, C), rs.rand(n, C), rs.rand(n) + 1
+    Xd = padded(X, ld_x, torch.float64)  # NaN in the padding: never read into a result
+    rhs_d = padded(rhs, ld_r, torch.float64) if ld_r else T(rhs)
+    want = rhs - d[:, None] * X + A.astype(np.float64) @ X
+
+    def out_buf():
+        if not ld_y:
+            return T(np.zeros((n, C)))
+        buf = torch.full((n, ld_y), -7.0, dtype=torch.float64, device="cuda")
+        buf[:, :C] = 0.0
+        return buf[:, :C]
+
+    Y = out_buf()
+    kernels.spmm_axpy(W, Xd, a=T(d), alpha=-1.0, b=1.0, rhs=rhs_d, out=Y)
+    np.testing.assert_allclose(Y.cpu().numpy(), want, rtol=1e-12, atol=1e-12)
+    if ld_y:
+        assert (Y.as_strided((n, ld_y), (ld_y, 1))[:, C:] == -7.0).all()
+    Q = np.sort(rs.choice(n, 400, replace=False)).astype(np.int32)
+    Y = out_buf()
+    kernels.spmm_axpy(W, Xd, a=T(d), alpha=-1.0, b=1.0, rhs=rhs_d, out=Y, rows=T(Q))
+    Yn = Y.cpu().numpy()
+    np.testing.assert_allclose(Yn[Q], want[Q], rtol=1e-12, atol=1e-12)
+    assert (Yn[np.setdiff1d(np.arange(n), Q)] == 0).all()
+    Yc = kernels.spmm_axpy(W, Xd, rows=T(Q), compact=True)
+    np.testing.assert_allclose(Yc.cpu().numpy(), (A.astype(np.float64) @ X)[Q], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("n,C", [(1, 1), (1000, 9), (300_001, 9), (50, 300)])
+def test_cols_scale_all_ops(n, C):
+    """dlp_cols_scale, op 0 Y = X / s, 1 Y += X s, 2 Y = X s, 3 Y = X + Y s, for every precision pair,
+    on padded rows; columns beyond C untouched."""
+    rs = np.random.RandomState(n + C)
+    X, Y0, sc = rs.rand(n, C) - 0.5, rs.rand(n, C) - 0.5, rs.rand(C) + 0.5
+    ops = {0: lambda x, y: x / sc, 1: lambda x, y: y + x * sc, 2: lambda x, y: x * sc, 3: lambda x, y: x + y * sc}
+    pairs = [(torch.float64, torch.float32), (torch.float32, torch.float64), (torch.float64, torch.float64),
+             (torch.float32, torch.float32)]
+    s_d = T(sc)
+    for tx, ty in pairs:
+        Xd = padded(X, C + 3, tx)
+        xw = Xd.double().cpu().numpy()
+        for op, f in ops.items():
+            buf = torch.full((n, C + 5), 9.0, dtype=ty, device="cuda")
+            buf[:, :C] = T(Y0, ty)
+            Yd = buf[:, :C]
+            yw = Yd.double().cpu().numpy()
+            _lib.call("dlp_cols_scale", n, C, Xd.data_ptr(), Xd.stride(0), _lib_code(tx), s_d.data_ptr(), op,
+                      Yd.data_ptr(), Yd.stride(0), _lib_code(ty), torch.cuda.current_stream().cuda_stream)
+            tol = 1e-6 if torch.float32 in (tx, ty) else 1e-14
+            np.testing.assert_allclose(Yd.double().cpu().numpy(), f(xw, yw), rtol=tol, atol=tol)
+            assert (buf[:, C:] == 9.0).all()
+    Xd = padded(X, C + 3, torch.float32)
+    Yb = torch.zeros((n, C), dtype=torch.bfloat16, device="cuda")
+    _lib.call("dlp_cols_scale", n, C, Xd.data_ptr(), Xd.stride(0), _lib_code(torch.float32), s_d.data_ptr(), 2,
+              Yb.data_ptr(), Yb.stride(0), _lib_code(torch.bfloat16), torch.cuda.current_stream().cuda_stream)
+    np.testing.assert_allclose(Yb.double().cpu().numpy(), Xd.double().cpu().numpy() * sc, rtol=1e-2, atol=1e-2)
+
+
+def _lib_code(dt):
+    from dynlplus_b200.backend import DTYPES
+    return DTYPES[dt]
+
+
 def test_spmm_bf16_fp32_accumulation():
     rs = np.random.RandomState(3)
     A = O.symmetric_from_pairs(rs.randint(0, 3000, 30000), rs.randint(0, 3000, 30000), rs.rand(30000), 3000,

@@ -90,6 +90,23 @@ def test_fused_pcg_zero_start_is_the_same_solve(graph):
         np.testing.assert_allclose(out[1], g[f"{tag}_Z"], rtol=1e-8, atol=1e-11)
 
 
+@pytest.mark.parametrize("graph", [True, False])
+def test_fused_pcg_zero_start_ignores_incoming_z(graph):
+    """A zero start sets Z = 0 itself: a Z full of NaN gives the reference's iteration counts and the
+    same iterate as a zeroed Z."""
+    g, A, S = golden_system()
+    for tag in ("pcg_loose", "pcg_tight"):
+        out = []
+        for fill in (0.0, float("nan")):
+            Z = torch.full((A.shape[0], 3), fill, dtype=torch.float64, device="cuda")
+            st = solvers.Stats()
+            solvers.pcg(S, Z, S.rhs, g[f"{tag}_eps"].tolist(), solvers.jacobi_M(S), 10_000, st, use_graph=graph,
+                        zero_start=True)
+            assert st.iters == int(g[f"{tag}_iters"]), (tag, fill, st.iters)
+            out.append(Z.cpu().numpy())
+        np.testing.assert_array_equal(out[1], out[0])
+
+
 @pytest.mark.parametrize("dt", [torch.float32, torch.float64])
 @pytest.mark.parametrize("n,C", [(1, 1), (1000, 3), (300_000, 9), (50_000, 33)])
 def test_residual_stats_match_torch(dt, n, C):
