@@ -292,6 +292,13 @@ __global__ void k_park(const int32_t *__restrict__ rows, int32_t nr, const uint8
 }
 
 // Compact CSR of the solver operator: the entries with w != 0 of every row, in stored order.
+// Solver CSR from the slots. The count keeps one thread per row (its serial scan is cheaper than a
+// group of lanes per row, measured: 22 vs 50 us at n = 1M); the copy uses a group of kLiveGroup
+// lanes per row reading the row's slots kLiveGroup at a time (consecutive: coalesced), ballot +
+// popcount giving each live entry its place, so the compact row keeps the slot order (measured: 73
+// vs 104 us with one thread per row).
+constexpr int kLiveGroup = 8;
+
 __global__ void k_live_count(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
                              const float *__restrict__ w, int32_t *cnt) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -304,16 +311,23 @@ __global__ void k_live_count(int32_t n, const int32_t *__restrict__ rbeg, const 
 __global__ void k_live_copy(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
                             const int32_t *__restrict__ col, const float *__restrict__ w,
                             const int32_t *__restrict__ indptr, int32_t *col_out, float *w_out) {
-  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  int o = indptr[r];
-  for (int j = rbeg[r]; j < rend[r]; ++j) {
-    const float x = w[j];
-    if (x != 0.0f) {
-      col_out[o] = col[j];
-      w_out[o] = x;
-      ++o;
+  constexpr int G = kLiveGroup;
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1), gshift = lane & ~(G - 1);
+  const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool valid = r < n;
+  const int b = valid ? rbeg[r] : 0, e = valid ? rend[r] : 0;
+  int o = valid ? indptr[r] : 0;
+  for (int base = b; __any_sync(0xffffffffu, base < e); base += G) {
+    const int j = base + gl;
+    const float x = j < e ? w[j] : 0.0f;
+    const bool lv = x != 0.0f;
+    const unsigned m = (__ballot_sync(0xffffffffu, lv) >> gshift) & ((1u << G) - 1);
+    if (lv) {
+      const int p = o + __popc(m & ((1u << gl) - 1));
+      col_out[p] = col[j];
+      w_out[p] = x;
     }
+    o += __popc(m);
   }
 }
 
@@ -446,7 +460,8 @@ int dlp_graph_to_csr(int32_t n, const int32_t *rbeg, const int32_t *rend, const 
   const size_t scan_bytes = ws_bytes - ((sizeof(int32_t) * (size_t)(n > 0 ? n : 1) + 255) / 256 * 256);
   if (n > 0) k_live_count<<<grid1(n), kGThreads, 0, s>>>(n, rbeg, rend, w, cnt);
   DLP_TRY(exclusive_scan_i32(cnt, n, indptr, scan_ws, scan_bytes, s));
-  if (n > 0) k_live_copy<<<grid1(n), kGThreads, 0, s>>>(n, rbeg, rend, col, w, indptr, col_out, w_out);
+  if (n > 0)
+    k_live_copy<<<grid1((long long)n * kLiveGroup), kGThreads, 0, s>>>(n, rbeg, rend, col, w, indptr, col_out, w_out);
   return check_launch(n > 0 ? 2 : 0);
 }
 
