@@ -409,13 +409,20 @@ class EdgeStream:
         nmoved = self._ground()
         moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
         if nmoved:
-            moved = kernels.flatnonzero(self.in_t)
+            mv, _ = kernels.flatnonzero(self.in_t, sync=False)
+            moved = mv[:nmoved]  # the grounding counted the membership changes: no read-back
             _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(moved),
-                      int(moved.numel()), ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), s)
+                      nmoved, ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), s)
             self.counters["ground_changes"] += nmoved
-        Q = kernels.flatnonzero(self.changed)
-        self._system_rows(Q, int(Q.numel()))
+        # the changed rows and the batch's solver CSR are both queued before one host read of their
+        # two counts
+        Qb, qc = kernels.flatnonzero(self.changed, sync=False)
         self.t += 1
+        self._csr_launch()
+        nq, nnz = torch.cat([qc, self._csr_ptr[n:n + 1]]).tolist()
+        self._csr_set(nnz)
+        Q = Qb[:nq]
+        self._system_rows(Q, nq)
         self.last_changed, self.last_moved = Q, moved
         self.n_ins, self.n_del = ni, nd
         self.counters["applied"] += flags[2] + flags[3]
@@ -485,6 +492,12 @@ class EdgeStream:
         """Compact CSR of W_UU (live solver entries only) for the current batch (cached)."""
         if getattr(self, "_csr_t", None) == (self.t, id(self.G.indices)):
             return self._csr
+        self._csr_launch()
+        self._csr_set(int(self._csr_ptr[self.n].item()))
+        return self._csr
+
+    def _csr_launch(self):
+        """Queue the compact CSR build of the current slots (no host read)."""
         n, G = self.n, self.G
         cap = int(G.indices.numel())
         if getattr(self, "_csr_cap", 0) < cap:
@@ -495,7 +508,10 @@ class EdgeStream:
         ws = workspace("to_csr").get(_lib.lib().dlp_graph_to_csr_workspace_bytes(n))
         _lib.call("dlp_graph_to_csr", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.data), ptr(self._csr_ptr),
                   ptr(self._csr_col), ptr(self._csr_w), ptr(ws), ws.numel(), stream())
-        nnz = int(self._csr_ptr[n].item())
+
+    def _csr_set(self, nnz):
+        """The CSR of the build just queued, given its entry count."""
+        n, G = self.n, self.G
         self._csr = CSR(self._csr_w[:nnz], self._csr_col[:nnz], self._csr_ptr, (n, n))
         self._csr_t = (self.t, id(G.indices))
         return self._csr
