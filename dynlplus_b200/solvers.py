@@ -3,8 +3,9 @@
 DynLP+ (certified): A = diag - W is a nonsingular M-matrix, so |r| <= rho * diag implies
 |F - F*| <= rho * h with A h = diag (dynlp/solvers.py:10-12); h rides along as one extra column.
 The iterations run in libdlp's kernels: Jacobi-PCG is one fused C call (three kernels per
-iteration, CUDA-graph chunks, device-side stop rule), push and frontier Jacobi use the row
-kernels, and the fp64 refinement (solvers.py:322-337) uses fp64 residual SpMMs.
+iteration, the iteration loop as a CUDA graph WHILE node, device-side stop rule), push and
+frontier Jacobi use the row kernels, and the fp64 refinement (solvers.py:322-337) uses fp64
+residual SpMMs.
 
 Extension over the reference: `target_relres` adds a second stop rule, the relative residual
 max_c ||rhs_c - A F_c||_2 / ||rhs_c||_2 in fp64, which the certified loops must also meet.
