@@ -250,6 +250,22 @@ def spmm_roofline(es, C, peaks):
                     "gathered matrix (n x ld x 4 B) fits in L2"}
 
 
+def aggregate_replicas(dev_ms, e2e_ms, units_per_step, world, device="cpu"):
+    """Whole-job throughput of `world` independent replicas (one per rank): the slowest rank's summed
+    step times (max over ranks, on the device) against all ranks' units. Every rank takes the same
+    collective steps. Returns (t_dev_ms, t_e2e_ms, value, e2e) with value, e2e in units per second."""
+    import torch
+    total = torch.tensor([float(sum(dev_ms)), float(sum(e2e_ms))], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    t_dev, t_e2e = float(total[0]), float(total[1])
+    value = world * units_per_step * len(dev_ms) / (t_dev * 1e-3)
+    e2e = world * units_per_step * len(e2e_ms) / (t_e2e * 1e-3) if e2e_ms else float("nan")
+    return t_dev, t_e2e, value, e2e
+
+
 def pcg_iteration_bytes(n, nnz, C, s=4):
     """Algorithmic bytes of one fused PCG iteration on an n-row operator with nnz entries and C
     columns of s-byte values: the apply (row ranges, the gather model nnz (4 + s_w + C s), diag,
@@ -387,13 +403,7 @@ def ours(a):
         e2e_times.append(s.elapsed_time(e))
         relres.append(float(res[0]))
     clk = clocks.stop() if clocks else None
-    total = torch.tensor([sum(times), sum(e2e_times)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    t_dev, t_e2e = float(total[0]), float(total[1])
-    value = world * a.batch * len(times) / (t_dev * 1e-3)
-    e2e = world * a.batch * len(e2e_times) / (t_e2e * 1e-3)
+    t_dev, t_e2e, value, e2e = aggregate_replicas(times, e2e_times, a.batch, world, dev)
     roof = None
     if rank == 0:
         roof = pcg_roofline(pcg_events, es.solver_csr().nnz, peaks,

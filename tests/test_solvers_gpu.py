@@ -72,6 +72,35 @@ def test_fused_pcg_fp32_and_relres_target():
     assert rel <= 1e-5 * 1.01 and st.iters < 200, (rel, st.iters)
 
 
+@pytest.mark.parametrize("C", [9, 10, 11, 12])
+@pytest.mark.parametrize("graph", [True, False])
+def test_fused_pcg_fp32_whole_rows(C, graph):
+    """fp32 blocks of 9-12 columns take the apply's whole-row path (each gathered and own row of P in
+    one 256-bit and one 128-bit load, AP stored whole into its padded rows): the relative-residual
+    target holds in fp64 and the solve matches the direct one."""
+    rs = np.random.RandomState(C)
+    n = 3000
+    A = O.symmetric_from_pairs(rs.randint(0, n, 24000), rs.randint(0, n, 24000), rs.rand(24000) + 0.1, n,
+                               np.float64)
+    diag = np.asarray(A.sum(axis=1)).ravel() + 0.5
+    rhs = rs.rand(n, C)
+    S = stream.System(t=0, U=torch.arange(n, device="cuda"), W=CSR.from_scipy(A, dtype=torch.float32),
+                      s=T(diag, torch.float32), diag=T(diag, torch.float32), B=T(rhs, torch.float32),
+                      rhs=T(rhs, torch.float32), prior=T(np.full(C, 1 / C), torch.float32),
+                      is_new=torch.zeros(n, dtype=torch.bool, device="cuda"),
+                      seed=torch.zeros(n, dtype=torch.bool, device="cuda"), comps={}, K=C, C=C, eta=0.0,
+                      n_inserted=0, n_deleted=0, n_active=n)
+    Z = solvers.padded_empty(n, C, torch.float32, "cuda")
+    st = solvers.Stats()
+    solvers.pcg(S, Z, S.rhs, None, solvers.jacobi_M(S), 10_000, st, target_relres=1e-5, use_graph=graph,
+                zero_start=True)
+    Zn = Z.double().cpu().numpy()
+    Ad = ssp.diags(diag) - A
+    rel = np.linalg.norm(rhs - Ad @ Zn, axis=0) / np.linalg.norm(rhs, axis=0)
+    assert rel.max() <= 1e-5 * 1.01 and st.iters < 300, (rel.max(), st.iters)
+    np.testing.assert_allclose(Zn, direct_solve(Ad, rhs), rtol=1e-4, atol=1e-4)
+
+
 @pytest.mark.parametrize("graph", [True, False])
 def test_fused_pcg_zero_start_is_the_same_solve(graph):
     """Mode bit 2 (Z == 0 on entry: R = rhs, no SpMM) gives the reference's iteration counts and
