@@ -175,9 +175,11 @@ constexpr int apply_min_blocks() {
   return (sizeof(typename T::TA) == 4 && VPL * VW <= 12 && VPL <= 4) ? 4 : 1;
 }
 
-// ROW12 as in gather_row: fp32 12-float rows held whole by one lane, two loads per row, one row in
-// flight per lane (measured on B200 at n = 1M, degree 10, C = 9: 150 us against 166 us for two rows
-// in flight, which spill under the 64-register cap, and 160 us for per-vector loads).
+// ROW12 as in gather_row: fp32 12-float rows held whole by one lane, two loads per row. Its lanes
+// keep their pAp partials (about a dozen rows each) in fp32 and the rest of the sum runs in fp64,
+// which frees the registers for two rows in flight per lane within the 64-register cap (measured on
+// B200 at n = 1M, degree 10, C = 9: 123 us; fp64 lane partials allow one row in flight, 127 us; two
+// spill, 166 us; per-vector loads 160 us).
 template <class T, int VW, int VPL, bool ROW12 = false>
 __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_pcg_apply(ApplyArgs<T> p) {
   using TA = typename T::TA;
@@ -195,11 +197,12 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
   const int es = gl / LV;
   const int ES = G / LV;
   const int gpw = 32 / G;
-  double dot[VPL][VW];
+  using TD = typename std::conditional<ROW12, float, double>::type;  // a lane's pAp partials
+  TD dot[VPL][VW];
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
-    for (int i = 0; i < VW; ++i) dot[k][i] = 0.0;
+    for (int i = 0; i < VW; ++i) dot[k][i] = TD(0);
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long g0 = warp * gpw; g0 < p.n; g0 += nwarps * gpw) {
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 1 : gather_batch_lean<TA, VW, VPL>()),
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 2 : gather_batch_lean<TA, VW, VPL>()),
                (ROW12 ? kRow12F : kRowVec)>(
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
     if (valid && es == 0) {
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
             apv[k][i] = d * pv - acc[k][i];  // padding columns too when the whole row is stored
             if (c < p.C) {
               if (!p.ap_row12) p.AP[r * p.ldap + c] = apv[k][i];
-              dot[k][i] += (double)pv * (double)apv[k][i];
+              dot[k][i] += (TD)pv * (TD)apv[k][i];
             }
           }
         if (p.ap_row12) store_row12(p.AP + r * p.ldap, apv);
@@ -252,12 +255,16 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
       }
     }
   }
-  // lanes sharing a vector lane (same cl) hold the same columns: reduce over the other bits
+  // lanes sharing a vector lane (same cl) hold the same columns: reduce over the other bits, in fp64
+  double dsum[VPL][VW];
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
-    for (int i = 0; i < VW; ++i)
-      for (int off = LV; off < 32; off <<= 1) dot[k][i] += __shfl_xor_sync(0xffffffffu, dot[k][i], off);
+    for (int i = 0; i < VW; ++i) {
+      double x = (double)dot[k][i];
+      for (int off = LV; off < 32; off <<= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+      dsum[k][i] = x;
+    }
   if (lane < LV) {
 #pragma unroll
     for (int k = 0; k < VPL; ++k) {
@@ -266,7 +273,7 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
 #pragma unroll
         for (int i = 0; i < VW; ++i) {
           const int c = vi * VW + i;
-          if (c < p.C) sm[wid][c] = dot[k][i];
+          if (c < p.C) sm[wid][c] = dsum[k][i];
         }
       }
     }
