@@ -1,5 +1,6 @@
 // Block PCG with the Jacobi preconditioner, one CG per column (dynlp/solvers.py:66-97), fused for
-// B200: three kernels per iteration, fp64 inner products, convergence decided on the device, and
+// B200: three kernels per iteration, inner products summed in fp64 (fp32 only in the per-lane pAp
+// partials of the fp32 whole-row apply, about a dozen rows each), convergence decided on the device, and
 // the iteration loop itself on the device (a CUDA graph WHILE node whose flag K2 sets), so the host
 // waits once per solve instead of once per chunk of iterations.
 //

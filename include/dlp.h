@@ -201,8 +201,9 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
 /* ---- (d) fused block PCG, Jacobi preconditioner --------------------------------------------
  * Replaces solvers.pcg with jacobi_M (dynlp/solvers.py:62-97): one CG per column of
  * (diag - W) Z = rhs, starting from the Z given. Per iteration three kernels (SpMM + pAp, residual
- * update + rz/norms/violation, direction update); all inner products and norms in fp64, reduced
- * in a fixed order. Stop rule `mode`: bit 0 = the reference's max_uc |R_uc|/(eps_c diag_u) <= 1,
+ * update + rz/norms/violation, direction update); inner products and norms summed in fp64 (for fp32
+ * rows of 9-12 columns, each lane's pAp partial over its dozen or so rows is fp32), reduced in a
+ * fixed order. Stop rule `mode`: bit 0 = the reference's max_uc |R_uc|/(eps_c diag_u) <= 1,
  * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold); bit 2 = a zero
  * start: Z is set to 0 (its incoming values are ignored) and the initial residual is rhs itself (no
  * SpMM; R is written in the first sweep). A proposed
