@@ -1,8 +1,8 @@
 // Block PCG with the Jacobi preconditioner, one CG per column (dynlp/solvers.py:66-97), fused for
 // B200: three kernels per iteration, inner products summed in fp64 (fp32 only in the per-lane pAp
-// partials of the fp32 whole-row apply, about a dozen rows each), convergence decided on the device, and
-// the iteration loop itself on the device (a CUDA graph WHILE node whose flag K2 sets), so the host
-// waits once per solve instead of once per chunk of iterations.
+// partials of the fp32 whole-row apply, about a dozen rows each), convergence decided on the
+// device, and the iteration loop itself on the device (a CUDA graph WHILE node whose flag K2
+// sets), so the host waits once per solve instead of once per chunk of iterations.
 //
 //   K1 apply  : AP = diag*P - W P (row gather), pAp_c partials; last block: alpha_c = rz_c / pAp_c
 //   K2 update : R -= alpha AP; rz_c = sum R^2/diag, ss_c = sum R^2, viol = max |R|/(eps_c diag);
