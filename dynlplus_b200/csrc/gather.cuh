@@ -64,11 +64,12 @@ static inline int grid_for(long long groups, int G) {
 }
 
 
-// Entries per batch of a gather_row lane, by the registers the batch holds (VPL x VW values of TA
-// per entry). Measured on B200 (ER n = 1M, degree 10, 9 fp32 columns): the plain SpMM is fastest
-// with four gathers in flight (about 48 registers of batch, one resident block fewer per SM); the
-// PCG apply, which also holds fp64 dot accumulators and is capped at 64 registers for a fourth
-// resident block, with two.
+// Entries per batch of a gather_row lane on the per-vector path, by the registers the batch holds
+// (VPL x VW values of TA per entry). Measured on B200 (ER n = 1M, degree 10, 9 fp32 columns): the
+// plain SpMM is fastest with four gathers in flight (about 48 registers of batch, one resident
+// block fewer per SM); the PCG apply, capped at 64 registers for a fourth resident block, with two.
+// The whole-row paths (kRow12F, kRow10D below) pass their own batch: two rows in flight for the
+// fp32 SpMM and PCG apply, the wide batch for fp64.
 template <typename TA, int VW, int VPL>
 constexpr int gather_batch_wide() {
   return VPL * VW * (int)(sizeof(TA) / 4) <= 12 ? 4 : VPL * VW * (int)(sizeof(TA) / 4) <= 24 ? 2 : 1;
