@@ -74,6 +74,32 @@ class AdmissionError(RuntimeError):
     """The request cannot fit the HBM budget."""
 
 
+def take_batch(q, first, limit=None, cost=None, budget=None):
+    """The requests of one batch: `first`, then queued requests in arrival order while the batch
+    holds fewer than `limit` (None: no limit) and, given `cost`, while the summed cost stays within
+    `budget` (`first` is always taken). Returns (items, carry): `carry` is the queued request that
+    did not fit, which heads the next batch so that arrival order holds, or None. The shutdown
+    sentinel (None) ends the batch and goes back on the queue for the worker loop to see."""
+    items, carry = [first], None
+    used = cost(first) if cost is not None else 0
+    while limit is None or len(items) < limit:
+        try:
+            nxt = q.get_nowait()
+        except queue.Empty:
+            break
+        if nxt is None:
+            q.put(None)
+            break
+        if cost is not None:
+            need = cost(nxt)
+            if used + need > budget:  # admitted next, once this batch has freed its memory
+                carry = nxt
+                break
+            used += need
+        items.append(nxt)
+    return items, carry
+
+
 class Server:
     def __init__(self, ds, labeled, *, dtype="float32", target_relres=1e-6, tol=1e-3, hbm_budget_bytes=None,
                  max_fresh_batch=64, fresh_dtype=torch.float64, mode="continuous", lowp=False):
@@ -103,6 +129,7 @@ class Server:
         self._streams = {k: torch.cuda.Stream() for k in self._q}
         self._stop = threading.Event()
         self._lock = threading.Lock()
+        self._carry = {}  # per worker: the queued request that heads its next batch
         self.done: list[_Item] = []
         kinds = list(self._q) if mode == "continuous" else ["all"]
         self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in kinds]
@@ -124,11 +151,27 @@ class Server:
         return fut
 
     def close(self):
+        """Stops the workers after their current batch; requests still waiting fail with
+        RuntimeError("server closed")."""
         self._stop.set()
-        for q in {id(q): q for q in self._q.values()}.values():
+        queues = {id(q): q for q in self._q.values()}.values()
+        for q in queues:
             q.put(None)
         for t in self._threads:
             t.join(timeout=60)
+        left = [it for it in list(self._carry.values()) if it is not None]
+        self._carry.clear()
+        for q in queues:
+            while True:
+                try:
+                    it = q.get_nowait()
+                except queue.Empty:
+                    break
+                if it is not None:
+                    left.append(it)
+        for it in left:
+            if not it.fut.done():
+                it.fut.set_exception(RuntimeError("server closed"))
 
     def latency(self, kind=None):
         with self._lock:
@@ -154,32 +197,23 @@ class Server:
             else:
                 it.fut.set_result(r)
 
-    def _drain(self, kind, first, limit=None):
-        items = [first]
+    def _drain(self, kind, first):
         if self.mode == "sequential":
-            return items
-        q = self._q[kind]
-        while limit is None or len(items) < limit:
-            try:
-                nxt = q.get_nowait()
-            except queue.Empty:
-                break
-            if nxt is None:
-                q.put(None)
-                break
-            items.append(nxt)
-        return items
+            return [first]
+        return take_batch(self._q[kind], first)[0]
 
     def _worker(self, kind):
         torch.cuda.set_device(self._dev)
         q = self._q["update"] if kind == "all" else self._q[kind]
         with torch.cuda.stream(self._streams["update" if kind == "all" else kind]):
             while not self._stop.is_set():
-                first = q.get()
+                first = self._carry.pop(kind, None)
+                if first is None:
+                    first = q.get()
                 if first is None:
                     break
                 try:
-                    getattr(self, "_do_" + first.kind)(first)
+                    self._carry[kind] = getattr(self, "_do_" + first.kind)(first)
                 except BaseException as e:  # a failing batch fails its requests, not the server
                     self._finish([first], [e])
 
@@ -212,22 +246,10 @@ class Server:
         self._finish(items, [o.cpu().numpy() for o in outs])
 
     def _do_fresh(self, first):
-        items, used = [first], first.req.hbm_bytes(1 if first.req.ds.K == 2 else first.req.ds.K)
-        q = self._q["fresh"]
-        while len(items) < self.max_fresh_batch:
-            try:
-                nxt = q.get_nowait()
-            except queue.Empty:
-                break
-            if nxt is None:
-                q.put(None)
-                break
-            need = nxt.req.hbm_bytes(1 if nxt.req.ds.K == 2 else nxt.req.ds.K)
-            if used + need > self.budget:  # admit later, when this batch has freed its memory
-                q.put(nxt)
-                break
-            items.append(nxt)
-            used += need
+        """One batched launch of the fresh solves that fit the budget together; returns the queued
+        request that did not fit (the worker starts its next batch with it) or None."""
+        cost = lambda it: it.req.hbm_bytes(1 if it.req.ds.K == 2 else it.req.ds.K)  # noqa: E731
+        items, carry = take_batch(self._q[first.kind], first, self.max_fresh_batch, cost, self.budget)
         try:
             systems = []
             for it in items:
@@ -243,3 +265,4 @@ class Server:
             self._finish(items, outs)
         except BaseException as e:
             self._finish(items, [e] * len(items))
+        return carry
