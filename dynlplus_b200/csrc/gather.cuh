@@ -85,19 +85,27 @@ constexpr int gather_batch_lean() {
 // with one load instruction fewer per gathered row. The values stay in load order: raw[0..1] hold
 // the 256-bit half and raw[2] the 128-bit part; with hi (the row starts 16 bytes into a 32-byte
 // sector) columns 0-3 are raw[2], 4-11 raw[0..1], else columns 0-7 are raw[0..1], 8-11 raw[2].
+// Both loads carry an L2 evict-last policy: the gathered block (P in the PCG) is then the last thing
+// the streamed CSR (evict-first loads) pushes out of L2. Measured on B200 (n = 1M, degree 10, C = 9,
+// kernel harness): the direction sweep that reads P next drops from 41.1 to 37.0 us, the apply is
+// unchanged, and every iterate is bit-identical (a cache policy changes no value).
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
 __device__ __forceinline__ bool load_row12(const float *__restrict__ xr, float (&raw)[3][4]) {
   const bool hi = ((uintptr_t)xr & 16u) != 0;
   const float *p8 = xr + (hi ? 4 : 0);
   const float *p4 = xr + (hi ? 0 : 8);
-  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+  const uint64_t pol = l2_evict_last();
+  asm("ld.global.nc.L2::cache_hint.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
       : "=f"(raw[0][0]), "=f"(raw[0][1]), "=f"(raw[0][2]), "=f"(raw[0][3]), "=f"(raw[1][0]), "=f"(raw[1][1]),
         "=f"(raw[1][2]), "=f"(raw[1][3])
-      : "l"(p8));
-  const float4 f = __ldg(reinterpret_cast<const float4 *>(p4));
-  raw[2][0] = f.x;
-  raw[2][1] = f.y;
-  raw[2][2] = f.z;
-  raw[2][3] = f.w;
+      : "l"(p8), "l"(pol));
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(raw[2][0]), "=f"(raw[2][1]), "=f"(raw[2][2]), "=f"(raw[2][3])
+      : "l"(p4), "l"(pol));
   return hi;
 }
 
