@@ -1,7 +1,10 @@
-"""bench.py's roofline inputs without a GPU: the algorithmic bytes of one fused PCG iteration at the
-headline size, the committed ncu traffic file, and the flags of the profiling runs."""
+"""bench.py without a GPU: the roofline inputs (the algorithmic bytes of one fused PCG iteration at
+the headline size, the committed ncu traffic file), the flags of the profiling runs, and the
+reference arm's JSON line."""
 import json
 import os
+
+import pytest
 
 import bench
 
@@ -24,3 +27,24 @@ def test_profiling_flags_parse():
     a = bench.parse(["--steps", "1", "--warmup", "3", "--no-cpu-baseline", "--no-clocks", "--no-graphs"])
     assert a.no_graphs and a.no_clocks and a.no_cpu_baseline and a.steps == 1
     assert not bench.parse([]).no_graphs
+
+
+def test_reference_arm_prints_the_contract_line(capsys, monkeypatch):
+    """--impl reference on rank 0: the oracle port over a small graph prints one JSON line with the
+    arm's metric, config, cpu_baseline and a zero-copy e2e."""
+    monkeypatch.delenv("RANK", raising=False)
+    a = bench.parse(["--impl", "reference", "--n", "3000", "--batch", "200", "--steps", "3", "--warmup", "1",
+                     "--label-frac", "0.02"])
+    assert bench.reference_arm(a) == 0
+    lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    rec = json.loads(lines[0])
+    assert rec["impl"] == "reference" and rec["metric"] == bench.METRIC and rec["unit"] == "edge-updates/s"
+    assert rec["higher_is_better"] is True and rec["config"] == bench.config(a)
+    assert 1 <= rec["steps"] <= 3 and rec["value"] > 0
+    assert rec["ms_per_step"] == pytest.approx(1e3 * 200 / rec["value"], rel=1e-9)
+    cb = rec["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["value"] == rec["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert rec["e2e"] == {"value": rec["value"], "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
+                          "d2h_bytes_per_step": 0}
+    assert rec["latency_ms"]["p50"] <= rec["latency_ms"]["p99"]
