@@ -53,12 +53,20 @@ _SCRATCH: dict = {}
 
 
 def _scratch(tag, n, C, dt, dev, padded=False):
-    key = (tag, n, C, dt, dev, torch.cuda.current_stream().cuda_stream)  # per stream, like the workspaces
-    t = _SCRATCH.get(key)
-    if t is None:
-        t = padded_empty(n, C, dt, dev, 0.0) if padded else torch.zeros((n, C), dtype=dt, device=dev)
-        _SCRATCH[key] = t
-    return t
+    """n x C scratch matrix: one buffer per (tag, C, dtype, device, stream, padding), zero-filled when
+    allocated, grown by at least a quarter when a larger n arrives, and handed out as its first n
+    rows (same leading dimension), so systems of changing size (vertex-arrival batches, refinement of
+    systems of every size) reuse one allocation instead of keeping one per size. Its contents are
+    whatever the last user of the key left."""
+    dev = torch.device(dev)
+    sid = torch.cuda.current_stream().cuda_stream if dev.type == "cuda" else 0  # per stream, like workspaces
+    key = (tag, C, dt, dev, sid, padded)
+    buf = _SCRATCH.get(key)
+    if buf is None or buf.shape[0] < n:
+        rows = n if buf is None else max(n, buf.shape[0] + buf.shape[0] // 4)
+        buf = padded_empty(rows, C, dt, dev, 0.0) if padded else torch.zeros((rows, C), dtype=dt, device=dev)
+        _SCRATCH[key] = buf
+    return buf[:n]
 
 
 def spmm(W, X):
