@@ -15,7 +15,9 @@
 namespace dlp {
 
 namespace {
-cudaError_t g_last_cuda = cudaSuccess;
+// per calling thread, as cudaGetLastError: a thread reads the code of its own failed call even while
+// other threads (the serving loop's workers) call the library
+thread_local cudaError_t g_last_cuda = cudaSuccess;
 std::atomic<unsigned long long> g_launches{0};
 }
 
@@ -34,13 +36,12 @@ int check_launch(int kernels) {
 }
 
 int sm_count() {
-  static int cached = 0;
-  if (!cached) {
-    int dev = 0;
+  static const int cached = [] {  // initialised once, thread-safe
+    int dev = 0, c = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
-    if (cached <= 0) cached = 148;
-  }
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+    return c > 0 ? c : 148;
+  }();
   return cached;
 }
 

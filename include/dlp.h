@@ -33,7 +33,7 @@ enum {
   DLP_OK = 0,
   DLP_ERR_INVALID = 1,   /* bad pointer, size, shape or leading dimension */
   DLP_ERR_DTYPE = 2,     /* unsupported precision combination */
-  DLP_ERR_CUDA = 3,      /* a CUDA runtime call failed; dlp_last_cuda_error() has the code */
+  DLP_ERR_CUDA = 3,      /* a CUDA runtime call failed; dlp_last_cuda_error() on the calling thread has the code */
   DLP_ERR_CAP = 4,       /* iteration cap reached before convergence */
   DLP_ERR_CANCELLED = 5, /* the host cancel flag was set */
   DLP_ERR_WORKSPACE = 6, /* workspace missing or too small */
