@@ -479,7 +479,8 @@ static int b_chunk_graph(const BProblem &q, const BTiles &tl, const BCtl &c, con
   DLP_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return DLP_ERR_INVALID;
   char key[640];
-  snprintf(key, sizeof(key), "%d|%p|%p|%p|%d|%d|%p|%p|%p|%lld|%p|%lld|%p|%lld|%p|%lld|%d|%p|%p|%d|%d|%p|%d|%d|%d|%g|%d|%d",
+  // every field a captured kernel receives as an argument, exactly (the target to 17 digits)
+  snprintf(key, sizeof(key), "%d|%p|%p|%p|%d|%d|%p|%p|%p|%lld|%p|%lld|%p|%lld|%p|%lld|%d|%p|%p|%d|%d|%p|%d|%d|%d|%.17g|%d|%d",
            dev, (const void *)q.indptr, (const void *)q.col, (const void *)q.w, q.N, q.C, q.diag, q.rhs, q.Z,
            (long long)q.ldz, q.R, (long long)q.ldr, q.P, (long long)q.ldp, q.AP, (long long)q.ldap, q.dtype,
            (const void *)tl.tinst, (void *)c.done, tl.ntiles, tl.ninst, (void *)c.tp1, bp.mode, bp.patience,
