@@ -8,16 +8,22 @@ not the hot path). Generators:
   NumPy RandomState, so they reproduce the reference run on NumPy exactly.
 * `planted_partition`, `er_graph`: the benchmark workloads, seeded `numpy.random.default_rng`,
   duplicate pairs kept once (set semantics), self-loops dropped.
+* `synth`, `knn_graph`: the reference's synthetic cosine-kNN mixture (graphs.py:78-143), same
+  RandomState draws; `build_cached` / `load("synthN")` keep it as an edge-list npz under DATA_DIR.
 * `EdgeUpdates`: the edge-update stream (insert uniform non-edges / delete uniform edges).
 """
 from __future__ import annotations
 
+import os
+import re
 from dataclasses import dataclass
 
 import numpy as np
 import torch
 
 from .backend import CSR, to_dtype
+
+DATA_DIR = os.environ.get("DATA_DIR", "data")  # graph caches (dynlp/graphs.py:21)
 
 
 def _dev(device=None):
@@ -139,6 +145,72 @@ def erdos_renyi(n, K=2, deg=5.0, seed=0, dtype="float32", device=None) -> Datase
     dev = _dev(device)
     A = symmetric_from_pairs(u, v, w, n, dtype, dev)
     return Dataset(f"er-n{n}-d{deg:g}", A, _t(rs.randint(0, K, size=n).astype(np.int32), dev), K, _t(perm(n), dev))
+
+
+def knn_graph(X, k, dtype, device=None) -> CSR:
+    """Symmetric cosine kNN graph of the (L2-normalised) dense rows of X (dynlp/graphs.py:78-93):
+    each row's k most similar other rows (similarities of one row block at a time, top-k on the
+    device), every unordered pair kept once with the similarity of its first occurrence in row-major
+    order, clamped below at 1e-3. Sparse rows (the reference's TF-IDF documents) are not taken."""
+    if not torch.is_tensor(X) and not isinstance(X, np.ndarray):
+        raise TypeError("knn_graph takes dense rows (a NumPy array or a tensor)")
+    dev = _dev(device) if not torch.is_tensor(X) else X.device
+    Xt = _t(X, dev, torch.float32)
+    n = int(Xt.shape[0])
+    block = max(1, min(n, (1 << 26) // max(n, 1)))
+    nbr = torch.empty((n, k), dtype=torch.int64, device=dev)
+    sim = torch.empty((n, k), dtype=torch.float32, device=dev)
+    for s in range(0, n, block):
+        e = min(n, s + block)
+        S = Xt[s:e] @ Xt.T
+        S[torch.arange(e - s, device=dev), torch.arange(s, e, device=dev)] = -float("inf")
+        sim[s:e], nbr[s:e] = torch.topk(S, k, dim=1)
+    u = torch.arange(n, device=dev).repeat_interleave(k)
+    v = nbr.reshape(-1)
+    key = torch.minimum(u, v) * n + torch.maximum(u, v)
+    order = torch.argsort(key, stable=True)
+    ks = key[order]
+    head = torch.ones_like(ks, dtype=torch.bool)
+    head[1:] = ks[1:] != ks[:-1]
+    first = order[head]  # the first occurrence of each pair, in key order
+    return symmetric_from_pairs(u[first], v[first], sim.reshape(-1)[first].clamp(min=1e-3), n, dtype, dev)
+
+
+def synth(n=50_000, K=10, k=5, dim=16, subs=5, seed=0, dtype="float32", device=None) -> Dataset:
+    """The reference's mixture for DynLP's step 1 (dynlp/graphs.py:124-143): K classes of `subs`
+    Gaussian sub-clusters in `dim` dimensions with spreads over a factor 8, a quarter of the
+    tightest sub-clusters each shadowed by one of another class placed next to it, points on the
+    unit sphere, cosine kNN with k neighbours. The draws are the reference's, in its order, on a
+    NumPy RandomState (float32 arithmetic as there), so the points equal the reference run on NumPy."""
+    rs, perm = _rng(seed)
+    m = K * subs
+    f32 = np.float32
+    ctr = rs.standard_normal((m, dim)).astype(f32)
+    ctr *= 10 / np.linalg.norm(ctr, axis=1, keepdims=True)
+    spread = (0.4 * 8 ** rs.random_sample(m)).astype(f32)
+    for a in np.argsort(spread)[: max(2, m // 4)].tolist():
+        b = (a + subs * int(rs.randint(1, K))) % m if K > 1 else a
+        step = rs.standard_normal(dim).astype(f32)
+        spread[b] = spread[a]
+        ctr[b] = ctr[a] + step / np.linalg.norm(step) * spread[a] * dim ** 0.5
+    sub = rs.randint(0, m, size=n)
+    X = ctr[sub] + spread[sub, None] * rs.standard_normal((n, dim)).astype(f32)
+    X /= np.linalg.norm(X, axis=1, keepdims=True)
+    dev = _dev(device)
+    return Dataset(f"synth{K}", knn_graph(X, k, dtype, dev), _t((sub // subs).astype(np.int32), dev), K, _t(perm(n), dev))
+
+
+def build_cached(spec, data_dir=DATA_DIR, device=None):
+    """data_dir/<spec>.npz, built if missing (dynlp/graphs.py:187-204): `synthN` is synth(K=N) saved
+    as an upper-triangle edge list with labels (no order: loading draws the reference's). The IMDB
+    review graph (downloads, TF-IDF) is not built here."""
+    path = os.path.join(data_dir, f"{spec}.npz")
+    if os.path.exists(path):
+        return path
+    if not re.fullmatch(r"synth\d+", spec):
+        raise ValueError(f"unknown dataset {spec!r} (synthN, or an edge-list .npz; IMDB is not built here)")
+    os.makedirs(data_dir, exist_ok=True)
+    return save_npz(synth(K=int(spec[5:]), device=device), path, with_order=False)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -269,13 +341,14 @@ def save_npz(ds: Dataset, path, with_order=True):
     return path
 
 
-def load(spec: str, *, n=100_000, K=2, deg=10.0, p_in=0.85, seed=0, dtype="float32", device=None) -> Dataset:
-    """dynlp/graphs.py:207-214: the synthetic families and edge lists on disk (`*.npz`); the IMDB /
-    synth kNN sets (downloads and a kNN build) are out of scope."""
+def load(spec: str, *, n=100_000, K=2, deg=10.0, p_in=0.85, seed=0, dtype="float32", data_dir=DATA_DIR,
+         device=None) -> Dataset:
+    """dynlp/graphs.py:207-214: the synthetic families, edge lists on disk (`*.npz`) and the cached
+    synth kNN sets (`synthN`); the IMDB review graph (downloads) is out of scope."""
     if spec == "sbm":
         return sbm(n, K, deg, p_in, seed, dtype, device)
     if spec == "er":
         return erdos_renyi(n, K, deg, seed, dtype, device)
     if spec.endswith(".npz"):
         return from_npz(spec, dtype, seed, device=device)
-    raise ValueError(f"unknown dataset {spec!r} (sbm, er or an edge-list .npz)")
+    return from_npz(build_cached(spec, data_dir, device), dtype, seed, name=spec, device=device)

@@ -231,6 +231,25 @@ def gen_stream(dl):
     save("stream.npz", **out)
 
 
+def gen_graphs(dl):
+    """The synthetic kNN family (dynlp/graphs.py:78-143): two synth datasets (the reference's AMG
+    test parameters, tests/test_dynlp.py:160, and a 3-class one) and a kNN graph of random rows."""
+    from dynlp import graphs
+    out = {}
+    for i, kw in enumerate([dict(n=1200, K=2, k=6, subs=2, seed=7, dtype="float64"),
+                            dict(n=3000, K=3, k=5, dim=16, subs=5, seed=1, dtype="float32")]):
+        ds = graphs.synth(**kw)
+        out.update(csr_parts(f"s{i}_A", ds.A))
+        out.update({f"s{i}_y": np.asarray(ds.y, np.int32), f"s{i}_order": np.asarray(ds.order, np.int64),
+                    f"s{i}_K": np.int64(ds.K), f"s{i}_name": np.asarray(ds.name)})
+    rs = np.random.RandomState(5)
+    X = rs.standard_normal((700, 8)).astype(np.float32)
+    X /= np.linalg.norm(X, axis=1, keepdims=True)
+    out["knn_X"] = X
+    out.update(csr_parts("knn_A", graphs.knn_graph(X, 4, "float32")))
+    save("graphs.npz", **out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", default="/root/reference")
@@ -239,7 +258,7 @@ def main(argv=None):
     import cupy_shim
     dl = cupy_shim.install(a.reference)
     gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg,
-            "stream": gen_stream}
+            "stream": gen_stream, "graphs": gen_graphs}
     for name, fn in gens.items():
         if not a.only or name in a.only.split(","):
             fn(dl)
