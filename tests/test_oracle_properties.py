@@ -96,8 +96,8 @@ def test_path_graph_needs_the_fp64_correction():
 
 
 def test_amg_vcycle_is_symmetric_positive_definite():
-    """tests/test_dynlp.py:159-166 on an SBM system large enough for two levels (the reference's
-    kNN graph family is out of scope): the V-cycle applied to the identity is a symmetric matrix
+    """tests/test_dynlp.py:159-166 on a second graph family, an SBM system large enough for two
+    levels at the default coarsest size: the V-cycle applied to the identity is a symmetric matrix
     with positive eigenvalues."""
     S = next(batch_systems(4000, 3, 8, 7, 0.02, 0.9, 0))
     n = S["W"].shape[0]
@@ -105,4 +105,21 @@ def test_amg_vcycle_is_symmetric_positive_definite():
     assert len(amg.sizes) >= 2 and amg.sizes[0] > amg.sizes[-1]
     M = amg(np.eye(n))
     assert np.abs(M - M.T).max() <= 1e-10 * np.abs(M).max()
+    assert np.linalg.eigvalsh((M + M.T) / 2).min() > 0
+
+
+def test_amg_vcycle_spd_on_the_reference_graph():
+    """tests/test_dynlp.py:158-165 exactly: the synth kNN graph (n=1200, K=2, k=6, 2 sub-clusters,
+    seed 7), the whole graph active with 2% labels, AMG with max_coarse=50 (two levels or more)."""
+    ds = graphs.synth(1200, K=2, k=6, subs=2, seed=7, dtype="float64", device="cpu")
+    A, y = ds.A.to_scipy().astype(np.float64), ds.y.numpy()
+    lab, _, _, sched = O.stream_schedule(y, 2, ds.order.numpy(), label_frac=0.02, init_frac=1.0, n_batches=0)
+    active = np.zeros(A.shape[0], dtype=bool)
+    active[sched[0][0]] = True
+    S = O.build_system(A, y, 2, active, lab)
+    amg = O.AMGOracle(S["W"], S["s"], max_coarse=50)
+    assert len(amg.levels) >= 2
+    n = S["W"].shape[0]
+    M = amg(np.eye(n))
+    np.testing.assert_allclose(M, M.T, atol=1e-10)
     assert np.linalg.eigvalsh((M + M.T) / 2).min() > 0
