@@ -1,7 +1,8 @@
 """The oracle against the reference's own property tests (tests/test_dynlp.py), on the host: its block
 PCG matches a direct solve, the absorption bound holds for any iterate, joint class columns give the
-binary column, an fp64 correction certifies the path graph where the fp32 solve alone cannot, and
-its AMG V-cycle is a symmetric positive definite operator. These pin the checker itself; the GPU
+binary column, an fp64 correction certifies the path graph where the fp32 solve alone cannot, its
+AMG V-cycle is a symmetric positive definite operator, its FH components cut a bridge and merge a
+weak chain, and the synth kNN graph keeps its k neighbours. These pin the checker itself; the GPU
 tests compare the device path with it."""
 import numpy as np
 import pytest
@@ -123,3 +124,46 @@ def test_amg_vcycle_spd_on_the_reference_graph():
     M = amg(np.eye(n))
     np.testing.assert_allclose(M, M.T, atol=1e-10)
     assert np.linalg.eigvalsh((M + M.T) / 2).min() > 0
+
+
+def _same_partition(a, b):
+    a, b = [int(x) for x in a], [int(x) for x in b]
+    return len(set(zip(a, b))) == len(set(a)) == len(set(b))
+
+
+def _components(edges, m, tau, ground=None):
+    """new_components on an explicit undirected edge list, every vertex new (as the reference's
+    helper in tests/test_dynlp.py:49-53)."""
+    a, b, w = (np.asarray(x) for x in zip(*edges))
+    g = np.ones(m) if ground is None else np.asarray(ground, dtype=np.float64)
+    return O.new_components(m, np.concatenate([a, b]), np.concatenate([b, a]),
+                            np.concatenate([w, w]).astype(np.float32), tau, 1.0, g)
+
+
+def test_adaptive_components_cut_a_bridge_that_tau_chains():
+    """tests/test_dynlp.py:56-62: two tight cliques joined by an edge above the global mean but weak
+    relative to both are one tau component and two FH components."""
+    edges = [(a + o, b + o, 0.95 + 0.01 * ((a + b) % 3)) for o in (0, 6) for a in range(6) for b in range(a + 1, 6)]
+    edges.append((5, 6, 0.8))
+    comps = _components(edges, 12, tau=0.5)
+    assert comps["tau"][1] == 1
+    assert comps["fh"][1] == 2 and _same_partition(comps["fh"][0], [0] * 6 + [1] * 6)
+
+
+def test_adaptive_components_merge_a_sparse_cluster():
+    """tests/test_dynlp.py:65-71: a weak chain (every edge below tau) stays singletons under tau but
+    is one FH component, a component without labelled contact joining its strongest neighbour."""
+    edges = [(i, i + 1, 0.3 + 0.02 * (i % 3)) for i in range(7)]
+    comps = _components(edges, 8, tau=0.5, ground=[1, 0, 0, 0, 0, 0, 0, 0])
+    assert comps["tau"][1] == 8
+    assert comps["fh"][1] == 1
+
+
+def test_synth_graph():
+    """tests/test_dynlp.py:173-177 on graphs.synth: symmetric, similarities in (0, 1], and every
+    vertex keeps its k = 5 neighbours."""
+    ds = graphs.synth(3000, K=10, seed=1, device="cpu")
+    S = ds.A.to_scipy()
+    assert ds.n == 3000 and ds.K == 10 and abs(S - S.T).max() == 0
+    assert S.data.min() > 0 and S.data.max() <= 1
+    assert np.diff(S.indptr).min() >= 5
