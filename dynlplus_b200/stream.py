@@ -93,8 +93,36 @@ def _range_positions(beg, end):
     return beg.long()[seg] + (torch.arange(seg.numel(), device=beg.device) - excl[seg]), seg
 
 
-def new_components(rows, rbeg, rend, col, w, nl, tau, wmax, ground):
-    """DynLP step 1 for the m = len(rows) new vertices (dynlp/stream.py:67-81), on the device:
+def new_components(m, lr, lc, w, tau, wmax, ground):
+    """DynLP step 1 for m new vertices with the reference's arguments (dynlp/stream.py:67-81): every
+    stored entry lr -> lc of their rows with its weight w (lc = -1 where the neighbour is not new).
+    Each vertex's mean dissimilarity s over its live entries (w > 0) is summed in fp64 and rounded
+    to fp32; the components are those over the live entries heavier than tau between new vertices
+    ("tau") and the adaptive FH ones on 1 - w/wmax scaled by sqrt(s_u s_v) ("fh"); ground is each
+    vertex's label weight. Returns {"tau": (labels, count), "fh": (labels, count)}."""
+    dev = w.device if torch.is_tensor(w) else None
+    lr = torch.as_tensor(lr, device=dev).long()
+    lc = torch.as_tensor(lc, device=dev).long()
+    w = torch.as_tensor(w, device=dev)
+    dev = w.device
+    if m == 0:
+        z = torch.zeros(0, dtype=torch.int32, device=dev)
+        return {"tau": (z, 0), "fh": (z, 0)}
+    on = w > 0
+    dis = torch.where(on, 1 - w.double() / wmax, torch.zeros((), dtype=torch.float64, device=dev))
+    s = torch.zeros(m, dtype=torch.float64, device=dev).index_add_(0, lr, dis)
+    cnt = torch.zeros(m, dtype=torch.float64, device=dev).index_add_(0, lr, on.double())
+    s = (s / cnt.clamp(min=1)).float() + 1e-6
+    e = on & (lc >= 0)
+    r, c, we = lr[e], lc[e], w[e]
+    heavy = we > tau
+    gr = torch.as_tensor(ground, device=dev).to(torch.float32)
+    return {"tau": cc.connected_components(m, r[heavy].to(torch.int32), c[heavy].to(torch.int32)),
+            "fh": cc.adaptive_components(m, r, c, we, s[r], s[c], wmax, gr)}
+
+
+def new_components_rows(rows, rbeg, rend, col, w, nl, tau, wmax, ground):
+    """new_components over the rows of a CSR (the form the streams call), on the device:
     each one's mean dissimilarity s over its live entries (`dlp_new_dissim`, row order), then the
     components over edges heavier than tau between new vertices ("tau", the paper's) and the
     adaptive FH components on 1 - w/wmax scaled by sqrt(s_u s_v) ("fh"). `nl` maps a column id to
@@ -174,7 +202,7 @@ def build_system(ds: Dataset, active, labeled, *, eta=0.0, dtype="float32", t=0,
         nl = torch.full((n_u,), -1, dtype=torch.int64, device=dev)
         nl[new] = torch.arange(new.numel(), device=dev)
         Wd = W.data.to(dt)
-        comps = new_components(new, W.indptr[:-1], W.indptr[1:], W.indices, Wd, nl, tau, wmax,
+        comps = new_components_rows(new, W.indptr[:-1], W.indptr[1:], W.indices, Wd, nl, tau, wmax,
                                Bm[new].to(dt).sum(dim=1))
     sysd = dict(t=t, U=U, W=W, s=s.to(dt), diag=diag.to(dt), B=Bm.to(dt), rhs=rhs.to(dt).contiguous(),
                 prior=prior.to(dt), is_new=is_new, seed=seed, comps=comps, K=K, C=1 if K == 2 else K, eta=eta,
@@ -483,7 +511,7 @@ class EdgeStream:
             nl = torch.full((n,), -1, dtype=torch.int64, device=dev)
             nl[new] = torch.arange(new.numel(), device=dev)
             wd = G.data if self.dtype == torch.float32 else G.data.to(self.dtype)
-            comps = new_components(new, G.rbeg, G.rend, G.indices, wd, nl, tau, wmax, self.B[new].sum(dim=1))
+            comps = new_components_rows(new, G.rbeg, G.rend, G.indices, wd, nl, tau, wmax, self.B[new].sum(dim=1))
         self._vertex_batch = {"is_new": is_new, "seed": seed, "comps": comps}
         self._counts = None
         return self.system
