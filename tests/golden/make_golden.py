@@ -250,6 +250,39 @@ def gen_graphs(dl):
     save("graphs.npz", **out)
 
 
+def gen_api(dl):
+    """The reference's public API (the drop-in boundary): for the modules graphs, stream, solvers,
+    amg, cc and kernels, every public function's parameters, every public class's constructor and
+    public methods' parameters, and the public upper-case constants; read from the source (ast)."""
+    import ast
+    import json
+    ref = os.path.join(os.path.dirname(os.path.dirname(__import__("dynlp").__file__)), "dynlp")
+
+    def params(fn):
+        a = fn.args
+        return {"args": [x.arg for x in a.posonlyargs + a.args], "kwonly": [x.arg for x in a.kwonlyargs]}
+
+    api = {}
+    for m in ("graphs", "stream", "solvers", "amg", "cc", "kernels"):
+        tree = ast.parse(open(os.path.join(ref, m + ".py")).read())
+        mod = {"functions": {}, "classes": {}, "constants": []}
+        for node in tree.body:
+            if isinstance(node, ast.FunctionDef) and not node.name.startswith("_"):
+                mod["functions"][node.name] = params(node)
+            elif isinstance(node, ast.ClassDef) and not node.name.startswith("_"):
+                mod["classes"][node.name] = {sub.name: params(sub) for sub in node.body
+                                             if isinstance(sub, ast.FunctionDef)
+                                             and (sub.name == "__init__" or not sub.name.startswith("_"))}
+            elif isinstance(node, ast.Assign):
+                mod["constants"] += [t.id for t in node.targets
+                                     if isinstance(t, ast.Name) and t.id.isupper() and not t.id.startswith("_")]
+        api[m] = mod
+    path = os.path.join(HERE, "api.json")
+    with open(path, "w") as f:
+        json.dump(api, f, indent=1, sort_keys=True)
+    print(f"wrote {path}")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", default="/root/reference")
@@ -258,7 +291,7 @@ def main(argv=None):
     import cupy_shim
     dl = cupy_shim.install(a.reference)
     gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg,
-            "stream": gen_stream, "graphs": gen_graphs}
+            "stream": gen_stream, "graphs": gen_graphs, "api": gen_api}
     for name, fn in gens.items():
         if not a.only or name in a.only.split(","):
             fn(dl)
