@@ -26,9 +26,10 @@ from .stream import IncrementalStream, Stream
 
 # (flag, type, default, help); type None = a switch. The reference's flags (dynlp/bench.py:22-33).
 ARGS = [
-    ("--dataset", str, "sbm", "sbm | er | path/to/graph.npz"),
+    ("--dataset", str, "sbm", "sbm | er | synth2 | synth10 | path/to/graph.npz (imdb is not built here)"),
     ("--n", int, 100_000, "sbm/er size"), ("--classes", int, 2, "sbm/er classes"), ("--deg", float, 10.0, None),
     ("--p-in", float, 0.85, "SBM: fraction of intra-class edges"),
+    ("--data-dir", str, graphs.DATA_DIR, "graph caches (synthN); default: $DATA_DIR or ./data"),
     ("--label-frac", float, 0.01, None), ("--init-frac", float, 0.1, None), ("--batches", int, 10, None),
     ("--del-frac", float, 0.1, None), ("--eta-rel", float, 0.0, "grounding regulariser (x mean degree)"),
     ("--incremental", None, False, "keep the batch system resident (needed by dynlp+inc)"),
@@ -112,7 +113,8 @@ def main(argv=None):
     a, t_run = parse(argv), time.perf_counter()
     info = env_info()
     print("[env]", json.dumps(info), flush=True)
-    ds = graphs.load(a.dataset, n=a.n, K=a.classes, deg=a.deg, p_in=a.p_in, seed=a.seed, dtype=a.dtype)
+    ds = graphs.load(a.dataset, n=a.n, K=a.classes, deg=a.deg, p_in=a.p_in, seed=a.seed, dtype=a.dtype,
+                     data_dir=a.data_dir)
     sync()
     print(f"[data] {ds.name}: n={ds.n:,} nnz={ds.nnz:,} K={ds.K} ({time.perf_counter() - t_run:.1f}s, "
           f"gpu mem {mem_used_gb():.1f} GB)", flush=True)

@@ -277,6 +277,15 @@ def gen_api(dl):
                 mod["constants"] += [t.id for t in node.targets
                                      if isinstance(t, ast.Name) and t.id.isupper() and not t.id.startswith("_")]
         api[m] = mod
+    # the streaming benchmark's command line and CSV columns (dynlp/bench.py:21-38)
+    tree = ast.parse(open(os.path.join(ref, "bench.py")).read())
+    for node in tree.body:
+        if isinstance(node, ast.Assign) and isinstance(node.targets[0], ast.Name):
+            if node.targets[0].id == "ARGS":
+                api["bench_args"] = [{"flag": e.elts[0].value, "switch": isinstance(e.elts[1], ast.Constant),
+                                      "default": ast.unparse(e.elts[2])} for e in node.value.elts]
+            elif node.targets[0].id == "FIELDS":
+                api["bench_fields"] = [e.value for e in node.value.elts]
     path = os.path.join(HERE, "api.json")
     with open(path, "w") as f:
         json.dump(api, f, indent=1, sort_keys=True)

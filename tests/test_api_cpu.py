@@ -2,6 +2,7 @@
 amg, cc and kernels exists here with its parameters in the same order (positional) or among ours
 (keyword-only), as recorded from the reference's source in tests/golden/api.json. The IMDB review
 pipeline (downloads, TF-IDF over sparse rows) is the one part left out."""
+import ast
 import importlib
 import inspect
 import json
@@ -34,6 +35,8 @@ def test_public_api_matches_the_reference():
         api = json.load(f)
     problems = []
     for m, spec in api.items():
+        if m.startswith("bench_"):
+            continue
         ours = importlib.import_module(f"dynlplus_b200.{m}")
         for c in spec["constants"]:
             if not hasattr(ours, c):
@@ -55,3 +58,24 @@ def test_public_api_matches_the_reference():
                     continue
                 _check(f"{m}.{cls}.{meth}", getattr(getattr(ours, cls), meth), want, problems)
     assert not problems, "\n".join(problems)
+
+
+def test_streaming_benchmark_flags_and_columns_match_the_reference():
+    """dynlp/bench.py:21-38: the same flags (switches as switches, the same defaults except the
+    dataset, whose reference default is the IMDB graph) and the same CSV columns in order."""
+    from dynlplus_b200 import bench
+    with open(os.path.join(GOLDEN, "api.json")) as f:
+        api = json.load(f)
+    assert bench.FIELDS == api["bench_fields"]
+    ours = {flag: (typ is None, default) for flag, typ, default, _ in bench.ARGS}
+    for a in api["bench_args"]:
+        assert a["flag"] in ours, a["flag"]
+        switch, default = ours[a["flag"]]
+        assert switch == a["switch"], a["flag"]
+        if a["flag"] == "--dataset":
+            assert default == "sbm"  # imdb needs downloads; the synthetic graphs stay available
+        elif a["flag"] == "--data-dir":
+            from dynlplus_b200 import graphs
+            assert default == graphs.DATA_DIR
+        else:
+            assert default == ast.literal_eval(a["default"]), a["flag"]
