@@ -286,6 +286,14 @@ def gen_api(dl):
                                       "default": ast.unparse(e.elts[2])} for e in node.value.elts]
             elif node.targets[0].id == "FIELDS":
                 api["bench_fields"] = [e.value for e in node.value.elts]
+    # the kernel micro-benchmark's flags and CSV columns (dynlp/kernelbench.py:21-63)
+    tree = ast.parse(open(os.path.join(ref, "kernelbench.py")).read())
+    api["kernelbench_args"] = [{"flag": t.elts[0].value, "default": ast.unparse(t.elts[2])} for t in ast.walk(tree)
+                               if isinstance(t, ast.Tuple) and len(t.elts) == 3 and isinstance(t.elts[0], ast.Constant)
+                               and isinstance(t.elts[0].value, str) and t.elts[0].value.startswith("--")]
+    api["kernelbench_fields"] = next([k.arg for k in c.keywords] for c in ast.walk(tree)
+                                     if isinstance(c, ast.Call) and isinstance(c.func, ast.Name)
+                                     and c.func.id == "dict" and c.keywords)
     path = os.path.join(HERE, "api.json")
     with open(path, "w") as f:
         json.dump(api, f, indent=1, sort_keys=True)
