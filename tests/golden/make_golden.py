@@ -300,6 +300,58 @@ def gen_api(dl):
     print(f"wrote {path}")
 
 
+def gen_matrix(dl):
+    """The reference's results matrix (scripts/matrix.py) on a synthetic results directory: CSV rows
+    of the streaming benchmark's FIELDS for two datasets and five solvers; stores the inputs and the
+    matrix.csv / matrix.md the reference's script writes for them."""
+    import importlib.util
+    import shutil
+    import tempfile
+    from dynlp.bench import FIELDS
+    rs = np.random.RandomState(3)
+    out_dir = os.path.join(HERE, "matrix")
+    shutil.rmtree(out_dir, ignore_errors=True)
+    os.makedirs(out_dir)
+    with tempfile.TemporaryDirectory() as d:
+        for tag, nb in (("sbm-20k", 3), ("er-50k", 4)):
+            rows = []
+            for solver in ("dynlp", "itlp", "dynlp+auto", "dynlp-fh", "dynlp+inc"):
+                for b in range(nb):
+                    r = {f: "" for f in FIELDS}
+                    r.update(tag=tag, dataset=tag.split("-")[0], K=3, batch=b, solver=solver, n_active=1000 * (b + 5),
+                             n_u=900 * (b + 5), nnz=8000 * (b + 5), inserted=500, deleted=50,
+                             iters=int(rs.randint(5, 400)), edges=int(rs.randint(10**5, 10**7)),
+                             sweeps=float(rs.randint(1, 90)), ms=round(float(rs.uniform(1, 300)), 3),
+                             setup_ms=round(float(rs.uniform(0, 5)), 3),
+                             path=["inc-push", "inc-pcg"][int(rs.randint(0, 2))] if solver == "dynlp+inc" else "pcg",
+                             err_max=float(rs.uniform(1e-6, 1e-2)) if solver != "itlp" or b else "",
+                             cert_self=float(rs.uniform(1e-5, 1e-3)), cert_post=float(rs.uniform(1e-5, 1e-3)),
+                             hmax=float(rs.uniform(1, 50)), hmax_ref=float(rs.uniform(1, 50)),
+                             agree=float(rs.uniform(0.9, 1)), acc_true=round(float(rs.uniform(0.6, 0.99)), 4),
+                             build_ms=round(float(rs.uniform(5, 50)), 3), ref_ms=round(float(rs.uniform(10, 90)), 3),
+                             run_s=round(float(rs.uniform(20, 40)), 2), delta=1e-4, tol=1e-3, dtype="float32",
+                             group="auto")
+                    rows.append(r)
+            path = os.path.join(d, f"{tag}.csv")
+            import csv as _csv
+            with open(path, "w", newline="") as fh:
+                w = _csv.DictWriter(fh, fieldnames=FIELDS)
+                w.writeheader()
+                w.writerows(rows)
+            shutil.copy(path, os.path.join(out_dir, f"{tag}.csv"))
+        root = os.path.dirname(os.path.dirname(os.path.abspath(dl.__file__)))
+        spec = importlib.util.spec_from_file_location("ref_matrix", os.path.join(root, "scripts", "matrix.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        import contextlib
+        with open(os.devnull, "w", encoding="utf-8") as sink, contextlib.redirect_stdout(sink):
+            mod.main(d)
+        for name in ("matrix.csv", "matrix.md"):
+            text = open(os.path.join(d, name), encoding="utf-8").read().replace(d, "RESULTS_DIR")
+            open(os.path.join(out_dir, "expected_" + name), "w", encoding="utf-8").write(text)
+    print(f"wrote {out_dir}")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", default="/root/reference")
@@ -308,7 +360,7 @@ def main(argv=None):
     import cupy_shim
     dl = cupy_shim.install(a.reference)
     gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg,
-            "stream": gen_stream, "graphs": gen_graphs, "api": gen_api}
+            "stream": gen_stream, "graphs": gen_graphs, "api": gen_api, "matrix": gen_matrix}
     for name, fn in gens.items():
         if not a.only or name in a.only.split(","):
             fn(dl)
