@@ -142,16 +142,20 @@ __global__ void k_dedupe(const int32_t *__restrict__ iu, const int32_t *__restri
   atomicExch(err, DLP_ERR_DEVICE);  // table full: cannot happen with 2x capacity
 }
 
+// Insertions run in two launches so that no row is searched while another thread appends to it.
+// k_insert_find looks up both directed entries of every owned insertion in the rows as they stand
+// before the batch's appends (stale column ids beyond rend are never read), and k_insert_apply then
+// appends the missing ones and sets the weights. Each undirected pair has one owner (the dedupe), so
+// the entries a pass touches are its own.
 __global__ void __launch_bounds__(kGThreads)
-    k_graph_insert(int32_t n, const int32_t *__restrict__ rbeg, int32_t *rend, const int32_t *__restrict__ rcap,
-                   int32_t *col, float *aw, float *w, const int32_t *__restrict__ iu, const int32_t *__restrict__ iv,
-                   const float *__restrict__ iw, int32_t ni, const unsigned long long *__restrict__ keys,
-                   const int32_t *__restrict__ best, uint32_t mask, const uint8_t *__restrict__ umask,
-                   const uint8_t *__restrict__ labeled, const int32_t *__restrict__ y, int32_t K, double *rowsum,
-                   double *B, uint8_t *changed, int32_t *overflow, int32_t *n_applied) {
+    k_insert_find(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+                  const int32_t *__restrict__ col, const int32_t *__restrict__ iu, const int32_t *__restrict__ iv,
+                  int32_t ni, const unsigned long long *__restrict__ keys, const int32_t *__restrict__ best,
+                  uint32_t mask, int32_t *__restrict__ slot_a, int32_t *__restrict__ slot_b) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ni) return;
   int32_t a = iu[i], b = iv[i];
+  slot_a[i] = -2;  // -2: not this insertion's edge (invalid, a self-loop or a later duplicate owns it)
   if ((unsigned)a >= (unsigned)n || (unsigned)b >= (unsigned)n || a == b) return;
   if (a > b) {
     const int32_t t = a;
@@ -164,35 +168,53 @@ __global__ void __launch_bounds__(kGThreads)
     if (keys[h] == key) break;
     h = (h + 1) & mask;
   }
-  if (keys[h] != key || best[h] != (int32_t)i) return;  // a later duplicate owns this edge
+  if (keys[h] != key || best[h] != (int32_t)i) return;
+  slot_a[i] = find_entry(col, rbeg[a], rend[a], b);
+  slot_b[i] = find_entry(col, rbeg[b], rend[b], a);
+}
+
+__global__ void __launch_bounds__(kGThreads)
+    k_insert_apply(int32_t n, int32_t *rend, const int32_t *__restrict__ rcap, int32_t *col, float *aw, float *w,
+                   const int32_t *__restrict__ iu, const int32_t *__restrict__ iv, const float *__restrict__ iw,
+                   int32_t ni, const int32_t *__restrict__ slot_a, const int32_t *__restrict__ slot_b,
+                   const uint8_t *__restrict__ umask, const uint8_t *__restrict__ labeled,
+                   const int32_t *__restrict__ y, int32_t K, double *rowsum, double *B, uint8_t *changed,
+                   int32_t *overflow, int32_t *n_applied) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ni) return;
+  int ja = slot_a[i];
+  if (ja == -2) return;
+  int jb = slot_b[i];
+  int32_t a = iu[i], b = iv[i];
+  if (a > b) {
+    const int32_t t = a;
+    a = b;
+    b = t;
+  }
   const float wn = iw ? iw[i] : 1.0f;
-  float old = 0.0f;
-  int ja = find_entry(col, rbeg[a], rend[a], b);
-  if (ja >= 0) {
-    old = atomicExch(aw + ja, wn);
-  } else {
+  const float old = ja >= 0 ? aw[ja] : 0.0f;
+  if (ja < 0) {
     ja = atomicAdd(rend + a, 1);
     if (ja >= rcap[a]) {
       atomicExch(overflow, 1);
       return;
     }
     col[ja] = b;
-    aw[ja] = wn;
+    aw[ja] = 0.0f;  // a tombstone until the mirror entry is in place too
     w[ja] = 0.0f;
   }
-  int jb = find_entry(col, rbeg[b], rend[b], a);
   if (jb < 0) {
     jb = atomicAdd(rend + b, 1);
     if (jb >= rcap[b]) {
-      // keep the graph symmetric: row a's entry goes back to its old weight (a tombstone when new);
-      // the retry after the rebuild finds it and completes the insertion
+      // row a keeps its entry at the old weight (a tombstone when new): the retry after the
+      // rebuild finds it and completes the insertion
       atomicExch(overflow, 1);
-      aw[ja] = old;
       return;
     }
     col[jb] = a;
     w[jb] = 0.0f;
   }
+  aw[ja] = wn;
   aw[jb] = wn;
   if (wn != old) account(a, b, ja, jb, wn, wn - old, w, umask, labeled, y, K, rowsum, B, changed);
   if (n_applied) atomicAdd(n_applied, 1);
@@ -407,7 +429,8 @@ int dlp_graph_delete(int32_t n, const int32_t *rbeg, int32_t *rend, int32_t *col
 
 size_t dlp_graph_insert_workspace_bytes(int32_t ni) {
   const size_t ts = table_size(ni > 0 ? ni : 1);
-  return ts * sizeof(unsigned long long) + ts * sizeof(int32_t) + 256;
+  const size_t m = (size_t)(ni > 0 ? ni : 1);
+  return ts * sizeof(unsigned long long) + ts * sizeof(int32_t) + 2 * m * sizeof(int32_t) + 256;
 }
 
 int dlp_graph_insert(int32_t n, const int32_t *rbeg, int32_t *rend, const int32_t *rcap, int32_t *col, float *aw,
@@ -425,13 +448,16 @@ int dlp_graph_insert(int32_t n, const int32_t *rbeg, int32_t *rend, const int32_
   const uint32_t ts = table_size(ni);
   unsigned long long *keys = (unsigned long long *)ws;
   int32_t *best = (int32_t *)(keys + ts);
+  int32_t *slot_a = best + ts;
+  int32_t *slot_b = slot_a + ni;
   DLP_CUDA(cudaMemsetAsync(keys, 0xff, ts * sizeof(unsigned long long), s));
   DLP_CUDA(cudaMemsetAsync(best, 0xff, ts * sizeof(int32_t), s));
   k_dedupe<<<grid1(ni), kGThreads, 0, s>>>(iu, iv, ni, keys, best, ts - 1, n, err);
-  k_graph_insert<<<grid1(ni), kGThreads, 0, s>>>(n, rbeg, rend, rcap, col, aw, w, iu, iv, iw, ni, keys, best, ts - 1,
-                                                  umask, labeled, y, K, rowsum, B, changed, overflow, n_applied);
+  k_insert_find<<<grid1(ni), kGThreads, 0, s>>>(n, rbeg, rend, col, iu, iv, ni, keys, best, ts - 1, slot_a, slot_b);
+  k_insert_apply<<<grid1(ni), kGThreads, 0, s>>>(n, rend, rcap, col, aw, w, iu, iv, iw, ni, slot_a, slot_b, umask,
+                                                  labeled, y, K, rowsum, B, changed, overflow, n_applied);
   k_clamp_rend<<<grid1(n), kGThreads, 0, s>>>(n, rend, rcap);
-  return check_launch(3);
+  return check_launch(4);
 }
 
 int dlp_graph_toggle(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *aw, float *w,

@@ -335,3 +335,63 @@ def test_incremental_push_path_on_small_batches():
         err = np.abs(solver.Z.cpu().numpy()[U, :K] - Fd[U]).max()
         assert st.cert <= 1e-3 * 1.0001 and err <= st.cert * 1.05 + 1e-9, (st.path, err, st.cert)
     assert "inc-push" in paths, paths
+
+
+def _empty_i32():
+    return np.zeros(0, np.int32)
+
+
+@pytest.mark.parametrize("order", ["appends_first", "reinserts_first"])
+def test_reinsert_of_squeezed_edges_next_to_appends(order):
+    """Edges deleted in one batch and inserted again in the next, in the same batch as insertions
+    of new edges into the same rows. Each deleted edge is its row's last stored entry, so after the
+    squeeze its column id is still in the freed slot, which the new edges of that row are appended
+    into: a lookup that ran while appends were in flight could take that slot for the deleted edge.
+    The resident graph must equal the oracle's graph after each batch, symmetric and with every
+    weight in place."""
+    n, K = 20_000, 3
+    ds = graphs.er_graph(n, 8, K, seed=21)
+    lab = graphs.label_mask(n, 0.02, seed=21)
+    es = stream.EdgeStream(ds, lab)
+    A_sc = ds.A.to_scipy().astype(np.float64)
+    rbeg, rend = es.G.rbeg.cpu().numpy(), es.G.rend.cpu().numpy()
+    col = es.G.indices.cpu().numpy()
+    rng = np.random.default_rng(0)
+    rows = rng.choice(n, 6000, replace=False)
+    last = {}
+    for a in rows:
+        if rend[a] > rbeg[a]:
+            c = int(col[rend[a] - 1])
+            last[(min(a, c), max(a, c))] = a
+    du = np.array([k[0] for k in last], np.int32)
+    dv = np.array([k[1] for k in last], np.int32)
+    es.apply_edges(del_u=du, del_v=dv)
+    A_sc = O.apply_edges(A_sc, _empty_i32(), _empty_i32(), np.zeros(0), du, dv)
+    G = es.G.to_csr("aw").to_scipy().astype(np.float64)
+    assert abs(G - A_sc).max() == 0
+    # the next batch: the deleted edges again (weight 2) and a new edge (weight 3) on each of their rows
+    Acoo = A_sc.tolil()
+    nu, nv = [], []
+    for (a, c), r in last.items():
+        while True:
+            b = int(rng.integers(0, n))
+            if b != r and Acoo[r, b] == 0 and (min(r, b), max(r, b)) not in last:
+                break
+        nu.append(r)
+        nv.append(b)
+    nu, nv = np.array(nu, np.int32), np.array(nv, np.int32)
+    if order == "appends_first":
+        iu, iv = np.concatenate([nu, du]), np.concatenate([nv, dv])
+        iw = np.concatenate([np.full(nu.size, 3.0), np.full(du.size, 2.0)]).astype(np.float32)
+    else:
+        iu, iv = np.concatenate([du, nu]), np.concatenate([dv, nv])
+        iw = np.concatenate([np.full(du.size, 2.0), np.full(nu.size, 3.0)]).astype(np.float32)
+    S = es.apply_edges(ins_u=iu, ins_v=iv, ins_w=iw)
+    A_sc = O.apply_edges(A_sc, iu, iv, iw.astype(np.float64), _empty_i32(), _empty_i32())
+    G = es.G.to_csr("aw").to_scipy().astype(np.float64)
+    assert abs(G - G.T).max() == 0
+    assert abs(G - A_sc).max() == 0
+    # the grounded system follows the graph
+    ref = _oracle_edge_system(A_sc, ds.y.cpu().numpy(), K, lab.cpu().numpy())
+    np.testing.assert_array_equal(np.flatnonzero(S.solved.cpu().numpy()), ref["U"])
+    np.testing.assert_allclose(S.astype(torch.float64).diag.cpu().numpy()[ref["U"]], ref["diag"], rtol=1e-12)
