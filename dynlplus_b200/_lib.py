@@ -26,6 +26,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_last_cuda_error": ("", ct.c_int),
     "dlp_sm_count": ("", ct.c_int),
     "dlp_launch_count": ("", ct.c_ulonglong),
+    "dlp_set_cancel_word": ("p", ct.c_int),
     "dlp_spmm": ("ppppiipipqipddpqdpqiiidp", ct.c_int),
     "dlp_spmm_lowp": ("ppppiipqpqpddpqidp", ct.c_int),
     "dlp_frontier_jacobi": ("ppppipiipqpqpdpqipppidp", ct.c_int),
@@ -62,6 +63,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cols_scale": ("iipqipipqip", ct.c_int),
     "dlp_fused_push_workspace_bytes": ("ii", ct.c_size_t),
     "dlp_fused_push": ("ppppiiippqpqippiiiipzpppp", ct.c_int),
+    "dlp_fused_push_counts": ("ppp", ct.c_int),
     "dlp_amg_match_workspace_bytes": ("i", ct.c_size_t),
     "dlp_amg_match": ("ipppipppzp", ct.c_int),
     "dlp_amg_members_workspace_bytes": ("i", ct.c_size_t),
@@ -109,11 +111,22 @@ def lib():
     return _lib
 
 
-def call(name: str, *args) -> None:
-    """Call an int-returning entry point and raise DLPError on a non-zero status."""
+class Cancelled(DLPError):
+    """A device-side loop stopped because the registered cancel word was set (DLP_ERR_CANCELLED)."""
+
+
+DLP_ERR_CAP, DLP_ERR_CANCELLED = 4, 5
+
+
+def call(name: str, *args, allow: tuple = ()) -> int:
+    """Call an int-returning entry point; returns its status when it is 0 or listed in `allow`,
+    raises Cancelled for DLP_ERR_CANCELLED and DLPError for any other non-zero status."""
     st = getattr(lib(), name)(*args)
-    if st != 0:
+    if st != 0 and st not in allow:
+        if st == DLP_ERR_CANCELLED:
+            raise Cancelled(name, st)
         raise DLPError(name, st, lib().dlp_last_cuda_error() if st == 3 else 0)
+    return st
 
 
 def exported_symbols() -> list[str]:

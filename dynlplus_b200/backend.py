@@ -172,3 +172,24 @@ class CSR:
 
 def csr(data, indices, indptr, shape) -> CSR:
     return CSR(data, indices, indptr, tuple(shape))
+
+
+_CANCEL = None  # the registered cancel word (kept alive while registered)
+
+
+def set_cancel_word(word):
+    """Register a one-element int32 tensor that the device-side solve loops poll (dlp_set_cancel_word):
+    while it holds a non-zero value, a running PCG stops at its next stop decision and a running push
+    at its next round, and the call raises `_lib.Cancelled`. The tensor lives in device memory or in
+    pinned host memory (`torch.zeros(1, dtype=torch.int32).pin_memory()`, writable from the host
+    while the solve runs). None unregisters."""
+    global _CANCEL
+    from . import _lib
+    if word is not None:
+        if word.dtype != torch.int32 or word.numel() < 1:
+            raise ValueError("the cancel word is a one-element int32 tensor")
+        if not (word.is_cuda or word.is_pinned()):
+            raise ValueError("the cancel word must be in device memory or pinned host memory")
+    # pinned host memory is addressed by the same pointer on the device (unified addressing)
+    _lib.call("dlp_set_cancel_word", word.data_ptr() if word is not None else None)
+    _CANCEL = word

@@ -18,6 +18,13 @@ void set_cuda_error(cudaError_t e);
 int check_launch(int kernels = 1);  // cudaGetLastError -> status; counts `kernels` launches
 int sm_count();
 void note_launches(unsigned long long k);  // kernels launched outside check_launch (graph replays)
+// The word dlp_set_cancel_word registered (NULL: none). Device loops read it with volatile loads.
+const int32_t *cancel_word();
+
+// One thread's read of the cancel word (host-mapped or device memory; NULL reads as 0).
+__device__ __forceinline__ int read_cancel(const int32_t *word) {
+  return word ? *(const volatile int32_t *)word : 0;
+}
 
 #define DLP_TRY(expr)                 \
   do {                                \
@@ -120,6 +127,20 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t value, int32_t *o
   if (lane == leader) base = atomicAdd(count, __popc(ballot));
   base = __shfl_sync(mask, base, leader);
   if (pred) out[base + __popc(ballot & ((1u << lane) - 1u))] = value;
+}
+
+// Warp-aggregated slot reservation: the lanes with pred=true get consecutive slots of `count`
+// (lane order within the warp, one atomic per warp); returns the lane's slot, or -1 without pred.
+__device__ __forceinline__ int warp_reserve(bool pred, int32_t *count) {
+  const unsigned mask = __activemask();
+  const unsigned ballot = __ballot_sync(mask, pred);
+  if (!ballot) return -1;
+  const int lane = lane_id();
+  const int leader = __ffs(ballot) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(ballot));
+  base = __shfl_sync(mask, base, leader);
+  return pred ? base + __popc(ballot & ((1u << lane) - 1u)) : -1;
 }
 
 // Deterministic warp-wide sum (or max) of base[b * stride] over b < nb: lane l takes b = l, l+32,

@@ -24,7 +24,8 @@ namespace dlp {
 
 struct PcgCtl {
   int32_t iters;
-  int32_t done;   // 0 running, 1 stop proposed, 2 stalled, 3 iteration cap, 5 converged (confirmed)
+  int32_t done;   // 0 running, 1 stop proposed, 2 stalled, 3 iteration cap, 5 converged (confirmed),
+                  // 6 cancelled (the host's cancel word was set)
   int32_t stall;
   int32_t go;     // set by K1 for the iteration in flight
   uint32_t cnt1, cnt2;
@@ -41,6 +42,7 @@ struct PcgBufs {
   // set only in the kernels of the device-side loop graph: K2 writes the loop's continue flag
   int has_cond;
   cudaGraphConditionalHandle cond;
+  const int32_t *cancel;  // the registered cancel word (NULL: none), read at every stop decision
 };
 
 constexpr int kUpdBlocksPerSM = 8;
@@ -76,6 +78,7 @@ static PcgBufs carve(void *ws, int C) {
   B.nbmax = (int)nb;
   B.has_cond = 0;
   B.cond = 0;
+  B.cancel = nullptr;
   return B;
 }
 
@@ -481,6 +484,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
         else if (phase == 1) ctl->done = 0;
       }
       if (ctl->done == 0 && ctl->iters >= ctl->max_iter) ctl->done = 3;
+      if (ctl->done == 0 && read_cancel(B.cancel)) ctl->done = 6;
       if (ctl->bad) ctl->done = 4;
       ctl->cnt2 = 0;
       // the device-side loop runs another iteration only while the solve is running
@@ -813,7 +817,7 @@ static int graph_key(const PcgProblem &q, const PcgBufs &B, int k, GraphKey *key
                    (uintptr_t)q.ldz, (uintptr_t)q.R, (uintptr_t)q.ldr, (uintptr_t)q.P, (uintptr_t)q.ldp,
                    (uintptr_t)q.AP, (uintptr_t)q.ldap, (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)k,
                    (uintptr_t)q.w_lo, (uintptr_t)q.P_lo, (uintptr_t)q.ld_lo, (uintptr_t)L.G, (uintptr_t)L.LV,
-                   (uintptr_t)L.VW, (uintptr_t)L.VPL}};
+                   (uintptr_t)L.VW, (uintptr_t)L.VPL, (uintptr_t)B.cancel}};
   return DLP_OK;
 }
 
@@ -972,6 +976,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   PcgProblem q{rbeg, rend, col, w, w_dtype, n, C, diag, rhs, ldrhs, Z, ldz, R, ldr, P, ldp, AP, ldap, dtype, avg_deg,
                w_lo, P_lo, ld_lo};
   PcgBufs B = carve(ws, C);
+  B.cancel = cancel_word();
   PcgCtl h{};
   h.mode = mode & 3;
   h.patience = patience > 0 ? patience : 400;
@@ -1056,6 +1061,8 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   if (viol_out) *viol_out = cur.viol;
   if (relres_out) *relres_out = cur.relres;
   if (status_out) *status_out = cur.done;
+  if (cur.done == 3) return DLP_ERR_CAP;
+  if (cur.done == 6) return DLP_ERR_CANCELLED;
   return DLP_OK;
 }
 

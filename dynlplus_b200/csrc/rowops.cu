@@ -19,7 +19,10 @@ namespace {
 // other threads (the serving loop's workers) call the library
 thread_local cudaError_t g_last_cuda = cudaSuccess;
 std::atomic<unsigned long long> g_launches{0};
+std::atomic<const int32_t *> g_cancel{nullptr};
 }
+
+const int32_t *cancel_word() { return g_cancel.load(std::memory_order_acquire); }
 
 void set_cuda_error(cudaError_t e) { g_last_cuda = e; }
 
@@ -430,6 +433,11 @@ int dlp_last_cuda_error(void) { return (int)g_last_cuda; }
 unsigned long long dlp_launch_count(void) { return g_launches.load(); }
 
 int dlp_sm_count(void) { return sm_count(); }
+
+int dlp_set_cancel_word(const int32_t *word) {
+  g_cancel.store(word, std::memory_order_release);
+  return DLP_OK;
+}
 
 int dlp_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype,
              int32_t n_rows, const int32_t *rows, int32_t C, const void *X, int64_t ldx, int x_dtype,

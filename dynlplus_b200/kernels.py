@@ -97,12 +97,21 @@ class FusedPush:
         eps_h = (ct.c_double * C)(*[float(e) for e in (eps.tolist() if torch.is_tensor(eps) else eps)])
         ws = workspace("fused_push").get(_lib.lib().dlp_fused_push_workspace_bytes(n, C))
         rounds, ok, edges = ct.c_int32(0), ct.c_int32(0), ct.c_ulonglong(0)
+        # a run cut short by max_rounds reports converged=False, as the reference's does (:424-433)
         _lib.call("dlp_fused_push", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C,
                   ptr(diag.to(Z.dtype).contiguous()), ptr(Z), ld(Z), ptr(R), ld(R), code(Z), eps_h, ptr(cand),
                   int(cand.numel()), int(max_rounds), int(check_every), int(bool(use_graph)), ptr(ws), ws.numel(),
-                  ct.byref(rounds), ct.byref(ok), ct.byref(edges), stream())
+                  ct.byref(rounds), ct.byref(ok), ct.byref(edges), stream(), allow=(_lib.DLP_ERR_CAP,))
         self.edges = int(edges.value)
+        self._ws = ws
         return int(rounds.value), bool(ok.value), int(edges.value)
+
+    def counts(self):
+        """(rounds, frontier rows, touched rows, edge visits) summed over the last run's rounds."""
+        import ctypes as ct
+        out = (ct.c_ulonglong * 4)()
+        _lib.call("dlp_fused_push_counts", ptr(self._ws), out, stream())
+        return tuple(int(x) for x in out)
 
 
 class FrontierOps:

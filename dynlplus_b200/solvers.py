@@ -223,7 +223,8 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
               float(target_relres or 0.0), mode, int(max_iter), int(patience), int(check_every),
               int(bool(GRAPHS if use_graph is None else use_graph)),
               W.nnz / max(n, 1), ptr(ws), ws.numel(), ct.byref(it), ct.byref(viol), ct.byref(rel), ct.byref(status),
-              stream(), ptr(w_lo), ptr(P_lo), ld(P_lo) if P_lo is not None else 0)
+              stream(), ptr(w_lo), ptr(P_lo), ld(P_lo) if P_lo is not None else 0,
+              allow=(_lib.DLP_ERR_CAP,))  # at the iteration cap the iterate stands, as in the reference
     if ev is not None:
         ev[1].record()
         PCG_EVENTS.append((ev[0], ev[1], it.value, n, C))

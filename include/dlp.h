@@ -55,6 +55,15 @@ int dlp_sm_count(void);
 /* kernels this library has launched in the process so far (graph replays count their kernels) */
 unsigned long long dlp_launch_count(void);
 
+/* Cancellation of the device-side loops (no reference counterpart: the reference has no way to stop
+ * a solve). `word` points at an int32 the device can read: device memory, or pinned host memory
+ * (cudaHostAlloc / cudaMallocHost, usable on the device under unified addressing). While it holds a
+ * non-zero value, dlp_pcg stops at its next stop decision (once per iteration) and dlp_fused_push
+ * at its next round, each returning DLP_ERR_CANCELLED with consistent outputs (the iterate and its
+ * residual, or Z and R with no residual taken but not pushed). NULL unregisters. One word per
+ * process; calls already running keep the word they started with. */
+int dlp_set_cancel_word(const int32_t *word);
+
 /* ---- (a) row-major SpMM with fused axpy / residual epilogue -------------------------------
  * Replaces kernels.spmm_axpy (dynlp/kernels.py:140-166, :240-266, launcher :377-393),
  * solvers.apply_A (dynlp/solvers.py:46-49) and the changed-row residual refresh of
@@ -218,8 +227,9 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
  * where conditional nodes are unavailable, chunks of check_every iterations are replayed as graphs.
  * use_graph == 0 launches the kernels directly and reads the control block every check_every
  * iterations.
- * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap,
- * 4 breakdown (a non-finite residual entry). eps may be NULL when bit 0 is unused.
+ * Synchronous: returns after the solve; *status_out = 5 converged, 2 stalled, 3 iteration cap
+ * (the call returns DLP_ERR_CAP), 4 breakdown (a non-finite residual entry), 6 cancelled (returns
+ * DLP_ERR_CANCELLED); the outputs are filled in every case. eps may be NULL when bit 0 is unused.
  * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C).
  * Mixed precision (fp32 only): with w_lo (bf16 copy of w) and P_lo (a bf16 n x C buffer, ld_lo) the
  * SpMM gathers the bf16 mirror of P that the direction update keeps (fp32 accumulation), while the
@@ -325,21 +335,33 @@ int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, ui
                       int32_t *count, dlp_stream_t stream);
 
 
-/* ---- (b) asynchronous residual push with device-resident frontiers ---------------------------
- * Replaces FusedPush (push_round + compact_frontier, dynlp/kernels.py:269-350; run :415-433):
- * starting from the candidate rows cand[0..ncand) (device), repeat rounds of
- *   r = atomicExch(R[u,:], 0); d = r / diag[u]; Z[u,:] += d; R[v,:] += w_uv d (live entries only)
- * and keep the touched rows with any_c |R[v,c]| > eps[c] * diag[v] as the next frontier, until the
- * frontier is empty or max_rounds rounds ran. The host reads one counter every check_every rounds
- * (chunks replayed as a CUDA graph when use_graph != 0). eps is a HOST array of C doubles. C <= 33.
+/* ---- (b) residual push with device-resident frontiers ------------------------------------------
+ * Replaces FusedPush.run (dynlp/kernels.py:396-433; its kernels push_round + compact_frontier,
+ * :269-350) with the round semantics of the synchronous push (dynlp/solvers.py:100-125): starting
+ * from the candidate rows cand[0..ncand) (device, distinct), every round takes the residual of all
+ * its frontier rows first,
+ *   d = R[u,:] / diag[u]; Z[u,:] += d; R[u,:] = 0,
+ * then pushes R[v,:] += w_uv d over their live entries, and the touched rows with
+ * any_c |R[v,c]| > eps[c] * diag[v] (compared in the working precision) form the next frontier,
+ * until the frontier is empty or max_rounds rounds ran. The frontiers are those of the synchronous
+ * push up to the order of the floating-point atomic sums. With use_graph != 0 the rounds run as a
+ * device-side loop (a CUDA graph with a conditional WHILE node; check_every unused); otherwise the
+ * host reads the control block every check_every rounds. eps is a HOST array of C doubles. C <= 33.
  * (dtype, w_dtype) in {(f32,f32), (f64,f32), (f64,f64)}. Workspace: dlp_fused_push_workspace_bytes.
- * Synchronous: *rounds_out, *converged_out (1 = no row violates), *edges_out (edge visits). */
+ * Synchronous: *rounds_out, *converged_out (1 = no row violates), *edges_out (stored entries of the
+ * frontier rows, the reference's edge visits). Returns DLP_ERR_CAP when rows still violate after
+ * max_rounds rounds and DLP_ERR_CANCELLED when the cancel word stopped it; in both cases the outputs
+ * are filled and R is the residual of Z (every taken residual was pushed). */
 size_t dlp_fused_push_workspace_bytes(int32_t n, int32_t C);
 int dlp_fused_push(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w, int w_dtype,
                    int32_t n, int32_t C, const void *diag, void *Z, int64_t ldz, void *R, int64_t ldr, int dtype,
                    const double *eps, const int32_t *cand, int32_t ncand, int32_t max_rounds, int32_t check_every,
                    int32_t use_graph, void *ws, size_t ws_bytes, int32_t *rounds_out, int32_t *converged_out,
                    unsigned long long *edges_out, dlp_stream_t stream);
+/* Totals of the last dlp_fused_push run on the workspace `ws`: out[0] = rounds, out[1] = frontier
+ * rows summed over the rounds, out[2] = touched rows, out[3] = stored entries streamed (the byte
+ * model of the push kernels is per frontier row, per entry and per touched row). Synchronous. */
+int dlp_fused_push_counts(const void *ws, unsigned long long *out, dlp_stream_t stream);
 
 
 /* ---- (e) aggregation AMG: setup and V-cycle (dynlp/amg.py) ---------------------------------
