@@ -55,6 +55,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-budget-s", type=float, default=150.0, help="wall budget of the CPU reference legs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true",
+                    help="skip the fp64 reference solve between timed steps (err_vs_fp64, label agreement)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch the PCG kernels one by one instead of as a CUDA graph (for kernel profilers)")
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
@@ -330,7 +332,7 @@ def ours(a):
     seed = a.seed + 1000 * rank  # independent replicas
     ds = graphs.er_graph(a.n, a.deg, a.k, seed=seed)
     lab = graphs.label_mask(a.n, a.label_frac, seed=seed)
-    es = stream.EdgeStream(ds, lab)
+    es = stream.EdgeStream(ds, lab, components=True)  # component ids after every batch (side stream)
     solver = solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres,
                                    full_every=16, lowp=a.lowp)
     solver.solve(es.system)  # the static solve of the initial graph (untimed)
@@ -348,13 +350,69 @@ def ours(a):
     def to_pinned(b):
         return {k: torch.from_numpy(v).pin_memory() for k, v in b.items()}
 
+    cap = 4096  # relabelled rows read back with the counts in one round trip (more: a second one)
+    h_cnt = torch.zeros(3, dtype=torch.int32).pin_memory()
+    h_rows = torch.zeros(cap, dtype=torch.int32).pin_memory()
+    h_labs = torch.zeros(cap, dtype=torch.int32).pin_memory()
+    d2h = []
+
     def step(b, host_result=False):
+        """One batch: patch, grounding, component ids (side stream), solve, labels. With host_result
+        the step's result comes back to the host: the number of relabelled rows, the component and
+        active-unlabelled counts, and every relabelled row with its new label."""
         S = es.apply_edges(**b)
         st = solver.solve(S)
-        if host_result:  # the step's result read back to the host: the fp64 relative residual + bound
-            res = torch.tensor([st.relres, st.cert], dtype=torch.float64, device=dev).cpu()
-            return st, res
-        return st, None
+        _, chg, chg_lab, nchg = solver.relabel(S)
+        es.join_components()
+        if not host_result:
+            return st, None
+        h_cnt[0:1].copy_(nchg, non_blocking=True)
+        h_cnt[1:3].copy_(es._cc_counts[0:2], non_blocking=True)
+        h_rows.copy_(chg[:cap], non_blocking=True)
+        h_labs.copy_(chg_lab[:cap], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        k = int(h_cnt[0])
+        nbytes = 12 + 8 * cap
+        rows, labs = h_rows[:min(k, cap)].numpy().copy(), h_labs[:min(k, cap)].numpy().copy()
+        if k > cap:
+            rows = np.concatenate([rows, chg[cap:k].cpu().numpy()])
+            labs = np.concatenate([labs, chg_lab[cap:k].cpu().numpy()])
+            nbytes += 8 * (k - cap)
+        d2h.append(nbytes)
+        return st, (k, int(h_cnt[1]), int(h_cnt[2]), rows, labs)
+
+    fstar = {}
+
+    def check_fp64(S):
+        """Outside the timed region: the scores against an fp64 solve of the same system (fp64 block
+        PCG to a relative residual of 1e-11, started from the previous batch's fp64 solution): the
+        score error relative to the largest score, label agreement and near-ties (rows whose two
+        best fp64 scores differ by at most twice the score error)."""
+        S64 = S.astype(torch.float64)
+        C = solver.C
+        Zs = fstar.get("Z")
+        if Zs is None:
+            Zs = solvers.padded_empty(a.n, C, torch.float64, dev, fill=0.0)
+        st = solvers.Stats()
+        rhs = S64.rhs.contiguous()
+        ev, solvers.PCG_EVENTS = solvers.PCG_EVENTS, None  # not part of the timed PCG calls
+        solvers.pcg(S64, Zs, rhs, None, solvers.jacobi_M(S64), 10_000, st, target_relres=1e-11)
+        solvers.PCG_EVENTS = ev
+        fstar["Z"] = Zs
+        U = S.solved
+        F, Fs = solver.Z[:, :C][U], Zs[U]
+        err = float((F - Fs).abs().max())
+        scale = float(Fs.abs().max())
+        labels = solver._labels[U]
+        want = Fs.argmax(dim=1).to(torch.int32) if C > 1 else (Fs[:, 0] > 0.5).to(torch.int32)
+        if C > 1:
+            top = torch.topk(Fs, 2, dim=1).values
+            tie = top[:, 0] - top[:, 1] <= 2 * err
+        else:
+            tie = (Fs[:, 0] - 0.5).abs() <= err
+        bad = labels != want
+        return {"err": err / scale, "agree": float(1.0 - bad.double().mean()), "near_ties": int(tie.sum()),
+                "mismatch_outside_ties": int((bad & ~tie).sum()), "fp64_iters": st.iters, "fp64_relres": st.relres}
 
     dev_batches = [to_dev(b) for b in batches[a.warmup: a.warmup + a.steps]]
     host_batches = [to_pinned(b) for b in batches[a.warmup + a.steps:]]
@@ -374,7 +432,7 @@ def ours(a):
     launches0 = _lib.lib().dlp_launch_count()
     solvers.PCG_EVENTS = []  # CUDA events around the fused PCG calls of the timed steps
     torch.cuda.nvtx.range_push("timed")  # lets a profiler filter the timed steps (--nvtx-include timed/)
-    times, relres, paths, iters, events = [], [], [], [], {}
+    times, relres, paths, iters, events, checks = [], [], [], [], {}, []
     for k, b in enumerate(dev_batches):
         c0 = dict(es.counters)
         flush.fill_(0.0)
@@ -385,6 +443,10 @@ def ours(a):
         e.record()
         e.synchronize()
         times.append(s.elapsed_time(e))
+        if rank == 0 and not a.no_fp64_check:  # between timed steps, outside the timed region
+            c_before = _lib.lib().dlp_launch_count()
+            checks.append(check_fp64(es.system))
+            launches0 += _lib.lib().dlp_launch_count() - c_before
         relres.append(st.relres)
         paths.append(st.path)
         iters.append(st.iters)
@@ -397,6 +459,7 @@ def ours(a):
     # end to end: host arrays in, host result out (the clock sampling covers this region too)
     e2e_times = []
     h2d = sum(v.numel() * v.element_size() for v in host_batches[0].values()) if host_batches else 0
+    relabelled, res = [], None
     for b in host_batches:
         flush.fill_(0.0)
         torch.cuda.synchronize()
@@ -406,7 +469,9 @@ def ours(a):
         e.record()
         e.synchronize()
         e2e_times.append(s.elapsed_time(e))
-        relres.append(float(res[0]))
+        relres.append(st.relres)
+        relabelled.append(res[0])
+    cc_last = res[1:3] if res is not None else None
     clk = clocks.stop() if clocks else None
     t_dev, t_e2e, value, e2e = aggregate_replicas(times, e2e_times, a.batch, world, dev)
     roof = None
@@ -434,7 +499,18 @@ def ours(a):
                 "pcg_iters_per_batch": float(np.mean(iters)),
                 "step_ms": [round(t, 3) for t in times],
                 "e2e": {"value": e2e, "unit": "edge-updates/s", "h2d_bytes_per_step": int(h2d),
-                        "d2h_bytes_per_step": 16},
+                        "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0,
+                        "result": "relabelled rows with their new labels; component and active-unlabelled counts",
+                        "relabelled_rows_per_step": float(np.mean(relabelled)) if relabelled else None},
+                "parity_vs_fp64": ({"err_vs_fp64_max": max(c["err"] for c in checks),
+                                    "label_agree_min": min(c["agree"] for c in checks),
+                                    "near_ties_max": max(c["near_ties"] for c in checks),
+                                    "mismatch_outside_near_ties": sum(c["mismatch_outside_ties"] for c in checks),
+                                    "batches": len(checks),
+                                    "reference": "fp64 block Jacobi-PCG of the same system to rel-res 1e-11"}
+                                   if checks else None),
+                "components": {"n_comp": cc_last[0], "label_free_vertices": cc_last[1] - es.system.n_solved}
+                if cc_last else None,
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "precision": ("bf16 gathers (fp32 accumulation)" if a.lowp else "fp32 sweeps (SpMM, PCG)") +
                              " with fp64 residual refinement, fp64 inner products"}

@@ -44,6 +44,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cc_graph": ("ippppipppppzp", ct.c_int),
     "dlp_ground_reach_workspace_bytes": ("i", ct.c_size_t),
     "dlp_ground_reach": ("ippppippppppppzp", ct.c_int),
+    "dlp_cc_mask_labels_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_cc_mask_labels": ("ippppppzp", ct.c_int),
     "dlp_cc_relabel": ("ippppzp", ct.c_int),
     "dlp_residual_stats_workspace_bytes": ("i", ct.c_size_t),
     "dlp_residual_stats": ("iipqpqppqippzp", ct.c_int),
@@ -52,6 +54,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_graph_delete": ("ipppppppipppippppppp", ct.c_int),
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
+    "dlp_predict_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_predict": ("iipqiippppppzp", ct.c_int),
     "dlp_label_update": ("pidpppppipppp", ct.c_int),
     "dlp_new_dissim": ("pipppidpp", ct.c_int),
     "dlp_graph_toggle": ("ppppppippppp", ct.c_int),

@@ -9,6 +9,10 @@ namespace dlp {
 
 int compact_roots(const int32_t *parent, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
                   cudaStream_t s);
+int compact_masked_roots(const int32_t *parent, const uint8_t *mask, int32_t n, int32_t *pos, int32_t *count,
+                         void *ws, size_t ws_bytes, cudaStream_t s);
+int compact_positions(const uint8_t *flag, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
+                      cudaStream_t s);
 size_t compact_ws_bytes(int32_t n);
 
 constexpr int kCcThreads = 256;
@@ -264,6 +268,14 @@ __global__ void k_ground_apply(int32_t n, const uint8_t *__restrict__ reached, c
   if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
 }
 
+// label[lpos[v]] = rank[parent[v]] for every masked v: the rank of its component's minimum id,
+// written at the vertex's place among the masked vertices.
+__global__ void k_cc_mask_gather(int32_t n, const int32_t *__restrict__ parent, const uint8_t *__restrict__ vmask,
+                                 const int32_t *__restrict__ rank, const int32_t *__restrict__ lpos, int32_t *label) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n && vmask[v]) label[lpos[v]] = rank[parent[v]];
+}
+
 static int grid_persist(long long work) {
   long long blocks = (work + kCcThreads - 1) / kCcThreads;
   const long long cap = (long long)sm_count() * 8;
@@ -398,6 +410,27 @@ int dlp_ground_reach(int32_t n, const int32_t *rbeg, const int32_t *rend, const 
   }
   k_ground_apply<<<ceil_div_i(n, 256), 256, 0, s>>>(n, reached, parent, vmask, umask, in_t, count);
   return check_launch();
+}
+
+size_t dlp_cc_mask_labels_workspace_bytes(int32_t n) {
+  const size_t v = ((size_t)(n > 0 ? n : 1) * sizeof(int32_t) + 255) / 256 * 256;
+  return 2 * v + compact_ws_bytes(n);
+}
+
+int dlp_cc_mask_labels(int32_t n, const int32_t *parent, const uint8_t *vmask, int32_t *label, int32_t *n_comp,
+                       int32_t *n_masked, void *ws, size_t ws_bytes, dlp_stream_t stream) {
+  if (n < 0 || !n_comp || !n_masked || (n > 0 && (!parent || !vmask || !label))) return DLP_ERR_INVALID;
+  if (!ws || ws_bytes < dlp_cc_mask_labels_workspace_bytes(n)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t v = ((size_t)(n > 0 ? n : 1) * sizeof(int32_t) + 255) / 256 * 256;
+  int32_t *rank = (int32_t *)ws;
+  int32_t *lpos = (int32_t *)((char *)ws + v);
+  void *cws = (char *)ws + 2 * v;
+  const size_t cbytes = ws_bytes - 2 * v;
+  DLP_TRY(compact_masked_roots(parent, vmask, n, rank, n_comp, cws, cbytes, s));
+  DLP_TRY(compact_positions(vmask, n, lpos, n_masked, cws, cbytes, s));
+  if (n > 0) k_cc_mask_gather<<<ceil_div_i(n, kCcThreads), kCcThreads, 0, s>>>(n, parent, vmask, rank, lpos, label);
+  return check_launch(n > 0 ? 1 : 0);
 }
 
 int dlp_cc_relabel(int32_t n, const int32_t *parent, int32_t *label, int32_t *n_comp, void *ws, size_t ws_bytes,

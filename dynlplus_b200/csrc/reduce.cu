@@ -99,6 +99,12 @@ struct RootPred {
   __device__ bool operator()(long long g) const { return parent[g] == (int32_t)g; }
 };
 
+struct MaskedRootPred {
+  const int32_t *parent;
+  const uint8_t *mask;
+  __device__ bool operator()(long long g) const { return mask[g] != 0 && parent[g] == (int32_t)g; }
+};
+
 template <typename Pred>
 static int compact_impl(Pred pred, const int32_t *idx, int32_t n, int32_t *out, int32_t *pos, int32_t *count,
                         void *ws, size_t ws_bytes, cudaStream_t s) {
@@ -168,6 +174,24 @@ size_t compact_ws_bytes(int32_t n) { return ((size_t)n_tiles(n) * sizeof(int32_t
 int compact_roots(const int32_t *parent, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
                   cudaStream_t s) {
   return compact_impl(RootPred{parent}, nullptr, n, nullptr, pos, count, ws, ws_bytes, s);
+}
+
+// pos[root] = rank of each masked root (mask[g] && parent[g] == g) among them; *count = their number.
+int compact_masked_roots(const int32_t *parent, const uint8_t *mask, int32_t n, int32_t *pos, int32_t *count,
+                         void *ws, size_t ws_bytes, cudaStream_t s) {
+  return compact_impl(MaskedRootPred{parent, mask}, nullptr, n, nullptr, pos, count, ws, ws_bytes, s);
+}
+
+// out[0..*count) = the flagged g in ascending order (numpy.flatnonzero).
+int compact_flags(const uint8_t *flag, int32_t n, int32_t *out, int32_t *count, void *ws, size_t ws_bytes,
+                  cudaStream_t s) {
+  return compact_impl(FlagPred{flag}, nullptr, n, out, nullptr, count, ws, ws_bytes, s);
+}
+
+// pos[g] = rank of g among the flagged entries (flag[g] != 0); *count = their number.
+int compact_positions(const uint8_t *flag, int32_t n, int32_t *pos, int32_t *count, void *ws, size_t ws_bytes,
+                      cudaStream_t s) {
+  return compact_impl(FlagPred{flag}, nullptr, n, nullptr, pos, count, ws, ws_bytes, s);
 }
 
 // ------------------------------------------------------------------------------------------------

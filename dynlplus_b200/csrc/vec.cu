@@ -65,6 +65,46 @@ __global__ void k_ground_update(int32_t n, const int32_t *__restrict__ parent, c
   if ((threadIdx.x & 31) == 0 && b) atomicAdd(counts, __popc(b));
 }
 
+// Labels (solvers.predict, dynlp/solvers.py:166-167): binary: F[r,0] > 0.5; otherwise the first
+// column holding the row's maximum (numpy argmax). Rows outside the mask get -1. flag[r] = the label
+// differs from the one labels[r] held on entry; labels[r] takes the new one.
+template <typename T>
+__global__ void k_predict(int32_t n, int32_t C, const T *__restrict__ F, int64_t ldf, int32_t binary,
+                          const uint8_t *__restrict__ mask, int32_t *labels, uint8_t *flag) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int32_t lab = -1;
+  if (!mask || mask[r]) {
+    const T *f = F + r * ldf;
+    if (binary) {
+      lab = f[0] > T(0.5) ? 1 : 0;
+    } else {
+      T best = f[0];
+      lab = 0;
+      for (int c = 1; c < C; ++c) {
+        const T x = f[c];
+        if (x > best) {
+          best = x;
+          lab = c;
+        }
+      }
+    }
+  }
+  flag[r] = labels[r] != lab ? 1 : 0;
+  labels[r] = lab;
+}
+
+// out_label[i] = labels[rows[i]] for i < *count.
+__global__ void k_gather_labels(const int32_t *__restrict__ rows, const int32_t *__restrict__ count,
+                                const int32_t *__restrict__ labels, int32_t *out_label, int32_t cap) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cap && i < *count) out_label[i] = labels[rows[i]];
+}
+
+int compact_flags(const uint8_t *flag, int32_t n, int32_t *out, int32_t *count, void *ws, size_t ws_bytes,
+                  cudaStream_t s);
+size_t compact_ws_bytes(int32_t n);
+
 }  // namespace dlp
 
 using namespace dlp;
@@ -95,6 +135,38 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
   else
     return DLP_ERR_DTYPE;
   return check_launch();
+}
+
+size_t dlp_predict_workspace_bytes(int32_t n) {
+  return ((size_t)(n > 0 ? n : 1) + 255) / 256 * 256 + compact_ws_bytes(n);
+}
+
+int dlp_predict(int32_t n, int32_t C, const void *F, int64_t ldf, int dtype, int32_t binary, const uint8_t *mask,
+                int32_t *labels, int32_t *changed, int32_t *changed_label, int32_t *n_changed, void *ws,
+                size_t ws_bytes, dlp_stream_t stream) {
+  if (n < 0 || C <= 0 || ldf < C || !n_changed || (n > 0 && (!F || !labels || !changed))) return DLP_ERR_INVALID;
+  if (!ws || ws_bytes < dlp_predict_workspace_bytes(n)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {
+    DLP_CUDA(cudaMemsetAsync(n_changed, 0, sizeof(int32_t), s));
+    return DLP_OK;
+  }
+  uint8_t *flag = (uint8_t *)ws;
+  const size_t fb = ((size_t)n + 255) / 256 * 256;
+  const int grid = ceil_div_i(n, 256);
+  if (dtype == DLP_F64)
+    k_predict<double><<<grid, 256, 0, s>>>(n, C, (const double *)F, ldf, binary, mask, labels, flag);
+  else if (dtype == DLP_F32)
+    k_predict<float><<<grid, 256, 0, s>>>(n, C, (const float *)F, ldf, binary, mask, labels, flag);
+  else
+    return DLP_ERR_DTYPE;
+  DLP_TRY(check_launch());
+  DLP_TRY(compact_flags(flag, n, changed, n_changed, (char *)ws + fb, ws_bytes - fb, s));
+  if (changed_label) {
+    k_gather_labels<<<grid, 256, 0, s>>>(changed, n_changed, labels, changed_label, n);
+    DLP_TRY(check_launch());
+  }
+  return DLP_OK;
 }
 
 int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, uint8_t *umask, uint8_t *in_t,

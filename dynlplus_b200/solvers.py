@@ -781,6 +781,25 @@ class IncrementalLP(DynLPPlus):
         return st
 
 
+    def relabel(self, sys):
+        """Labels after the last solve (predict, dynlp/solvers.py:166-167) on every row of the
+        global-index system (-1 outside the solved set), and the rows whose label changed since the
+        previous call. Returns device tensors (labels, changed rows, their labels, count[1]); the
+        first `count` entries of the two lists are valid. No host read."""
+        Z = self.Z
+        n, dev = Z.shape[0], Z.device
+        if getattr(self, "_labels", None) is None or self._labels.numel() != max(n, 1):
+            self._labels = torch.full((max(n, 1),), -2, dtype=torch.int32, device=dev)
+            self._chg = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+            self._chg_lab = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+            self._nchg = torch.zeros(1, dtype=torch.int32, device=dev)
+        sol = sys.solved.view(torch.uint8) if sys.solved.dtype == torch.bool else sys.solved.to(torch.uint8)
+        ws = workspace("predict").get(_lib.lib().dlp_predict_workspace_bytes(n))
+        _lib.call("dlp_predict", n, self.C, ptr(Z), ld(Z), code(Z), int(self.K == 2), ptr(sol), ptr(self._labels),
+                  ptr(self._chg), ptr(self._chg_lab), ptr(self._nchg), ptr(ws), ws.numel(), stream())
+        return self._labels[:n], self._chg, self._chg_lab, self._nchg
+
+
 class Reference:
     """High-accuracy float64 solution F* and absorption bound (dynlp/solvers.py:437-445)."""
 

@@ -314,7 +314,7 @@ class EdgeStream:
     """
 
     def __init__(self, ds: Dataset, labeled, *, eta_rel=0.0, dtype="float32", with_h=True, slack_frac=0.25, slack_min=8,
-                 active=None):
+                 active=None, components=False):
         A, K = ds.A, ds.K
         self.ds, self.K, self.dtype = ds, K, to_dtype(dtype)
         self.C = 1 if K == 2 else K
@@ -359,6 +359,17 @@ class EdgeStream:
         self.rhs32 = torch.zeros((n, self.ld32), dtype=torch.float32, device=dev)
         self._system_rows(None, n)
         self.t = 0
+        # connected components of the active unlabelled subgraph after every batch (the reference
+        # labels them in Stream._build, dynlp/stream.py:150-153): computed on a side stream that
+        # overlaps the solve; the next batch's patch waits for it
+        self.with_components = bool(components)
+        self._cc_done = None
+        if self.with_components:
+            self._cc_stream = torch.cuda.Stream(device=dev)
+            self._cc_parent = torch.empty(n + 1, dtype=torch.int32, device=dev)
+            self._cc_label = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+            self._cc_counts = torch.zeros(3, dtype=torch.int32, device=dev)  # n_comp, n_masked, error
+            self._components_launch()
         self.last_changed = torch.arange(n, dtype=torch.int32, device=dev)
         self.last_moved = torch.zeros(0, dtype=torch.int32, device=dev)
         self.n_ins = self.n_del = 0
@@ -375,6 +386,41 @@ class EdgeStream:
         self.counters["ground_fallbacks"] += sweeps < 0
         self._stat[4].fill_(changes)
         return changes
+
+    def _components_launch(self):
+        """Queue the component labelling of the current graph on the side stream."""
+        G, n = self.G, self.n
+        main = torch.cuda.current_stream(self.dev)
+        side = self._cc_stream
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            ws = workspace("cc_graph").get(_lib.lib().dlp_cc_graph_workspace_bytes())
+            _lib.call("dlp_cc_graph", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), code(G.aw),
+                      ptr(self.vmask), None, ptr(self._cc_parent), ptr(self._cc_counts[2:3]), ptr(ws), ws.numel(),
+                      stream())
+            wl = workspace("cc_labels").get(_lib.lib().dlp_cc_mask_labels_workspace_bytes(n))
+            _lib.call("dlp_cc_mask_labels", n, ptr(self._cc_parent), ptr(self.vmask), ptr(self._cc_label),
+                      ptr(self._cc_counts[0:1]), ptr(self._cc_counts[1:2]), ptr(wl), wl.numel(), stream())
+            self._cc_done = torch.cuda.Event()
+            self._cc_done.record(side)
+
+    def join_components(self):
+        """Make the current stream wait for this batch's component labelling (no host wait)."""
+        if self._cc_done is not None:
+            torch.cuda.current_stream(self.dev).wait_event(self._cc_done)
+
+    def components(self):
+        """(labels, n_comp) of the active unlabelled subgraph after the last batch, numbered as the
+        reference's connected_components numbers them over its local ids (dynlp/stream.py:150-153,
+        dynlp/cc.py:22): labels[i] belongs to the i-th active unlabelled vertex in ascending id order.
+        Device int32 labels; one host read for the counts."""
+        if not self.with_components:
+            raise RuntimeError("EdgeStream(..., components=True) computes the component labels")
+        self.join_components()
+        n_comp, n_masked, err = self._cc_counts.tolist()
+        if err:
+            raise RuntimeError("component labelling: entry column outside [0, n)")
+        return self._cc_label[:n_masked], n_comp
 
     def _system_rows(self, rows, nr):
         ch = self.C + (1 if self.with_h else 0)
@@ -406,6 +452,7 @@ class EdgeStream:
         iw = self._upload(ins_w, torch.float32)
         nd = int(du.numel()) if du is not None else 0
         ni = int(iu.numel()) if iu is not None else 0
+        self.join_components()  # the previous batch's labelling reads the graph this batch patches
         self.changed.zero_()
         self._stat.zero_()
         st = self._stat
@@ -433,6 +480,8 @@ class EdgeStream:
             flags = st[0:4].tolist()
         if flags[0]:
             raise ValueError(f"edge batch rejected: {_lib.STATUS.get(flags[0])} (vertex id out of range?)")
+        if self.with_components:
+            self._components_launch()
         # grounding: components of the unlabelled subgraph with the labelled vertices as a sink
         nmoved = self._ground()
         moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
@@ -471,6 +520,7 @@ class EdgeStream:
         dele = dele.to(device=dev, dtype=torch.int64)
         prev_u = self.umask.bool().clone()
         self._vertex_batch = None
+        self.join_components()
         self.changed.zero_()
         lab_all = self.labeled_all
         for ids, on in ((dele, False), (ins, True)):
@@ -485,6 +535,8 @@ class EdgeStream:
                 _lib.call("dlp_label_update", ptr(L), int(L.numel()), 1.0 if on else -1.0, ptr(G.rbeg), ptr(G.rend),
                           ptr(G.indices), ptr(G.aw), ptr(self.y), self.K, ptr(self.B), ptr(self.umask),
                           ptr(self.changed), s)
+        if self.with_components:
+            self._components_launch()
         nmoved = self._ground()
         moved = torch.zeros(0, dtype=torch.int32, device=dev)
         if nmoved:

@@ -189,6 +189,16 @@ int dlp_ground_reach(int32_t n, const int32_t *rbeg, const int32_t *rend, const 
                      int32_t *count, int32_t *err, int32_t *sweeps_out, void *ws, size_t ws_bytes,
                      dlp_stream_t stream);
 
+/* The reference's component labels of the masked vertices: connected_components over the
+ * subgraph that vmask induces, numbered as dynlp/stream.py:150-153 with dynlp/cc.py:22 number them
+ * (local ids = the masked vertices in ascending order; a component's label = the rank of its smallest
+ * local id among the components'). Input: parent of dlp_cc_graph with the same vmask (fully
+ * compressed; roots are minimum vertex ids). Output: label[i] for the i-th masked vertex, *n_comp =
+ * components, *n_masked = masked vertices (device ints). Workspace: dlp_cc_mask_labels_workspace_bytes. */
+size_t dlp_cc_mask_labels_workspace_bytes(int32_t n);
+int dlp_cc_mask_labels(int32_t n, const int32_t *parent, const uint8_t *vmask, int32_t *label, int32_t *n_comp,
+                       int32_t *n_masked, void *ws, size_t ws_bytes, dlp_stream_t stream);
+
 /* Canonical relabel: label[i] = rank of parent[i] among the roots (parent[r] == r; parent must be
  * fully compressed, as dlp_cc_edges/dlp_cc_graph leave it), i.e. the
  * labels numpy.unique(parent, return_inverse=True) gives (dynlp/cc.py:22-23); *n_comp = number
@@ -314,6 +324,17 @@ int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t
  * scale is a device double[C]. Precisions: f32/f64. */
 int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
                    void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream);
+
+/* Labels of the rows (solvers.predict, dynlp/solvers.py:166-167): binary != 0 (the K == 2 column):
+ * label = F[r,0] > 0.5; otherwise the first column of the row's maximum over C columns (numpy
+ * argmax). Rows with mask[r] == 0 get -1 (mask NULL: every row). labels[0..n) holds the previous
+ * labels on entry and the new ones on exit; the rows whose label changed are listed in ascending
+ * order in changed[0..*n_changed) (device int), and, with changed_label != NULL, their new labels in
+ * changed_label[]. dtype of F: f32/f64. Workspace: dlp_predict_workspace_bytes(n). */
+size_t dlp_predict_workspace_bytes(int32_t n);
+int dlp_predict(int32_t n, int32_t C, const void *F, int64_t ldf, int dtype, int32_t binary, const uint8_t *mask,
+                int32_t *labels, int32_t *changed, int32_t *changed_label, int32_t *n_changed, void *ws,
+                size_t ws_bytes, dlp_stream_t stream);
 
 /* Labelled vertices L entering (sign = +1) or leaving (sign = -1) the active set
  * (IncrementalStream._label_update, dynlp/stream.py:230-235): B[v, y[l]] += sign * aw(l, v) for every

@@ -262,7 +262,9 @@ def build_system(A, y, K, active, labeled, eta=0.0, dtype=np.float64):
     s = Bm.sum(axis=1) + eta
     diag = s + np.asarray(W.sum(axis=1)).ravel()
     rhs = (Bm[:, 1:2] if K == 2 else Bm) + eta * prior[None, :]
-    return dict(U=U, W=W, s=s, diag=diag, B=Bm, rhs=rhs, prior=prior, n_ungrounded=int((~grounded).sum()))
+    # cc_labels: the reference's component labels of the active unlabelled vertices U0 (stream.py:153)
+    return dict(U=U, W=W, s=s, diag=diag, B=Bm, rhs=rhs, prior=prior, n_ungrounded=int((~grounded).sum()),
+                U0=U0, cc_labels=lab, n_comp=ncomp)
 
 
 # ---------------------------------------------------------------------------------------------
