@@ -79,17 +79,3 @@ def test_streaming_benchmark_flags_and_columns_match_the_reference():
             assert default == graphs.DATA_DIR
         else:
             assert default == ast.literal_eval(a["default"]), a["flag"]
-
-
-def test_kernel_benchmark_flags_and_columns_match_the_reference():
-    """dynlp/kernelbench.py:21-63: the same flags and defaults, the same CSV columns."""
-    from dynlplus_b200 import graphs, kernelbench
-    with open(os.path.join(GOLDEN, "api.json")) as f:
-        api = json.load(f)
-    assert kernelbench.FIELDS == api["kernelbench_fields"]
-    ours = {flag: default for flag, _, default in kernelbench.ARGS}
-    assert set(ours) == {a["flag"] for a in api["kernelbench_args"]}
-    for a in api["kernelbench_args"]:
-        want = graphs.DATA_DIR if a["default"] == "graphs.DATA_DIR" else ast.literal_eval(a["default"])
-        assert ours[a["flag"]] == want, a["flag"]
-    assert [kernelbench.kernel_name(g) for g in ("8", "32", "128", "cols")] == ["lanes8", "lanes32", "block128", "cols"]

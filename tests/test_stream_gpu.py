@@ -148,3 +148,10 @@ def test_streaming_benchmark_rows(tmp_path, incremental):
         if row["solver"].startswith("dynlp+"):
             assert row["err_max"] <= max(1.05 * row["cert_self"], 1e-9), row
         assert 0.0 <= row["acc_true"] <= 1.0
+    # the run's CSV through the results matrix: one line per solver, iterations summed over batches
+    from dynlplus_b200 import matrix
+    agg = matrix.main(str(tmp_path))
+    assert [g["solver"] for g in agg] == names.split(",")
+    for g in agg:
+        assert g["iters"] == sum(r["iters"] for r in rows if r["solver"] == g["solver"])
+    assert (tmp_path / "matrix.md").read_text(encoding="utf-8").startswith("# Method matrix:")
