@@ -148,7 +148,9 @@ size_t dlp_colreduce_workspace_bytes(int32_t C);
  * wider inputs return DLP_ERR_SCRATCH_LIMIT. The first call on each device looks the array's
  * device address up (cudaGetSymbolAddress), so make that first call before any stream capture.
  * All calls on a device share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. It allocates nothing and calls no allocating routine. */
+ * serialised by the caller. It allocates nothing and calls no allocating routine. The looked-up
+ * address is kept for the life of the process: after a cudaDeviceReset of a device, do not call it
+ * on that device again in the same process. */
 int dlp_colreduce_noalloc(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,
                           const void *diag, int dtype, const uint8_t *mask, double *out, dlp_stream_t stream);
 int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, const void *Y, int64_t ldy,

@@ -46,3 +46,38 @@ def test_noalloc_refuses_more_columns_than_its_scratch():
     with pytest.raises(_lib.DLPError) as e:
         _noalloc(2, X)
     assert e.value.status == 9
+
+
+def _numpy_reference(kind, X, Y=None, diag=None, mask=None):
+    """The reduction in fp64 NumPy, independent of the library."""
+    X = X.double().cpu().numpy()
+    rows = np.ones(X.shape[0], bool) if mask is None else mask.cpu().numpy().astype(bool)
+    X = X[rows]
+    if kind == 0:
+        return (np.abs(X) / diag.double().cpu().numpy()[rows][:, None]).max(axis=0, initial=0.0)
+    if kind == 1:
+        return (X * Y.double().cpu().numpy()[rows]).sum(axis=0)
+    if kind == 2:
+        return (X * X).sum(axis=0)
+    return np.abs(X).max(axis=0, initial=0.0)
+
+
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+def test_noalloc_matches_numpy_up_to_its_column_limit(dt):
+    """Every kind, with and without a row mask, at the widest input the fixed scratch takes (64
+    columns) and at sizes that leave partial blocks, on two calls in a row."""
+    rs = np.random.RandomState(7)
+    for call in range(2):
+        for n, C in ((5, 64), (1_000, 64), (123_457, 64), (70_001, 17)):
+            X = torch.as_tensor(rs.randn(n, C)).to(dt).cuda()
+            Y = torch.as_tensor(rs.randn(n, C)).to(dt).cuda()
+            d = torch.as_tensor(rs.rand(n) + 0.5).to(dt).cuda()
+            mask = torch.as_tensor((rs.rand(n) < 0.3).astype(np.uint8)).cuda()
+            for m in (None, mask):
+                for kind, kw in ((0, dict(diag=d)), (1, dict(Y=Y)), (2, {}), (3, {})):
+                    got = _noalloc(kind, X, mask=m, **kw).cpu().numpy()
+                    want = _numpy_reference(kind, X, mask=m, **kw)
+                    # maxima of |x| exact; |x| / d is formed as |x| * (1 / d), one rounding from
+                    # NumPy's quotient; sums accumulate in fp64 in a different order
+                    tol = {3: dict(rtol=0, atol=0), 0: dict(rtol=1e-15, atol=0)}.get(kind, dict(rtol=1e-10, atol=1e-10))
+                    np.testing.assert_allclose(got, want, **tol, err_msg=f"call {call} n {n} kind {kind}")
