@@ -61,7 +61,7 @@ def parse(argv=None):
                     help="launch the PCG kernels one by one instead of as a CUDA graph (for kernel profilers)")
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
     ap.add_argument("--workload", default="edge-stream",
-                    choices=["edge-stream", "static", "amg", "batched", "serving"],
+                    choices=["edge-stream", "static", "amg", "batched", "serving", "kernels"],
                     help="edge-stream: the headline (ER 1M edge batches); static: SBM 100k solve + one "
                          "1000-update batch; amg: SBM 1M lognormal, AMG-PCG to rel-res 1e-8; batched: 256 SBM "
                          "instances in one batched solve; serving: resident SBM with mixed Poisson requests")
@@ -676,6 +676,121 @@ def wl_serving(a):
                                  "update_p99": p99(seq) / p99(best)})
 
 
+def wl_kernels(a):
+    """The row kernels one by one on the headline graph (ER n=1M, mean degree 10, k=8 plus the h
+    column) after one batch of updates, each timed alone with CUDA events on its launching stream
+    after an L2 flush, against its algorithmic bytes:
+      spmm             the apply_A SpMM over all rows (fp32, the PCG's gather);
+      frontier_jacobi  the batch's changed rows (fp32): 12 nf + e (8 + 4C) + nf (12C + 5);
+      push_fp64 / _fp32  the residual push from the batch's residual to eps = tol / (1.25 hmax) (the
+                       incremental solver's small-batch branch), the whole dlp_fused_push call:
+                       per frontier row 12 + 2C s_r + 2C s_z + s_d, per live entry 8 + s_w + 2C s_r,
+                       per touched row 8 + C s_r + s_d."""
+    import ctypes as ct
+    import torch
+    from dynlplus_b200 import _lib, graphs, kernels, solvers, stream
+    from dynlplus_b200.backend import code, ld, ptr
+    from dynlplus_b200.backend import stream as cur_stream
+    dev = torch.device("cuda", torch.cuda.current_device())
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("hbm_gbs") or 6650.0
+    ds = graphs.er_graph(a.n, a.deg, a.k, seed=a.seed)
+    lab = graphs.label_mask(a.n, a.label_frac, seed=a.seed)
+    es = stream.EdgeStream(ds, lab)
+    solver = solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres)
+    solver.solve(es.system)
+    Zprev = solver.Z.clone()
+    S = es.apply_edges(**graphs.EdgeUpdates(ds.A, seed=a.seed).next(a.batch))
+    C = solver.C + 1
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def timed(fn, reps):
+        ms = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s0.record()
+            fn()
+            s1.record()
+            s1.synchronize()
+            ms.append(s0.elapsed_time(s1))
+        return float(np.median(ms))
+
+    def line(name, algo, ms, **extra):
+        gbs = algo / (ms * 1e-3) / 1e9
+        return {"kernel": name, "algorithmic_bytes": int(algo), "ms": ms, "achieved_gbs": gbs, "peak_gbs": peak,
+                "frac": gbs / peak, **extra}
+
+    out = {"spmm": spmm_roofline(es, C, peaks)}
+    # frontier Jacobi over the batch's changed rows
+    W = es.solver_csr()
+    f = S.changed.to(torch.int32).contiguous()
+    nf = int(f.numel())
+    rows = f.long()
+    e_f = int((W.indptr[1:][rows] - W.indptr[:-1][rows]).sum())
+    X = solvers.padded_empty(a.n, C, torch.float32, dev)
+    X.copy_(solver.Z[:, :C])
+    rhs = S.rhs_h
+    Y = torch.empty((max(nf, 1), C), dtype=torch.float32, device=dev)
+    ch = torch.empty(max(nf, 1), dtype=torch.uint8, device=dev)
+
+    def jac():
+        _lib.call("dlp_frontier_jacobi", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), ptr(f),
+                  nf, C, ptr(X), ld(X), ptr(rhs), ld(rhs), ptr(S.diag), 1e-4, ptr(Y), ld(Y), code(X), ptr(ch), None,
+                  None, 0, W.nnz / a.n, cur_stream())
+    for _ in range(3):
+        jac()
+    algo = 12 * nf + e_f * (8 + 4 * C) + nf * (12 * C + 5)
+    out["frontier_jacobi"] = line("k_frontier_jacobi", algo, timed(jac, 20), rows=nf, entries=e_f)
+    # the push from the batch's residual
+    s64 = S.astype(torch.float64)
+    hmax = solver.hmax or 1.0
+    eps = [a.tol / (1.25 * hmax)] * solver.C + [solver.eps_h]
+    for name, dt in (("push_fp64", torch.float64), ("push_fp32", torch.float32)):
+        sw = S.astype(dt)
+        diag = sw.diag.to(dt)
+        rhs_d = (s64.rhs_h if dt == torch.float64 else S.rhs_h).to(dt)
+        Z0 = solvers.padded_empty(a.n, C, dt, dev)
+        R0 = solvers.padded_empty(a.n, C, dt, dev)
+        Z0.copy_(Zprev[:, :C])
+        R0.copy_(solvers.residual(s64, Zprev, s64.rhs_h))
+        Z, R = solvers.padded_empty(a.n, C, dt, dev), solvers.padded_empty(a.n, C, dt, dev)
+        eps_d = torch.as_tensor(eps, dtype=torch.float64, device=dev)
+        cand = kernels.flatnonzero(kernels.violating(R0, diag, eps_d))
+        fp = kernels.FusedPush(W, C)
+        res = {}
+
+        def push():
+            Z.copy_(Z0)
+            R.copy_(R0)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            res["run"] = fp.run(Z, R, diag, eps, cand, 100_000)
+            ev1.record()
+            ev1.synchronize()
+            res["ms"] = ev0.elapsed_time(ev1)
+        push()
+        ms = []
+        for _ in range(5):
+            flush.fill_(1.0)
+            push()
+            ms.append(res["ms"])
+        rounds, ok, edges = res["run"]
+        _, frows, trows, _ = fp.counts()
+        sz = 8 if dt == torch.float64 else 4
+        algo = frows * (12 + 4 * C * sz + 4) + edges * (8 + 4 + 2 * C * sz) + trows * (8 + C * sz + sz)
+        out[name] = line("k_push_scatter + k_push_sift (whole dlp_fused_push call)", algo, float(np.median(ms)),
+                         rounds=rounds, converged=ok, candidates=int(cand.numel()), frontier_rows=frows,
+                         touched_rows=trows, entries=edges)
+    del ct
+    _line(a, "row kernels on the headline graph: achieved HBM GB/s per kernel (CUDA events, after an L2 flush)",
+          out["spmm"]["achieved_after_l2_flush"], "GB/s", out["spmm"]["ms_per_launch_after_l2_flush"],
+          {"workload": workload_name(a), "frontier": "the changed rows of one batch of %d updates" % a.batch},
+          kernels=out)
+
+
 def main(argv=None):
     a = parse(argv)
     if a.no_graphs:
@@ -684,7 +799,8 @@ def main(argv=None):
     if a.impl == "reference":
         return reference_arm(a)
     if a.workload != "edge-stream":
-        return {"static": wl_static, "amg": wl_amg, "batched": wl_batched, "serving": wl_serving}[a.workload](a) or 0
+        return {"static": wl_static, "amg": wl_amg, "batched": wl_batched, "serving": wl_serving,
+                "kernels": wl_kernels}[a.workload](a) or 0
     return ours(a)
 
 
