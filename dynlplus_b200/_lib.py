@@ -42,6 +42,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_cc_edges": ("ippqppp", ct.c_int),
     "dlp_cc_graph_workspace_bytes": ("", ct.c_size_t),
     "dlp_cc_graph": ("ippppipppppzp", ct.c_int),
+    "dlp_cc_graph_warm_workspace_bytes": ("i", ct.c_size_t),
+    "dlp_cc_graph_warm": ("ippppippppzp", ct.c_int),
     "dlp_ground_reach_workspace_bytes": ("i", ct.c_size_t),
     "dlp_ground_reach": ("ippppippppppppzp", ct.c_int),
     "dlp_cc_mask_labels_workspace_bytes": ("i", ct.c_size_t),

@@ -3,6 +3,8 @@
 // compresses every vertex to its root. Because a root is only ever hooked under a smaller id, the
 // root of each component is its minimum vertex id, whatever the schedule: the result is the
 // reference's canonical labelling before its rank relabel (cc.py:22), bit-exact.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace dlp {
@@ -276,6 +278,127 @@ __global__ void k_cc_mask_gather(int32_t n, const int32_t *__restrict__ parent, 
   if (v < n && vmask[v]) label[lpos[v]] = rank[parent[v]];
 }
 
+// ------------------------------------------------------------------------------------------------
+// Components of a graph that changes by small batches between calls (warm start). The masked
+// subgraph of the workloads is one giant component plus a few tiny ones, so instead of Afforest's
+// sampling rounds the giant component is found by a breadth-first search from the root the previous
+// call found for its most frequent component: top-down levels (8 lanes per frontier vertex,
+// first-touch bits, warp-aggregated appends) while the frontier is small, then bottom-up sweeps over
+// the bitmap. Every reached vertex is connected to the seed, so the reached set R is one connected
+// set whatever the seed; its vertices start under R's minimum id, and the union-find then hooks the
+// rows outside R in full (k_cc_graph with R as the skipped component). The result is the exact
+// minimum-id labelling of dlp_cc_graph; a poor seed (a vertex cut off by the batch) only leaves more
+// rows to the union-find. No host read: the schedule of levels is fixed and levels past the end of
+// the search return at once.
+// ------------------------------------------------------------------------------------------------
+constexpr int kWarmDown = 7;  // top-down levels at most
+constexpr int kWarmUp = 4;    // bottom-up sweeps at most
+// control words: [0] seed, then R's root (k_cc_graph's skipped root), [1] sink flag of k_cc_graph
+// (unused: no sink), [2] bottom-up switch, [3] minimum reached id, [4 + l] frontier size of level l
+enum { kWSeed = 0, kWUp = 2, kWMin = 3, kWCnt = 4 };
+
+__global__ void k_warm_seed(int32_t n, const uint8_t *__restrict__ vmask, uint32_t *bits, int32_t *front0,
+                            int32_t *ctl) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int32_t sd = ctl[kWSeed];
+  ctl[1] = 0;
+  ctl[kWUp] = 0;
+  ctl[kWMin] = 0x7fffffff;
+  for (int l = 0; l <= kWarmDown; ++l) ctl[kWCnt + l] = 0;
+  if (sd >= 0 && sd < n && (!vmask || vmask[sd])) {
+    bits[sd >> 5] |= 1u << (sd & 31);
+    front0[0] = sd;
+    ctl[kWCnt] = 1;
+  }
+}
+
+template <typename TW>
+__global__ void __launch_bounds__(kCcThreads)
+    k_bfs_down(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+               const int32_t *__restrict__ col, const TW *__restrict__ w, const uint8_t *__restrict__ vmask,
+               uint32_t *bits, const int32_t *__restrict__ front_in, int32_t *front_out, int32_t *ctl, int level,
+               int cap) {
+  constexpr int G = 8, kGroups = 32 / G;
+  const int nf = ctl[kWCnt + level];
+  if (nf == 0) return;
+  if (nf > cap) {  // a large frontier: the bottom-up sweeps take over from the bitmap
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[kWUp] = 1;
+    return;
+  }
+  const int lane = lane_id(), gl = lane % G;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long stride = (((long long)gridDim.x * blockDim.x) >> 5) * kGroups;
+  for (long long base = warp * kGroups; base < nf; base += stride) {  // warp-uniform bounds
+    const long long g = base + lane / G;
+    int beg = 0, end = 0;
+    if (g < nf) {
+      const int32_t u = front_in[g];
+      beg = rbeg[u];
+      end = rend[u];
+    }
+    const int trips = __reduce_max_sync(0xffffffffu, (end - beg + G - 1) / G);
+    for (int t = 0; t < trips; ++t) {
+      const int j = beg + gl + t * G;
+      bool fresh = false;
+      int32_t v = 0;
+      if (j < end && live(w, j)) {
+        v = col[j];
+        if ((unsigned)v < (unsigned)n && (!vmask || vmask[v])) {
+          const uint32_t bit = 1u << (v & 31);
+          fresh = (atomicOr(bits + (v >> 5), bit) & bit) == 0u;
+        }
+      }
+      warp_append(fresh, v, front_out, ctl + kWCnt + level + 1);
+    }
+  }
+}
+
+// Bottom-up sweep: an unreached vertex of the mask joins when one of its live in-mask entries
+// leads to a reached vertex (bits read and written in place, so a sweep carries marks many hops).
+template <typename TW>
+__global__ void __launch_bounds__(kCcThreads)
+    k_bfs_up(int32_t n, const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+             const int32_t *__restrict__ col, const TW *__restrict__ w, const uint8_t *__restrict__ vmask,
+             uint32_t *bits_, const int32_t *ctl) {
+  if (!ctl[kWUp] && !ctl[kWCnt + kWarmDown]) return;  // the top-down levels finished the search
+  volatile uint32_t *bits = bits_;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (long long)gridDim.x * blockDim.x) {
+    if (vmask && !vmask[u]) continue;
+    const uint32_t ub = 1u << (u & 31);
+    if (bits[u >> 5] & ub) continue;
+    const int end = rend[u];
+    for (int j = rbeg[u]; j < end; ++j) {
+      if (!live(w, j)) continue;
+      const int32_t v = col[j];
+      if ((unsigned)v >= (unsigned)n || (vmask && !vmask[v])) continue;
+      if (bits[v >> 5] & (1u << (v & 31))) {
+        atomicOr(bits_ + (u >> 5), ub);
+        break;
+      }
+    }
+  }
+}
+
+// Smallest reached id: the first set bit of each word, then a minimum.
+__global__ void k_warm_min(int32_t n, const uint32_t *__restrict__ bits, int32_t *ctl) {
+  const long long wd = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int32_t m = 0x7fffffff;
+  if (wd < ((long long)n + 31) / 32 && bits[wd]) m = (int32_t)(wd * 32 + __ffs(bits[wd]) - 1);
+  m = __reduce_min_sync(0xffffffffu, m);
+  if (lane_id() == 0 && m != 0x7fffffff) atomicMin(ctl + kWMin, m);
+}
+
+// parent[v] = R's minimum id for the reached vertices, v otherwise (parent[n] = n, the unused sink);
+// control word 0 becomes R's root for k_cc_graph (-1 when nothing was reached).
+__global__ void k_warm_parent(int32_t n, const uint32_t *__restrict__ bits, int32_t *parent, int32_t *ctl) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t m = ctl[kWMin];
+  if (v < n) parent[v] = (bits[v >> 5] >> (v & 31)) & 1u ? m : (int32_t)v;
+  else if (v == n) parent[v] = (int32_t)n;
+  if (v == 0) ctl[kWSeed] = m == 0x7fffffff ? -1 : m;
+}
+
 static int grid_persist(long long work) {
   long long blocks = (work + kCcThreads - 1) / kCcThreads;
   const long long cap = (long long)sm_count() * 8;
@@ -340,6 +463,17 @@ int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int3
   return check_launch(launches);
 }
 
+static size_t warm_ws_layout(int32_t n, size_t *off_bits, size_t *off_f0, size_t *off_f1) {
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  size_t b = 256;  // control words
+  *off_bits = b;
+  b += ((nn + 31) / 32 * 4 + 255) / 256 * 256;
+  *off_f0 = b;
+  b += (nn * 4 + 255) / 256 * 256;
+  *off_f1 = b;
+  return b + (nn * 4 + 255) / 256 * 256;
+}
+
 constexpr int kReachBatch = 4;      // sweeps between host checks
 constexpr int kReachMaxSweeps = 32; // then the union-find finishes the job
 
@@ -351,6 +485,55 @@ static size_t reach_ws_layout(int32_t n, size_t *off_flags, size_t *off_parent, 
   b += ((size_t)n + 1 + 63) / 64 * 256;      // parent of the fallback (n + 1 ints)
   *off_cc = b;
   return b + 256;                            // dlp_cc_graph workspace
+}
+
+size_t dlp_cc_graph_warm_workspace_bytes(int32_t n) {
+  size_t a, b, c;
+  return warm_ws_layout(n, &a, &b, &c);
+}
+
+int dlp_cc_graph_warm(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                      int w_dtype, const uint8_t *vmask, int32_t *parent, int32_t *err, void *ws, size_t ws_bytes,
+                      dlp_stream_t stream) {
+  if (n < 0 || !parent) return DLP_ERR_INVALID;
+  if (n > 0 && (!rbeg || !rend || !col)) return DLP_ERR_INVALID;
+  if (w && w_dtype != DLP_F32 && w_dtype != DLP_F64 && w_dtype != DLP_BF16) return DLP_ERR_DTYPE;
+  size_t off_bits, off_f0, off_f1;
+  if (!ws || ws_bytes < warm_ws_layout(n, &off_bits, &off_f0, &off_f1)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {
+    k_cc_init<<<1, kCcThreads, 0, s>>>(parent, 1);
+    return check_launch();
+  }
+  char *base = (char *)ws;
+  int32_t *ctl = (int32_t *)base;
+  uint32_t *bits = (uint32_t *)(base + off_bits);
+  int32_t *front[2] = {(int32_t *)(base + off_f0), (int32_t *)(base + off_f1)};
+  DLP_CUDA(cudaMemsetAsync(bits, 0, ((size_t)n + 31) / 32 * 4, s));
+  k_warm_seed<<<1, 32, 0, s>>>(n, vmask, bits, front[0], ctl);
+  const int cap = std::max(n / 16, 1024);
+  const int grid = grid_persist((long long)n * 8);
+  const int grid1 = grid_persist(n);
+#define DLP_WARM_PASSES(TW)                                                                                       \
+  for (int l = 0; l < kWarmDown; ++l)                                                                            \
+    k_bfs_down<TW><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const TW *)w, vmask, bits, front[l & 1],      \
+                                               front[(l + 1) & 1], ctl, l, cap);                                  \
+  for (int u = 0; u < kWarmUp; ++u)                                                                              \
+    k_bfs_up<TW><<<grid1, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const TW *)w, vmask, bits, ctl);               \
+  k_warm_min<<<ceil_div_i(((long long)n + 31) / 32, kCcThreads), kCcThreads, 0, s>>>(n, bits, ctl);              \
+  k_warm_parent<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(n, bits, parent, ctl);           \
+  k_cc_graph<TW><<<grid, kCcThreads, 0, s>>>(n, rbeg, rend, col, (const TW *)w, vmask, nullptr, parent, err, ctl);
+  if (!w || w_dtype == DLP_F32) {
+    DLP_WARM_PASSES(float)
+  } else if (w_dtype == DLP_F64) {
+    DLP_WARM_PASSES(double)
+  } else {
+    DLP_WARM_PASSES(bf16)
+  }
+#undef DLP_WARM_PASSES
+  k_cc_compress<<<ceil_div_i((long long)n + 1, kCcThreads), kCcThreads, 0, s>>>(parent, n + 1, err);
+  k_cc_big<<<1, kCcModeSample, 0, s>>>(n, vmask, parent, ctl);  // the next call's seed
+  return check_launch(kWarmDown + kWarmUp + 6);
 }
 
 size_t dlp_ground_reach_workspace_bytes(int32_t n) {

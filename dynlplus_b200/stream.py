@@ -369,6 +369,9 @@ class EdgeStream:
             self._cc_parent = torch.empty(n + 1, dtype=torch.int32, device=dev)
             self._cc_label = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
             self._cc_counts = torch.zeros(3, dtype=torch.int32, device=dev)  # n_comp, n_masked, error
+            # the warm labelling's state between batches (its search seed): zeroed once
+            self._cc_ws = torch.zeros(int(_lib.lib().dlp_cc_graph_warm_workspace_bytes(n)), dtype=torch.uint8,
+                                      device=dev)
             self._components_launch()
         self.last_changed = torch.arange(n, dtype=torch.int32, device=dev)
         self.last_moved = torch.zeros(0, dtype=torch.int32, device=dev)
@@ -394,10 +397,9 @@ class EdgeStream:
         side = self._cc_stream
         side.wait_stream(main)
         with torch.cuda.stream(side):
-            ws = workspace("cc_graph").get(_lib.lib().dlp_cc_graph_workspace_bytes())
-            _lib.call("dlp_cc_graph", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), code(G.aw),
-                      ptr(self.vmask), None, ptr(self._cc_parent), ptr(self._cc_counts[2:3]), ptr(ws), ws.numel(),
-                      stream())
+            _lib.call("dlp_cc_graph_warm", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), code(G.aw),
+                      ptr(self.vmask), ptr(self._cc_parent), ptr(self._cc_counts[2:3]), ptr(self._cc_ws),
+                      self._cc_ws.numel(), stream())
             wl = workspace("cc_labels").get(_lib.lib().dlp_cc_mask_labels_workspace_bytes(n))
             _lib.call("dlp_cc_mask_labels", n, ptr(self._cc_parent), ptr(self.vmask), ptr(self._cc_label),
                       ptr(self._cc_counts[0:1]), ptr(self._cc_counts[1:2]), ptr(wl), wl.numel(), stream())

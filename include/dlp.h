@@ -177,6 +177,19 @@ int dlp_cc_graph(int32_t n, const int32_t *rbeg, const int32_t *rend, const int3
                  int w_dtype, const uint8_t *vmask, const uint8_t *sink, int32_t *parent, int32_t *err, void *ws,
                  size_t ws_bytes, dlp_stream_t stream);
 
+/* dlp_cc_graph without a sink, for a graph that changes by small batches between calls (the
+ * per-batch components of the resident stream; no reference counterpart beyond dynlp/cc.py:8-23 run
+ * per batch in dynlp/stream.py:150-153). Same parent (n + 1 entries; minimum vertex id of every
+ * component of the vmask-induced subgraph over live entries, parent[n] = n) as dlp_cc_graph with
+ * sink = NULL. The workspace carries state between calls: zero it before the first call; each call
+ * starts a breadth-first search from the root of the previous call's most frequent component and
+ * leaves the rows it did not reach to the union-find. Asynchronous (no host read).
+ * Workspace: dlp_cc_graph_warm_workspace_bytes(n). */
+size_t dlp_cc_graph_warm_workspace_bytes(int32_t n);
+int dlp_cc_graph_warm(int32_t n, const int32_t *rbeg, const int32_t *rend, const int32_t *col, const void *w,
+                      int w_dtype, const uint8_t *vmask, int32_t *parent, int32_t *err, void *ws, size_t ws_bytes,
+                      dlp_stream_t stream);
+
 /* The grounded set (dynlp/stream.py:150-159, :275-280) without a full labelling: on entry umask
  * holds the previous grounded set; on exit umask[u] = 1 iff vmask[u] and u's component in the
  * graph form of dlp_cc_graph (same arguments, same symmetric row ranges) reaches the sink, i.e.

@@ -160,3 +160,73 @@ def test_ground_reach_matches_components(case):
         assert sweeps < 0  # the fallback ran
     elif case == "dense":
         assert 0 < sweeps <= 32  # settled by the sweeps (a near-critical sparse graph may need the fallback)
+
+
+def _warm_case(kind, rng):
+    """(n, symmetric scipy CSR with some zero-weight entries, vmask) for the warm labelling."""
+    import scipy.sparse as ssp
+    if kind == "er":
+        n = 30_000
+        m = 5 * n
+        u, v = rng.integers(0, n, m), rng.integers(0, n, m)
+    elif kind == "path":  # one long chain: far deeper than the search's levels and sweeps
+        n = 20_000
+        u, v = np.arange(n - 1), np.arange(1, n)
+    else:  # many small components
+        n = 20_000
+        u = rng.integers(0, n, n // 2)
+        v = np.minimum(n - 1, u + rng.integers(1, 4, n // 2))
+    ok = u != v
+    u, v = u[ok], v[ok]
+    w = np.where(rng.random(u.size) < 0.1, 0.0, 1.0).astype(np.float32)  # inert entries
+    A = ssp.coo_matrix((np.concatenate([w, w]), (np.concatenate([u, v]), np.concatenate([v, u]))), shape=(n, n))
+    A = A.tocsr()
+    A.sum_duplicates()
+    A.data = np.where(A.data > 0, 1.0, 0.0).astype(np.float32)
+    return n, A, (rng.random(n) < 0.95).astype(np.uint8)
+
+
+@pytest.mark.parametrize("kind", ["er", "path", "pieces"])
+def test_warm_labelling_matches_union_find_over_calls(kind):
+    """dlp_cc_graph_warm equals dlp_cc_graph (no sink) call after call while the graph changes and
+    the seed the workspace carries goes stale: edges deleted around it, its vertex cut off, new
+    edges merging components."""
+    from dynlplus_b200 import _lib
+    from dynlplus_b200.backend import code, ptr, stream
+    rng = np.random.default_rng({"er": 1, "path": 2, "pieces": 3}[kind])
+    n, A, vm = _warm_case(kind, rng)
+    ws = torch.zeros(int(_lib.lib().dlp_cc_graph_warm_workspace_bytes(n)), dtype=torch.uint8, device="cuda")
+    wsg = torch.zeros(int(_lib.lib().dlp_cc_graph_workspace_bytes()), dtype=torch.uint8, device="cuda")
+    vmask = T(vm)
+    for call in range(6):
+        G = CSR.from_scipy(A)
+        got = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        want = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        err = torch.zeros(2, dtype=torch.int32, device="cuda")
+        _lib.call("dlp_cc_graph_warm", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.data), code(G.data),
+                  ptr(vmask), ptr(got), ptr(err[0:1]), ptr(ws), ws.numel(), stream())
+        _lib.call("dlp_cc_graph", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.data), code(G.data),
+                  ptr(vmask), None, ptr(want), ptr(err[1:2]), ptr(wsg), wsg.numel(), stream())
+        assert int(err.sum()) == 0
+        np.testing.assert_array_equal(got.cpu().numpy(), want.cpu().numpy(), err_msg=f"{kind} call {call}")
+        # the next graph: cut the seed the workspace now holds off from everything, then flip
+        # the weights of random entries (deletions and revivals, kept symmetric)
+        seed = int(ws[:4].view(torch.int32).item())
+        A = A.tolil()
+        if 0 <= seed < n:
+            A[seed, :] = 0
+            A[:, seed] = 0
+        A = A.tocsr()
+        A.eliminate_zeros()
+        k = rng.integers(0, A.nnz, max(A.nnz // 20, 1))
+        r = np.repeat(np.arange(n), np.diff(A.indptr))[k]
+        c = A.indices[k]
+        A = A.tolil()
+        for a, b in zip(r, c):
+            A[a, b] = A[b, a] = 0.0 if rng.random() < 0.7 else 1.0
+        u = rng.integers(0, n, 200)
+        v = rng.integers(0, n, 200)
+        for a, b in zip(u, v):
+            if a != b:
+                A[a, b] = A[b, a] = 1.0
+        A = A.tocsr()
