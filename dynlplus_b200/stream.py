@@ -457,35 +457,42 @@ class EdgeStream:
         self.join_components()  # the previous batch's labelling reads the graph this batch patches
         self.changed.zero_()
         self._stat.zero_()
-        st = self._stat
+        st = self._stat  # [error, overflow, deleted, inserted, ground changes, ground error, changed rows, -]
         s = stream()
         if nd:
             _lib.call("dlp_graph_delete", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(du),
                       ptr(dv), nd, ptr(self.umask), ptr(self.labeled), ptr(self.y), self.K, ptr(self.rowsum),
                       ptr(self.B), ptr(self.changed), ptr(st[2:3]), ptr(st[0:1]), ptr(self._squeeze), s)
-        if ni:
-            for attempt in range(4):
-                ws = workspace("insert").get(_lib.lib().dlp_graph_insert_workspace_bytes(ni))
-                st[1].zero_()
-                _lib.call("dlp_graph_insert", n, ptr(G.rbeg), ptr(G.rend), ptr(G.rcap), ptr(G.indices), ptr(G.aw),
-                          ptr(G.data), ptr(iu), ptr(iv), ptr(iw), ni, ptr(self.umask), ptr(self.labeled), ptr(self.y),
-                          self.K, ptr(self.rowsum), ptr(self.B), ptr(self.changed), ptr(st[1:2]), ptr(st[3:4]),
-                          ptr(st[0:1]), ptr(ws), ws.numel(), s)
-                flags = st[0:4].tolist()  # [error, overflow, deleted, inserted]: one read-back
-                if flags[1] == 0:
-                    break
-                G.rebuild()  # a row ran out of slack: repack with more and apply the batch again
-                self.counters["rebuilds"] += 1
-            else:
-                raise RuntimeError("edge insertion kept overflowing after repacking")
+        # Everything below is queued before the first host read: the insertion, the grounding, the
+        # changed rows and the solver CSR; one read then brings every flag and count. An overflow
+        # (rare) or a membership change (rare) redoes what depends on it.
+        for attempt in range(4):
+            if ni:
+                self._insert(iu, iv, iw, ni)
+            if self.with_components:
+                self._components_launch()
+            self._ground_launch()
+            Qb, _ = kernels.flatnonzero(self.changed, count=st[6:7], sync=False)
+            self._csr_launch()
+            flags = self._read_counts()
+            if flags["overflow"] == 0:
+                break
+            self.join_components()
+            G.rebuild()  # a row ran out of slack: repack with more and apply the insertions again
+            self.counters["rebuilds"] += 1
+            st[1].zero_()
+            # the grounding of the incomplete graph flipped in_t's vertices: back to the batch's start,
+            # so the next grounding counts every membership change against it
+            self.umask.bitwise_xor_(self.in_t)
         else:
-            flags = st[0:4].tolist()
-        if flags[0]:
-            raise ValueError(f"edge batch rejected: {_lib.STATUS.get(flags[0])} (vertex id out of range?)")
-        if self.with_components:
-            self._components_launch()
-        # grounding: components of the unlabelled subgraph with the labelled vertices as a sink
-        nmoved = self._ground()
+            raise RuntimeError("edge insertion kept overflowing after repacking")
+        if flags["error"]:
+            raise ValueError(f"edge batch rejected: {_lib.STATUS.get(flags['error'])} (vertex id out of range?)")
+        if flags["ground_error"]:
+            raise ValueError("grounding: entry column outside [0, n)")
+        nmoved = flags["moved"]
+        self.counters["ground_sweeps"] += abs(self._sweeps.value)
+        self.counters["ground_fallbacks"] += self._sweeps.value < 0
         moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
         if nmoved:
             mv, _ = kernels.flatnonzero(self.in_t, sync=False)
@@ -493,21 +500,51 @@ class EdgeStream:
             _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(moved),
                       nmoved, ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), s)
             self.counters["ground_changes"] += nmoved
-        # the changed rows and the batch's solver CSR are both queued before one host read of their
-        # two counts
-        Qb, qc = kernels.flatnonzero(self.changed, sync=False)
+            Qb, _ = kernels.flatnonzero(self.changed, count=st[6:7], sync=False)
+            self._csr_launch()
+            flags = self._read_counts()
+            self._counts = None
+        nq, nnz = flags["changed"], flags["nnz"]
         self.t += 1
-        self._csr_launch()
-        nq, nnz = torch.cat([qc, self._csr_ptr[n:n + 1]]).tolist()
         self._csr_set(nnz)
         Q = Qb[:nq]
         self._system_rows(Q, nq)
         self.last_changed, self.last_moved = Q, moved
         self.n_ins, self.n_del = ni, nd
-        self.counters["applied"] += flags[2] + flags[3]
-        if nmoved:
-            self._counts = None
+        self.counters["applied"] += flags["deleted"] + flags["inserted"]
         return self.system
+
+    def _insert(self, iu, iv, iw, ni):
+        G, st = self.G, self._stat
+        ws = workspace("insert").get(_lib.lib().dlp_graph_insert_workspace_bytes(ni))
+        _lib.call("dlp_graph_insert", self.n, ptr(G.rbeg), ptr(G.rend), ptr(G.rcap), ptr(G.indices), ptr(G.aw),
+                  ptr(G.data), ptr(iu), ptr(iv), ptr(iw), ni, ptr(self.umask), ptr(self.labeled), ptr(self.y),
+                  self.K, ptr(self.rowsum), ptr(self.B), ptr(self.changed), ptr(st[1:2]), ptr(st[3:4]),
+                  ptr(st[0:1]), ptr(ws), ws.numel(), stream())
+
+    def _ground_launch(self):
+        """The grounding check (reachability from the labelled vertices through unlabelled ones,
+        dynlp/stream.py:150-159): umask and in_t updated, the number of membership changes counted
+        into the batch's stat word 4 (its sweeps synchronise the stream internally)."""
+        import ctypes as ct
+        G, n, st = self.G, self.n, self._stat
+        self._sweeps = ct.c_int32(0)
+        ws = workspace("ground_reach").get(_lib.lib().dlp_ground_reach_workspace_bytes(n))
+        _lib.call("dlp_ground_reach", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), code(G.aw),
+                  ptr(self.vmask), ptr(self.labeled), ptr(self.umask), ptr(self.in_t), ptr(st[4:5]), ptr(st[5:6]),
+                  ct.addressof(self._sweeps), ptr(ws), ws.numel(), stream())
+
+    def _read_counts(self):
+        """One host read of the batch's flags and counts (and the solver CSR's entry count)."""
+        if getattr(self, "_h_stat", None) is None:
+            self._h_stat = torch.zeros(9, dtype=torch.int32, pin_memory=torch.cuda.is_available())
+        h = self._h_stat
+        h[0:8].copy_(self._stat, non_blocking=True)
+        h[8:9].copy_(self._csr_ptr[self.n:self.n + 1], non_blocking=True)
+        torch.cuda.current_stream(self.dev).synchronize()
+        v = h.tolist()
+        return {"error": v[0], "overflow": v[1], "deleted": v[2], "inserted": v[3], "moved": v[4],
+                "ground_error": v[5], "changed": v[6], "nnz": v[8]}
 
     def apply_vertices(self, ins, dele, tau=None, wmax=None) -> System:
         """One vertex-arrival batch (IncrementalStream.batches, dynlp/stream.py:300-346): the
