@@ -56,7 +56,6 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_graph_delete": ("ipppppppipppippppppp", ct.c_int),
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
-    "dlp_refine_residual": ("iipqpqpqipp", ct.c_int),
     "dlp_predict_workspace_bytes": ("i", ct.c_size_t),
     "dlp_predict": ("iipqiippppppzp", ct.c_int),
     "dlp_label_update": ("pidpppppipppp", ct.c_int),

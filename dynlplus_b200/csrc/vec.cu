@@ -65,37 +65,6 @@ __global__ void k_ground_update(int32_t n, const int32_t *__restrict__ parent, c
   if ((threadIdx.x & 31) == 0 && b) atomicAdd(counts, __popc(b));
 }
 
-// R64 += scale[c] * (Rt - Rs): the fp64 residual after a working-precision correction A D = Rs,
-// from the correction's own true residual Rt = Rs - A D (same thread map as k_cols_scale).
-template <typename T>
-__global__ void __launch_bounds__(kColsThreads) k_refine_residual(int32_t n, int32_t C, double *R64, int64_t ld64,
-                                                                  const T *__restrict__ Rt, int64_t ldt,
-                                                                  const T *__restrict__ Rs, int64_t lds,
-                                                                  const double *__restrict__ scale) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long RS = (long long)gridDim.x * blockDim.x / C;
-  const long long r0 = t / C;
-  const int c = (int)(t - r0 * C);
-  if (r0 >= RS) return;
-  const double sc = scale[c];
-  for (long long r = r0; r < n; r += kColsUnroll * RS) {
-    double a[kColsUnroll], b[kColsUnroll], y[kColsUnroll];
-#pragma unroll
-    for (int u = 0; u < kColsUnroll; ++u) {
-      const long long rr = r + u * RS;
-      const bool ok = rr < n;
-      a[u] = ok ? (double)Rt[rr * ldt + c] : 0.0;
-      b[u] = ok ? (double)Rs[rr * lds + c] : 0.0;
-      y[u] = ok ? R64[rr * ld64 + c] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < kColsUnroll; ++u) {
-      const long long rr = r + u * RS;
-      if (rr < n) R64[rr * ld64 + c] = y[u] + sc * (a[u] - b[u]);
-    }
-  }
-}
-
 // Labels (solvers.predict, dynlp/solvers.py:166-167): binary: F[r,0] > 0.5; otherwise the first
 // column holding the row's maximum (numpy argmax). Rows outside the mask get -1. flag[r] = the label
 // differs from the one labels[r] held on entry; labels[r] takes the new one.
@@ -163,26 +132,6 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
     k_cols_scale<float, float><<<grid, kColsThreads, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (float *)Y, ldy);
   else if (x_dtype == DLP_F32 && y_dtype == DLP_BF16 && op == 2)
     k_cols_scale<float, bf16><<<grid, kColsThreads, 0, s>>>(n, C, (const float *)X, ldx, scale, op, (bf16 *)Y, ldy);
-  else
-    return DLP_ERR_DTYPE;
-  return check_launch();
-}
-
-int dlp_refine_residual(int32_t n, int32_t C, double *R64, int64_t ld64, const void *Rt, int64_t ldt, const void *Rs,
-                        int64_t lds, int dtype, const double *scale, dlp_stream_t stream) {
-  if (n < 0 || C <= 0 || ld64 < C || ldt < C || lds < C) return DLP_ERR_INVALID;
-  if (n == 0) return DLP_OK;
-  if (!R64 || !Rt || !Rs || !scale) return DLP_ERR_INVALID;
-  long long blocks = ceil_div_i((long long)n * C, (long long)kColsThreads * kColsUnroll);
-  blocks = std::min(blocks, (long long)sm_count() * 8);
-  blocks = std::max(blocks, (long long)ceil_div_i((long long)C, kColsThreads));
-  cudaStream_t s = (cudaStream_t)stream;
-  if (dtype == DLP_F32)
-    k_refine_residual<float><<<(int)blocks, kColsThreads, 0, s>>>(n, C, R64, ld64, (const float *)Rt, ldt,
-                                                                 (const float *)Rs, lds, scale);
-  else if (dtype == DLP_F64)
-    k_refine_residual<double><<<(int)blocks, kColsThreads, 0, s>>>(n, C, R64, ld64, (const double *)Rt, ldt,
-                                                                  (const double *)Rs, lds, scale);
   else
     return DLP_ERR_DTYPE;
   return check_launch();

@@ -231,8 +231,6 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     st.iters += it.value
     st.edges += (it.value + 2) * W.nnz + work_M * it.value
     st.relres = rel.value
-    # status 5: the stop was confirmed on the true residual, which R now holds (rhs - A Z)
-    st.pcg_status, st.pcg_R = status.value, R
     if status.value == 4:
         raise FloatingPointError("PCG breakdown: non-finite residual")
     return Z
@@ -610,19 +608,10 @@ class DynLPPlus(Solver):
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs), ld(Rs),
                       code(Rs), stream())
             D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)  # zeroed by the zero start
-            st.pcg_status, st.pcg_R = None, None
             D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, zero_start=True, **kw)
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(D), ld(D), code(D), ptr(sc), 1, ptr(Z64), ld(Z64),
                       code(Z64), stream())
-            Rt = st.pcg_R
-            if st.pcg_status == 5 and Rt is not None and not self.lowp and Rt.shape == Rs.shape:
-                # the correction's confirmed true residual Rs - A D gives the new fp64 residual
-                # without a second fp64 product: R64 += scale (Rt - Rs)
-                _lib.call("dlp_refine_residual", Z64.shape[0], C + 1, ptr(R64), ld(R64), ptr(Rt), ld(Rt), ptr(Rs),
-                          ld(Rs), code(Rs), ptr(sc), stream())
-                stats = None
-            else:
-                R64, stats = None, None
+            R64, stats = None, None
         if R64 is None:
             R64 = residual(s64, Z64, rhs64)
             st.edges += s64.nnz

@@ -340,16 +340,6 @@ int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t
 int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
                    void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream);
 
-/* The fp64 residual after a working-precision correction (refinement round, dynlp/solvers.py:333-337):
- * the correction solved A D = Rs with Rs = R64 / scale cast to the working precision, and Rt is its
- * confirmed true residual Rs - A D (what dlp_pcg leaves in R when it returns status 5). Then
- *   R64[r,c] += scale[c] * (Rt[r,c] - Rs[r,c])
- * is the residual of Z64 + scale D without a new fp64 product; its error is that of Rt (a few
- * working-precision ulps of Rs, i.e. of the residual being corrected, not of rhs). Rt, Rs: dtype
- * f32/f64; scale: device double[C]. */
-int dlp_refine_residual(int32_t n, int32_t C, double *R64, int64_t ld64, const void *Rt, int64_t ldt, const void *Rs,
-                        int64_t lds, int dtype, const double *scale, dlp_stream_t stream);
-
 /* Labels of the rows (solvers.predict, dynlp/solvers.py:166-167): binary != 0 (the K == 2 column):
  * label = F[r,0] > 0.5; otherwise the first column of the row's maximum over C columns (numpy
  * argmax). Rows with mask[r] == 0 get -1 (mask NULL: every row). labels[0..n) holds the previous
