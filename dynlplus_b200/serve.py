@@ -220,9 +220,9 @@ class Server:
     def _do_update(self, first):
         items = self._drain("update", first)
         try:
-            for it in items:  # sequential patch semantics
+            for i, it in enumerate(items):  # sequential patch semantics, one solve for all of them
                 r = it.req
-                self.es.apply_edges(r.ins_u, r.ins_v, r.ins_w, r.del_u, r.del_v)
+                self.es.apply_edges(r.ins_u, r.ins_v, r.ins_w, r.del_u, r.del_v, keep_pending=i > 0)
             st = self.solver.solve(self.es.system)
             labels = self._snapshot()
             torch.cuda.current_stream().synchronize()

@@ -442,8 +442,12 @@ class EdgeStream:
         return t.to(self.dev, non_blocking=True)
 
     # -- the batch -----------------------------------------------------------------------------
-    def apply_edges(self, ins_u=None, ins_v=None, ins_w=None, del_u=None, del_v=None) -> System:
-        """Apply one edge batch (deletions, then insertions) and return the updated system."""
+    def apply_edges(self, ins_u=None, ins_v=None, ins_w=None, del_u=None, del_v=None, keep_pending=False) -> System:
+        """Apply one edge batch (deletions, then insertions) and return the updated system.
+
+        keep_pending: the previous batch has not been solved yet (several batches patched before one
+        solve): its changed and moved rows stay in this batch's lists, so the solve refreshes the
+        equations and residuals of every row any of the batches touched."""
         G, n = self.G, self.n
         self._vertex_batch = None
         for name, x in (("ins_u", ins_u), ("ins_v", ins_v), ("del_u", del_u), ("del_v", del_v)):
@@ -455,7 +459,9 @@ class EdgeStream:
         nd = int(du.numel()) if du is not None else 0
         ni = int(iu.numel()) if iu is not None else 0
         self.join_components()  # the previous batch's labelling reads the graph this batch patches
-        self.changed.zero_()
+        prev_moved = self.last_moved if keep_pending else None
+        if not keep_pending:
+            self.changed.zero_()
         self._stat.zero_()
         st = self._stat  # [error, overflow, deleted, inserted, ground changes, ground error, changed rows, -]
         s = stream()
@@ -481,6 +487,7 @@ class EdgeStream:
             G.rebuild()  # a row ran out of slack: repack with more and apply the insertions again
             self.counters["rebuilds"] += 1
             st[1].zero_()
+            st[3:6].zero_()  # counts the next attempt makes again (insertions, membership changes)
             # the grounding of the incomplete graph flipped in_t's vertices: back to the batch's start,
             # so the next grounding counts every membership change against it
             self.umask.bitwise_xor_(self.in_t)
@@ -509,6 +516,8 @@ class EdgeStream:
         self._csr_set(nnz)
         Q = Qb[:nq]
         self._system_rows(Q, nq)
+        if prev_moved is not None and prev_moved.numel():
+            moved = torch.cat([prev_moved, moved])  # parked again by the solve: idempotent
         self.last_changed, self.last_moved = Q, moved
         self.n_ins, self.n_del = ni, nd
         self.counters["applied"] += flags["deleted"] + flags["inserted"]

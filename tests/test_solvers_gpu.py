@@ -395,3 +395,28 @@ def test_reinsert_of_squeezed_edges_next_to_appends(order):
     ref = _oracle_edge_system(A_sc, ds.y.cpu().numpy(), K, lab.cpu().numpy())
     np.testing.assert_array_equal(np.flatnonzero(S.solved.cpu().numpy()), ref["U"])
     np.testing.assert_allclose(S.astype(torch.float64).diag.cpu().numpy()[ref["U"]], ref["diag"], rtol=1e-12)
+
+
+def test_coalesced_batches_then_one_solve():
+    """Several edge batches patched before one solve (the serving loop's coalescing,
+    apply_edges(keep_pending=True)): the solve refreshes every row any batch changed, so the scores
+    meet the relative residual on the oracle's system rebuilt from the final graph."""
+    n, K = 20_000, 4
+    ds = graphs.er_graph(n, 10, K, seed=12)
+    lab = graphs.label_mask(n, 0.01, seed=12)
+    es = stream.EdgeStream(ds, lab)
+    up = graphs.EdgeUpdates(ds.A, seed=12)
+    solver = solvers.IncrementalLP(n, K, "float32", tol=1e-3, method="pcg", target_relres=1e-6, full_every=64)
+    solver.solve(es.system)
+    A_sc = ds.A.to_scipy().astype(np.float64)
+    for rnd in range(2):
+        for i in range(3):
+            b = up.next(500)
+            S = es.apply_edges(**b, keep_pending=i > 0)
+            A_sc = O.apply_edges(A_sc, b["ins_u"], b["ins_v"], b["ins_w"].astype(np.float64), b["del_u"], b["del_v"])
+        st = solver.solve(S)
+        ref = _oracle_edge_system(A_sc, ds.y.cpu().numpy(), K, lab.cpu().numpy())
+        U = ref["U"]
+        F = solver.Z[:, :K].cpu().numpy()[U]
+        rel = O.relres(ref["W"], ref["diag"], F, ref["rhs"])
+        assert rel <= 1e-6 and st.relres <= 1e-6, (rnd, rel, st.relres)
