@@ -237,7 +237,8 @@ __global__ void __launch_bounds__(kGThreads)
   const long long g = t >> 3;
   const int l = (int)(t & 7);
   if (g >= nt) return;
-  const int32_t u = T[g];
+  const int32_t u = T ? T[g] : (int32_t)g;  // no list: every row flagged in in_t
+  if (!T && !in_t[u]) return;
   const bool uu = umask[u];
   for (int j = rbeg[u] + l; j < rend[u]; j += 8) {
     const int32_t x = col[j];
@@ -254,6 +255,17 @@ __global__ void __launch_bounds__(kGThreads)
     }
   }
   if (l == 0) changed[u] = 1;
+}
+
+// rowsum[r] for the rows flagged in flag (the toggled rows when they come without a list).
+__global__ void k_rowsum_flagged(const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
+                                 const float *__restrict__ w, const uint8_t *__restrict__ flag, int32_t nr,
+                                 double *rowsum) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nr || !flag[r]) return;
+  double s = 0.0;
+  for (int j = rbeg[r]; j < rend[r]; ++j) s += (double)w[j];
+  rowsum[r] = s;
 }
 
 __global__ void k_rowsum(const int32_t *__restrict__ rbeg, const int32_t *__restrict__ rend,
@@ -465,11 +477,14 @@ int dlp_graph_toggle(const int32_t *rbeg, const int32_t *rend, const int32_t *co
                      uint8_t *changed, dlp_stream_t stream) {
   if (nt < 0) return DLP_ERR_INVALID;
   if (nt == 0) return DLP_OK;
-  if (!rbeg || !rend || !col || !aw || !w || !T || !in_t || !umask || !rowsum || !changed) return DLP_ERR_INVALID;
+  if (!rbeg || !rend || !col || !aw || !w || !in_t || !umask || !rowsum || !changed) return DLP_ERR_INVALID;
   cudaStream_t s = (cudaStream_t)stream;
   k_graph_toggle<<<grid1((long long)nt * 8), kGThreads, 0, s>>>(rbeg, rend, col, aw, w, T, nt, in_t, umask, rowsum,
                                                                  changed);
-  k_rowsum<<<grid1(nt), kGThreads, 0, s>>>(rbeg, rend, w, T, nt, rowsum);
+  if (T)
+    k_rowsum<<<grid1(nt), kGThreads, 0, s>>>(rbeg, rend, w, T, nt, rowsum);
+  else
+    k_rowsum_flagged<<<grid1(nt), kGThreads, 0, s>>>(rbeg, rend, w, in_t, nt, rowsum);
   return check_launch(2);
 }
 

@@ -469,28 +469,32 @@ class EdgeStream:
             _lib.call("dlp_graph_delete", n, ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(du),
                       ptr(dv), nd, ptr(self.umask), ptr(self.labeled), ptr(self.y), self.K, ptr(self.rowsum),
                       ptr(self.B), ptr(self.changed), ptr(st[2:3]), ptr(st[0:1]), ptr(self._squeeze), s)
-        # Everything below is queued before the first host read: the insertion, the grounding, the
-        # changed rows and the solver CSR; one read then brings every flag and count. An overflow
-        # (rare) or a membership change (rare) redoes what depends on it.
+        # Everything below is queued in dependency order before one host read of every flag and
+        # count: the insertion, the grounding (its sweeps synchronise internally), the membership
+        # toggle of the rows it flagged, the changed rows and the solver CSR. An overflow (rare)
+        # undoes the toggle, repacks and redoes the rest.
         for attempt in range(4):
             if ni:
                 self._insert(iu, iv, iw, ni)
             if self.with_components:
                 self._components_launch()
             self._ground_launch()
+            self._toggle_flagged()
+            mv, _ = kernels.flatnonzero(self.in_t, count=st[7:8], sync=False)
             Qb, _ = kernels.flatnonzero(self.changed, count=st[6:7], sync=False)
             self._csr_launch()
             flags = self._read_counts()
             if flags["overflow"] == 0:
                 break
             self.join_components()
+            # back to the batch's start membership: umask before the grounding, then the same rows
+            # toggled again put their weights and their neighbours' row sums back
+            self.umask.bitwise_xor_(self.in_t)
+            self._toggle_flagged()
             G.rebuild()  # a row ran out of slack: repack with more and apply the insertions again
             self.counters["rebuilds"] += 1
             st[1].zero_()
-            st[3:6].zero_()  # counts the next attempt makes again (insertions, membership changes)
-            # the grounding of the incomplete graph flipped in_t's vertices: back to the batch's start,
-            # so the next grounding counts every membership change against it
-            self.umask.bitwise_xor_(self.in_t)
+            st[3:8].zero_()  # counts the next attempt makes again
         else:
             raise RuntimeError("edge insertion kept overflowing after repacking")
         if flags["error"]:
@@ -500,16 +504,9 @@ class EdgeStream:
         nmoved = flags["moved"]
         self.counters["ground_sweeps"] += abs(self._sweeps.value)
         self.counters["ground_fallbacks"] += self._sweeps.value < 0
-        moved = torch.zeros(0, dtype=torch.int32, device=self.dev)
+        moved = mv[:nmoved]
         if nmoved:
-            mv, _ = kernels.flatnonzero(self.in_t, sync=False)
-            moved = mv[:nmoved]  # the grounding counted the membership changes: no read-back
-            _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), ptr(moved),
-                      nmoved, ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), s)
             self.counters["ground_changes"] += nmoved
-            Qb, _ = kernels.flatnonzero(self.changed, count=st[6:7], sync=False)
-            self._csr_launch()
-            flags = self._read_counts()
             self._counts = None
         nq, nnz = flags["changed"], flags["nnz"]
         self.t += 1
@@ -543,6 +540,13 @@ class EdgeStream:
                   ptr(self.vmask), ptr(self.labeled), ptr(self.umask), ptr(self.in_t), ptr(st[4:5]), ptr(st[5:6]),
                   ct.addressof(self._sweeps), ptr(ws), ws.numel(), stream())
 
+    def _toggle_flagged(self):
+        """Membership change of every row the grounding flagged in in_t (dlp_graph_toggle without a
+        list; nothing to do when no row moved)."""
+        G = self.G
+        _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), None, self.n,
+                  ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), stream())
+
     def _read_counts(self):
         """One host read of the batch's flags and counts (and the solver CSR's entry count)."""
         if getattr(self, "_h_stat", None) is None:
@@ -552,7 +556,7 @@ class EdgeStream:
         h[8:9].copy_(self._csr_ptr[self.n:self.n + 1], non_blocking=True)
         torch.cuda.current_stream(self.dev).synchronize()
         v = h.tolist()
-        return {"error": v[0], "overflow": v[1], "deleted": v[2], "inserted": v[3], "moved": v[4],
+        return {"error": v[0], "overflow": v[1], "deleted": v[2], "inserted": v[3], "moved": v[7],
                 "ground_error": v[5], "changed": v[6], "nnz": v[8]}
 
     def apply_vertices(self, ins, dele, tau=None, wmax=None) -> System:

@@ -300,7 +300,8 @@ int dlp_graph_insert(int32_t n, const int32_t *rbeg, int32_t *rend, const int32_
 /* Membership change of the vertices T[0..nt) (in_t[v] = 1 marks them; umask already holds the new
  * U): solver weights of their entries and mirror entries follow umask, neighbours' row sums move
  * by the difference and are flagged changed, and the row sums of T are recomputed
- * (IncrementalStream._toggle, dynlp/stream.py:206-228). */
+ * (IncrementalStream._toggle, dynlp/stream.py:206-228). T == NULL: the rows u < nt with in_t[u] != 0
+ * (pass nt = n; no list and no host count needed). */
 int dlp_graph_toggle(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *aw, float *w,
                      const int32_t *T, int32_t nt, const uint8_t *in_t, const uint8_t *umask, double *rowsum,
                      uint8_t *changed, dlp_stream_t stream);
