@@ -84,12 +84,23 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_amg_scale_rows": ("iidpqppqip", ct.c_int),
     "dlp_amg_jacobi_sweep": ("iippppqpqpdpqip", ct.c_int),
     "dlp_dense_apply": ("iippqpqip", ct.c_int),
+    "dlp_amg_vcycle_workspace_bytes": ("piii", ct.c_size_t),
+    "dlp_amg_vcycle": ("pipidiiipqpqpzp", ct.c_int),
+    "dlp_pcg_amg_workspace_bytes": ("piii", ct.c_size_t),
+    "dlp_pcg_amg": ("ppppiippqpqpqpqpqpqippdiiiidpipidipzpppp", ct.c_int),
     "dlp_pcg_batched_workspace_bytes": ("iii", ct.c_size_t),
     "dlp_pcg_batched": ("pppiippqpqpqpqpqiiippppppdiiiiiidpzpppp", ct.c_int),
     "dlp_ground_update": ("ipppppp", ct.c_int),
 }
 
 _lib = None
+
+
+class AmgLevel(ct.Structure):
+    """dlp_amg_level (include/dlp.h): one level of an AMG hierarchy."""
+    _fields_ = [("n", ct.c_int32), ("nnz", ct.c_int64), ("indptr", ct.c_void_p), ("col", ct.c_void_p),
+                ("w", ct.c_void_p), ("diag", ct.c_void_p), ("agg", ct.c_void_p), ("off", ct.c_void_p),
+                ("members", ct.c_void_p)]
 
 
 class DLPError(RuntimeError):

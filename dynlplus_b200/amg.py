@@ -13,7 +13,11 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib, kernels
-from .backend import CSR, code, ld, ptr, stream, workspace
+from .backend import CSR, DTYPES, code, ld, ptr, stream, workspace
+
+
+def code_of(dt):
+    return DTYPES[dt]
 
 
 @dataclass
@@ -194,13 +198,40 @@ class AMG:
         _lib.call("dlp_amg_prolong_add", n, C, ptr(L.agg), ptr(Xc), ld(Xc), ptr(X), ld(X), code(R), stream())
         return self._smooth(L, X, R, self.nu, lvl)
 
+    def levels_desc(self, dt):
+        """The hierarchy as the library's level descriptors (dlp_amg_level), diagonals in dt; cached
+        per precision together with the tensors it points at."""
+        import ctypes as ct
+        key = ("desc", dt)
+        d = self._buf.get(key)
+        if d is None:
+            lv = self.levels + [self.coarse]
+            arr = (_lib.AmgLevel * len(lv))()
+            keep = []
+            for i, L in enumerate(lv):
+                diag = self._diag(L, i, dt)
+                w = L.W.data if L.W.data.dtype == torch.float32 else L.W.data.float().contiguous()
+                keep.append(w)
+                last = i == len(lv) - 1
+                arr[i] = _lib.AmgLevel(int(L.W.shape[0]), int(L.W.nnz), ptr(L.W.indptr), ptr(L.W.indices), ptr(w),
+                                       ptr(diag), None if last else ptr(L.agg), None if last else ptr(L.off),
+                                       None if last else ptr(L.members))
+            d = (arr, len(lv), keep)
+            self._buf[key] = d
+            del ct
+        return d
+
+    def vcycle_workspace(self, C, dt):
+        arr, nlev, _ = self.levels_desc(dt)
+        return workspace("amg_vcycle").get(_lib.lib().dlp_amg_vcycle_workspace_bytes(arr, nlev, C, code_of(dt)))
+
     def __call__(self, R):
-        """M(R): one V-cycle; returns a new tensor (the cycle's buffers are reused across calls).
-        Inputs wider than 64 columns are cycled 64 columns at a time (the columns are independent)."""
+        """M(R): one V-cycle (dlp_amg_vcycle: every level in one library call); returns a new tensor."""
         R = R.contiguous()
-        if R.shape[1] <= 64:
-            return self._cycle(0, R).clone()
-        out = torch.empty_like(R)
-        for c0 in range(0, R.shape[1], 64):
-            out[:, c0:c0 + 64] = self._cycle(0, R[:, c0:c0 + 64].contiguous())
-        return out
+        n, C = R.shape
+        Y = torch.empty_like(R)
+        arr, nlev, _ = self.levels_desc(R.dtype)
+        ws = self.vcycle_workspace(C, R.dtype)
+        _lib.call("dlp_amg_vcycle", arr, nlev, ptr(self.inv), self.nu, float(self.omega), self.coarse_sweeps, C,
+                  code(R), ptr(R), ld(R), ptr(Y), ld(Y), ptr(ws), ws.numel(), stream())
+        return Y

@@ -179,7 +179,11 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
         raise ValueError("pcg needs eps and/or target_relres")
     if M is not None and not isinstance(M, JacobiM):
         if zero_start:
-            Z.zero_()  # the generic loop starts from the Z it is given
+            Z.zero_()  # these loops start from the Z they are given
+        from .amg import AMG
+        if isinstance(M, AMG) and not lowp:
+            return _pcg_amg(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm,
+                            check_every, use_graph)
         return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, lowp)
     n, C = Z.shape
     if n == 0:
@@ -228,6 +232,47 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     if ev is not None:
         ev[1].record()
         PCG_EVENTS.append((ev[0], ev[1], it.value, n, C))
+    st.iters += it.value
+    st.edges += (it.value + 2) * W.nnz + work_M * it.value
+    st.relres = rel.value
+    if status.value == 4:
+        raise FloatingPointError("PCG breakdown: non-finite residual")
+    return Z
+
+
+def _pcg_amg(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, check_every, use_graph):
+    """PCG with the AMG V-cycle as preconditioner, its loop on the device (dlp_pcg_amg): the
+    reference's pcg (dynlp/solvers.py:66-97) with M = amg.AMG, one host read per device-side loop
+    and per confirmation of a proposed stop."""
+    n, C = Z.shape
+    if n == 0:
+        return Z
+    dt, dev = Z.dtype, Z.device
+    W = sys.W
+    w32 = W.data if W.data.dtype == torch.float32 else W.data.float().contiguous()
+    diag = sys.diag.to(dt).contiguous()
+    rhs = rhs.to(dt)
+    R = _scratch("amg_R", n, C, dt, dev)
+    P = _scratch("amg_P", n, C, dt, dev)
+    AP = _scratch("amg_AP", n, C, dt, dev)
+    Y = _scratch("amg_Y", n, C, dt, dev)
+    arr, nlev, _ = M.levels_desc(dt)
+    ws = workspace("pcg_amg").get(_lib.lib().dlp_pcg_amg_workspace_bytes(arr, nlev, C, code(Z)))
+    mode = 1 if eps is not None else 0
+    eps_h = (ct.c_double * C)(*[float(e) for e in eps]) if eps is not None else None
+    rn = None
+    if target_relres is not None:
+        mode |= 2
+        if rhs_norm is None:
+            rhs_norm = col_norms(rhs).cpu().tolist()
+        rn = (ct.c_double * C)(*[float(x) for x in rhs_norm])
+    it, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_int32(0)
+    _lib.call("dlp_pcg_amg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(w32), n, C, ptr(diag), ptr(rhs), ld(rhs),
+              ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), ptr(Y), ld(Y), code(Z), eps_h, rn,
+              float(target_relres or 0.0), mode, int(max_iter), int(patience),
+              int(bool(GRAPHS if use_graph is None else use_graph)), W.nnz / max(n, 1), arr, nlev, ptr(M.inv),
+              int(M.nu), float(M.omega), int(M.coarse_sweeps), ptr(ws), ws.numel(), ct.byref(it), ct.byref(rel),
+              ct.byref(status), stream(), allow=(_lib.DLP_ERR_CAP,))
     st.iters += it.value
     st.edges += (it.value + 2) * W.nnz + work_M * it.value
     st.relres = rel.value

@@ -457,6 +457,55 @@ int dlp_dense_apply(int32_t nc, int32_t C, const double *M, const void *X, int64
                     int dtype, dlp_stream_t stream);
 
 
+/* ---- (e) the V-cycle and the AMG-preconditioned PCG on the device ------------------------------
+ * A hierarchy is described level by level (level 0 = the operator of the solve): the level's
+ * operator W as plain CSR with fp32 weights, its diagonal s + rowsum(W) in the working precision,
+ * and the aggregation to the next level (agg: level row -> next-level row; off/members: the rows of
+ * each next-level aggregate in ascending order). The coarsest level has no aggregation. */
+typedef struct {
+  int32_t n;                    /* rows of the level */
+  int64_t nnz;                  /* stored entries of its W */
+  const int32_t *indptr, *col;  /* W (plain CSR) */
+  const float *w;
+  const void *diag;             /* s + rowsum(W), working precision */
+  const int32_t *agg;           /* level -> next level (NULL on the coarsest) */
+  const int32_t *off, *members; /* next-level aggregates (NULL on the coarsest) */
+} dlp_amg_level;
+
+/* One V-cycle Y = M(R) (dynlp/amg.py:114-134 _smooth / _cycle): on each level X = omega R / diag,
+ * nu - 1 damped Jacobi sweeps, the residual restricted to the next level, the cycle there, its result
+ * prolonged and added, nu sweeps; on the coarsest level the dense fp64 inverse coarse_inv (row-major
+ * n x n) when given, else coarse_sweeps sweeps. nu >= 1. dtype f32/f64 (R, Y, every diag). All
+ * intermediate vectors live in the workspace: dlp_amg_vcycle_workspace_bytes(levels, nlev, C, dtype). */
+size_t dlp_amg_vcycle_workspace_bytes(const dlp_amg_level *levels, int32_t nlev, int32_t C, int dtype);
+int dlp_amg_vcycle(const dlp_amg_level *levels, int32_t nlev, const double *coarse_inv, int32_t nu, double omega,
+                   int32_t coarse_sweeps, int32_t C, int dtype, const void *R, int64_t ldr, void *Y, int64_t ldy,
+                   void *ws, size_t ws_bytes, dlp_stream_t stream);
+
+/* Replaces solvers.pcg with the AMG preconditioner (dynlp/solvers.py:66-97, M = amg.AMG): one CG per
+ * column of (diag - W) Z = rhs from the Z given, with M(R) = dlp_amg_vcycle over `levels` (level 0
+ * is the operator rbeg/rend/col/w of the solve). Per iteration: AP = A P, pAp, alpha, Z += alpha P,
+ * R -= alpha AP, the stop metric (mode bit 0: max_uc |R_uc| / (eps_c diag_u) <= 1; bit 1:
+ * max_c ||R_c|| / rhs_norm[c] <= target_relres), Y = M(R), rz = R.Y, beta, P = Y + beta P; inner
+ * products in fp64 with a fixed reduction order. With use_graph != 0 the iterations run on the device
+ * as one CUDA graph with a conditional WHILE node (cached per problem), stopping at a proposed stop,
+ * the patience rule (no 10% improvement in `patience` iterations), the cap or the cancel word; a
+ * proposed stop is confirmed on the true residual as the reference does (solvers.py:85-89), and a
+ * failed confirmation resumes from the true residual. Y is an n x C scratch like R, P and AP.
+ * eps and rhs_norm are HOST arrays of C doubles. Synchronous: *status_out = 5 converged, 2 stalled,
+ * 3 cap (returns DLP_ERR_CAP), 4 breakdown, 6 cancelled (returns DLP_ERR_CANCELLED).
+ * Workspace: dlp_pcg_amg_workspace_bytes(levels, nlev, C, dtype). */
+size_t dlp_pcg_amg_workspace_bytes(const dlp_amg_level *levels, int32_t nlev, int32_t C, int dtype);
+int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *w, int32_t n, int32_t C,
+                const void *diag, const void *rhs, int64_t ldrhs, void *Z, int64_t ldz, void *R, int64_t ldr, void *P,
+                int64_t ldp, void *AP, int64_t ldap, void *Y, int64_t ldy, int dtype, const double *eps,
+                const double *rhs_norm, double target_relres, int32_t mode, int32_t max_iter, int32_t patience,
+                int32_t use_graph, double avg_deg, const dlp_amg_level *levels, int32_t nlev,
+                const double *coarse_inv, int32_t nu, double omega, int32_t coarse_sweeps, void *ws,
+                size_t ws_bytes, int32_t *iters_out, double *relres_out, int32_t *status_out,
+                dlp_stream_t stream);
+
+
 /* ---- batched independent solves (config: many instances in one launch sequence) -------------
  * No reference counterpart (the reference solves one system at a time). Block PCG with the Jacobi
  * preconditioner over a concatenated block-diagonal CSR (indptr/col/w fp32, N rows, C <= 64

@@ -86,3 +86,61 @@ def test_bf16_sweeps_with_fp64_refinement_reach_1e8(method):
     import scipy.sparse.linalg as sla
     Fd = direct_solve(ssp.diags(S64.diag.cpu().numpy()) - A, S64.rhs.cpu().numpy())
     assert np.abs(F - Fd).max() <= max(st.cert, 1e-6)
+
+
+def _unit_sbm_system(n, seed, dtype="float64"):
+    """An SBM with unit weights: fp32 level weights and their coarse sums are exact, so the
+    device hierarchy equals the oracle's fp64 one entry for entry."""
+    ds = graphs.planted_partition(n, 4, 9.0, 3.0, seed=seed)
+    lab = graphs.label_mask(n, 0.01, seed=seed)
+    return stream.build_system(ds, torch.ones(n, dtype=torch.bool, device="cuda"), lab, dtype=dtype)
+
+
+def test_device_amg_pcg_matches_oracle():
+    """dlp_pcg_amg (the loop on the device) against the oracle's pcg with its AMG (dynlp/solvers.py:66-97
+    with M = amg.AMG) in fp64: the same iteration count and the same iterate."""
+    S = _unit_sbm_system(30_000, 8)
+    M = amg.AMG(S.W, S.s, max_coarse=200)
+    C = S.rhs.shape[1]
+    eps = [1e-7] * C
+    Z = torch.zeros((S.n_u, C), dtype=torch.float64, device="cuda")
+    st = solvers.Stats()
+    solvers.pcg(S, Z, S.rhs, eps, M, 10_000, st)
+    W = S.W.to_scipy().astype(np.float64)
+    Mo = O.AMGOracle(W, S.s.cpu().numpy(), max_coarse=200)
+    assert Mo.sizes == M.sizes
+    Zo, it = O.pcg(W, S.diag.cpu().numpy(), np.zeros((S.n_u, C)), S.rhs.cpu().numpy(), eps, M=Mo)
+    assert st.iters == it, (st.iters, it)
+    np.testing.assert_allclose(Z.cpu().numpy(), Zo, rtol=1e-9, atol=1e-12 * np.abs(Zo).max())
+
+
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+def test_device_amg_pcg_graph_equals_host_loop_and_caps(dt):
+    """The device-side loop (CUDA graph WHILE node) and the host-driven launches give bit-identical
+    iterates; a cap of 3 iterations stops at 3 with DLP_ERR_CAP handled as the reference's cap."""
+    S = _unit_sbm_system(20_000, 9, "float32" if dt == torch.float32 else "float64")
+    M = amg.AMG(S.W, S.s, max_coarse=200)
+    C = S.rhs.shape[1]
+    eps = [1e-5] * C
+    out = []
+    for graph in (True, False):
+        Z = torch.zeros((S.n_u, C), dtype=dt, device="cuda")
+        st = solvers.Stats()
+        solvers.pcg(S, Z, S.rhs, eps, M, 10_000, st, use_graph=graph, target_relres=1e-6)
+        out.append((Z, st.iters, st.relres))
+    assert out[0][1] == out[1][1] and torch.equal(out[0][0], out[1][0])
+    assert out[0][2] <= 1e-6
+    Z = torch.zeros((S.n_u, C), dtype=dt, device="cuda")
+    st = solvers.Stats()
+    solvers.pcg(S, Z, S.rhs, eps, M, 3, st)
+    assert st.iters == 3
+
+
+def test_vcycle_one_call_matches_oracle_cycle():
+    """dlp_amg_vcycle (every level in one library call) against the oracle's V-cycle, fp64."""
+    S = _unit_sbm_system(30_000, 10)
+    M = amg.AMG(S.W, S.s, max_coarse=200)
+    W = S.W.to_scipy().astype(np.float64)
+    Mo = O.AMGOracle(W, S.s.cpu().numpy(), max_coarse=200)
+    R = torch.as_tensor(np.random.RandomState(0).randn(S.n_u, 5)).cuda()
+    np.testing.assert_allclose(M(R).cpu().numpy(), Mo(R.cpu().numpy()), rtol=1e-10, atol=1e-12)
