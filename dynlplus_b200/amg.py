@@ -127,9 +127,12 @@ class AMG:
                 rows = torch.repeat_interleave(torch.arange(n, device=dev), torch.diff(cur.W.indptr.long()))
                 Ad[rows, cur.W.indices.long()] = -cur.W.data.double()
             Ad[torch.arange(n, device=dev), torch.arange(n, device=dev)] += cur.diag
-            # the dense coarse operator is inverted once at setup (fp64 LU); each cycle applies the
-            # inverse with a libdlp kernel
-            self.inv = torch.linalg.inv(Ad).contiguous() if n else Ad
+            # the dense coarse operator is inverted once at setup (Gauss-Jordan in fp64, in place);
+            # each cycle applies the inverse with a libdlp kernel
+            if n:
+                ws = workspace("amg_inverse").get(_lib.lib().dlp_dense_spd_inverse_workspace_bytes(n))
+                _lib.call("dlp_dense_spd_inverse", n, ptr(Ad), ptr(ws), ws.numel(), stream())
+            self.inv = Ad
         self.work_per_apply = sum(2 * nu * L.W.nnz + 2 * L.W.shape[0] for L in self.levels)
         self.work_per_apply += n * n if self.inv is not None else coarse_sweeps * cur.W.nnz
         self.sizes = [L.W.shape[0] for L in self.levels] + [n]
@@ -226,12 +229,20 @@ class AMG:
         return workspace("amg_vcycle").get(_lib.lib().dlp_amg_vcycle_workspace_bytes(arr, nlev, C, code_of(dt)))
 
     def __call__(self, R):
-        """M(R): one V-cycle (dlp_amg_vcycle: every level in one library call); returns a new tensor."""
+        """M(R): one V-cycle (dlp_amg_vcycle: every level in one library call); returns a new tensor.
+        Inputs wider than 64 columns are cycled 64 columns at a time (the columns are independent)."""
         R = R.contiguous()
         n, C = R.shape
         Y = torch.empty_like(R)
         arr, nlev, _ = self.levels_desc(R.dtype)
-        ws = self.vcycle_workspace(C, R.dtype)
-        _lib.call("dlp_amg_vcycle", arr, nlev, ptr(self.inv), self.nu, float(self.omega), self.coarse_sweeps, C,
-                  code(R), ptr(R), ld(R), ptr(Y), ld(Y), ptr(ws), ws.numel(), stream())
+        for c0 in range(0, C, 64):
+            Rc = R[:, c0:c0 + 64] if C > 64 else R
+            Yc = torch.empty_like(Rc.contiguous()) if C > 64 else Y
+            Rc = Rc.contiguous()
+            cw = Rc.shape[1]
+            ws = self.vcycle_workspace(cw, R.dtype)
+            _lib.call("dlp_amg_vcycle", arr, nlev, ptr(self.inv), self.nu, float(self.omega), self.coarse_sweeps, cw,
+                      code(R), ptr(Rc), ld(Rc), ptr(Yc), ld(Yc), ptr(ws), ws.numel(), stream())
+            if C > 64:
+                Y[:, c0:c0 + 64] = Yc
         return Y

@@ -25,16 +25,19 @@ static size_t al256a(size_t x) { return (x + 255) / 256 * 256; }
 // ---- the V-cycle ------------------------------------------------------------------------------
 struct VcPlan {
   // per level: two smoothing buffers, the level residual, and for levels >= 1 the restricted input
-  // and the cycle's output there (ld = C for all of them)
+  // and the cycle's output there; rows padded to 16 bytes (ld) so the level SpMMs gather vectors
   std::vector<char *> A, B, Rr, Rin, Xout;
+  int64_t ld = 0;
   size_t bytes = 0;
 };
 
 static size_t vc_plan(const dlp_amg_level *lv, int nlev, int C, size_t es, char *base, VcPlan *p) {
   size_t off = 0;
+  const int per16 = (int)(16 / es);
+  p->ld = (C + per16 - 1) / per16 * per16;
   auto take = [&](int n) {
     char *q = base ? base + off : nullptr;
-    off += al256a((size_t)(n > 0 ? n : 1) * (size_t)C * es);
+    off += al256a((size_t)(n > 0 ? n : 1) * (size_t)p->ld * es);
     return q;
   };
   p->A.assign(nlev, nullptr);
@@ -65,59 +68,83 @@ struct VcArgs {
   cudaStream_t s;
 };
 
-static int vc_sweep(const VcArgs &a, int l, const void *X, const void *R, int64_t ldr, void *Y) {
+// Y = X + omega * res / diag, res = the level residual RHS - A X (damped Jacobi from the residual).
+template <typename T>
+__global__ void k_jacobi_update(int32_t n, int32_t C, const T *__restrict__ X, int64_t ldx, const T *__restrict__ res,
+                                int64_t ldres, const T *__restrict__ diag, double omega, T *Y, int64_t ldy) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * C) return;
+  const long long u = t / C;
+  const int c = (int)(t - u * C);
+  Y[u * ldy + c] = X[u * ldx + c] + (T)omega * res[u * ldres + c] / diag[u];
+}
+
+// One damped Jacobi sweep on level l, Y = X + omega (R - A X) / diag: the level residual by the
+// row-gather SpMM into the level's residual buffer, then the update (X in the plan's ld, Y in ldy).
+static int vc_sweep(const VcArgs &a, int l, const void *X, const void *R, int64_t ldr, void *Y, int64_t ldy) {
   const dlp_amg_level &L = a.lv[l];
-  return dlp_amg_jacobi_sweep(L.n, a.C, L.indptr, L.col, L.w, X, a.C, R, ldr, L.diag, a.omega, Y, a.C, a.dtype,
-                              (dlp_stream_t)a.s);
+  const int64_t ld = a.plan->ld;
+  char *res = a.plan->Rr[l];
+  DLP_TRY(dlp_spmm(L.indptr, L.indptr + 1, L.col, L.w, DLP_F32, L.n, nullptr, a.C, X, ld, a.dtype, L.diag, -1.0, 1.0,
+                   R, ldr, 1.0, res, ld, a.dtype, 0, 0, L.n > 0 ? (double)L.nnz / L.n : 1.0, (dlp_stream_t)a.s));
+  if (L.n == 0) return DLP_OK;
+  const long long t = (long long)L.n * a.C;
+  if (a.dtype == DLP_F32)
+    k_jacobi_update<float><<<ceil_div_i(t, 256), 256, 0, a.s>>>(L.n, a.C, (const float *)X, ld, (const float *)res, ld,
+                                                                (const float *)L.diag, a.omega, (float *)Y, ldy);
+  else
+    k_jacobi_update<double><<<ceil_div_i(t, 256), 256, 0, a.s>>>(L.n, a.C, (const double *)X, ld, (const double *)res,
+                                                                 ld, (const double *)L.diag, a.omega, (double *)Y,
+                                                                 ldy);
+  return check_launch();
 }
 
 // Y (ld ldy) = the cycle's correction for R (ld ldr) on level l.
 static int vc_cycle(const VcArgs &a, int l, const void *R, int64_t ldr, void *Y, int64_t ldy) {
   const dlp_amg_level &L = a.lv[l];
   const int C = a.C;
+  const int64_t ld = a.plan->ld;
   const dlp_stream_t st = (dlp_stream_t)a.s;
   char *bufA = a.plan->A[l], *bufB = a.plan->B[l];
   if (l == a.nlev - 1) {  // the coarsest level
     if (a.inv) return dlp_dense_apply(L.n, C, a.inv, R, ldr, Y, ldy, a.dtype, st);
     if (a.coarse_sweeps <= 1) return dlp_amg_scale_rows(L.n, C, a.omega, R, ldr, L.diag, Y, ldy, a.dtype, st);
-    DLP_TRY(dlp_amg_scale_rows(L.n, C, a.omega, R, ldr, L.diag, bufA, C, a.dtype, st));
+    DLP_TRY(dlp_amg_scale_rows(L.n, C, a.omega, R, ldr, L.diag, bufA, ld, a.dtype, st));
     char *cur = bufA;
     for (int i = 0; i < a.coarse_sweeps - 1; ++i) {
-      const bool last = i == a.coarse_sweeps - 2;
-      char *tgt = cur == bufA ? bufB : bufA;
-      if (last) {
-        DLP_TRY(dlp_amg_jacobi_sweep(L.n, C, L.indptr, L.col, L.w, cur, C, R, ldr, L.diag, a.omega, Y, ldy, a.dtype,
-                                     st));
+      if (i == a.coarse_sweeps - 2) {
+        DLP_TRY(vc_sweep(a, l, cur, R, ldr, Y, ldy));
       } else {
-        DLP_TRY(vc_sweep(a, l, cur, R, ldr, tgt));
+        char *tgt = cur == bufA ? bufB : bufA;
+        DLP_TRY(vc_sweep(a, l, cur, R, ldr, tgt, ld));
         cur = tgt;
       }
     }
     return DLP_OK;
   }
   // pre-smoothing: X = omega R / diag, then nu - 1 sweeps
-  DLP_TRY(dlp_amg_scale_rows(L.n, C, a.omega, R, ldr, L.diag, bufA, C, a.dtype, st));
+  DLP_TRY(dlp_amg_scale_rows(L.n, C, a.omega, R, ldr, L.diag, bufA, ld, a.dtype, st));
   char *cur = bufA;
   for (int i = 0; i < a.nu - 1; ++i) {
     char *tgt = cur == bufA ? bufB : bufA;
-    DLP_TRY(vc_sweep(a, l, cur, R, ldr, tgt));
+    DLP_TRY(vc_sweep(a, l, cur, R, ldr, tgt, ld));
     cur = tgt;
   }
   // restriction of R - A X: Rr = R - diag X + W X
   char *Rr = a.plan->Rr[l];
-  DLP_TRY(dlp_spmm(L.indptr, L.indptr + 1, L.col, L.w, DLP_F32, L.n, nullptr, C, cur, C, a.dtype, L.diag, -1.0, 1.0,
-                   R, ldr, 1.0, Rr, C, a.dtype, 0, 0, L.n > 0 ? (double)L.nnz / L.n : 1.0, st));
+  DLP_TRY(dlp_spmm(L.indptr, L.indptr + 1, L.col, L.w, DLP_F32, L.n, nullptr, C, cur, ld, a.dtype, L.diag, -1.0, 1.0,
+                   R, ldr, 1.0, Rr, ld, a.dtype, 0, 0, L.n > 0 ? (double)L.nnz / L.n : 1.0, st));
   const dlp_amg_level &N = a.lv[l + 1];
-  DLP_TRY(dlp_amg_restrict(N.n, C, L.off, L.members, Rr, C, a.plan->Rin[l + 1], C, a.dtype, st));
-  DLP_TRY(vc_cycle(a, l + 1, a.plan->Rin[l + 1], C, a.plan->Xout[l + 1], C));
-  DLP_TRY(dlp_amg_prolong_add(L.n, C, L.agg, a.plan->Xout[l + 1], C, cur, C, a.dtype, st));
+  DLP_TRY(dlp_amg_restrict(N.n, C, L.off, L.members, Rr, ld, a.plan->Rin[l + 1], ld, a.dtype, st));
+  DLP_TRY(vc_cycle(a, l + 1, a.plan->Rin[l + 1], ld, a.plan->Xout[l + 1], ld));
+  DLP_TRY(dlp_amg_prolong_add(L.n, C, L.agg, a.plan->Xout[l + 1], ld, cur, ld, a.dtype, st));
   // post-smoothing: nu sweeps, the last one into Y
   for (int i = 0; i < a.nu; ++i) {
     if (i == a.nu - 1) {
-      DLP_TRY(dlp_amg_jacobi_sweep(L.n, C, L.indptr, L.col, L.w, cur, C, R, ldr, L.diag, a.omega, Y, ldy, a.dtype, st));
+      DLP_TRY(vc_sweep(a, l, cur, R, ldr, Y, ldy));
     } else {
       char *tgt = cur == bufA ? bufB : bufA;
-      DLP_TRY(vc_sweep(a, l, cur, R, ldr, tgt));
+      DLP_TRY(vc_sweep(a, l, cur, R, ldr, tgt, ld));
       cur = tgt;
     }
   }
@@ -619,6 +646,59 @@ int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, co
   if (cur.done == 3) return DLP_ERR_CAP;
   if (cur.done == 6) return DLP_ERR_CANCELLED;
   return DLP_OK;
+}
+
+}  // extern "C"
+
+// ---- the coarse operator's inverse (setup) ---------------------------------------------------------
+// Gauss-Jordan elimination in place on a symmetric positive definite matrix (no pivoting needed):
+// for each pivot k, the scaled pivot row and the pivot column are saved first (k_gj_save), then
+// every element takes its update from the saved vectors (k_gj_update), so no thread reads what
+// another thread of the same launch writes. After the last pivot A holds its inverse.
+namespace dlp {
+
+__global__ void k_gj_save(int32_t n, int32_t k, const double *__restrict__ A, double *fcol, double *rowk) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double piv = A[(long long)k * n + k];
+  fcol[t] = A[t * n + k];
+  rowk[t] = (t == k ? 1.0 : A[(long long)k * n + t]) / piv;
+}
+
+__global__ void k_gj_update(int32_t n, int32_t k, double *A, const double *__restrict__ fcol,
+                            const double *__restrict__ rowk) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const long long i = t / n;
+  const int j = (int)(t - i * n);
+  if (i == k) {
+    A[t] = rowk[j];
+  } else {
+    const double a = j == k ? 0.0 : A[t];
+    A[t] = a - fcol[i] * rowk[j];
+  }
+}
+
+}  // namespace dlp
+
+extern "C" {
+
+size_t dlp_dense_spd_inverse_workspace_bytes(int32_t n) { return 2 * al256a(sizeof(double) * (size_t)(n > 0 ? n : 1)); }
+
+int dlp_dense_spd_inverse(int32_t n, double *A, void *ws, size_t ws_bytes, dlp_stream_t stream) {
+  if (n < 0 || (n > 0 && !A)) return DLP_ERR_INVALID;
+  if (n > 46340) return DLP_ERR_INVALID;  // n * n elements index an int64 but the grid is int
+  if (!ws || ws_bytes < dlp_dense_spd_inverse_workspace_bytes(n)) return DLP_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  double *fcol = (double *)ws;
+  double *rowk = (double *)((char *)ws + al256a(sizeof(double) * (size_t)(n > 0 ? n : 1)));
+  const int g1 = ceil_div_i(n, 256);
+  const int g2 = ceil_div_i((long long)n * n, 256);
+  for (int k = 0; k < n; ++k) {
+    k_gj_save<<<g1, 256, 0, s>>>(n, k, A, fcol, rowk);
+    k_gj_update<<<g2, 256, 0, s>>>(n, k, A, fcol, rowk);
+  }
+  return check_launch(2 * n);
 }
 
 }  // extern "C"

@@ -506,6 +506,14 @@ int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, co
                 dlp_stream_t stream);
 
 
+/* The inverse of a dense symmetric positive definite fp64 matrix A (n x n, row-major), in place:
+ * Gauss-Jordan elimination without pivoting, two launches per pivot (the coarsest AMG level's solve,
+ * dynlp/amg.py:105-108 inverts it with the library's LU). Asynchronous.
+ * Workspace: dlp_dense_spd_inverse_workspace_bytes(n). */
+size_t dlp_dense_spd_inverse_workspace_bytes(int32_t n);
+int dlp_dense_spd_inverse(int32_t n, double *A, void *ws, size_t ws_bytes, dlp_stream_t stream);
+
+
 /* ---- batched independent solves (config: many instances in one launch sequence) -------------
  * No reference counterpart (the reference solves one system at a time). Block PCG with the Jacobi
  * preconditioner over a concatenated block-diagonal CSR (indptr/col/w fp32, N rows, C <= 64
