@@ -79,6 +79,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_amg_coarse_keys": ("ippppippp", ct.c_int),
     "dlp_amg_coarse_reduce_workspace_bytes": ("qi", ct.c_size_t),
     "dlp_amg_coarse_reduce": ("qppipppppppppzp", ct.c_int),
+    "dlp_sort_pairs_workspace_bytes": ("q", ct.c_size_t),
+    "dlp_sort_pairs": ("qqpppppzp", ct.c_int),
     "dlp_amg_restrict": ("iipppqpqip", ct.c_int),
     "dlp_amg_prolong_add": ("iippqpqip", ct.c_int),
     "dlp_amg_scale_rows": ("iidpqppqip", ct.c_int),

@@ -64,8 +64,8 @@ def members(agg, nc):
 def coarsen(W: CSR, s, agg, nc, off=None, mem=None):
     """(W_c, s_c) of the aggregation (dynlp/amg.py:67-74): sorted CSR rows, fp64 sums in the fine
     CSR order. Every fine entry gets the key (aggregate of its row, aggregate of its column); a
-    stable sort by key brings each coarse entry's contributions together in their original order
-    and one kernel sums the runs (the reference's coalesce)."""
+    stable radix sort by key (dlp_sort_pairs) brings each coarse entry's contributions together in
+    their original order and one kernel sums the runs (the reference's coalesce)."""
     dev = W.indices.device
     n, m = W.shape[0], int(W.indices.numel())
     if s is not None and off is None:
@@ -74,8 +74,13 @@ def coarsen(W: CSR, s, agg, nc, off=None, mem=None):
     val = torch.empty(max(m, 1), dtype=torch.float64, device=dev)
     _lib.call("dlp_amg_coarse_keys", n, ptr(W.indptr), ptr(W.indices), ptr(W.data.float().contiguous()),
               ptr(agg.to(torch.int32).contiguous()), nc, ptr(key), ptr(val), stream())
-    key, order = torch.sort(key[:m], stable=True)
-    val = val[:m][order]
+    key, val = key[:m], val[:m]
+    if m > 1:  # stable radix sort by coarse entry; the "no entry" marker sorts last
+        kt = torch.empty_like(key)
+        vt = torch.empty_like(val)
+        ws = workspace("amg_sort").get(_lib.lib().dlp_sort_pairs_workspace_bytes(m))
+        _lib.call("dlp_sort_pairs", m, nc * nc, ptr(key), ptr(val), ptr(kt), ptr(vt), ptr(ws), ws.numel(), stream())
+        del kt, vt
     indptr_c = torch.empty(nc + 1, dtype=torch.int32, device=dev)
     col_c = torch.empty(max(m, 1), dtype=torch.int32, device=dev)
     w_c = torch.empty(max(m, 1), dtype=torch.float32, device=dev)

@@ -1,4 +1,5 @@
 // Ordered stream compaction (numpy.flatnonzero semantics) and deterministic column reductions.
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -167,6 +168,82 @@ int exclusive_scan_i32(const int32_t *in, int32_t n, int32_t *out, void *ws, siz
   k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile, nt, nullptr);
   k_tile_scan_i32<<<nt, kScanThreads, 0, s>>>(in, n, tile, out);
   return check_launch(3);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Stable LSD radix sort of (int64 key, fp64 value) pairs, 8 bits per pass (the AMG coarsening's
+// sort by coarse entry). Keys above max_key order as max_key (the "no entry" marker sorts last).
+// Per pass: tile histograms stored digit-major, one exclusive scan of them (each (digit, tile) gets
+// its first output slot), then a stable scatter: a tile is taken in chunks of 256 elements in input
+// order; inside a chunk equal digits are ranked by __match_any_sync per warp and per-warp counts in
+// shared memory, and a running count per digit carries over to the next chunk.
+// ------------------------------------------------------------------------------------------------
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kScanThreads * kRsItems;
+
+__device__ __forceinline__ int rs_digit(long long k, long long maxk, int shift) {
+  k = k > maxk ? maxk : k;
+  return (int)((k >> shift) & 255);
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_rs_hist(long long m, const long long *__restrict__ keys,
+                                                          long long maxk, int shift, int32_t *hist, int ntiles) {
+  __shared__ int32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * kRsTile;
+#pragma unroll
+  for (int i = 0; i < kRsItems; ++i) {
+    const long long e = base + (long long)i * kScanThreads + threadIdx.x;
+    if (e < m) atomicAdd(&h[rs_digit(keys[e], maxk, shift)], 1);
+  }
+  __syncthreads();
+  hist[(long long)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_rs_scatter(long long m, const long long *__restrict__ keys, const double *__restrict__ vals, long long maxk,
+                 int shift, const int32_t *__restrict__ offs, int ntiles, long long *keys_out, double *vals_out) {
+  __shared__ int32_t s_base[256];
+  __shared__ int32_t s_cnt[kScanThreads / 32][256];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  s_base[tid] = offs[(long long)tid * ntiles + blockIdx.x];
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) s_cnt[w][tid] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * kRsTile;
+  for (int i = 0; i < kRsItems; ++i) {
+    const long long e = base + (long long)i * kScanThreads + tid;
+    const bool valid = e < m;
+    long long k = 0;
+    double v = 0.0;
+    int d = 256;  // no digit: past the end
+    if (valid) {
+      k = keys[e];
+      v = vals[e];
+      d = rs_digit(k, maxk, shift);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const int wrank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && wrank == 0) s_cnt[wid][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      int pre = 0;
+      for (int w = 0; w < wid; ++w) pre += s_cnt[w][d];
+      const int dest = s_base[d] + pre + wrank;
+      keys_out[dest] = k;
+      vals_out[dest] = v;
+    }
+    __syncthreads();
+    int tot = 0;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+      tot += s_cnt[w][tid];
+      s_cnt[w][tid] = 0;
+    }
+    s_base[tid] += tot;
+    __syncthreads();
+  }
 }
 
 size_t compact_ws_bytes(int32_t n) { return ((size_t)n_tiles(n) * sizeof(int32_t) + 255) / 256 * 256 + 256; }
@@ -361,6 +438,51 @@ int dlp_colreduce(int kind, int32_t n, int32_t C, const void *X, int64_t ldx, co
   }
   k_colreduce_final<<<(C + 7) / 8, 256, 0, s>>>(kind, C, nb, partial, out);
   return check_launch(nb > 0 ? 2 : 1);
+}
+
+
+size_t dlp_sort_pairs_workspace_bytes(int64_t m) {
+  const long long nt = (m + kRsTile - 1) / kRsTile;
+  const long long h = 256 * (nt > 0 ? nt : 1);
+  return (((size_t)h * 4 + 255) / 256 * 256) + (((size_t)(h + 1) * 4 + 255) / 256 * 256) +
+         compact_ws_bytes((int32_t)std::min<long long>(h, INT32_MAX - 1));
+}
+
+int dlp_sort_pairs(int64_t m, int64_t max_key, int64_t *keys, double *vals, int64_t *keys_tmp, double *vals_tmp,
+                   void *ws, size_t ws_bytes, dlp_stream_t stream) {
+  if (m < 0 || max_key < 0 || (m > 0 && (!keys || !vals || !keys_tmp || !vals_tmp))) return DLP_ERR_INVALID;
+  if (m >= ((long long)INT32_MAX / 2)) return DLP_ERR_INVALID;
+  if (!ws || ws_bytes < dlp_sort_pairs_workspace_bytes(m)) return DLP_ERR_WORKSPACE;
+  if (m <= 1) return DLP_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ntiles = (int)((m + kRsTile - 1) / kRsTile);
+  const long long h = 256LL * ntiles;
+  char *p = (char *)ws;
+  int32_t *hist = (int32_t *)p;
+  p += ((size_t)h * 4 + 255) / 256 * 256;
+  int32_t *offs = (int32_t *)p;
+  p += ((size_t)(h + 1) * 4 + 255) / 256 * 256;
+  const size_t scan_bytes = ws_bytes - (size_t)(p - (char *)ws);
+  int bits = 0;
+  for (unsigned long long x = (unsigned long long)max_key; x; x >>= 1) ++bits;
+  const int passes = bits > 0 ? (bits + 7) / 8 : 1;
+  long long *kin = (long long *)keys, *kout = (long long *)keys_tmp;
+  double *vin = vals, *vout = vals_tmp;
+  int launches = 0;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int shift = 8 * pass;
+    k_rs_hist<<<ntiles, kScanThreads, 0, s>>>(m, kin, max_key, shift, hist, ntiles);
+    DLP_TRY(exclusive_scan_i32(hist, (int32_t)h, offs, p, scan_bytes, s));
+    k_rs_scatter<<<ntiles, kScanThreads, 0, s>>>(m, kin, vin, max_key, shift, offs, ntiles, kout, vout);
+    launches += 2;
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  if (kin != (long long *)keys) {  // an odd number of passes: the result is in the spare arrays
+    DLP_CUDA(cudaMemcpyAsync(keys, kin, sizeof(long long) * (size_t)m, cudaMemcpyDeviceToDevice, s));
+    DLP_CUDA(cudaMemcpyAsync(vals, vin, sizeof(double) * (size_t)m, cudaMemcpyDeviceToDevice, s));
+  }
+  return check_launch(launches);
 }
 
 }  // extern "C"

@@ -440,6 +440,15 @@ int dlp_amg_coarse_reduce(int64_t m, const int64_t *key, const double *val, int3
                           int32_t *col_c, float *w_c, int32_t *nnz_c, void *ws, size_t ws_bytes,
                           dlp_stream_t stream);
 
+/* Stable ascending sort of m (key, value) pairs in place, keys above max_key ordered as max_key (the
+ * coarsening's "no entry" marker, INT64_MAX, sorts last): LSD radix, 8 bits per pass over the bits
+ * of max_key. keys_tmp / vals_tmp: m spare entries each. m < 2^30. (The sort of the reference's
+ * coalesce, dynlp/graphs.py:36-44 as used by dynlp/amg.py:67-74.)
+ * Workspace: dlp_sort_pairs_workspace_bytes(m). */
+size_t dlp_sort_pairs_workspace_bytes(int64_t m);
+int dlp_sort_pairs(int64_t m, int64_t max_key, int64_t *keys, double *vals, int64_t *keys_tmp, double *vals_tmp,
+                   void *ws, size_t ws_bytes, dlp_stream_t stream);
+
 /* V-cycle pieces (amg.py:28-31 Level.apply, :114-131 _smooth / _cycle):
  * restrict Rc[a,:] = sum over members of R (ordered); prolong X[u,:] += Xc[agg[u],:];
  * scale_rows X = omega R / diag; jacobi_sweep Y = X + omega ((RHS + W X) / diag - X);

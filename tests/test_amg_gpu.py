@@ -163,3 +163,23 @@ def test_dense_spd_inverse_matches_numpy(n):
     _lib.call("dlp_dense_spd_inverse", n, ptr(At), ptr(ws), ws.numel(), stream())
     want = np.linalg.inv(A)
     np.testing.assert_allclose(At.cpu().numpy(), want, rtol=0, atol=1e-10 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("m,nc", [(1, 3), (2047, 40), (300_001, 1000), (2_000_003, 250_000)])
+def test_radix_sort_of_pairs_is_stable(m, nc):
+    """dlp_sort_pairs against torch's stable sort: equal keys keep their order (the values are the
+    positions), and the no-entry marker (INT64_MAX) sorts last."""
+    from dynlplus_b200 import _lib
+    from dynlplus_b200.backend import ptr, stream, workspace
+    g = torch.Generator(device="cuda").manual_seed(m)
+    key = torch.randint(0, nc * nc, (m,), generator=g, device="cuda", dtype=torch.int64)
+    key = key // 7  # many equal keys
+    key[torch.rand(m, generator=g, device="cuda") < 0.2] = 2**63 - 1
+    val = torch.arange(m, dtype=torch.float64, device="cuda")
+    want_k, order = torch.sort(key, stable=True)
+    k2, v2 = key.clone(), val.clone()
+    ws = workspace("sort_test").get(_lib.lib().dlp_sort_pairs_workspace_bytes(m))
+    _lib.call("dlp_sort_pairs", m, nc * nc, ptr(k2), ptr(v2), ptr(torch.empty_like(k2)), ptr(torch.empty_like(v2)),
+              ptr(ws), ws.numel(), stream())
+    assert torch.equal(k2, want_k)
+    assert torch.equal(v2, val[order])
