@@ -569,24 +569,47 @@ def wl_static(a):
 
 def wl_amg(a):
     """Config 3: SBM n=1,000,000, 16 blocks, degree 24 in + 8 cross, lognormal(0, 0.5) weights,
-    1% labelled, k=16: AMG-preconditioned PCG (fp32 sweeps) with fp64 refinement to rel-res 1e-8."""
+    1% labelled, k=16: AMG-preconditioned block PCG with BF16 SpMM (bf16 weights and scores, fp32
+    accumulation) and fp64 residual refinement to rel-res 1e-8, the loop on the device. Beside it,
+    on the same system: fp32 sweeps with AMG and with the Jacobi preconditioner, each with its error
+    against an fp64 solve (fp64 Jacobi-PCG to rel-res 1e-12), the hierarchy and one V-cycle's time."""
     import torch
+    from dynlplus_b200 import amg as amg_mod
     from dynlplus_b200 import graphs, solvers, stream
     ds = graphs.planted_partition(1_000_000, 16, 24.0, 8.0, weights="lognormal", seed=3)
     lab = graphs.label_mask(1_000_000, 0.01, seed=3)
     S = stream.build_system(ds, torch.ones(ds.n, dtype=torch.bool, device="cuda"), lab, dtype="float32")
-    times, rels, iters, setups = [], [], [], []
-    for rep in range(a.warmup + a.steps):
-        solver = solvers.DynLPPlus(ds.n, 16, "float32", method="amg", tol=1e-3, target_relres=1e-8)
-        t, st = _events(lambda: solver.solve(S))
-        if rep >= a.warmup:
-            times.append(t)
-            rels.append(st.relres)
-            iters.append(st.iters)
-            setups.append(st.setup_ms)
-    _line(a, "AMG-PCG solve time to rel-res 1e-8 (fp32 sweeps, fp64 refinement)", float(np.mean(times)), "ms",
-          float(np.mean(times)), {"workload": "sbm-n1000000-b16-d24+8-lognormal-lab0.01-k16"}, hib=False,
-          relres_max=float(max(rels)), pcg_iters=float(np.mean(iters)), amg_setup_ms=float(np.mean(setups)))
+    S64 = S.astype(torch.float64)
+    C = S.rhs.shape[1]
+    Fs = torch.zeros((S.n_u, C), dtype=torch.float64, device="cuda")
+    solvers.pcg(S64, Fs, S64.rhs.contiguous(), None, solvers.jacobi_M(S64), 100_000, solvers.Stats(),
+                target_relres=1e-12)
+    scale = float(Fs.abs().max())
+
+    def run(method, lowp):
+        times, st, solver = [], None, None
+        for rep in range(a.warmup + a.steps):
+            solver = solvers.DynLPPlus(ds.n, 16, "float32", method=method, tol=1e-3, target_relres=1e-8, lowp=lowp)
+            t, st = _events(lambda: solver.solve(S))
+            if rep >= a.warmup:
+                times.append(t)
+        err = float((solver.scores(S).double() - Fs).abs().max()) / scale
+        return {"ms": float(np.mean(times)), "pcg_iters": st.iters, "relres": st.relres, "err_vs_fp64": err,
+                "setup_ms": st.setup_ms}
+
+    res = {"amg_bf16": run("amg", True), "amg_fp32": run("amg", False), "jacobi_fp32": run("pcg", False)}
+    M = amg_mod.AMG(S.W, S.s)
+    R = torch.randn((S.n_u, C + 1), dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        M(R)
+    t_cycle, _ = _events(lambda: [M(R) for _ in range(10)])
+    head = res["amg_bf16"]
+    _line(a, "AMG-PCG solve time to rel-res 1e-8 (BF16 SpMM, fp32 accumulation, fp64 refinement)", head["ms"], "ms",
+          head["ms"], {"workload": "sbm-n1000000-b16-d24+8-lognormal-lab0.01-k16"}, hib=False,
+          relres_max=head["relres"], err_vs_fp64=head["err_vs_fp64"], pcg_iters=head["pcg_iters"],
+          amg_setup_ms=head["setup_ms"], variants=res, amg_levels=M.sizes, vcycle_ms=t_cycle / 10,
+          precision="bf16 SpMM (weights and gathered scores) with fp32 accumulation in the CG, fp32 V-cycle, "
+                    "fp64 refinement; error relative to the largest fp64 score")
 
 
 def wl_batched(a):

@@ -89,7 +89,7 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_amg_vcycle_workspace_bytes": ("piii", ct.c_size_t),
     "dlp_amg_vcycle": ("pipidiiipqpqpzp", ct.c_int),
     "dlp_pcg_amg_workspace_bytes": ("piii", ct.c_size_t),
-    "dlp_pcg_amg": ("ppppiippqpqpqpqpqpqippdiiiidpipidipzpppp", ct.c_int),
+    "dlp_pcg_amg": ("ppppiippqpqpqpqpqpqippdiiiidpipidipzppppppq", ct.c_int),
     "dlp_dense_spd_inverse_workspace_bytes": ("i", ct.c_size_t),
     "dlp_dense_spd_inverse": ("ippzp", ct.c_int),
     "dlp_pcg_batched_workspace_bytes": ("iii", ct.c_size_t),

@@ -249,7 +249,8 @@ __global__ void __launch_bounds__(kGThreads)
 // loop that proposed it keeps P for a resume after a failed confirmation).
 template <typename T>
 __global__ void __launch_bounds__(kGThreads)
-    k_gpcg_dir(int init, int32_t n, int32_t C, T *P, int64_t ldp, const T *__restrict__ Y, int64_t ldy, GBufs B) {
+    k_gpcg_dir(int init, int32_t n, int32_t C, T *P, int64_t ldp, const T *__restrict__ Y, int64_t ldy, GBufs B,
+               bf16 *P_lo, int64_t ld_lo) {
   if (!init && B.ctl->done != 0) return;
   const GIdx g = g_index(C);
   if (!g.on) return;
@@ -267,7 +268,11 @@ __global__ void __launch_bounds__(kGThreads)
 #pragma unroll
     for (int u = 0; u < kGUnroll; ++u) {
       const long long rr = r + u * g.RS;
-      if (rr < n) P[rr * ldp + c] = yv[u] + be * pv[u];
+      if (rr < n) {
+        const T pn = yv[u] + be * pv[u];
+        P[rr * ldp + c] = pn;
+        if (P_lo) P_lo[rr * ld_lo + c] = cvt<bf16>(pn);  // the mirror the bf16 apply gathers
+      }
     }
   }
 }
@@ -334,6 +339,9 @@ struct GProblem {
   int dtype;
   double avg_deg;
   VcArgs vc;
+  const void *w_lo;  // bf16 weights and the bf16 mirror of P for the apply (NULL: full precision)
+  void *P_lo;
+  int64_t ld_lo;
 };
 
 static int g_grid(int32_t n, int32_t C) {
@@ -368,7 +376,8 @@ static int g_precond(const GProblem &q, const GBufs &B, cudaStream_t s) {
 
 template <typename T>
 static int g_dir(int init, const GProblem &q, const GBufs &B, cudaStream_t s) {
-  k_gpcg_dir<T><<<g_grid(q.n, q.C), kGThreads, 0, s>>>(init, q.n, q.C, (T *)q.P, q.ldp, (const T *)q.Y, q.ldy, B);
+  k_gpcg_dir<T><<<g_grid(q.n, q.C), kGThreads, 0, s>>>(init, q.n, q.C, (T *)q.P, q.ldp, (const T *)q.Y, q.ldy, B,
+                                                       (bf16 *)q.P_lo, q.ld_lo);
   return check_launch();
 }
 
@@ -385,8 +394,13 @@ static int g_decide(int phase, const GProblem &q, const GBufs &B, cudaStream_t s
 template <typename T>
 static int g_iteration(const GProblem &q, const GBufs &B, cudaStream_t s) {
   const dlp_stream_t st = (dlp_stream_t)s;
-  DLP_TRY(dlp_spmm(q.rbeg, q.rend, q.col, q.w, DLP_F32, q.n, nullptr, q.C, q.P, q.ldp, q.dtype, q.diag, 1.0, -1.0,
-                   nullptr, q.C, 0.0, q.AP, q.ldap, q.dtype, 0, 0, q.avg_deg, st));
+  if (q.w_lo) {  // bf16 weights and gathered rows, fp32 accumulation; the own-row term from fp32 P
+    DLP_TRY(dlp_spmm_lowp(q.rbeg, q.rend, q.col, q.w_lo, q.n, q.C, q.P_lo, q.ld_lo, q.P, q.ldp, q.diag, 1.0, -1.0,
+                          q.AP, q.ldap, 0, q.avg_deg, st));
+  } else {
+    DLP_TRY(dlp_spmm(q.rbeg, q.rend, q.col, q.w, DLP_F32, q.n, nullptr, q.C, q.P, q.ldp, q.dtype, q.diag, 1.0, -1.0,
+                     nullptr, q.C, 0.0, q.AP, q.ldap, q.dtype, 0, 0, q.avg_deg, st));
+  }
   DLP_TRY(dlp_colreduce(1, q.n, q.C, q.P, q.ldp, q.AP, q.ldap, nullptr, q.dtype, nullptr, B.pAp, B.red_ws,
                         B.red_bytes, st));
   k_gpcg_step<T><<<g_grid(q.n, q.C), kGThreads, 0, s>>>(q.n, q.C, (T *)q.Z, q.ldz, (T *)q.R, q.ldr, (const T *)q.P,
@@ -427,7 +441,8 @@ static int g_key(const GProblem &q, const GBufs &B, GKey *key) {
                               (uintptr_t)q.ldz, (uintptr_t)q.R, (uintptr_t)q.ldr, (uintptr_t)q.P, (uintptr_t)q.ldp,
                               (uintptr_t)q.AP, (uintptr_t)q.ldap, (uintptr_t)q.Y, (uintptr_t)q.ldy,
                               (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)B.cancel, (uintptr_t)q.vc.inv,
-                              (uintptr_t)q.vc.nu, (uintptr_t)q.vc.coarse_sweeps, (uintptr_t)q.vc.nlev};
+                              (uintptr_t)q.vc.nu, (uintptr_t)q.vc.coarse_sweeps, (uintptr_t)q.vc.nlev,
+                              (uintptr_t)q.w_lo, (uintptr_t)q.P_lo, (uintptr_t)q.ld_lo};
   uint64_t om;
   std::memcpy(&om, &q.vc.omega, sizeof(om));
   v.push_back((uintptr_t)om);
@@ -552,8 +567,9 @@ int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, co
                 int32_t use_graph, double avg_deg, const dlp_amg_level *levels, int32_t nlev,
                 const double *coarse_inv, int32_t nu, double omega, int32_t coarse_sweeps, void *ws,
                 size_t ws_bytes, int32_t *iters_out, double *relres_out, int32_t *status_out,
-                dlp_stream_t stream) {
+                dlp_stream_t stream, const void *w_lo, void *P_lo, int64_t ld_lo) {
   DLP_TRY(vc_check(levels, nlev, C, dtype));
+  if ((w_lo || P_lo) && (!w_lo || !P_lo || ld_lo < C || dtype != DLP_F32)) return DLP_ERR_INVALID;
   if (n < 0 || levels[0].n != n || nu < 1) return DLP_ERR_INVALID;
   if (ldz < C || ldr < C || ldp < C || ldap < C || ldy < C || ldrhs < C) return DLP_ERR_INVALID;
   if ((mode & 3) == 0 || mode > 3 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
@@ -583,7 +599,7 @@ int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, co
   vc_plan(levels, nlev, C, dtype == DLP_F64 ? 8 : 4, B.vc, &plan);
   GProblem q{rbeg, rend, col, w, n, C, diag, rhs, ldrhs, Z, R, P, AP, Y, ldz, ldr, ldp, ldap, ldy, dtype,
              avg_deg > 0 ? avg_deg : 1.0,
-             VcArgs{levels, nlev, coarse_inv, nu, coarse_sweeps, C, dtype, omega, &plan, s}};
+             VcArgs{levels, nlev, coarse_inv, nu, coarse_sweeps, C, dtype, omega, &plan, s}, w_lo, P_lo, ld_lo};
   GCtl h{};
   h.patience = patience > 0 ? patience : 400;
   h.max_iter = max_iter;

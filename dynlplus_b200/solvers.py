@@ -181,9 +181,9 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
         if zero_start:
             Z.zero_()  # these loops start from the Z they are given
         from .amg import AMG
-        if isinstance(M, AMG) and not lowp:
+        if isinstance(M, AMG) and (not lowp or Z.dtype == torch.float32):
             return _pcg_amg(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm,
-                            check_every, use_graph)
+                            check_every, use_graph, lowp)
         return _pcg_generic(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, lowp)
     n, C = Z.shape
     if n == 0:
@@ -240,7 +240,8 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
     return Z
 
 
-def _pcg_amg(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, check_every, use_graph):
+def _pcg_amg(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres, rhs_norm, check_every, use_graph,
+             lowp=False):
     """PCG with the AMG V-cycle as preconditioner, its loop on the device (dlp_pcg_amg): the
     reference's pcg (dynlp/solvers.py:66-97) with M = amg.AMG, one host read per device-side loop
     and per confirmation of a proposed stop."""
@@ -266,13 +267,18 @@ def _pcg_amg(sys, Z, rhs, eps, M, max_iter, st, work_M, patience, target_relres,
         if rhs_norm is None:
             rhs_norm = col_norms(rhs).cpu().tolist()
         rn = (ct.c_double * C)(*[float(x) for x in rhs_norm])
+    w_lo = P_lo = None
+    if lowp:  # bf16 weights and a bf16 mirror of P in the apply (fp32 accumulation)
+        w_lo = bf16_weights(W)
+        P_lo = _scratch("amg_Plo", n, C, torch.bfloat16, dev, padded=True)
     it, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_int32(0)
     _lib.call("dlp_pcg_amg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(w32), n, C, ptr(diag), ptr(rhs), ld(rhs),
               ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), ptr(Y), ld(Y), code(Z), eps_h, rn,
               float(target_relres or 0.0), mode, int(max_iter), int(patience),
               int(bool(GRAPHS if use_graph is None else use_graph)), W.nnz / max(n, 1), arr, nlev, ptr(M.inv),
               int(M.nu), float(M.omega), int(M.coarse_sweeps), ptr(ws), ws.numel(), ct.byref(it), ct.byref(rel),
-              ct.byref(status), stream(), allow=(_lib.DLP_ERR_CAP,))
+              ct.byref(status), stream(), ptr(w_lo), ptr(P_lo), ld(P_lo) if P_lo is not None else 0,
+              allow=(_lib.DLP_ERR_CAP,))
     st.iters += it.value
     st.edges += (it.value + 2) * W.nnz + work_M * it.value
     st.relres = rel.value

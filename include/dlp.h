@@ -503,6 +503,8 @@ int dlp_amg_vcycle(const dlp_amg_level *levels, int32_t nlev, const double *coar
  * failed confirmation resumes from the true residual. Y is an n x C scratch like R, P and AP.
  * eps and rhs_norm are HOST arrays of C doubles. Synchronous: *status_out = 5 converged, 2 stalled,
  * 3 cap (returns DLP_ERR_CAP), 4 breakdown, 6 cancelled (returns DLP_ERR_CANCELLED).
+ * Mixed precision (fp32 only), as in dlp_pcg: with w_lo (bf16 copy of w) and P_lo (bf16 n x C, ld_lo)
+ * the apply gathers the bf16 mirror of P that the direction update keeps (fp32 accumulation).
  * Workspace: dlp_pcg_amg_workspace_bytes(levels, nlev, C, dtype). */
 size_t dlp_pcg_amg_workspace_bytes(const dlp_amg_level *levels, int32_t nlev, int32_t C, int dtype);
 int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const float *w, int32_t n, int32_t C,
@@ -512,7 +514,7 @@ int dlp_pcg_amg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, co
                 int32_t use_graph, double avg_deg, const dlp_amg_level *levels, int32_t nlev,
                 const double *coarse_inv, int32_t nu, double omega, int32_t coarse_sweeps, void *ws,
                 size_t ws_bytes, int32_t *iters_out, double *relres_out, int32_t *status_out,
-                dlp_stream_t stream);
+                dlp_stream_t stream, const void *w_lo, void *P_lo, int64_t ld_lo);
 
 
 /* The inverse of a dense symmetric positive definite fp64 matrix A (n x n, row-major), in place:
