@@ -105,7 +105,7 @@ class BatchedSystems:
         return arg
 
     def solve(self, target_relres=1e-6, eps=None, max_iter=100_000, patience=400, check_every=8, use_graph=True,
-              group=None, Z0=None):
+              group=None, Z0=None, inst_targets=None):
         """Solve every instance; returns (Z (N x Ch), iters, status, relres) with per-instance arrays."""
         B, Ch, N, dev, dt = len(self.systems), self.Ch, self.N, self.dev, self.dtype
         Z = padded_empty(N, Ch, dt, dev)
@@ -123,7 +123,11 @@ class BatchedSystems:
                                                                                         device=dev)
         if Ch > self.C:
             rn[:, self.C:] *= 1e3
-        rn = torch.where(rn > 0, rn, torch.ones_like(rn)).contiguous()
+        rn = torch.where(rn > 0, rn, torch.ones_like(rn))
+        if inst_targets is not None:  # instance i stops at ||R_c|| <= inst_targets[i] ||rhs_c||
+            t = torch.as_tensor(np.asarray(inst_targets, dtype=np.float64) / target_relres, device=dev)
+            rn = rn * t[:, None]
+        rn = rn.contiguous()
         mode = 2
         epsd = torch.full((B, Ch), 1e300, dtype=torch.float64, device=dev)
         if eps is not None:
@@ -163,4 +167,60 @@ def solve_many(systems, target_relres=1e-6, dtype=torch.float64, tile_rows=1024,
             out[j] = F
         for k, j in enumerate(idx):
             info[j] = (int(it[k]), int(stt[k]), float(rel[k]))
+    return out, info
+
+
+def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6):
+    """solve_many in mixed precision: the batched PCG sweeps run in fp32 and the accuracy is won back
+    by refinement against the fp64 residual (dynlp/solvers.py:322-337 applied to the batch): after a
+    solve from zero, every round computes R = rhs - A Z in fp64 for all instances at once, stops when
+    every instance's relative residual meets the target, and otherwise solves A D = R / scale in fp32
+    and adds D * scale. The scale (column maxima of R) and the correction's target are each
+    instance's own, so an instance's result does not depend on the others in its batch. Returns F per
+    system and (iterations, status, relative residual) per system."""
+    out, info = [None] * len(systems), [None] * len(systems)
+    by_c: dict = {}
+    for i, s in enumerate(systems):
+        by_c.setdefault(s.C, []).append(i)
+    for C, idx in by_c.items():
+        group = [systems[i] for i in idx]
+        bs = BatchedSystems(group, tile_rows=tile_rows, dtype=torch.float32)
+        dev, N, Ch = bs.dev, bs.N, bs.Ch
+        s64 = [s.astype(torch.float64) for s in group]
+        diag64 = torch.cat([s.diag for s in s64]).contiguous()
+        rhs64 = torch.cat([torch.cat([s.rhs, s.diag[:, None]], 1) for s in s64]).contiguous()
+        A = CSR(bs.w, bs.col, bs.indptr, (N, N))
+        spans = list(zip(bs.offsets[:-1], bs.offsets[1:]))
+        ones = torch.ones(C, dtype=torch.float64, device=dev)
+        rhs_n = [kernels.colreduce(2, rhs64[a:b, :C]).sqrt() if b > a else ones for a, b in spans]
+        Z64 = padded_empty(N, Ch, torch.float64, dev, 0.0)
+        Zf, it, _, _ = bs.solve(target_relres=target_relres)
+        Z64 += Zf.double()
+        iters = it.astype(np.int64)
+        rel = np.zeros(len(group))
+        for rnd in range(rounds + 1):
+            R64 = kernels.spmm_axpy(A, Z64, a=diag64, alpha=-1.0, b=1.0, rhs=rhs64)
+            rn = [kernels.colreduce(2, R64[a:b, :C]).sqrt() if b > a else 0 * ones for a, b in spans]
+            rel = np.array([float((r / torch.where(h > 0, h, torch.ones_like(h))).max()) for r, h in zip(rn, rhs_n)])
+            if (rel <= target_relres).all() or rnd == rounds:
+                break
+            scales, rhs32 = [], torch.empty((N, Ch), dtype=torch.float32, device=dev)
+            for a, b in spans:
+                sc = kernels.colreduce(3, R64[a:b]) if b > a else torch.ones(Ch, dtype=torch.float64, device=dev)
+                sc = torch.where(sc > 0, sc, torch.ones_like(sc))
+                rhs32[a:b] = (R64[a:b] / sc[None, :]).float()
+                scales.append(sc)
+            bs.rhs = rhs32
+            # each instance's correction brings its residual to a fifth of the target, as far as one
+            # fp32 solve resolves (a few 1e-6 of the correction's right-hand side)
+            need = [max(0.2 * target_relres / max(r, 1e-300), 3e-6) for r in rel]
+            D, it2, _, _ = bs.solve(target_relres=target_relres, inst_targets=need)
+            for k, ((a, b), sc) in enumerate(zip(spans, scales)):
+                if rel[k] > target_relres:  # a converged instance keeps its scores (same as alone)
+                    Z64[a:b] += D[a:b].double() * sc[None, :]
+                    iters[k] += it2[k]
+        for k, j in enumerate(idx):
+            a, b = spans[k]
+            out[j] = Z64[a:b, :C]
+            info[j] = (int(iters[k]), 5 if rel[k] <= target_relres else 2, float(rel[k]))
     return out, info

@@ -851,6 +851,45 @@ class IncrementalLP(DynLPPlus):
         return self._labels[:n], self._chg, self._chg_lab, self._nchg
 
 
+class PlainFP32LP(Solver):
+    """The plain FP32 path the serving loop is measured against: scores kept in fp32 on the global-index
+    system and every batch solved by fp32 Jacobi-PCG from the previous scores until the fp32 relative
+    residual meets the target -- no fp64 residual, no refinement (the reference's solver run in one
+    precision, dynlp/solvers.py:66-97). `relres` is still reported against the fp64 system."""
+
+    name = "plain-fp32"
+
+    def __init__(self, n_total, K, target_relres=1e-6, max_iter=100_000):
+        super().__init__(n_total, K, "float32")
+        self.target_relres, self.max_iter = target_relres, max_iter
+        self.Z = None
+
+    def solve(self, sys):
+        st = Stats(path="plain-fp32")
+        sw = sys.astype(torch.float32)
+        with Timer() as tm:
+            n, C = sw.rhs.shape[0], self.C
+            if self.Z is None:
+                self.Z = padded_empty(n, C, torch.float32, sw.diag.device, fill=0.0)
+                self.Z[:] = torch.where(sw.solved[:, None], sw.prior.to(torch.float32)[None, :], torch.zeros_like(self.Z))
+            if sys.moved is not None and sys.moved.numel():  # rows entering U start at the prior, rows leaving at 0
+                mv = sys.moved.long()
+                self.Z[mv] = torch.where(sys.solved[mv, None], sw.prior.to(torch.float32)[None, :],
+                                         torch.zeros_like(self.Z[mv]))
+            rhs = sw.rhs.contiguous()
+            pcg(sw, self.Z, rhs, None, jacobi_M(sw), self.max_iter, st, target_relres=self.target_relres)
+            s64 = sys.astype(F64)
+            R = residual(s64, self.Z.double(), s64.rhs.contiguous())
+            st.relres = float((col_norms(R) / torch.clamp(col_norms(s64.rhs), min=1e-300)).max())
+        st.ms = tm.ms
+        self.F = self.Z
+        return st
+
+    def relabel(self, sys):
+        """Labels of every row (-1 outside the solved set) and the rows whose label changed."""
+        return IncrementalLP.relabel(self, sys)
+
+
 class Reference:
     """High-accuracy float64 solution F* and absorption bound (dynlp/solvers.py:437-445)."""
 
