@@ -170,13 +170,14 @@ def solve_many(systems, target_relres=1e-6, dtype=torch.float64, tile_rows=1024,
     return out, info
 
 
-def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6):
+def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6, autotune=False):
     """solve_many in mixed precision: the batched PCG sweeps run in fp32 and the accuracy is won back
     by refinement against the fp64 residual (dynlp/solvers.py:322-337 applied to the batch): after a
     solve from zero, every round computes R = rhs - A Z in fp64 for all instances at once, stops when
     every instance's relative residual meets the target, and otherwise solves A D = R / scale in fp32
     and adds D * scale. The scale (column maxima of R) and the correction's target are each
-    instance's own, so an instance's result does not depend on the others in its batch. Returns F per
+    instance's own, so an instance's result does not depend on the others in its batch (autotune: the
+    rows-per-warp and tile shape of the fp32 sweeps picked by BatchedSystems.autotune). Returns F per
     system and (iterations, status, relative residual) per system."""
     out, info = [None] * len(systems), [None] * len(systems)
     by_c: dict = {}
@@ -185,6 +186,8 @@ def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6):
     for C, idx in by_c.items():
         group = [systems[i] for i in idx]
         bs = BatchedSystems(group, tile_rows=tile_rows, dtype=torch.float32)
+        if autotune:
+            bs.autotune()
         dev, N, Ch = bs.dev, bs.N, bs.Ch
         s64 = [s.astype(torch.float64) for s in group]
         diag64 = torch.cat([s.diag for s in s64]).contiguous()

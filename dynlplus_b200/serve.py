@@ -21,11 +21,12 @@ returns it when the batch completes; a request that does not fit waits for the n
 request larger than the whole budget is refused. Each kind has its own worker thread and CUDA
 stream, so their device work overlaps; libdlp calls release the GIL.
 
-Precision. mode="continuous" is the mixed-precision loop: FP32 (or BF16, lowp=True) sweeps with
-refinement against an FP64 residual. mode="sequential" is the plain FP32 path it is measured
-against: one request at a time in arrival order, every update solved alone by FP32 PCG without an
-FP64 residual, every fresh solve launched alone in FP32. Every request records its submit and
-completion times (p50/p99 latency).
+Precision. The continuous loop is mixed precision: FP32 (or BF16, lowp=True) sweeps with refinement
+against an FP64 residual. mode="sequential" serves one request at a time in arrival order; by
+default in plain FP32, the path the loop is measured against (every update solved alone by FP32 PCG
+without an FP64 residual, every fresh solve launched alone in FP32), and with precision="mixed" the
+loop's own solvers one request at a time (which isolates what batching buys). Every request records
+its submit and completion times (p50/p99 latency).
 """
 from __future__ import annotations
 
@@ -160,17 +161,22 @@ def take_batch(q, first, limit=None, cost=None, budget=None, size=None, slot=Non
 class Server:
     def __init__(self, ds, labeled, *, dtype="float32", target_relres=1e-6, tol=1e-3, hbm_budget_bytes=None,
                  max_fresh_batch=64, update_slot_edges=200_000, query_slot_ids=4_000_000, mode="continuous",
-                 lowp=False):
-        """mode="continuous": the mixed-precision loop described above (lowp: BF16 gathers in the update
-        solves' sweeps). mode="sequential": the plain FP32 path it is measured against. The slots cap
-        the edges patched before one update solve and the ids of one query batch."""
+                 lowp=False, precision=None):
+        """mode="continuous": the continuous-batching loop described above; mode="sequential": one
+        request at a time in arrival order. precision="mixed" (the default of the continuous loop):
+        FP32 sweeps (lowp: BF16 gathers in the update solves' sweeps) with refinement against the
+        FP64 residual; precision="fp32" (the default of the sequential mode): the plain FP32 path. The
+        slots cap the edges patched before one update solve and the ids of one query batch."""
         if mode not in ("continuous", "sequential"):
             raise ValueError(f"unknown serving mode {mode!r}")
-        self.mode = mode
+        precision = precision or ("mixed" if mode == "continuous" else "fp32")
+        if precision not in ("mixed", "fp32"):
+            raise ValueError(f"unknown serving precision {precision!r}")
+        self.mode, self.precision = mode, precision
         self.target = target_relres
         self.K = ds.K
         self.es = stream.EdgeStream(ds, labeled, dtype=dtype)
-        if mode == "continuous":
+        if precision == "mixed":
             self.solver = solvers.IncrementalLP(ds.n, ds.K, dtype, tol=tol, method="pcg",
                                                 target_relres=target_relres, full_every=16, lowp=lowp)
         else:
@@ -330,7 +336,7 @@ class Server:
                 ds = it.req.ds
                 systems.append(stream.build_system(ds, torch.ones(ds.n, dtype=torch.bool, device=ds.A.indices.device),
                                                    it.req.labeled, dtype="float32"))
-            if self.mode == "continuous":  # FP32 sweeps, refinement against the FP64 residual
+            if self.precision == "mixed":  # FP32 sweeps, refinement against the FP64 residual
                 Fs, info = batched.solve_many_mixed(systems, target_relres=self.target)
             else:  # the plain FP32 solve
                 Fs, info = batched.solve_many(systems, target_relres=self.target, dtype=torch.float32)

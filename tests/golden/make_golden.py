@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running the REFERENCE (shishir9159/DynLPlus) on the CPU.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>   (or DLP_REFERENCE=<path>)
 
 The reference is pure Python over CuPy; `cupy_shim.install` maps CuPy onto NumPy/SciPy and routes
 its three NVRTC-kernel entry points to its own vectorised fallbacks (see cupy_shim.py). Each
@@ -354,10 +354,13 @@ def gen_matrix(dl):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("DLP_REFERENCE"),
+                    help="the reference checkout (default: $DLP_REFERENCE)")
     ap.add_argument("--only", default="")
     a = ap.parse_args(argv)
     import cupy_shim
+    if not a.reference:
+        ap.error("--reference (or DLP_REFERENCE) names the reference checkout")
     dl = cupy_shim.install(a.reference)
     gens = {"cc": gen_cc, "kernels": gen_kernels, "system": gen_system, "solvers": gen_solvers, "amg": gen_amg,
             "stream": gen_stream, "graphs": gen_graphs, "api": gen_api, "matrix": gen_matrix}
