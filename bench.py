@@ -60,6 +60,8 @@ def parse(argv=None):
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch the PCG kernels one by one instead of as a CUDA graph (for kernel profilers)")
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
+    ap.add_argument("--three-kernel", action="store_true",
+                    help="edge-stream: the three-kernel PCG iteration instead of the two-kernel one")
     ap.add_argument("--workload", default="edge-stream",
                     choices=["edge-stream", "static", "amg", "batched", "serving", "kernels"],
                     help="edge-stream: the headline (ER 1M edge batches); static: SBM 100k solve + one "
@@ -77,7 +79,8 @@ def workload_name(a):
 def config(a):
     return {"workload": workload_name(a), "n": a.n, "mean_degree": a.deg, "k": a.k, "label_frac": a.label_frac,
             "batch_updates": a.batch, "insert_frac": 0.5, "target_relres": a.target_relres, "tol": a.tol,
-            "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas"}
+            "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas",
+            "pcg_iteration": "three kernels" if a.three_kernel else "two kernels (fp32 whole rows)"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -247,14 +250,39 @@ def spmm_roofline(es, C, peaks):
     algo = 4 * (n + 1) + nnz * (4 + 4 + C * sx) + n * 4 + n * C * sx + n * C * 4
     achieved = algo / (ms * 1e-3) / 1e9
     peak = peaks.get("hbm_gbs") or 6650.0
-    del _lib
+    # the same product with the gathered rows and the weights in bf16 (fp32 accumulation, fp32 own
+    # row and output; dlp_spmm_lowp, the SpMM of the BF16 sweeps): 4(n+1) + nnz (4 + 2 + 2C) + n s_a
+    # + n C 4 (own row) + n C 4 (output)
+    from dynlplus_b200.backend import ld as _ld, ptr as _ptr, stream as _stream
+    wb = solvers.bf16_weights(G)
+    Xb = solvers.padded_empty(n, C, torch.bfloat16, es.dev)
+    Xb.copy_(X)
+
+    def lowp():
+        _lib.call("dlp_spmm_lowp", _ptr(G.rbeg), _ptr(G.rend), _ptr(G.indices), _ptr(wb), n, C, _ptr(Xb), _ld(Xb),
+                  _ptr(X), _ld(X), _ptr(a), 1.0, -1.0, _ptr(Y), _ld(Y), 0, G.nnz / max(n, 1), _stream())
+
+    for _ in range(3):
+        lowp()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        lowp()
+    e.record()
+    e.synchronize()
+    ms_lo = s.elapsed_time(e) / reps
+    algo_lo = 4 * (n + 1) + nnz * (4 + 2 + C * 2) + n * 4 + n * C * 4 + n * C * 4
+    bf16 = {"kernel": "dlp_spmm_lowp (k_spmm, apply_A form, bf16 weights and gathered rows, fp32 accumulation, own row "
+                      "and output, C=%d, ld=%d)" % (C, Xb.stride(0)),
+            "achieved": algo_lo / (ms_lo * 1e-3) / 1e9, "frac": algo_lo / (ms_lo * 1e-3) / 1e9 / (peaks.get("hbm_gbs") or 6650.0),
+            "algorithmic_bytes": int(algo_lo), "ms_per_launch": ms_lo}
     return {"bound": "hbm", "kernel": "k_spmm (apply_A form, fp32, C=%d, ld=%d, compact CSR of W_UU)" % (C, X.stride(0)),
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback",
             "algorithmic_bytes": int(algo), "ms_per_launch": ms, "ms_per_launch_after_l2_flush": float(np.mean(cold)),
             "achieved_after_l2_flush": algo / (float(np.mean(cold)) * 1e-3) / 1e9, "traffic": None,
             "note": "gather model counts every neighbour-row gather as HBM bytes; on this graph the "
-                    "gathered matrix (n x ld x 4 B) fits in L2"}
+                    "gathered matrix (n x ld x 4 B) fits in L2", "bf16": bf16}
 
 
 def aggregate_replicas(dev_ms, e2e_ms, units_per_step, world, device="cpu"):
@@ -275,20 +303,47 @@ def aggregate_replicas(dev_ms, e2e_ms, units_per_step, world, device="cpu"):
 
 def pcg_iteration_bytes(n, nnz, C, s=4):
     """Algorithmic bytes of one fused PCG iteration on an n-row operator with nnz entries and C
-    columns of s-byte values: the apply (row ranges, the gather model nnz (4 + s_w + C s), diag,
-    own row of P, AP written), the residual update (R read and written, AP read, diag) and the
-    direction update (P and Z read and written, R read, diag)."""
-    apply = 8 * n + nnz * (4 + 4 + C * s) + n * s + n * C * s + n * C * s
-    update = 3 * n * C * s + n * s
-    direction = 5 * n * C * s + n * s
-    return apply + update + direction
+    columns of s-byte values, the byte model of the hot-path measurement spec: the SpMM by the gather
+    model, B_spmm = 4 (n + 1) + nnz (4 + s_w + C s) + n C s (AP written) + n s (diag) + n C s (own row
+    of P), plus 6 n C s (R, P and Z read and written) and n s (diag). The implementation moves more
+    (AP is read back by the residual update and R twice; its three kernels are separate passes), so
+    this is the floor its time is measured against."""
+    spmm = 4 * (n + 1) + nnz * (4 + 4 + C * s) + n * C * s + n * s + n * C * s
+    return spmm + 6 * n * C * s + n * s
 
 
-def pcg_roofline(events, nnz, peaks, traffic_file):
+def pcg_steady(es, C, iters=100):
+    """The PCG iteration in steady state on the stream's final system: one dlp_pcg call from zero
+    that runs `iters` iterations to its cap (a target it cannot meet), timed with CUDA events on the
+    launching stream, so the per-call start and host reads weigh 1/iters of it."""
+    import torch
+    from dynlplus_b200 import solvers
+    S = es.system.astype(torch.float32)
+    rhs = S.rhs_h.to(torch.float32).contiguous()
+    Z = solvers.padded_empty(rhs.shape[0], rhs.shape[1], torch.float32, rhs.device, fill=0.0)
+    rn = [1.0] * rhs.shape[1]
+    ev, solvers.PCG_EVENTS = solvers.PCG_EVENTS, None
+    try:
+        for _ in range(2):  # the first call captures the loop graph
+            st = solvers.Stats()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s.record()
+            solvers.pcg(S, Z, rhs, None, solvers.jacobi_M(S), iters, st, target_relres=1e-30, rhs_norm=rn,
+                        zero_start=True)
+            e.record()
+            e.synchronize()
+    finally:
+        solvers.PCG_EVENTS = ev
+    return s.elapsed_time(e) / max(st.iters, 1), st.iters
+
+
+def pcg_roofline(events, nnz, peaks, traffic_file, steady=None):
     """The fused PCG iteration (k_pcg_apply + k_pcg_update + k_pcg_dir), timed live: CUDA events
     around every dlp_pcg call of the timed steps (on the launching stream); time per iteration =
     the calls' total device time / their iterations (so it also carries each call's start, stop
-    checks and recheck, a conservative figure)."""
+    checks and recheck, a conservative figure). steady: (ms per iteration, iterations) of
+    pcg_steady, reported beside it."""
     ms = sum(s.elapsed_time(e) for s, e, _, _, _ in events)
     iters = sum(it for _, _, it, _, _ in events)
     if not iters:
@@ -308,7 +363,12 @@ def pcg_roofline(events, nnz, peaks, traffic_file):
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback",
             "traffic": traffic, "traffic_source": tsrc, "algorithmic_bytes_per_iteration": int(algo),
-            "ms_per_iteration": t, "iterations_timed": int(iters), "pcg_calls": len(events)}
+            "ms_per_iteration": t, "iterations_timed": int(iters), "pcg_calls": len(events),
+            "byte_model": "4(n+1) + nnz(4 + s_w + C s) + n C s (AP) + n s (diag) + n C s (own P) + 6 n C s + n s",
+            "steady": None if steady is None else {
+                "ms_per_iteration": steady[0], "iterations": steady[1],
+                "achieved": algo / (steady[0] * 1e-3) / 1e9, "frac": algo / (steady[0] * 1e-3) / 1e9 / peak,
+                "note": "one dlp_pcg call of that many iterations on the final system, outside the timed steps"}}
 
 
 def ours(a):
@@ -329,6 +389,7 @@ def ours(a):
     if os.path.exists(pk):
         peaks = json.load(open(pk))
 
+    solvers.TWO_KERNEL = not a.three_kernel
     seed = a.seed + 1000 * rank  # independent replicas
     ds = graphs.er_graph(a.n, a.deg, a.k, seed=seed)
     lab = graphs.label_mask(a.n, a.label_frac, seed=seed)
@@ -477,7 +538,8 @@ def ours(a):
     roof = None
     if rank == 0:
         roof = pcg_roofline(pcg_events, es.solver_csr().nnz, peaks,
-                            os.path.join(ROOT, "profiles", "pcg_iteration_traffic.json"))
+                            os.path.join(ROOT, "profiles", "pcg_iteration_traffic.json"),
+                            steady=pcg_steady(es, a.k + 1))
         if roof is not None:
             roof["spmm_alone"] = spmm_roofline(es, a.k + 1, peaks)
     cpu = None
@@ -634,20 +696,27 @@ def wl_batched(a):
                 times.append(t)
         return float(np.mean(times)), info
 
-    # the headline: fp32 sweeps over the concatenated CSR with fp64 refinement (relres on the fp64
-    # residual); beside it the same batch solved in fp64 throughout
-    t_mix, info = timed(lambda: batched.solve_many_mixed(systems, target_relres=1e-6, autotune=True))
+    # two precisions on the same 256 systems: fp32 sweeps with fp64 refinement, and fp64 sweeps
+    # (fp32 weights both); the faster is the headline, the other is reported beside it
+    t_mix, info_mix = timed(lambda: batched.solve_many_mixed(systems, target_relres=1e-6, autotune=True))
     t64, info64 = timed(lambda: batched.solve_many(systems, target_relres=1e-6, dtype=torch.float64, autotune=True))
     rows = sum(s.n_u for s in systems)
+    runs = {"fp32 sweeps + fp64 refinement": (t_mix, info_mix), "fp64 sweeps": (t64, info64)}
+    head = min(runs, key=lambda k: runs[k][0])
+    t, info = runs[head]
+
+    def summary(t, info):
+        return {"solves_per_s": 256 / (t * 1e-3), "ms": t, "relres_max": float(max(r for _, _, r in info)),
+                "converged": int(sum(s == 5 for _, s, _ in info)),
+                "iterations_total": int(sum(i for i, _, _ in info))}
+
     _line(a, "independent harmonic solves per second, 256 instances batched (rel-res 1e-6)",
-          256 / (t_mix * 1e-3), "solves/s", t_mix,
+          256 / (t * 1e-3), "solves/s", t,
           {"workload": "256x sbm n~logU[2e3,2e5] k in {2,4,8} deg~U[8,24] lab0.01", "rows": int(rows),
-           "precision": "fp32 sweeps + fp64 refinement"},
+           "precision": head},
           relres_max=float(max(r for _, _, r in info)), converged=int(sum(s == 5 for _, s, _ in info)),
-          iterations_total=int(sum(i for i, _, _ in info)),
-          fp64_throughout={"solves_per_s": 256 / (t64 * 1e-3), "ms": t64,
-                           "relres_max": float(max(r for _, _, r in info64)),
-                           "iterations_total": int(sum(i for i, _, _ in info64))})
+          iterations_total=int(sum(i for i, _, _ in info)), dtype="f64" if head == "fp64 sweeps" else "f32",
+          variants={k: summary(*v) for k, v in runs.items()})
 
 
 def wl_serving(a):

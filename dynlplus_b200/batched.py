@@ -170,15 +170,16 @@ def solve_many(systems, target_relres=1e-6, dtype=torch.float64, tile_rows=1024,
     return out, info
 
 
-def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6, autotune=False):
+def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6, autotune=False, inner=1e-4):
     """solve_many in mixed precision: the batched PCG sweeps run in fp32 and the accuracy is won back
     by refinement against the fp64 residual (dynlp/solvers.py:322-337 applied to the batch): after a
     solve from zero, every round computes R = rhs - A Z in fp64 for all instances at once, stops when
     every instance's relative residual meets the target, and otherwise solves A D = R / scale in fp32
     and adds D * scale. The scale (column maxima of R) and the correction's target are each
     instance's own, so an instance's result does not depend on the others in its batch (autotune: the
-    rows-per-warp and tile shape of the fp32 sweeps picked by BatchedSystems.autotune). Returns F per
-    system and (iterations, status, relative residual) per system."""
+    rows-per-warp and tile shape of the fp32 sweeps picked by BatchedSystems.autotune; inner: the
+    smallest relative residual asked of one fp32 solve). Returns F per system and (iterations,
+    status, relative residual) per system."""
     out, info = [None] * len(systems), [None] * len(systems)
     by_c: dict = {}
     for i, s in enumerate(systems):
@@ -197,7 +198,9 @@ def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6, auto
         ones = torch.ones(C, dtype=torch.float64, device=dev)
         rhs_n = [kernels.colreduce(2, rhs64[a:b, :C]).sqrt() if b > a else ones for a, b in spans]
         Z64 = padded_empty(N, Ch, torch.float64, dev, 0.0)
-        Zf, it, _, _ = bs.solve(target_relres=target_relres)
+        # the fp32 solves aim no lower than `inner`: below their precision floor (about 1e-6 of
+        # ||rhs|| on these systems, lower for some) a solve only stalls until its patience runs out
+        Zf, it, _, _ = bs.solve(target_relres=max(target_relres, inner))
         Z64 += Zf.double()
         iters = it.astype(np.int64)
         rel = np.zeros(len(group))
@@ -214,9 +217,9 @@ def solve_many_mixed(systems, target_relres=1e-6, tile_rows=1024, rounds=6, auto
                 rhs32[a:b] = (R64[a:b] / sc[None, :]).float()
                 scales.append(sc)
             bs.rhs = rhs32
-            # each instance's correction brings its residual to a fifth of the target, as far as one
-            # fp32 solve resolves (a few 1e-6 of the correction's right-hand side)
-            need = [max(0.2 * target_relres / max(r, 1e-300), 3e-6) for r in rel]
+            # each instance's correction brings its residual to a fifth of the target, or by `inner`
+            # when that is further than one fp32 solve safely resolves (another round follows)
+            need = [max(0.2 * target_relres / max(r, 1e-300), inner) for r in rel]
             D, it2, _, _ = bs.solve(target_relres=target_relres, inst_targets=need)
             for k, ((a, b), sc) in enumerate(zip(spans, scales)):
                 if rel[k] > target_relres:  # a converged instance keeps its scores (same as alone)

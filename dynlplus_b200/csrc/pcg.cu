@@ -31,13 +31,15 @@ struct PcgCtl {
   uint32_t cnt1, cnt2;
   int32_t mode, patience;
   int32_t max_iter, bad;  // bad: non-finite residual entries seen (breakdown)
+  int32_t par, pad;       // two-kernel iteration: which of P / AP holds the current direction
   double best, viol, relres, target;
 };
 
 // Per-block partials are stored output-major: output o of block b at part[o * nbmax + b].
 struct PcgBufs {
   PcgCtl *ctl;
-  double *alpha, *beta, *rz, *eps, *rhsn, *epsinv, *part1, *part2;
+  // rzprev: rz of the iteration in flight, kept for the beta of a resume after a failed recheck
+  double *alpha, *beta, *rz, *eps, *rhsn, *epsinv, *rzprev, *part1, *part2;
   int nbmax;
   // set only in the kernels of the device-side loop graph: K2 writes the loop's continue flag
   int has_cond;
@@ -55,8 +57,8 @@ static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 static size_t pcg_ws_bytes(int C) {
   const size_t nb = (size_t)std::max(upd_blocks(), apply_blocks());
   size_t b = align256(sizeof(PcgCtl));
-  b += 6 * align256(sizeof(double) * C);
-  b += align256(sizeof(double) * nb * C);            // part1 (pAp)
+  b += 7 * align256(sizeof(double) * C);
+  b += align256(sizeof(double) * nb * 2 * C);        // part1 (pAp; q of the two-kernel iteration)
   b += align256(sizeof(double) * nb * (2 * C + 1));  // part2 (rz, ss, violation)
   return b;
 }
@@ -67,13 +69,13 @@ static PcgBufs carve(void *ws, int C) {
   PcgBufs B;
   B.ctl = (PcgCtl *)p;
   p += align256(sizeof(PcgCtl));
-  double **vecs[6] = {&B.alpha, &B.beta, &B.rz, &B.eps, &B.rhsn, &B.epsinv};
+  double **vecs[7] = {&B.alpha, &B.beta, &B.rz, &B.eps, &B.rhsn, &B.epsinv, &B.rzprev};
   for (auto v : vecs) {
     *v = (double *)p;
     p += align256(sizeof(double) * C);
   }
   B.part1 = (double *)p;
-  p += align256(sizeof(double) * nb * C);
+  p += align256(sizeof(double) * nb * 2 * C);
   B.part2 = (double *)p;
   B.nbmax = (int)nb;
   B.has_cond = 0;
@@ -184,13 +186,26 @@ constexpr int apply_min_blocks() {
 // which frees the registers for two rows in flight per lane within the 64-register cap (measured on
 // B200 at n = 1M, degree 10, C = 9: 123 us; fp64 lane partials allow one row in flight, 127 us; two
 // spill, 166 us; per-vector loads 160 us).
-template <class T, int VW, int VPL, bool ROW12 = false>
+//
+// FUSE (fp32 whole rows only): the apply of the two-kernel iteration. P and AP trade places every
+// iteration (ctl->par says which buffer holds the direction), and the lanes also sum
+// q_c = sum AP^2 / diag, from which the last block predicts the iteration's beta before the residual
+// update: with alpha = rz / pAp and the A-conjugacy of successive directions ((P_prev, A P) = 0, so
+// (R / diag) . AP = pAp), rz_next = sum (R - alpha AP)^2 / diag = alpha^2 q - rz, and
+// beta = rz_next / rz = alpha^2 q / rz - 1. The exact rz_next of the stored residual, summed by the
+// fused sweep, is the one the next alpha uses.
+template <class T, int VW, int VPL, bool ROW12 = false, bool FUSE = false>
 __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_pcg_apply(ApplyArgs<T> p) {
   using TA = typename T::TA;
   PcgCtl *ctl = p.B.ctl;
   if (ctl->done != 0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->go = 0;
     return;
+  }
+  if (FUSE && ctl->par) {  // this iteration's direction is in the AP buffer; AP goes to the P buffer
+    const typename T::TX *tp = p.P;
+    p.P = (const typename T::TX *)p.AP;
+    p.AP = (typename T::TY *)tp;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->go = 1;
   __shared__ double sm[kThreads / 32][256];
@@ -207,6 +222,10 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
     for (int i = 0; i < VW; ++i) dot[k][i] = TD(0);
+  // FUSE: q is summed over the warp's 32 rows after each batch (a reduce-scatter across the lanes:
+  // lanes 2c and 2c + 1 end with column c's sum), so a lane keeps one running q partial instead of
+  // a row's worth
+  float qacc = 0.f;
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long g0 = warp * gpw; g0 < p.n; g0 += nwarps * gpw) {
@@ -215,9 +234,14 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 2 : gather_batch_lean<TA, VW, VPL>()),
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? (FUSE ? 1 : 2) : gather_batch_lean<TA, VW, VPL>()),
                (ROW12 ? kRow12F : kRowVec)>(
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
+    float qv[FUSE ? 12 : 1];  // FUSE: this row's AP^2 / diag per column (0 past C and on invalid lanes)
+    if constexpr (FUSE) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) qv[c] = 0.f;
+    }
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);
       if constexpr (ROW12) {
@@ -232,13 +256,23 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
             const int c = k * 4 + i;
             const float pv = k == 0 ? (hi ? pw[2][i] : pw[0][i]) : k == 1 ? (hi ? pw[0][i] : pw[1][i])
                                                                         : (hi ? pw[1][i] : pw[2][i]);
-            apv[k][i] = d * pv - acc[k][i];  // padding columns too when the whole row is stored
+            // padding columns too when the whole row is stored; zeros there when AP becomes the next
+            // direction (FUSE), so the gathered padding stays zero
+            apv[k][i] = (FUSE && c >= p.C) ? 0.f : d * pv - acc[k][i];
             if (c < p.C) {
               if (!p.ap_row12) p.AP[r * p.ldap + c] = apv[k][i];
               dot[k][i] += (TD)pv * (TD)apv[k][i];
             }
           }
         if (p.ap_row12) store_row12(p.AP + r * p.ldap, apv);
+        if constexpr (FUSE) {
+          const float rinv = __frcp_rn((float)d);
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (k * 4 + i < p.C) qv[k * 4 + i] = apv[k][i] * apv[k][i] * rinv;
+        }
       } else {
 #pragma unroll
         for (int k = 0; k < VPL; ++k) {
@@ -258,42 +292,78 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
         }
       }
     }
+    if constexpr (FUSE) {  // reduce-scatter of the 12 (padded to 16) column values over the warp
+      float v8[8], v4[4], v2[2], v1;
+      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float lo = qv[j], hi = j + 8 < 12 ? qv[j + 8] : 0.f;
+        v8[j] = (b4 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b4 ? lo : hi, 16);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v4[j] = (b3 ? v8[j + 4] : v8[j]) + __shfl_xor_sync(0xffffffffu, b3 ? v8[j] : v8[j + 4], 8);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) v2[j] = (b2 ? v4[j + 2] : v4[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v4[j] : v4[j + 2], 4);
+      v1 = (b1 ? v2[1] : v2[0]) + __shfl_xor_sync(0xffffffffu, b1 ? v2[0] : v2[1], 2);
+      qacc += v1 + __shfl_xor_sync(0xffffffffu, v1, 1);
+    }
   }
   // lanes sharing a vector lane (same cl) hold the same columns: reduce over the other bits, in fp64
-  double dsum[VPL][VW];
+  constexpr int NQ = FUSE ? 2 : 1;  // pAp, and q when fused
+  {
+    double dsum[VPL][VW];
 #pragma unroll
-  for (int k = 0; k < VPL; ++k)
+    for (int k = 0; k < VPL; ++k)
 #pragma unroll
-    for (int i = 0; i < VW; ++i) {
-      double x = (double)dot[k][i];
-      for (int off = LV; off < 32; off <<= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-      dsum[k][i] = x;
-    }
-  if (lane < LV) {
+      for (int i = 0; i < VW; ++i) {
+        double x = (double)dot[k][i];
+        for (int off = LV; off < 32; off <<= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        dsum[k][i] = x;
+      }
+    if (lane < LV) {
 #pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      const int vi = lane + k * LV;
-      if (vi < NV) {
+      for (int k = 0; k < VPL; ++k) {
+        const int vi = lane + k * LV;
+        if (vi < NV) {
 #pragma unroll
-        for (int i = 0; i < VW; ++i) {
-          const int c = vi * VW + i;
-          if (c < p.C) sm[wid][c] = dsum[k][i];
+          for (int i = 0; i < VW; ++i) {
+            const int c = vi * VW + i;
+            if (c < p.C) sm[wid][c] = dsum[k][i];
+          }
         }
       }
     }
   }
+  if constexpr (FUSE) {  // lanes 2c hold the warp's q for column c (slot of lane bits 4..1)
+    const int slot = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+    if ((lane & 1) == 0 && slot < p.C) sm[wid][p.C + slot] = (double)qacc;
+  }
   __syncthreads();
-  for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
+  for (int c = threadIdx.x; c < NQ * p.C; c += blockDim.x) {
     double s = 0.0;
     for (int w = 0; w < kThreads / 32; ++w) s += sm[w][c];
     p.B.part1[(long long)c * p.B.nbmax + blockIdx.x] = s;
   }
   if (last_block(&ctl->cnt1)) {
     const PcgBufs &B = p.B;
-    block_partials_reduce<kThreads, 2>(B.part1, B.nbmax, (int)gridDim.x, p.C, p.C, [&](int c, double s) {
-      const double al = s > 0.0 ? B.rz[c] / s : 0.0;
-      B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
-    });
+    if constexpr (FUSE) {
+      __shared__ double s_pq[2 * 12];
+      block_partials_reduce<kThreads, 2>(B.part1, B.nbmax, (int)gridDim.x, 2 * p.C, 2 * p.C,
+                                         [&](int o, double s) { s_pq[o] = s; });
+      for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
+        const double pap = s_pq[c], q = s_pq[p.C + c], rz = B.rz[c];
+        double al = pap > 0.0 ? rz / pap : 0.0;
+        al = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
+        B.alpha[c] = al;
+        const double be = rz > 0.0 ? al * al * q / rz - 1.0 : 0.0;
+        B.beta[c] = isfinite(be) && be > 0.0 && be < 1e30 ? be : 0.0;
+      }
+    } else {
+      block_partials_reduce<kThreads, 2>(B.part1, B.nbmax, (int)gridDim.x, p.C, p.C, [&](int c, double s) {
+        const double al = s > 0.0 ? B.rz[c] / s : 0.0;
+        B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
+      });
+    }
     if (threadIdx.x == 0) ctl->cnt1 = 0;
   }
 }
@@ -343,6 +413,75 @@ __device__ __forceinline__ double block_column_sum(const double *v, int c, int64
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
   return s;
+}
+
+// The last block of a residual sweep (K2, or the fused sweep of the two-kernel iteration): reduces
+// the partials (rz_c, ss_c, violation), keeps rz for the next alpha and the one it replaces
+// (rzprev: the beta of a resume after a failed recheck, rz_true / rz of the iteration, as the
+// reference's loop has it), sets K3's beta (three-kernel phases 0 and 1), and takes the stop
+// decision: violation <= 1 and/or max_c ||R_c||/||rhs_c|| <= target, patience, iteration cap,
+// cancel word; the fused sweep flips which buffer holds the direction.
+__device__ void finish_sweep(int phase, int32_t C, const PcgBufs &B, bool fused) {
+  PcgCtl *ctl = B.ctl;
+  const int tid = threadIdx.x;
+  // outputs: rz_c (c < C), ss_c (C + c), violation (2C)
+  __shared__ double s_out[2 * 256 + 1];
+  block_partials_reduce<kSweepThreads, 2>(B.part2, B.nbmax, (int)gridDim.x, 2 * C + 1, 2 * C,
+                                          [&](int o, double v) { s_out[o] = v; });
+  __shared__ double s_rel;
+  if (tid == 0) s_rel = 0.0;
+  __syncthreads();
+  for (int c = tid; c < C; c += kSweepThreads) {
+    const double a = s_out[c], b = s_out[C + c];
+    const double rzo = B.rz[c];
+    if (phase == 0) B.rzprev[c] = rzo;
+    if (!fused) {
+      const double den = phase == 1 ? B.rzprev[c] : rzo;
+      const double be = (phase < 2 && den > 0.0) ? a / den : 0.0;
+      B.beta[c] = isfinite(be) && fabs(be) < 1e30 ? be : 0.0;
+    }
+    B.rz[c] = a;
+    const double rel = B.rhsn[c] > 0.0 ? sqrt(b) / B.rhsn[c] : sqrt(b);
+    // fmax over non-negative doubles: the int64 view is monotone
+    atomicMax((unsigned long long *)&s_rel, __double_as_longlong(rel));
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const double v = s_out[2 * C];
+    const double rel = s_rel;
+    ctl->viol = v;
+    ctl->relres = rel;
+    double m = 0.0;
+    if (ctl->mode & 1) m = fmax(m, v);
+    if (ctl->mode & 2) m = fmax(m, ctl->target > 0.0 ? rel / ctl->target : rel);
+    const bool conv = m <= 1.0 && !ctl->bad;
+    if (phase == 0) ctl->iters += 1;
+    if (phase == 0 && fused) ctl->par ^= 1;  // the next direction went into the other buffer
+    if (phase >= 2) {  // the initial residual
+      ctl->best = m;
+      ctl->stall = 0;
+      ctl->done = conv ? 5 : 0;
+    } else if (phase == 0 && conv) {
+      ctl->done = 1;  // proposed: confirmed against the true residual by the host
+    } else if (phase == 1 && conv) {
+      ctl->done = 5;
+    } else {
+      if (m < 0.9 * ctl->best) {
+        ctl->best = m;
+        ctl->stall = 0;
+      } else {
+        ctl->stall += 1;
+      }
+      if (ctl->stall >= ctl->patience) ctl->done = 2;
+      else if (phase == 1) ctl->done = 0;
+    }
+    if (ctl->done == 0 && ctl->iters >= ctl->max_iter) ctl->done = 3;
+    if (ctl->done == 0 && read_cancel(B.cancel)) ctl->done = 6;
+    if (ctl->bad) ctl->done = 4;
+    ctl->cnt2 = 0;
+    // the device-side loop runs another iteration only while the solve is running
+    if (B.has_cond) cudaGraphSetConditional(B.cond, ctl->done == 0 ? 1u : 0u);
+  }
 }
 
 // K2: residual update + reductions + stop decision
@@ -435,62 +574,99 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
     for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
     B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
   }
-  if (last_block(&ctl->cnt2)) {
-    // outputs: rz_c (c < C), ss_c (C + c), violation (2C)
-    __shared__ double s_out[2 * 256 + 1];
-    block_partials_reduce<kSweepThreads, 2>(B.part2, B.nbmax, (int)gridDim.x, 2 * C + 1, 2 * C,
-                                            [&](int o, double v) { s_out[o] = v; });
-    __shared__ double s_rel;
-    if (tid == 0) s_rel = 0.0;
-    __syncthreads();
-    for (int c = tid; c < C; c += kSweepThreads) {
-      const double a = s_out[c], b = s_out[C + c];
-      const double rzo = B.rz[c];
-      const double be = (phase < 2 && rzo > 0.0) ? a / rzo : 0.0;
-      B.beta[c] = isfinite(be) && fabs(be) < 1e30 ? be : 0.0;
-      B.rz[c] = a;
-      const double rel = B.rhsn[c] > 0.0 ? sqrt(b) / B.rhsn[c] : sqrt(b);
-      // fmax over non-negative doubles: the int64 view is monotone
-      atomicMax((unsigned long long *)&s_rel, __double_as_longlong(rel));
-    }
-    __syncthreads();
-    const double s_vmax = s_out[2 * C];
-    if (tid == 0) {
-      const double v = s_vmax;
-      const double rel = s_rel;
-      ctl->viol = v;
-      ctl->relres = rel;
-      double m = 0.0;
-      if (ctl->mode & 1) m = fmax(m, v);
-      if (ctl->mode & 2) m = fmax(m, ctl->target > 0.0 ? rel / ctl->target : rel);
-      const bool conv = m <= 1.0 && !ctl->bad;
-      if (phase == 0) ctl->iters += 1;
-      if (phase >= 2) {  // the initial residual
-        ctl->best = m;
-        ctl->stall = 0;
-        ctl->done = conv ? 5 : 0;
-      } else if (phase == 0 && conv) {
-        ctl->done = 1;  // proposed: confirmed against the true residual by the host
-      } else if (phase == 1 && conv) {
-        ctl->done = 5;
-      } else {
-        if (m < 0.9 * ctl->best) {
-          ctl->best = m;
-          ctl->stall = 0;
-        } else {
-          ctl->stall += 1;
-        }
-        if (ctl->stall >= ctl->patience) ctl->done = 2;
-        else if (phase == 1) ctl->done = 0;
+  if (last_block(&ctl->cnt2)) finish_sweep(phase, C, B, false);
+}
+
+// K2 of the two-kernel iteration: the residual update, the solution update and the next direction
+// in one sweep, with the beta the apply predicted (k_pcg_apply, FUSE):
+//   R -= alpha AP; Z += alpha P; P_next = R / diag + beta P; rz_c, ss_c, violation of the new R
+// P_next is written over AP (the same element is read first), so the current direction stays intact
+// for a resume after a failed recheck; the last block takes the stop decision as K2 does and
+// flips ctl->par. buf0 / buf1 are the P and AP buffers (same leading dimension ld).
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>()))
+    k_pcg_fused(int32_t n, int32_t C, T *__restrict__ R, int64_t ldr, T *__restrict__ Z, int64_t ldz, T *buf0,
+                T *buf1, int64_t ld, const T *__restrict__ diag, PcgBufs B) {
+  PcgCtl *ctl = B.ctl;
+  if (!ctl->go) {
+    if (B.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(B.cond, 0u);  // loop ends
+    return;
+  }
+  if (B.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(B.cond, 0u);
+  __shared__ double s_rz[kSweepThreads], s_ss[kSweepThreads], s_v[kSweepThreads / 32];
+  const bool par = ctl->par != 0;
+  const T *P = par ? buf1 : buf0;
+  T *AP = par ? buf0 : buf1;  // AP in, the next direction out
+  const SweepIdx ix = sweep_index(ldr, C);
+  double rz = 0.0, ss = 0.0, vmax = 0.0;
+  bool bad = false;
+  if (ix.on) {
+    const int c = ix.c;
+    const T al = (T)B.alpha[c], be = (T)B.beta[c];
+    const long long rstep = ix.RS * ldr, zstep = ix.RS * ldz, pstep = ix.RS * ld;
+    long long offr = ix.r0 * ldr + c, offz = ix.r0 * ldz + c, offp = ix.r0 * ld + c;
+    double rmax = 0.0;
+    for (long long r = ix.r0; r < n; r += kSweepUnroll * ix.RS) {
+      // every load of the batch is issued before any store
+      T rv[kSweepUnroll], av[kSweepUnroll], pv[kSweepUnroll], zv[kSweepUnroll], dv[kSweepUnroll];
+#pragma unroll
+      for (int u = 0; u < kSweepUnroll; ++u) {
+        const long long rr = r + u * ix.RS;
+        const bool ok = rr < n;
+        rv[u] = ok ? R[offr + u * rstep] : T(0);
+        av[u] = ok ? AP[offp + u * pstep] : T(0);
+        pv[u] = ok ? P[offp + u * pstep] : T(0);
+        zv[u] = ok ? Z[offz + u * zstep] : T(0);
+        dv[u] = ok ? diag[rr] : T(1);
       }
-      if (ctl->done == 0 && ctl->iters >= ctl->max_iter) ctl->done = 3;
-      if (ctl->done == 0 && read_cancel(B.cancel)) ctl->done = 6;
-      if (ctl->bad) ctl->done = 4;
-      ctl->cnt2 = 0;
-      // the device-side loop runs another iteration only while the solve is running
-      if (B.has_cond) cudaGraphSetConditional(B.cond, ctl->done == 0 ? 1u : 0u);
+#pragma unroll
+      for (int u = 0; u < kSweepUnroll; ++u) {
+        const long long rr = r + u * ix.RS;
+        if (rr < n) {
+          const T rn = rv[u] - al * av[u];
+          R[offr + u * rstep] = rn;
+          Z[offz + u * zstep] = zv[u] + al * pv[u];
+          const double r64 = (double)rn;
+          const double dinv = __drcp_rn((double)dv[u]);  // correctly rounded: the value of 1.0 / d
+          // R / diag rounded to T: for fp32 operands the fp64 product with the correctly rounded
+          // reciprocal rounds to the same value as the fp32 quotient (the quotient is never within
+          // 2^-49 relative of an fp32 rounding midpoint; the product is within 2^-52 of it)
+          AP[offp + u * pstep] = (T)(r64 * dinv) + be * pv[u];
+          const double r2 = r64 * r64;
+          rz += r2 * dinv;
+          ss += r2;
+          rmax = fmax(rmax, fabs(r64) * dinv);
+        }
+      }
+      offr += kSweepUnroll * rstep;
+      offz += kSweepUnroll * zstep;
+      offp += kSweepUnroll * pstep;
+    }
+    bad = !isfinite(ss);
+    vmax = rmax * B.epsinv[c];
+  }
+  if (bad) ctl->bad = 1;
+  const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  s_rz[tid] = rz;
+  s_ss[tid] = ss;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+  if (lane == 0) s_v[wid] = vmax;
+  __syncthreads();
+  for (int c = wid; c < C; c += kSweepThreads / 32) {
+    const double a = block_column_sum(s_rz, c, ldr);
+    const double b = block_column_sum(s_ss, c, ldr);
+    if (lane == 0) {
+      B.part2[(long long)c * B.nbmax + blockIdx.x] = a;
+      B.part2[(long long)(C + c) * B.nbmax + blockIdx.x] = b;
     }
   }
+  if (tid == 0) {
+    double v = 0.0;
+    for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
+    B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
+  }
+  if (last_block(&ctl->cnt2)) finish_sweep(0, C, B, true);
 }
 
 // K3: Z += alpha P; P = R/diag + beta P
@@ -498,12 +674,19 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
 //   mode 2: P = R/diag      mode 4: P = R/diag and Z = 0 (a zero start)
 template <typename T>
 __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_dir(int mode, int32_t n, int32_t C, T *__restrict__ Z,
-                                                           int64_t ldz, T *__restrict__ P, int64_t ldp,
+                                                           int64_t ldz, T *P, int64_t ldp,
                                                            const T *__restrict__ R, int64_t ldr,
                                                            const T *__restrict__ diag, PcgBufs B, bf16 *P_lo,
-                                                           int64_t ld_lo) {
+                                                           int64_t ld_lo, T *P2) {
   PcgCtl *ctl = B.ctl;
   if (mode == 0 && !ctl->go) return;
+  // two-kernel iteration (P2 = its AP buffer): the new direction goes to the buffer ctl->par names,
+  // from the old one in the other (a resume after a failed recheck keeps the reference's beta)
+  T *Pin = P, *Pout = P;
+  if (P2 && mode == 1) {
+    if (ctl->par) Pout = P2;  // direction of the iteration in buf0 = P, the resumed one to buf1
+    else Pin = P2;
+  }
   const bool upd_p = mode != 0 || ctl->done == 0;
   const SweepIdx ix = sweep_index(ldr, C);
   if (!ix.on) return;
@@ -520,7 +703,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
     for (int u = 0; u < kSweepUnroll; ++u) {
       const long long rr = r + u * ix.RS;
       const bool ok = rr < n;
-      pv[u] = (ok && !init) ? P[offp + u * pstep] : T(0);
+      pv[u] = (ok && !init) ? Pin[offp + u * pstep] : T(0);
       zv[u] = (ok && mode == 0) ? Z[offz + u * zstep] : T(0);
       rv[u] = (ok && upd_p) ? R[offr + u * rstep] : T(0);
       dv[u] = (ok && upd_p) ? diag[rr] : T(1);
@@ -534,7 +717,7 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
         if (upd_p) {
           const T y = rv[u] / dv[u];
           const T pn = init ? y : y + be * pv[u];
-          P[offp + u * pstep] = pn;
+          Pout[offp + u * pstep] = pn;
           if (P_lo) P_lo[rr * ld_lo + c] = cvt<bf16>(pn);
         }
       }
@@ -674,9 +857,10 @@ struct PcgProblem {
   const void *w_lo;  // bf16 weights and the bf16 mirror of P (NULL: full precision gathers)
   void *P_lo;
   int64_t ld_lo;
+  bool fused;  // the two-kernel iteration (fp32 whole rows, P and AP trade places)
 };
 
-template <class T>
+template <class T, bool FUSE = false>
 static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, bool launch = true) {
   Layout L;
   const bool lo = sizeof(typename T::TX) == 2;
@@ -705,7 +889,11 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, b
     default: return DLP_ERR_INVALID;                                                    \
   }
   constexpr bool row12 = std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value;
-  if (row12 && L.VW == 4 && L.VPL == 3 && L.LV == 1) {
+  if constexpr (FUSE) {
+    if (!(row12 && L.VW == 4 && L.VPL == 3 && L.LV == 1) || q.ldp != q.ldap) return DLP_ERR_INVALID;
+    static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, row12, true>, kThreads);
+    if (launch) k_pcg_apply<T, VWV, 3, row12, true><<<sm_count() * per, kThreads, 0, s>>>(a);
+  } else if (row12 && L.VW == 4 && L.VPL == 3 && L.LV == 1) {
     // fp32 rows of 12 floats held whole by one lane: the two-load gather (load_row12)
     static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, row12>, kThreads);
     if (launch) k_pcg_apply<T, VWV, 3, row12><<<sm_count() * per, kThreads, 0, s>>>(a);
@@ -734,11 +922,27 @@ template <typename TS>
 static int launch_dir(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   k_pcg_dir<TS><<<dir_grid<TS>(), kSweepThreads, 0, s>>>(mode, q.n, q.C, (TS *)q.Z, q.ldz, (TS *)q.P, q.ldp,
                                                          (const TS *)q.R, q.ldr, (const TS *)q.diag, B,
-                                                         (bf16 *)q.P_lo, q.ld_lo);
+                                                         (bf16 *)q.P_lo, q.ld_lo, q.fused ? (TS *)q.AP : nullptr);
+  return check_launch();
+}
+
+static int fused_grid() {
+  static const int per = resident_per_sm(k_pcg_fused<float>, kSweepThreads);
+  return sm_count() * per;
+}
+
+static int launch_fused(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  k_pcg_fused<float><<<fused_grid(), kSweepThreads, 0, s>>>(q.n, q.C, (float *)q.R, q.ldr, (float *)q.Z, q.ldz,
+                                                            (float *)q.P, (float *)q.AP, q.ldp,
+                                                            (const float *)q.diag, B);
   return check_launch();
 }
 
 static int iteration(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  if (q.fused) {
+    DLP_TRY((launch_apply<T_F32, true>(q, B, s)));
+    return launch_fused(q, B, s);
+  }
   if (q.dtype == DLP_F32) {
     if (q.w_lo) DLP_TRY(launch_apply<T_BF16F>(q, B, s));
     else DLP_TRY(launch_apply<T_F32>(q, B, s));
@@ -753,6 +957,10 @@ static int iteration(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
 
 // Fills the one-wave grid caches of the kernels iteration() launches, without launching.
 static int prime_grids(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  if (q.fused) {
+    (void)fused_grid();
+    return launch_apply<T_F32, true>(q, B, s, false);
+  }
   if (q.dtype == DLP_F32) {
     (void)update_grid<float>();
     (void)dir_grid<float>();
@@ -817,7 +1025,7 @@ static int graph_key(const PcgProblem &q, const PcgBufs &B, int k, GraphKey *key
                    (uintptr_t)q.ldz, (uintptr_t)q.R, (uintptr_t)q.ldr, (uintptr_t)q.P, (uintptr_t)q.ldp,
                    (uintptr_t)q.AP, (uintptr_t)q.ldap, (uintptr_t)q.dtype, (uintptr_t)B.ctl, (uintptr_t)k,
                    (uintptr_t)q.w_lo, (uintptr_t)q.P_lo, (uintptr_t)q.ld_lo, (uintptr_t)L.G, (uintptr_t)L.LV,
-                   (uintptr_t)L.VW, (uintptr_t)L.VPL, (uintptr_t)B.cancel}};
+                   (uintptr_t)L.VW, (uintptr_t)L.VPL, (uintptr_t)B.cancel, (uintptr_t)q.fused}};
   return DLP_OK;
 }
 
@@ -963,7 +1171,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   if (n < 0 || C <= 0 || C > 256 || ldz < C || ldr < C || ldp < C || ldap < C || ldrhs < C) return DLP_ERR_INVALID;
   if (ldr > (int64_t)sm_count() * kSweepThreads) return DLP_ERR_INVALID;
   if ((w_lo || P_lo) && (!w_lo || !P_lo || ld_lo < C || dtype != DLP_F32)) return DLP_ERR_INVALID;
-  if ((mode & 3) == 0 || mode > 7 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
+  if ((mode & 3) == 0 || mode > 31 || ((mode & 1) && !eps) || ((mode & 2) && !rhs_norm)) return DLP_ERR_INVALID;
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
     return DLP_ERR_DTYPE;
   if (!ws || ws_bytes < pcg_ws_bytes(C)) return DLP_ERR_WORKSPACE;
@@ -974,7 +1182,14 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   }
   cudaStream_t s = (cudaStream_t)stream;
   PcgProblem q{rbeg, rend, col, w, w_dtype, n, C, diag, rhs, ldrhs, Z, ldz, R, ldr, P, ldp, AP, ldap, dtype, avg_deg,
-               w_lo, P_lo, ld_lo};
+               w_lo, P_lo, ld_lo, false};
+  if (dtype == DLP_F32 && w_dtype == DLP_F32 && !w_lo && !(mode & 8) && ldp == ldap &&
+      (uintptr_t)AP % 16 == 0) {
+    // the two-kernel iteration where the apply takes the fp32 whole-row path for P and for AP
+    Layout L;
+    DLP_TRY(choose_layout(C, sizeof(float), P, ldp, 0, avg_deg, &L));
+    q.fused = L.VW == 4 && L.VPL == 3 && L.LV == 1 && ldap >= 12 && ldap % 4 == 0;
+  }
   PcgBufs B = carve(ws, C);
   B.cancel = cancel_word();
   PcgCtl h{};
@@ -1040,6 +1255,9 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
       } else {
         for (int i = 0; i < k; ++i) DLP_TRY(iteration(q, B, s));
       }
+    } else if (mode & 16) {
+      cur.done = 5;  // the caller confirms the stop on a residual of its own (no recheck here)
+      break;
     } else {
       // a stop was proposed: recheck on the true residual (dynlp/solvers.py:85-89)
       DLP_TRY(true_residual(q, s));

@@ -166,15 +166,20 @@ PCG_EVENTS = None
 # kernels one by one (False: the same kernels, for kernel-level profilers that do not follow graph
 # control flow).
 GRAPHS = True
+# fp32 solves with whole-row gathers run the two-kernel iteration (dlp_pcg mode bit 3 off); False
+# forces the three-kernel one (for comparisons)
+TWO_KERNEL = True
 
 
 def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400, *, target_relres=None,
-        rhs_norm=None, check_every=8, use_graph=None, lowp=False, zero_start=False):
+        rhs_norm=None, check_every=8, use_graph=None, lowp=False, zero_start=False, confirm=True):
     """Block PCG (one CG per column) until |r_c| <= eps_c * diag (dynlp/solvers.py:66-97).
 
     Jacobi-preconditioned solves run as one fused libdlp call. With `target_relres` the relative
     residual ||R_c|| / rhs_norm_c <= target must hold as well (rhs_norm defaults to ||rhs_c||).
-    zero_start: the solve starts from Z = 0 whatever Z holds, with rhs as the initial residual."""
+    zero_start: the solve starts from Z = 0 whatever Z holds, with rhs as the initial residual.
+    confirm=False: a proposed stop is final without the recheck on the true residual (for a caller
+    that computes the fp64 residual next; the AMG-preconditioned loops always recheck)."""
     if eps is None and target_relres is None:
         raise ValueError("pcg needs eps and/or target_relres")
     if M is not None and not isinstance(M, JacobiM):
@@ -209,6 +214,10 @@ def pcg(sys: System, Z, rhs, eps, M, max_iter, st: Stats, work_M=0, patience=400
         rn = (ct.c_double * C)(*[float(x) for x in rhs_norm])
     if zero_start:
         mode |= 4  # Z == 0 on entry: the initial residual is rhs (no SpMM)
+    if not TWO_KERNEL:
+        mode |= 8  # the three-kernel iteration even where the two-kernel one applies
+    if not confirm:
+        mode |= 16  # the caller confirms the stop on its own (fp64) residual
     ws = workspace("pcg").get(_lib.lib().dlp_pcg_workspace_bytes(C))
     it, viol, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_double(0), ct.c_int32(0)
     rhs = rhs.to(dt)
@@ -654,7 +663,9 @@ class DynLPPlus(Solver):
                 fl = (2e-3 if self.lowp else 3e-6) if self.dtype == torch.float32 else 1e-13
                 allowed = [max(self.refine_share * self.target_relres * float(rhs_norm[c]), fl * rnR[c], 1e-300) /
                            scale[c] for c in range(C)]
-                kw = dict(target_relres=1.0, rhs_norm=allowed + [1e300])
+                # the fp64 residual computed next confirms the correction's stop, so the solve skips
+                # its own recheck on the working-precision residual
+                kw = dict(target_relres=1.0, rhs_norm=allowed + [1e300], confirm=False)
             Rs = _scratch("ref_Rs", Z64.shape[0], C + 1, self.dtype, dev)
             _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs), ld(Rs),
                       code(Rs), stream())

@@ -240,9 +240,19 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
  * fixed order. Stop rule `mode`: bit 0 = the reference's max_uc |R_uc|/(eps_c diag_u) <= 1,
  * bit 1 = max_c ||R_c||_2 / rhs_norm[c] <= target_relres (both bits: both must hold); bit 2 = a zero
  * start: Z is set to 0 (its incoming values are ignored) and the initial residual is rhs itself (no
- * SpMM; R is written in the first sweep). A proposed
- * stop is confirmed on the true residual rhs - A Z (solvers.py:85-89); `patience` iterations
- * without a 10% improvement stop the solve as the reference's stall rule does (:90-92).
+ * SpMM; R is written in the first sweep); bit 3 = always the three-kernel iteration; bit 4 = no
+ * recheck: a proposed stop is final (status 5) without the true-residual confirmation below, for a
+ * caller that confirms on its own residual (R then holds the recurrence residual). Without bit 3,
+ * fp32 solves whose rows take the whole-row gather (9-12 columns, ldp == ldap >= 12, P and AP on
+ * 16-byte boundaries, no bf16 mirror) run two kernels per iteration: the SpMM also sums
+ * q_c = sum AP^2/diag and predicts beta = alpha^2 q / rz - 1 (exact for A-conjugate successive
+ * directions), and one sweep updates R, Z and the next direction; P and AP trade places every
+ * iteration (on return either may hold the last direction), and rz of the stored residual stays
+ * exact for the next alpha. A proposed
+ * stop is confirmed on the true residual rhs - A Z (solvers.py:85-89), and a failed confirmation
+ * resumes with the reference's beta (rz of the true residual over rz of the iteration);
+ * `patience` iterations without a 10% improvement stop the solve as the reference's stall rule
+ * does (:90-92).
  * eps and rhs_norm are HOST arrays of C doubles (rhs_norm may be NULL when bit 1 is unused).
  * R, P, AP are caller-provided n x C scratch matrices (R holds the final residual; for fp32 rows of
  * 9-12 columns with ldap >= 12 on 16-byte boundaries AP is written whole, its padding columns

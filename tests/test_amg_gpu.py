@@ -179,8 +179,9 @@ def test_radix_sort_of_pairs_is_stable(m, nc):
     val = torch.arange(m, dtype=torch.float64, device="cuda")
     want_k, order = torch.sort(key, stable=True)
     k2, v2 = key.clone(), val.clone()
+    kt, vt = torch.empty_like(k2), torch.empty_like(v2)  # spare arrays, alive until the sort has run
     ws = workspace("sort_test").get(_lib.lib().dlp_sort_pairs_workspace_bytes(m))
-    _lib.call("dlp_sort_pairs", m, nc * nc, ptr(k2), ptr(v2), ptr(torch.empty_like(k2)), ptr(torch.empty_like(v2)),
-              ptr(ws), ws.numel(), stream())
+    _lib.call("dlp_sort_pairs", m, nc * nc, ptr(k2), ptr(v2), ptr(kt), ptr(vt), ptr(ws), ws.numel(), stream())
+    torch.cuda.synchronize()
     assert torch.equal(k2, want_k)
     assert torch.equal(v2, val[order])

@@ -72,6 +72,74 @@ def test_fused_pcg_fp32_and_relres_target():
     assert rel <= 1e-5 * 1.01 and st.iters < 200, (rel, st.iters)
 
 
+def _whole_row_system(C, n=3000, seed=None):
+    rs = np.random.RandomState(C if seed is None else seed)
+    A = O.symmetric_from_pairs(rs.randint(0, n, 24000), rs.randint(0, n, 24000), rs.rand(24000) + 0.1, n,
+                               np.float64)
+    diag = np.asarray(A.sum(axis=1)).ravel() + 0.5
+    rhs = rs.rand(n, C)
+    S = stream.System(t=0, U=torch.arange(n, device="cuda"), W=CSR.from_scipy(A, dtype=torch.float32),
+                      s=T(diag, torch.float32), diag=T(diag, torch.float32), B=T(rhs, torch.float32),
+                      rhs=T(rhs, torch.float32), prior=T(np.full(C, 1 / C), torch.float32),
+                      is_new=torch.zeros(n, dtype=torch.bool, device="cuda"),
+                      seed=torch.zeros(n, dtype=torch.bool, device="cuda"), comps={}, K=C, C=C, eta=0.0,
+                      n_inserted=0, n_deleted=0, n_active=n)
+    return S, A, diag, rhs
+
+
+@pytest.mark.parametrize("C", [9, 12])
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("eps", [None, 1e-6])
+def test_two_kernel_iteration_follows_three_kernel_one(C, graph, eps):
+    """fp32 solves whose rows take the whole-row gather run two kernels per iteration (the SpMM also
+    sums q = sum AP^2/diag and predicts beta; one sweep updates R, Z and the next direction, P and AP
+    trading places). Against the three-kernel iteration on the same system: iteration counts within
+    one, scores equal to fp32 rounding, and both meet the target on the fp64 residual."""
+    S, A, diag, rhs = _whole_row_system(C)
+    out = []
+    try:
+        for two in (True, False):
+            solvers.TWO_KERNEL = two
+            Z = solvers.padded_empty(A.shape[0], C, torch.float32, "cuda")
+            st = solvers.Stats()
+            solvers.pcg(S, Z, S.rhs, None if eps is None else [eps] * C, solvers.jacobi_M(S), 10_000, st,
+                        target_relres=1e-5, use_graph=graph, zero_start=True)
+            out.append((Z.double().cpu().numpy(), st.iters))
+    finally:
+        solvers.TWO_KERNEL = True
+    (Z2, it2), (Z3, it3) = out
+    assert abs(it2 - it3) <= 1, (it2, it3)
+    Ad = ssp.diags(diag) - A
+    for Zx in (Z2, Z3):
+        rel = np.linalg.norm(rhs - Ad @ Zx, axis=0) / np.linalg.norm(rhs, axis=0)
+        assert rel.max() <= 1e-5 * 1.01, rel.max()
+    np.testing.assert_allclose(Z2, Z3, rtol=0, atol=2e-5 * np.abs(Z3).max())
+
+
+def test_two_kernel_iteration_cap_and_odd_counts():
+    """The two-kernel loop stopped at 1, 2, 3 and 5 iterations (P and AP trade places every
+    iteration): the iterate equals the three-kernel one at the same count, in the device-side loop
+    and in host-driven chunks of 3."""
+    C = 9
+    S, A, diag, rhs = _whole_row_system(C, seed=3)
+    try:
+        for cap in (1, 2, 3, 5):
+            res = []
+            for two in (True, False):
+                solvers.TWO_KERNEL = two
+                for graph in (True, False):
+                    Z = solvers.padded_empty(A.shape[0], C, torch.float32, "cuda")
+                    st = solvers.Stats()
+                    solvers.pcg(S, Z, S.rhs, None, solvers.jacobi_M(S), cap, st, target_relres=1e-9,
+                                use_graph=graph, zero_start=True, check_every=3)
+                    assert st.iters == cap
+                    res.append(Z.double().cpu().numpy())
+            for Zx in res[1:]:
+                np.testing.assert_allclose(Zx, res[0], rtol=0, atol=1e-5 * np.abs(res[0]).max())
+    finally:
+        solvers.TWO_KERNEL = True
+
+
 @pytest.mark.parametrize("C", [9, 10, 11, 12])
 @pytest.mark.parametrize("graph", [True, False])
 def test_fused_pcg_fp32_whole_rows(C, graph):
