@@ -194,6 +194,24 @@ constexpr int apply_min_blocks() {
 // (R / diag) . AP = pAp), rz_next = sum (R - alpha AP)^2 / diag = alpha^2 q - rz, and
 // beta = rz_next / rz = alpha^2 q / rz - 1. The exact rz_next of the stored residual, summed by the
 // fused sweep, is the one the next alpha uses.
+// Reduce-scatter of 12 per-lane column values (padded to 16 slots) over the warp: lanes 2c and
+// 2c + 1 return column c's sum over the 32 lanes (slot c = lane bits 4..1), lanes of slots >= 12 zero.
+__device__ __forceinline__ float warp_scatter12(const float (&v)[12], int lane) {
+  float v8[8], v4[4], v2[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float lo = v[j], hi = j + 8 < 12 ? v[j + 8] : 0.f;
+    v8[j] = (b4 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b4 ? lo : hi, 16);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v4[j] = (b3 ? v8[j + 4] : v8[j]) + __shfl_xor_sync(0xffffffffu, b3 ? v8[j] : v8[j + 4], 8);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) v2[j] = (b2 ? v4[j + 2] : v4[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v4[j] : v4[j + 2], 4);
+  const float v1 = (b1 ? v2[1] : v2[0]) + __shfl_xor_sync(0xffffffffu, b1 ? v2[0] : v2[1], 2);
+  return v1 + __shfl_xor_sync(0xffffffffu, v1, 1);
+}
+
 template <class T, int VW, int VPL, bool ROW12 = false, bool FUSE = false>
 __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_pcg_apply(ApplyArgs<T> p) {
   using TA = typename T::TA;
@@ -222,10 +240,10 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
     for (int i = 0; i < VW; ++i) dot[k][i] = TD(0);
-  // FUSE: q is summed over the warp's 32 rows after each batch (a reduce-scatter across the lanes:
-  // lanes 2c and 2c + 1 end with column c's sum), so a lane keeps one running q partial instead of
-  // a row's worth
-  float qacc = 0.f;
+  // FUSE: pAp and q are summed over the warp's 32 rows after each batch (warp_scatter12), so a lane
+  // keeps one running partial of each instead of a row's worth: the registers go to a second row in
+  // flight. fp32 sums over 32 rows, accumulated in fp64.
+  double pacc = 0.0, qacc = 0.0;
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long g0 = warp * gpw; g0 < p.n; g0 += nwarps * gpw) {
@@ -234,13 +252,14 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? (FUSE ? 1 : 2) : gather_batch_lean<TA, VW, VPL>()),
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 2 : gather_batch_lean<TA, VW, VPL>()),
                (ROW12 ? kRow12F : kRowVec)>(
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
-    float qv[FUSE ? 12 : 1];  // FUSE: this row's AP^2 / diag per column (0 past C and on invalid lanes)
+    // FUSE: this row's P . AP and AP^2 / diag per column (0 past C and on invalid lanes)
+    float pv_[FUSE ? 12 : 1], qv[FUSE ? 12 : 1];
     if constexpr (FUSE) {
 #pragma unroll
-      for (int c = 0; c < 12; ++c) qv[c] = 0.f;
+      for (int c = 0; c < 12; ++c) pv_[c] = qv[c] = 0.f;
     }
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);
@@ -261,7 +280,8 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
             apv[k][i] = (FUSE && c >= p.C) ? 0.f : d * pv - acc[k][i];
             if (c < p.C) {
               if (!p.ap_row12) p.AP[r * p.ldap + c] = apv[k][i];
-              dot[k][i] += (TD)pv * (TD)apv[k][i];
+              if constexpr (FUSE) pv_[c] = pv * apv[k][i];
+              else dot[k][i] += (TD)pv * (TD)apv[k][i];
             }
           }
         if (p.ap_row12) store_row12(p.AP + r * p.ldap, apv);
@@ -292,25 +312,14 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
         }
       }
     }
-    if constexpr (FUSE) {  // reduce-scatter of the 12 (padded to 16) column values over the warp
-      float v8[8], v4[4], v2[2], v1;
-      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float lo = qv[j], hi = j + 8 < 12 ? qv[j + 8] : 0.f;
-        v8[j] = (b4 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b4 ? lo : hi, 16);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) v4[j] = (b3 ? v8[j + 4] : v8[j]) + __shfl_xor_sync(0xffffffffu, b3 ? v8[j] : v8[j + 4], 8);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) v2[j] = (b2 ? v4[j + 2] : v4[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v4[j] : v4[j + 2], 4);
-      v1 = (b1 ? v2[1] : v2[0]) + __shfl_xor_sync(0xffffffffu, b1 ? v2[0] : v2[1], 2);
-      qacc += v1 + __shfl_xor_sync(0xffffffffu, v1, 1);
+    if constexpr (FUSE) {
+      pacc += (double)warp_scatter12(pv_, lane);
+      qacc += (double)warp_scatter12(qv, lane);
     }
   }
   // lanes sharing a vector lane (same cl) hold the same columns: reduce over the other bits, in fp64
   constexpr int NQ = FUSE ? 2 : 1;  // pAp, and q when fused
-  {
+  if constexpr (!FUSE) {
     double dsum[VPL][VW];
 #pragma unroll
     for (int k = 0; k < VPL; ++k)
@@ -334,9 +343,12 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
       }
     }
   }
-  if constexpr (FUSE) {  // lanes 2c hold the warp's q for column c (slot of lane bits 4..1)
+  if constexpr (FUSE) {  // lanes 2c hold the warp's pAp and q of column c (slot of lane bits 4..1)
     const int slot = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
-    if ((lane & 1) == 0 && slot < p.C) sm[wid][p.C + slot] = (double)qacc;
+    if ((lane & 1) == 0 && slot < p.C) {
+      sm[wid][slot] = pacc;
+      sm[wid][p.C + slot] = qacc;
+    }
   }
   __syncthreads();
   for (int c = threadIdx.x; c < NQ * p.C; c += blockDim.x) {
