@@ -344,6 +344,7 @@ def pcg_roofline(events, nnz, peaks, traffic_file, steady=None):
     the calls' total device time / their iterations (so it also carries each call's start, stop
     checks and recheck, a conservative figure). steady: (ms per iteration, iterations) of
     pcg_steady, reported beside it."""
+    from dynlplus_b200 import solvers
     ms = sum(s.elapsed_time(e) for s, e, _, _, _ in events)
     iters = sum(it for _, _, it, _, _ in events)
     if not iters:
@@ -356,10 +357,10 @@ def pcg_roofline(events, nnz, peaks, traffic_file, steady=None):
     traffic, tsrc = None, None
     if os.path.exists(traffic_file):
         tr = json.load(open(traffic_file))
-        if tr.get("n") == n and tr.get("C") == C:
+        if tr.get("n") == n and tr.get("C") == C and ("k_pcg_fused" in tr.get("per_kernel", {})) == solvers.TWO_KERNEL:
             traffic, tsrc = tr.get("dram_bytes_per_iteration"), tr.get("source")
-    return {"bound": "hbm", "kernel": "fused PCG iteration: k_pcg_apply + k_pcg_update + k_pcg_dir "
-                                      "(fp32, C=%d, compact CSR of W_UU, nnz=%d)" % (C, nnz),
+    ks = "k_pcg_apply + k_pcg_fused" if solvers.TWO_KERNEL else "k_pcg_apply + k_pcg_update + k_pcg_dir"
+    return {"bound": "hbm", "kernel": "PCG iteration: %s (fp32, C=%d, compact CSR of W_UU, nnz=%d)" % (ks, C, nnz),
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback",
             "traffic": traffic, "traffic_source": tsrc, "algorithmic_bytes_per_iteration": int(algo),

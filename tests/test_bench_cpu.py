@@ -20,7 +20,7 @@ def test_traffic_file_is_consistent():
     t = json.load(open(p))
     assert (t["n"], t["C"]) == (1_000_000, 9)
     assert t["dram_bytes_per_iteration"] == sum(t["per_kernel"].values())
-    assert set(t["per_kernel"]) == {"k_pcg_apply", "k_pcg_update", "k_pcg_dir"}
+    assert set(t["per_kernel"]) == {"k_pcg_apply", "k_pcg_fused"}  # the two-kernel iteration
 
 
 def test_profiling_flags_parse():
