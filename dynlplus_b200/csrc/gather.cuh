@@ -131,6 +131,15 @@ __device__ __forceinline__ bool load_row10d(const double *__restrict__ xr, doubl
   return hi;
 }
 
+// A bf16 row of 16 values (32 bytes, 32-byte aligned) in one 256-bit load, kept packed: word j
+// holds columns 2j (low half) and 2j + 1 (high half). L2 evict-last as in load_row12.
+__device__ __forceinline__ void load_row16h(const void *__restrict__ xr, uint32_t (&q)[8]) {
+  const uint64_t pol = l2_evict_last();
+  asm("ld.global.nc.L2::cache_hint.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
+      : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7])
+      : "l"(xr), "l"(pol));
+}
+
 // Column c (0-9) of a row read by load_row10d.
 __device__ __forceinline__ double row10_col(const double (&raw)[5][2], bool hi, int c) {
   const int fh = c < 2 ? 8 + c : c - 2;  // c is a compile-time index at every (unrolled) call
@@ -192,7 +201,9 @@ __device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {
 // row); kRow12F the two loads of load_row12 (fp32 rows of three 16-byte vectors: VW 4, VPL 3) and
 // kRow10D the three loads of load_row10d (fp64 rows of five: VW 2, VPL 5), each with the whole row
 // held by one lane (the caller guarantees LV == 1).
-enum RowPath : int { kRowVec = 0, kRow12F = 1, kRow10D = 2 };
+// kRow16H reads a bf16 row of 16 values (two 16-byte vectors: VW 8, VPL 2) in one 256-bit load from a
+// 32-byte aligned address and widens it to fp32 at the multiply-adds.
+enum RowPath : int { kRowVec = 0, kRow12F = 1, kRow10D = 2, kRow16H = 3 };
 
 template <typename TW, typename TX, typename TA, int VW, int VPL, int U = gather_batch_wide<TA, VW, VPL>(),
           int ROW = kRowVec>
@@ -205,6 +216,9 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
   static_assert(ROW != kRow10D ||
                     (std::is_same<TX, double>::value && std::is_same<TA, double>::value && VW == 2 && VPL == 5),
                 "the three-load path gathers fp64 rows of five 16-byte vectors");
+  static_assert(ROW != kRow16H ||
+                    (std::is_same<TX, bf16>::value && std::is_same<TA, float>::value && VW == 8 && VPL == 2),
+                "the one-load path gathers bf16 rows of two 16-byte vectors");
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
 #pragma unroll
@@ -218,6 +232,28 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
       v[u] = j < end ? ld_stream(col + j) : -1;
       wv[u] = j < end ? cvt<TA>(ld_stream(w + j)) : TA(0);
     }
+    if constexpr (ROW == kRow16H) {
+      uint32_t q[U][8];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (v[u] >= 0) {
+          load_row16h(X + (long long)v[u] * ldx, q[u]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) q[u][k] = 0u;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {  // bf16 -> fp32 widening is a 16-bit shift of the bit pattern
+          const int c = 2 * k;
+          acc[c / 8][c % 8] = fmaa(wv[u], __uint_as_float(q[u][k] << 16), acc[c / 8][c % 8]);
+          acc[(c + 1) / 8][(c + 1) % 8] = fmaa(wv[u], __uint_as_float(q[u][k] & 0xffff0000u),
+                                               acc[(c + 1) / 8][(c + 1) % 8]);
+        }
+      continue;
+    }
     TA t[U][VPL][VW];
     bool hi[U];
 #pragma unroll
@@ -227,7 +263,7 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
       if constexpr (ROW != kRowVec) {
         if (v[u] >= 0) {
           if constexpr (ROW == kRow12F) hi[u] = load_row12(xr, t[u]);
-          else hi[u] = load_row10d(xr, t[u]);
+          else if constexpr (ROW == kRow10D) hi[u] = load_row10d(xr, t[u]);
         } else {
 #pragma unroll
           for (int k = 0; k < VPL; ++k)

@@ -100,7 +100,8 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, TX, TA, VW, VPL, (ROW == kRow12F ? 2 : gather_batch_wide<TA, VW, VPL>()), ROW>(
+    gather_row<typename T::TW, TX, TA, VW, VPL,
+               (ROW == kRow12F ? 2 : ROW == kRow16H ? 4 : gather_batch_wide<TA, VW, VPL>()), ROW>(
         p.col, p.w, p.X, p.ldx, beg, end, es, ES, cl, LV, NV, G, acc);
     if constexpr (ROW == kRow10D) {
       if (valid && es == 0) {  // same arithmetic, in the same order, as the per-column epilogue below
@@ -177,9 +178,18 @@ static int launch_spmm_vw(const SpmmArgs<T> &a, int VPL, dlp_stream_t s) {
       VW == 4 && std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value;
   constexpr bool kRow10 =
       VW == 2 && std::is_same<typename T::TX, double>::value && std::is_same<typename T::TA, double>::value;
+  constexpr bool kRow16 =
+      VW == 8 && std::is_same<typename T::TX, bf16>::value && std::is_same<typename T::TA, float>::value;
   switch (VPL) {
     case 1: k_spmm<T, VW, 1><<<grid, kThreads, 0, (cudaStream_t)s>>>(a); break;
-    case 2: k_spmm<T, VW, 2><<<grid, kThreads, 0, (cudaStream_t)s>>>(a); break;
+    case 2:
+      // bf16 rows of 16 values held whole by one lane: one 256-bit load per gathered row
+      if (kRow16 && a.LV == 1 && (uintptr_t)a.X % 32 == 0 && (a.ldx * 2) % 32 == 0) {
+        k_spmm<T, VW, 2, (kRow16 ? kRow16H : kRowVec)><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
+      } else {
+        k_spmm<T, VW, 2><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
+      }
+      break;
     case 3:
       if (kRow12 && a.LV == 1) {  // fp32 12-float rows held whole by one lane: two loads per row
         k_spmm<T, VW, 3, (kRow12 ? kRow12F : kRowVec)><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);

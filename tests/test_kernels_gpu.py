@@ -284,3 +284,31 @@ def test_invalid_arguments_raise():
     # 300 columns fit (75 vectors) and are exact
     X = np.random.RandomState(0).rand(4, 300).astype(np.float32)
     np.testing.assert_allclose(kernels.spmm_axpy(CSR.from_scipy(A), T(X)).cpu().numpy(), A @ X, rtol=1e-6)
+
+
+@pytest.mark.parametrize("C", [3, 9, 16])
+def test_spmm_lowp_whole_bf16_rows(C):
+    """dlp_spmm_lowp, the SpMM of the BF16 sweeps: Y = a*X_own - W X_lo with bf16 weights and gathered
+    rows and fp32 accumulation, own row and output. Rows of 16 bf16 values (ld 16, 32 bytes) are
+    gathered whole by one 256-bit load; against the same product in fp64 of the bf16 values."""
+    from dynlplus_b200.backend import ld, ptr, stream
+    from dynlplus_b200.solvers import padded_empty
+    rs = np.random.RandomState(C)
+    n = 5000
+    A = O.symmetric_from_pairs(rs.randint(0, n, 60000), rs.randint(0, n, 60000), rs.rand(60000) + 0.1, n,
+                               np.float32)
+    W = CSR.from_scipy(A, dtype=torch.float32)
+    wb = W.data.to(torch.bfloat16)
+    X = T(rs.rand(n, C) - 0.5, torch.float32)
+    Xo = padded_empty(n, C, torch.float32, "cuda")
+    Xo.copy_(X)
+    Xl = torch.zeros((n, 16), dtype=torch.bfloat16, device="cuda")[:, :C]  # 32-byte rows
+    Xl.copy_(X)
+    a = T(rs.rand(n) + 1.0, torch.float32)
+    Y = torch.empty((n, C), dtype=torch.float32, device="cuda")
+    for rep in range(2):
+        _lib.call("dlp_spmm_lowp", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(wb), n, C, ptr(Xl), ld(Xl), ptr(Xo),
+                  ld(Xo), ptr(a), 1.0, -1.0, ptr(Y), ld(Y), 0, W.nnz / n, stream())
+    Ab = ssp.csr_matrix((wb.float().cpu().numpy().astype(np.float64), A.indices, A.indptr), shape=A.shape)
+    want = a.double().cpu().numpy()[:, None] * X.double().cpu().numpy() - Ab @ Xl.float().double().cpu().numpy()
+    np.testing.assert_allclose(Y.double().cpu().numpy(), want, rtol=1e-5, atol=1e-5 * np.abs(want).max())
