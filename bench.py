@@ -221,7 +221,7 @@ def spmm_roofline(es, C, peaks):
     X = solvers.padded_empty(n, C, torch.float32, es.dev)
     X.copy_(torch.rand((n, C), device=es.dev))
     a = es.diag32
-    Y = torch.empty((n, C), dtype=torch.float32, device=es.dev)
+    Y = solvers.padded_empty(n, C, torch.float32, es.dev)  # 16-byte rows: whole-row stores, as the PCG's AP
     for _ in range(3):
         kernels.spmm_axpy(G, X, a=a, b=-1.0, out=Y)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=es.dev)
@@ -276,7 +276,7 @@ def spmm_roofline(es, C, peaks):
                       "and output, C=%d, ld=%d)" % (C, Xb.stride(0)),
             "achieved": algo_lo / (ms_lo * 1e-3) / 1e9, "frac": algo_lo / (ms_lo * 1e-3) / 1e9 / (peaks.get("hbm_gbs") or 6650.0),
             "algorithmic_bytes": int(algo_lo), "ms_per_launch": ms_lo}
-    return {"bound": "hbm", "kernel": "k_spmm (apply_A form, fp32, C=%d, ld=%d, compact CSR of W_UU)" % (C, X.stride(0)),
+    return {"bound": "hbm", "kernel": "k_spmm (apply_A form, fp32, C=%d, ld=%d for X and Y, compact CSR of W_UU)" % (C, X.stride(0)),
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback",
             "algorithmic_bytes": int(algo), "ms_per_launch": ms, "ms_per_launch_after_l2_flush": float(np.mean(cold)),

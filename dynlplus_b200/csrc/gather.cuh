@@ -175,6 +175,43 @@ __device__ __forceinline__ void store_row10d(double *yr, const double (&v)[10]) 
 
 // Store counterpart of load_row12: the 12 values v (columns 0-11) of a row at a 16-byte aligned
 // address in one 256-bit store (the 32-byte aligned half) and one 128-bit store.
+// Column c (0-11) of a row read by load_row12.
+__device__ __forceinline__ float row12_col(const float (&raw)[3][4], bool hi, int c) {
+  const int k = c / 4, i = c % 4;
+  return hi ? (k == 0 ? raw[2][i] : k == 1 ? raw[0][i] : raw[1][i]) : (k == 0 ? raw[0][i] : k == 1 ? raw[1][i] : raw[2][i]);
+}
+
+// The first C (9-12) values v of an fp32 row at a 16-byte aligned address, and nothing past them:
+// a 32-byte aligned run of 8 in one 256-bit store, 16-byte runs in 128-bit stores, the rest
+// scalar (C = 9: two stores when the row starts on a 32-byte boundary, three otherwise).
+__device__ __forceinline__ void store_row_exact12(float *yr, const float (&v)[12], int C) {
+  const bool hi = ((uintptr_t)yr & 16u) != 0;
+  if (!hi) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(yr), "f"(v[0]), "f"(v[1]),
+                 "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+    if (C == 12) {
+      *reinterpret_cast<float4 *>(yr + 8) = make_float4(v[8], v[9], v[10], v[11]);
+    } else {
+#pragma unroll
+      for (int c = 8; c < 11; ++c)
+        if (c < C) yr[c] = v[c];
+    }
+  } else {
+    *reinterpret_cast<float4 *>(yr) = make_float4(v[0], v[1], v[2], v[3]);
+    if (C == 12) {
+      asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(yr + 4), "f"(v[4]), "f"(v[5]),
+                   "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11])
+                   : "memory");
+    } else {
+      *reinterpret_cast<float4 *>(yr + 4) = make_float4(v[4], v[5], v[6], v[7]);
+#pragma unroll
+      for (int c = 8; c < 11; ++c)
+        if (c < C) yr[c] = v[c];
+    }
+  }
+}
+
 __device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {
   const bool hi = ((uintptr_t)yr & 16u) != 0;
   float *p8 = yr + (hi ? 4 : 0);

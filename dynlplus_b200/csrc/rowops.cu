@@ -75,6 +75,10 @@ struct SpmmArgs {
   // written in three or four vector stores (exactly its C values) when their rows are 16-byte
   // aligned and hold 10 values
   int own10, rhs10, y10;
+  // kRow12F epilogue: the own row is read whole (two loads) when its rows are 16-byte aligned and
+  // hold 12 values, and the Y row is written in two or three vector stores (exactly its C values)
+  // when its rows start on 16-byte boundaries
+  int own12, y12;
 };
 
 // ROW as in gather_row. kRow12F runs with two rows in flight per lane (measured on B200 at n = 1M,
@@ -145,6 +149,45 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
         }
       }
       continue;
+    }
+    if constexpr (ROW == kRow12F || ROW == kRow16H) {
+      if (valid && es == 0 && (p.own12 || p.y12)) {  // the per-column arithmetic below, whole rows
+        const long long orow = p.compact ? gi : (long long)r;
+        const float av = p.a ? (float)p.alpha * (float)p.a[r] : 0.f;
+        float yv[12];
+#pragma unroll
+        for (int c = 0; c < 12; ++c) yv[c] = (float)p.b * acc[c / VW][c % VW];
+        if (p.a) {
+          if (p.own12) {
+            float xo[3][4];
+            const float *orow_x;  // the fp32 own row (the bf16 form reads it from Xo)
+            if constexpr (ROW == kRow16H) orow_x = (const float *)p.Xo + (long long)r * p.ldxo;
+            else orow_x = p.Xo ? (const float *)p.Xo + (long long)r * p.ldxo : (const float *)p.X + (long long)r * p.ldx;
+            const bool hx = load_row12(orow_x, xo);
+#pragma unroll
+            for (int c = 0; c < 12; ++c) yv[c] = fmaa(av, row12_col(xo, hx, c), yv[c]);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 12; ++c)
+              if (c < p.C)
+                yv[c] = fmaa(av, p.Xo ? (float)p.Xo[(long long)r * p.ldxo + c] : cvt<float>(p.X[(long long)r * p.ldx + c]),
+                             yv[c]);
+          }
+        }
+        if (p.rhs) {
+#pragma unroll
+          for (int c = 0; c < 12; ++c)
+            if (c < p.C) yv[c] += (float)p.cr * (float)p.rhs[(long long)r * p.ldr + c];
+        }
+        if (p.y12) {
+          store_row_exact12((float *)(p.Y + orow * p.ldy), yv, p.C);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 12; ++c)
+            if (c < p.C) p.Y[orow * p.ldy + c] = yv[c];
+        }
+        continue;
+      }
     }
     if (valid && es == 0) {
       const long long orow = p.compact ? gi : (long long)r;
@@ -227,7 +270,19 @@ static int run_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col
   }
   SpmmArgs<T> p{rbeg, rend, col, (const typename T::TW *)w, n_rows, rows, C, (const typename T::TX *)X, ldx,
                 (const typename T::TV *)a, alpha, b, (const typename T::TV *)RHS, ldr, cr,
-                (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV, (const typename T::TV *)Xo, ldxo, 0, 0, 0};
+                (typename T::TY *)Y, ldy, compact, L.G, L.LV, L.NV, (const typename T::TV *)Xo, ldxo, 0, 0, 0,
+                0, 0};
+  const bool f32_12 = std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value &&
+                      L.VW == 4 && L.VPL == 3 && L.LV == 1 && C >= 9;
+  const bool bf16_16 = std::is_same<typename T::TX, bf16>::value && std::is_same<typename T::TA, float>::value &&
+                       L.VW == 8 && L.VPL == 2 && L.LV == 1 && C >= 9 && C <= 12;
+  if (std::is_same<typename T::TY, float>::value && std::is_same<typename T::TV, float>::value && (f32_12 || bf16_16)) {
+    // the kRow12F / kRow16H layouts (launch_spmm_vw): whole-row epilogue (fp32 own row and output)
+    // where the rows allow it
+    auto rows12 = [](const void *q, int64_t ldq) { return q && (uintptr_t)q % 16 == 0 && ldq % 4 == 0 && ldq >= 12; };
+    p.own12 = Xo ? rows12(Xo, ldxo) : (f32_12 && rows12(X, ldx));
+    p.y12 = Y && (uintptr_t)Y % 16 == 0 && ldy % 4 == 0;
+  }
   if (L.VPL == 5 && L.LV == 1) {  // the kRow10D layout chosen above: whole-row epilogue where aligned
     auto rows10 = [](const void *q, int64_t ldq) { return q && (uintptr_t)q % 16 == 0 && ldq % 2 == 0 && ldq >= 10; };
     p.own10 = Xo ? rows10(Xo, ldxo) : 1;

@@ -305,10 +305,53 @@ def test_spmm_lowp_whole_bf16_rows(C):
     Xl = torch.zeros((n, 16), dtype=torch.bfloat16, device="cuda")[:, :C]  # 32-byte rows
     Xl.copy_(X)
     a = T(rs.rand(n) + 1.0, torch.float32)
-    Y = torch.empty((n, C), dtype=torch.float32, device="cuda")
-    for rep in range(2):
-        _lib.call("dlp_spmm_lowp", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(wb), n, C, ptr(Xl), ld(Xl), ptr(Xo),
-                  ld(Xo), ptr(a), 1.0, -1.0, ptr(Y), ld(Y), 0, W.nnz / n, stream())
     Ab = ssp.csr_matrix((wb.float().cpu().numpy().astype(np.float64), A.indices, A.indptr), shape=A.shape)
     want = a.double().cpu().numpy()[:, None] * X.double().cpu().numpy() - Ab @ Xl.float().double().cpu().numpy()
-    np.testing.assert_allclose(Y.double().cpu().numpy(), want, rtol=1e-5, atol=1e-5 * np.abs(want).max())
+    buf = torch.full((n, 16), -7.0, dtype=torch.float32, device="cuda")  # output rows of 16-byte pitch
+    for Y in (torch.empty((n, C), dtype=torch.float32, device="cuda"), buf[:, :C]):
+        for rep in range(2):
+            _lib.call("dlp_spmm_lowp", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(wb), n, C, ptr(Xl), ld(Xl),
+                      ptr(Xo), ld(Xo), ptr(a), 1.0, -1.0, ptr(Y), ld(Y), 0, W.nnz / n, stream())
+        np.testing.assert_allclose(Y.double().cpu().numpy(), want, rtol=1e-5, atol=1e-5 * np.abs(want).max())
+    assert (buf[:, C:] == -7.0).all()
+
+
+@pytest.mark.parametrize("C", [9, 10, 11, 12])
+@pytest.mark.parametrize("ld_x,ld_y", [(12, 12), (16, 16), (12, 0), (12, 13)])
+def test_spmm_fp32_whole_row_epilogue(C, ld_x, ld_y):
+    """fp32 rows of 9-12 values gathered whole (two loads per row): the own row of the diagonal term
+    read whole and the output written in vector stores of exactly its C values where the rows are
+    16-byte aligned (ld 0 = unpadded, odd ld = unaligned rows), against numpy: full rows, a row subset
+    in place, compact rows. Columns of the output beyond C keep their values; the results are the
+    same values as the per-column epilogue's (same FMAs in the same order)."""
+    rs = np.random.RandomState(C * 100 + ld_x + ld_y)
+    n = 3001
+    A = O.symmetric_from_pairs(rs.randint(0, n, 30000), rs.randint(0, n, 30000), rs.rand(30000), n, np.float32)
+    W = CSR.from_scipy(A, dtype=torch.float32)
+    X, d = rs.rand(n, C).astype(np.float32), (rs.rand(n) + 1).astype(np.float32)
+    Xd = padded(X, ld_x, torch.float32)  # NaN in the padding: never read into a result
+    want = d[:, None].astype(np.float64) * X - A.astype(np.float64) @ X.astype(np.float64)
+
+    def out_buf():
+        if not ld_y:
+            return torch.zeros((n, C), dtype=torch.float32, device="cuda")
+        buf = torch.full((n, ld_y), -7.0, dtype=torch.float32, device="cuda")
+        buf[:, :C] = 0.0
+        return buf[:, :C]
+
+    Y = out_buf()
+    kernels.spmm_axpy(W, Xd, a=T(d), b=-1.0, out=Y)
+    np.testing.assert_allclose(Y.cpu().numpy(), want, rtol=1e-5, atol=1e-5 * np.abs(want).max())
+    if ld_y:
+        assert (Y.as_strided((n, ld_y), (ld_y, 1))[:, C:] == -7.0).all()
+    Yu = kernels.spmm_axpy(W, T(X), a=T(d), b=-1.0)  # unpadded X and Y: the per-column epilogue
+    assert torch.equal(Y, Yu) or np.abs(Y.cpu().numpy() - Yu.cpu().numpy()).max() <= 1e-5 * np.abs(want).max()
+    Q = np.sort(rs.choice(n, 400, replace=False)).astype(np.int32)
+    Y = out_buf()
+    kernels.spmm_axpy(W, Xd, a=T(d), b=-1.0, out=Y, rows=T(Q))
+    Yn = Y.cpu().numpy()
+    np.testing.assert_allclose(Yn[Q], want[Q], rtol=1e-5, atol=1e-5 * np.abs(want).max())
+    assert (Yn[np.setdiff1d(np.arange(n), Q)] == 0).all()
+    Yc = kernels.spmm_axpy(W, Xd, rows=T(Q), compact=True)
+    np.testing.assert_allclose(Yc.cpu().numpy(), (A.astype(np.float64) @ X.astype(np.float64))[Q], rtol=1e-5,
+                               atol=1e-5 * np.abs(want).max())
