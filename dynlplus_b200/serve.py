@@ -19,7 +19,8 @@ of its kind, in arrival order, while they fit its slot (edges per update solve, 
 batch, instances per fresh batch) and the memory the budget has free, reserves that memory, and
 returns it when the batch completes; a request that does not fit waits for the next slot. A
 request larger than the whole budget is refused. Each kind has its own worker thread and CUDA
-stream, so their device work overlaps; libdlp calls release the GIL.
+stream, so their device work overlaps (updates and queries on high-priority streams, fresh solves on a
+normal one); libdlp calls release the GIL.
 
 Precision. The continuous loop is mixed precision: FP32 (or BF16, lowp=True) sweeps with refinement
 against an FP64 residual. mode="sequential" serves one request at a time in arrival order; by
@@ -31,6 +32,7 @@ its submit and completion times (p50/p99 latency).
 from __future__ import annotations
 
 import queue
+import sys
 import threading
 import time
 from concurrent.futures import Future
@@ -161,12 +163,13 @@ def take_batch(q, first, limit=None, cost=None, budget=None, size=None, slot=Non
 class Server:
     def __init__(self, ds, labeled, *, dtype="float32", target_relres=1e-6, tol=1e-3, hbm_budget_bytes=None,
                  max_fresh_batch=64, update_slot_edges=200_000, query_slot_ids=4_000_000, mode="continuous",
-                 lowp=False, precision=None):
+                 lowp=False, precision=None, switch_interval_s=0.0005):
         """mode="continuous": the continuous-batching loop described above; mode="sequential": one
         request at a time in arrival order. precision="mixed" (the default of the continuous loop):
         FP32 sweeps (lowp: BF16 gathers in the update solves' sweeps) with refinement against the
         FP64 residual; precision="fp32" (the default of the sequential mode): the plain FP32 path. The
-        slots cap the edges patched before one update solve and the ids of one query batch."""
+        slots cap the edges patched before one update solve and the ids of one query batch.
+        switch_interval_s: the interpreter's thread switch interval while the server runs."""
         if mode not in ("continuous", "sequential"):
             raise ValueError(f"unknown serving mode {mode!r}")
         precision = precision or ("mixed" if mode == "continuous" else "fp32")
@@ -193,7 +196,9 @@ class Server:
         if seq:  # one queue for every kind: arrival order, one request at a time
             one = queue.Queue()
             self._q = {k: one for k in self._q}
-        self._streams = {k: torch.cuda.Stream() for k in self._q}
+        # updates and queries on high-priority streams: their kernels go ahead of a fresh solve's when
+        # both are ready, so a large fresh batch does not hold the resident graph's answers back
+        self._streams = {k: torch.cuda.Stream(priority=0 if k == "fresh" else -1) for k in self._q}
         self._stop = threading.Event()
         self._lock = threading.Lock()
         self._carry = {}  # per worker: the queued request that heads its next batch
@@ -201,6 +206,11 @@ class Server:
         kinds = ["all"] if seq else list(self._q)
         self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in kinds]
         self._dev = torch.cuda.current_device()
+        # the workers hand the interpreter lock to each other at every device wait; the default 5 ms
+        # switch interval would let a worker busy with host-side bookkeeping hold a waiting one back
+        # for that long at each of its host reads (restored by close)
+        self._switch = sys.getswitchinterval()
+        sys.setswitchinterval(min(self._switch, switch_interval_s))
         for t in self._threads:
             t.start()
 
@@ -220,6 +230,7 @@ class Server:
         """Stops the workers after their current batch; requests still waiting fail with
         RuntimeError("server closed")."""
         self._stop.set()
+        sys.setswitchinterval(self._switch)
         queues = {id(q): q for q in self._q.values()}.values()
         for q in queues:
             q.put(None)
