@@ -60,6 +60,8 @@ def parse(argv=None):
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch the PCG kernels one by one instead of as a CUDA graph (for kernel profilers)")
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
+    ap.add_argument("--no-class-sum", action="store_true",
+                    help="edge-stream: corrections solve all k class columns (default: k-1 and derive the last)")
     ap.add_argument("--three-kernel", action="store_true",
                     help="edge-stream: the three-kernel PCG iteration instead of the two-kernel one")
     ap.add_argument("--workload", default="edge-stream",
@@ -80,7 +82,8 @@ def config(a):
     return {"workload": workload_name(a), "n": a.n, "mean_degree": a.deg, "k": a.k, "label_frac": a.label_frac,
             "batch_updates": a.batch, "insert_frac": 0.5, "target_relres": a.target_relres, "tol": a.tol,
             "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas",
-            "pcg_iteration": "three kernels" if a.three_kernel else "two kernels (fp32 whole rows)"}
+            "pcg_iteration": "three kernels" if a.three_kernel else "two kernels (fp32 whole rows)",
+            "class_sum": not a.no_class_sum}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -313,13 +316,18 @@ def pcg_iteration_bytes(n, nnz, C, s=4):
 
 
 def pcg_steady(es, C, iters=100):
-    """The PCG iteration in steady state on the stream's final system: one dlp_pcg call from zero
-    that runs `iters` iterations to its cap (a target it cannot meet), timed with CUDA events on the
-    launching stream, so the per-call start and host reads weigh 1/iters of it."""
+    """The PCG iteration in steady state on the stream's final system with the C columns of the timed
+    solves: one dlp_pcg call from zero that runs `iters` iterations to its cap (a target it cannot
+    meet), timed with CUDA events on the launching stream, so the per-call start and host reads
+    weigh 1/iters of it."""
     import torch
     from dynlplus_b200 import solvers
     S = es.system.astype(torch.float32)
-    rhs = S.rhs_h.to(torch.float32).contiguous()
+    rhs = S.rhs_h.to(torch.float32)
+    if C < rhs.shape[1]:  # the class-sum corrections: all class columns but the last, and h
+        k = rhs.shape[1] - 1
+        rhs = torch.cat([rhs[:, : k - 1], rhs[:, k:]], dim=1)
+    rhs = rhs.contiguous()
     Z = solvers.padded_empty(rhs.shape[0], rhs.shape[1], torch.float32, rhs.device, fill=0.0)
     rn = [1.0] * rhs.shape[1]
     ev, solvers.PCG_EVENTS = solvers.PCG_EVENTS, None
@@ -396,7 +404,7 @@ def ours(a):
     lab = graphs.label_mask(a.n, a.label_frac, seed=seed)
     es = stream.EdgeStream(ds, lab, components=True)  # component ids after every batch (side stream)
     solver = solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres,
-                                   full_every=16, lowp=a.lowp)
+                                   full_every=16, lowp=a.lowp, class_sum=not a.no_class_sum)
     solver.solve(es.system)  # the static solve of the initial graph (untimed)
     A0 = ds.A.to_scipy() if (rank == 0 and not a.no_cpu_baseline) else None
     Z0 = solver.Z.cpu().numpy() if A0 is not None else None
@@ -540,7 +548,7 @@ def ours(a):
     if rank == 0:
         roof = pcg_roofline(pcg_events, es.solver_csr().nnz, peaks,
                             os.path.join(ROOT, "profiles", "pcg_iteration_traffic.json"),
-                            steady=pcg_steady(es, a.k + 1))
+                            steady=pcg_steady(es, pcg_events[0][4] if pcg_events else a.k + 1))
         if roof is not None:
             roof["spmm_alone"] = spmm_roofline(es, a.k + 1, peaks)
     cpu = None

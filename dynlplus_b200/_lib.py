@@ -56,6 +56,8 @@ SIGNATURES: dict[str, tuple[str, object]] = {
     "dlp_graph_delete": ("ipppppppipppippppppp", ct.c_int),
     "dlp_graph_insert_workspace_bytes": ("i", ct.c_size_t),
     "dlp_graph_insert": ("ipppppppppipppipppppppzp", ct.c_int),
+    "dlp_class_sum_rhs": ("iipqppqp", ct.c_int),
+    "dlp_class_sum_update": ("iipqppqpp", ct.c_int),
     "dlp_predict_workspace_bytes": ("i", ct.c_size_t),
     "dlp_predict": ("iipqiippppppzp", ct.c_int),
     "dlp_label_update": ("pidpppppipppp", ct.c_int),

@@ -131,6 +131,21 @@ __device__ __forceinline__ bool load_row10d(const double *__restrict__ xr, doubl
   return hi;
 }
 
+// An fp32 row of 8 values at a 32-byte aligned address in one 256-bit load (L2 evict-last as in
+// load_row12), and its store counterpart.
+__device__ __forceinline__ void load_row8(const float *__restrict__ xr, float (&raw)[2][4]) {
+  const uint64_t pol = l2_evict_last();
+  asm("ld.global.nc.L2::cache_hint.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
+      : "=f"(raw[0][0]), "=f"(raw[0][1]), "=f"(raw[0][2]), "=f"(raw[0][3]), "=f"(raw[1][0]), "=f"(raw[1][1]),
+        "=f"(raw[1][2]), "=f"(raw[1][3])
+      : "l"(xr), "l"(pol));
+}
+__device__ __forceinline__ void store_row8(float *yr, const float (&v)[2][4]) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(yr), "f"(v[0][0]), "f"(v[0][1]),
+               "f"(v[0][2]), "f"(v[0][3]), "f"(v[1][0]), "f"(v[1][1]), "f"(v[1][2]), "f"(v[1][3])
+               : "memory");
+}
+
 // A bf16 row of 16 values (32 bytes, 32-byte aligned) in one 256-bit load, kept packed: word j
 // holds columns 2j (low half) and 2j + 1 (high half). L2 evict-last as in load_row12.
 __device__ __forceinline__ void load_row16h(const void *__restrict__ xr, uint32_t (&q)[8]) {
@@ -240,7 +255,9 @@ __device__ __forceinline__ void store_row12(float *yr, const float (&v)[3][4]) {
 // held by one lane (the caller guarantees LV == 1).
 // kRow16H reads a bf16 row of 16 values (two 16-byte vectors: VW 8, VPL 2) in one 256-bit load from a
 // 32-byte aligned address and widens it to fp32 at the multiply-adds.
-enum RowPath : int { kRowVec = 0, kRow12F = 1, kRow10D = 2, kRow16H = 3 };
+// kRow8F reads an fp32 row of 8 values (VW 4, VPL 2) in one 256-bit load from a 32-byte aligned
+// address.
+enum RowPath : int { kRowVec = 0, kRow12F = 1, kRow10D = 2, kRow16H = 3, kRow8F = 4 };
 
 template <typename TW, typename TX, typename TA, int VW, int VPL, int U = gather_batch_wide<TA, VW, VPL>(),
           int ROW = kRowVec>
@@ -253,6 +270,9 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
   static_assert(ROW != kRow10D ||
                     (std::is_same<TX, double>::value && std::is_same<TA, double>::value && VW == 2 && VPL == 5),
                 "the three-load path gathers fp64 rows of five 16-byte vectors");
+  static_assert(ROW != kRow8F ||
+                    (std::is_same<TX, float>::value && std::is_same<TA, float>::value && VW == 4 && VPL == 2),
+                "the one-load path gathers fp32 rows of two 16-byte vectors");
   static_assert(ROW != kRow16H ||
                     (std::is_same<TX, bf16>::value && std::is_same<TA, float>::value && VW == 8 && VPL == 2),
                 "the one-load path gathers bf16 rows of two 16-byte vectors");
@@ -301,6 +321,7 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
         if (v[u] >= 0) {
           if constexpr (ROW == kRow12F) hi[u] = load_row12(xr, t[u]);
           else if constexpr (ROW == kRow10D) hi[u] = load_row10d(xr, t[u]);
+          else if constexpr (ROW == kRow8F) load_row8(xr, t[u]);
         } else {
 #pragma unroll
           for (int k = 0; k < VPL; ++k)

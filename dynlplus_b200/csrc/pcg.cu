@@ -212,7 +212,7 @@ __device__ __forceinline__ float warp_scatter12(const float (&v)[12], int lane) 
   return v1 + __shfl_xor_sync(0xffffffffu, v1, 1);
 }
 
-template <class T, int VW, int VPL, bool ROW12 = false, bool FUSE = false>
+template <class T, int VW, int VPL, int ROWP = kRowVec, bool FUSE = false>
 __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_pcg_apply(ApplyArgs<T> p) {
   using TA = typename T::TA;
   PcgCtl *ctl = p.B.ctl;
@@ -234,7 +234,9 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
   const int es = gl / LV;
   const int ES = G / LV;
   const int gpw = 32 / G;
-  using TD = typename std::conditional<ROW12, float, double>::type;  // a lane's pAp partials
+  constexpr bool WHOLE = ROWP == kRow12F || ROWP == kRow8F;  // one lane holds a whole fp32 row
+  constexpr int NR = ROWP == kRow8F ? 2 : 3;                  // its 16-byte vectors
+  using TD = typename std::conditional<WHOLE, float, double>::type;  // a lane's pAp partials
   TD dot[VPL][VW];
 #pragma unroll
   for (int k = 0; k < VPL; ++k)
@@ -252,8 +254,8 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     const int beg = valid ? p.rbeg[r] : 0;
     const int end = valid ? p.rend[r] : 0;
     TA acc[VPL][VW];
-    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (ROW12 ? 2 : gather_batch_lean<TA, VW, VPL>()),
-               (ROW12 ? kRow12F : kRowVec)>(
+    gather_row<typename T::TW, typename T::TX, TA, VW, VPL, (WHOLE ? 2 : gather_batch_lean<TA, VW, VPL>()),
+               (WHOLE ? ROWP : kRowVec)>(
         p.col, p.w, p.P, p.ldp, beg, end, es, ES, cl, LV, NV, G, acc);
     // FUSE: this row's P . AP and AP^2 / diag per column (0 past C and on invalid lanes)
     float pv_[FUSE ? 12 : 1], qv[FUSE ? 12 : 1];
@@ -263,18 +265,22 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     }
     if (valid && es == 0) {
       const TA d = cvt<TA>(p.diag[r]);
-      if constexpr (ROW12) {
-        // the own row in two loads too (its 48 bytes are 16-byte aligned, as for every gathered row)
-        float pw[3][4];
-        const bool hi = load_row12(p.P + r * p.ldp, pw);
-        float apv[3][4];
+      if constexpr (WHOLE) {
+        // the own row whole too (two loads for 12 floats at a 16-byte boundary, one for 8 at 32)
+        float pw[NR][4];
+        bool hi = false;
+        if constexpr (ROWP == kRow8F) load_row8(p.P + r * p.ldp, pw);
+        else hi = load_row12(p.P + r * p.ldp, pw);
+        float apv[NR][4];
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < NR; ++k)
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int c = k * 4 + i;
-            const float pv = k == 0 ? (hi ? pw[2][i] : pw[0][i]) : k == 1 ? (hi ? pw[0][i] : pw[1][i])
-                                                                        : (hi ? pw[1][i] : pw[2][i]);
+            float pv;
+            if constexpr (ROWP == kRow8F) pv = pw[k][i];
+            else pv = k == 0 ? (hi ? pw[2][i] : pw[0][i]) : k == 1 ? (hi ? pw[0][i] : pw[1][i])
+                                                          : (hi ? pw[1][i] : pw[2][i]);
             // padding columns too when the whole row is stored; zeros there when AP becomes the next
             // direction (FUSE), so the gathered padding stays zero
             apv[k][i] = (FUSE && c >= p.C) ? 0.f : d * pv - acc[k][i];
@@ -284,11 +290,14 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
               else dot[k][i] += (TD)pv * (TD)apv[k][i];
             }
           }
-        if (p.ap_row12) store_row12(p.AP + r * p.ldap, apv);
+        if (p.ap_row12) {
+          if constexpr (ROWP == kRow8F) store_row8(p.AP + r * p.ldap, apv);
+          else store_row12(p.AP + r * p.ldap, apv);
+        }
         if constexpr (FUSE) {
           const float rinv = __frcp_rn((float)d);
 #pragma unroll
-          for (int k = 0; k < 3; ++k)
+          for (int k = 0; k < NR; ++k)
 #pragma unroll
             for (int i = 0; i < 4; ++i)
               if (k * 4 + i < p.C) qv[k * 4 + i] = apv[k][i] * apv[k][i] * rinv;
@@ -900,16 +909,38 @@ static int launch_apply(const PcgProblem &q, const PcgBufs &B, cudaStream_t s, b
     DLP_APPLY_ONE(VW_, 8)                                                               \
     default: return DLP_ERR_INVALID;                                                    \
   }
-  constexpr bool row12 = std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value;
-  if constexpr (FUSE) {
-    if (!(row12 && L.VW == 4 && L.VPL == 3 && L.LV == 1) || q.ldp != q.ldap) return DLP_ERR_INVALID;
-    static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, row12, true>, kThreads);
-    if (launch) k_pcg_apply<T, VWV, 3, row12, true><<<sm_count() * per, kThreads, 0, s>>>(a);
-  } else if (row12 && L.VW == 4 && L.VPL == 3 && L.LV == 1) {
-    // fp32 rows of 12 floats held whole by one lane: the two-load gather (load_row12)
-    static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, row12>, kThreads);
-    if (launch) k_pcg_apply<T, VWV, 3, row12><<<sm_count() * per, kThreads, 0, s>>>(a);
-  } else if (L.VW == 1) {
+  constexpr bool f32 = std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value;
+  // whole fp32 rows held by one lane: 12 floats in two loads (load_row12) or 8 in one (load_row8)
+  const bool w12 = f32 && L.VW == 4 && L.VPL == 3 && L.LV == 1;
+  const bool w8 = f32 && L.VW == 4 && L.VPL == 2 && L.LV == 1 && (uintptr_t)X % 32 == 0 && ldx % 8 == 0 &&
+                  (uintptr_t)q.AP % 32 == 0 && q.ldap % 8 == 0;
+  if (w8) a.ap_row12 = 1;  // the 8-float AP row in one 256-bit store
+  if constexpr (f32) {
+    if constexpr (FUSE) {
+      if (!(w12 || w8) || q.ldp != q.ldap) return DLP_ERR_INVALID;
+      if (w8) {
+        static const int per = resident_per_sm(k_pcg_apply<T, VWV, 2, kRow8F, true>, kThreads);
+        if (launch) k_pcg_apply<T, VWV, 2, kRow8F, true><<<sm_count() * per, kThreads, 0, s>>>(a);
+      } else {
+        static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, kRow12F, true>, kThreads);
+        if (launch) k_pcg_apply<T, VWV, 3, kRow12F, true><<<sm_count() * per, kThreads, 0, s>>>(a);
+      }
+      return launch ? check_launch() : DLP_OK;
+    }
+    if (w12) {
+      static const int per = resident_per_sm(k_pcg_apply<T, VWV, 3, kRow12F>, kThreads);
+      if (launch) k_pcg_apply<T, VWV, 3, kRow12F><<<sm_count() * per, kThreads, 0, s>>>(a);
+      return launch ? check_launch() : DLP_OK;
+    }
+    if (w8) {
+      static const int per = resident_per_sm(k_pcg_apply<T, VWV, 2, kRow8F>, kThreads);
+      if (launch) k_pcg_apply<T, VWV, 2, kRow8F><<<sm_count() * per, kThreads, 0, s>>>(a);
+      return launch ? check_launch() : DLP_OK;
+    }
+  } else if constexpr (FUSE) {
+    return DLP_ERR_INVALID;
+  }
+  if (L.VW == 1) {
     DLP_APPLY_CASE(1)
   } else {
     DLP_APPLY_CASE(VWV)
@@ -1200,7 +1231,9 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
     // the two-kernel iteration where the apply takes the fp32 whole-row path for P and for AP
     Layout L;
     DLP_TRY(choose_layout(C, sizeof(float), P, ldp, 0, avg_deg, &L));
-    q.fused = L.VW == 4 && L.VPL == 3 && L.LV == 1 && ldap >= 12 && ldap % 4 == 0;
+    q.fused = (L.VW == 4 && L.VPL == 3 && L.LV == 1 && ldap >= 12 && ldap % 4 == 0) ||
+              (L.VW == 4 && L.VPL == 2 && L.LV == 1 && ldp % 8 == 0 && (uintptr_t)P % 32 == 0 &&
+               (uintptr_t)AP % 32 == 0);
   }
   PcgBufs B = carve(ws, C);
   B.cancel = cancel_word();

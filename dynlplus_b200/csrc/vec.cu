@@ -137,6 +137,36 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
   return check_launch();
 }
 
+// Class-sum elimination: the right-hand side of a correction without its last class column, and the
+// update that adds the correction and sets the last class to one minus the others. One thread per row
+// (K + 1 <= 16 values), sums in ascending column order in fp64.
+__global__ void k_class_sum_rhs(int32_t n, int32_t K, const double *__restrict__ R, int64_t ldr,
+                                const double *__restrict__ scale, float *__restrict__ E, int64_t lde) {
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+    const double *rr = R + r * ldr;
+    float *er = E + r * lde;
+    for (int j = 0; j < K - 1; ++j) er[j] = (float)(rr[j] / scale[j]);
+    er[K - 1] = (float)(rr[K] / scale[K]);
+  }
+}
+
+__global__ void k_class_sum_update(int32_t n, int32_t K, const float *__restrict__ D, int64_t ldd,
+                                   const double *__restrict__ scale, double *__restrict__ Z, int64_t ldz,
+                                   const uint8_t *__restrict__ solved) {
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+    const float *dr = D + r * ldd;
+    double *zr = Z + r * ldz;
+    double sum = 0.0;
+    for (int j = 0; j < K - 1; ++j) {
+      const double z = zr[j] + (double)dr[j] * scale[j];
+      zr[j] = z;
+      sum += z;
+    }
+    zr[K] = zr[K] + (double)dr[K - 1] * scale[K];
+    zr[K - 1] = (!solved || solved[r]) ? 1.0 - sum : 0.0;
+  }
+}
+
 size_t dlp_predict_workspace_bytes(int32_t n) {
   return ((size_t)(n > 0 ? n : 1) + 255) / 256 * 256 + compact_ws_bytes(n);
 }
@@ -174,6 +204,26 @@ int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, ui
   if (n < 0 || !parent || !vmask || !umask || !in_t || !count) return DLP_ERR_INVALID;
   if (n == 0) return DLP_OK;
   k_ground_update<<<ceil_div_i(n, 256), 256, 0, (cudaStream_t)stream>>>(n, parent, vmask, umask, in_t, count);
+  return check_launch();
+}
+
+int dlp_class_sum_rhs(int32_t n, int32_t K, const double *R, int64_t ldr, const double *scale, float *E,
+                      int64_t lde, dlp_stream_t stream) {
+  if (n < 0 || K < 2 || K > 15 || ldr < K + 1 || lde < K) return DLP_ERR_INVALID;
+  if (n == 0) return DLP_OK;
+  if (!R || !scale || !E) return DLP_ERR_INVALID;
+  const int grid = (int)std::min<long long>(ceil_div_i((long long)n, 256LL), (long long)sm_count() * 8);
+  k_class_sum_rhs<<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, R, ldr, scale, E, lde);
+  return check_launch();
+}
+
+int dlp_class_sum_update(int32_t n, int32_t K, const float *D, int64_t ldd, const double *scale, double *Z,
+                         int64_t ldz, const uint8_t *solved, dlp_stream_t stream) {
+  if (n < 0 || K < 2 || K > 15 || ldd < K || ldz < K + 1) return DLP_ERR_INVALID;
+  if (n == 0) return DLP_OK;
+  if (!D || !scale || !Z) return DLP_ERR_INVALID;
+  const int grid = (int)std::min<long long>(ceil_div_i((long long)n, 256LL), (long long)sm_count() * 8);
+  k_class_sum_update<<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, D, ldd, scale, Z, ldz, solved);
   return check_launch();
 }
 

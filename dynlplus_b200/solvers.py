@@ -548,7 +548,7 @@ class DynLPPlus(Solver):
 
     def __init__(self, n_total, K, dtype="float32", method="auto", tol=1e-3, eps_h=0.05, group="auto",
                  push_frac=0.05, push_budget=30.0, amg_hmax=2000.0, max_iter=100_000, amg_opts=None,
-                 target_relres=None, lowp=False):
+                 target_relres=None, lowp=False, class_sum=False):
         super().__init__(n_total, K, dtype, store_dtype="float64")  # float64 master copy of F and h
         self.method, self.tol, self.eps_h, self.group = method, tol, eps_h, group
         self.push_frac, self.push_budget, self.amg_hmax = push_frac, push_budget, amg_hmax
@@ -558,6 +558,8 @@ class DynLPPlus(Solver):
         # working-precision rounding between the PCG's own residual and the fp64 one)
         self.refine_share = 0.2
         self.lowp = lowp  # SpMM sweeps on bf16 weights and scores (fp32 accumulation)
+        # refinement corrections solve K - 1 class columns and derive the last (_correct_class_sum)
+        self.class_sum = class_sum
         self.name, self.H, self.hmax = f"dynlp+{method}", None, None
 
     def _use_amg(self):
@@ -666,13 +668,16 @@ class DynLPPlus(Solver):
                 # the fp64 residual computed next confirms the correction's stop, so the solve skips
                 # its own recheck on the working-precision residual
                 kw = dict(target_relres=1.0, rhs_norm=allowed + [1e300], confirm=False)
-            Rs = _scratch("ref_Rs", Z64.shape[0], C + 1, self.dtype, dev)
-            _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs), ld(Rs),
-                      code(Rs), stream())
-            D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)  # zeroed by the zero start
-            D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, zero_start=True, **kw)
-            _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(D), ld(D), code(D), ptr(sc), 1, ptr(Z64), ld(Z64),
-                      code(Z64), stream())
+            if kw and self.dtype == torch.float32 and self._class_sum_applies(s64, C):
+                self._correct_class_sum(sw, s64, Z64, R64, sc, scale, eps_c, allowed, kw, ops, st, amg_box)
+            else:
+                Rs = _scratch("ref_Rs", Z64.shape[0], C + 1, self.dtype, dev)
+                _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(R64), ld(R64), code(R64), ptr(sc), 0, ptr(Rs),
+                          ld(Rs), code(Rs), stream())
+                D = _scratch("ref_D", Z64.shape[0], C + 1, self.dtype, dev, padded=True)  # zeroed by the zero start
+                D = self._run(sw, D, Rs, eps_c, ops, st, amg_box, zero_start=True, **kw)
+                _lib.call("dlp_cols_scale", Z64.shape[0], C + 1, ptr(D), ld(D), code(D), ptr(sc), 1, ptr(Z64),
+                          ld(Z64), code(Z64), stream())
             R64, stats = None, None
         if R64 is None:
             R64 = residual(s64, Z64, rhs64)
@@ -681,6 +686,41 @@ class DynLPPlus(Solver):
             hmax, bound = self._bound(rc, h_est)
             _, rel = self._relres_ok(ss, rhs_norm)
         return Z64, R64, hmax, bound, rel
+
+    def _class_sum_applies(self, s64, C):
+        """class_sum: more than one class column, and the system's right-hand sides sum to its
+        grounding on every solved row (sum_c rhs_c = s = A 1, so the scores sum to one there)."""
+        if not (self.class_sum and C > 2):
+            return False
+        key = id(s64.rhs)
+        if getattr(self, "_cs_key", None) != key:
+            d = (s64.rhs.sum(dim=1) - s64.s).abs()
+            if s64.solved is not None:
+                d = torch.where(s64.solved, d, torch.zeros_like(d))
+            self._cs_ok = bool(d.max() <= 1e-9 * max(float(s64.s.abs().max()), 1e-300)) if d.numel() else False
+            self._cs_key = key
+        return self._cs_ok
+
+    def _correct_class_sum(self, sw, s64, Z64, R64, sc, scale, eps_c, allowed, kw, ops, st, amg_box):
+        """The refinement's correction with the last class column eliminated: the scores of a grounded
+        row sum to one, so the PCG solves the first C - 1 class columns and h (C columns: 32-byte rows
+        for C = 8), and the last class is set to one minus the others. Its residual is minus the sum
+        of theirs, so each solved class column aims at the last one's target over sqrt(C - 1) (the
+        fp64 residual of every column, the derived one included, decides the next round)."""
+        C, n, dev = self.C, Z64.shape[0], Z64.device
+        absA = [allowed[c] * scale[c] for c in range(C)]
+        lim = absA[C - 1] / (C - 1) ** 0.5
+        allowed_e = [min(absA[c], lim) / scale[c] for c in range(C - 1)]
+        kw = dict(kw, rhs_norm=allowed_e + [1e300])
+        eps_e = list(eps_c[: C - 1]) + [eps_c[C]]
+        Re = _scratch("ref_Re", n, C, torch.float32, dev)
+        _lib.call("dlp_class_sum_rhs", n, C, ptr(R64), ld(R64), ptr(sc), ptr(Re), ld(Re), stream())
+        De = _scratch("ref_De", n, C, torch.float32, dev, padded=True)  # zeroed by the zero start
+        De = self._run(sw, De, Re, eps_e, ops, st, amg_box, zero_start=True, **kw)
+        sol = None
+        if s64.solved is not None:
+            sol = s64.solved.view(torch.uint8) if s64.solved.dtype == torch.bool else s64.solved.to(torch.uint8)
+        _lib.call("dlp_class_sum_update", n, C, ptr(De), ld(De), ptr(sc), ptr(Z64), ld(Z64), ptr(sol), stream())
 
     def _rhs_h(self, sys):
         if sys.rhs_h is not None:
@@ -743,8 +783,8 @@ class IncrementalLP(DynLPPlus):
     `full_every` batches to bound drift."""
 
     def __init__(self, n_total, K, dtype="float32", tol=1e-3, full_every=16, max_rounds=50_000, method="auto",
-                 **kw):
-        super().__init__(n_total, K, dtype, method=method, tol=tol, **kw)
+                 class_sum=True, **kw):
+        super().__init__(n_total, K, dtype, method=method, tol=tol, class_sum=class_sum, **kw)
         self.name, self.full_every, self.max_rounds = "dynlp+inc", full_every, max_rounds
         self.Z = self.R = None
         self.since_full = 0

@@ -351,6 +351,20 @@ int dlp_park_rows(const int32_t *rows, int32_t nr, const uint8_t *umask, int32_t
 int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype, const double *scale, int32_t op,
                    void *Y, int64_t ldy, int y_dtype, dlp_stream_t stream);
 
+/* Class-sum elimination for the refinement's corrections (no reference counterpart: the reference
+ * solves every class column). On a grounded row the class right-hand sides sum to the grounding
+ * (dynlp/stream.py:163-165: s = sum_c B_c + eta, rhs = B + eta * prior, sum_c prior_c = 1), so the
+ * scores sum to one and the last of the K class columns follows from the others.
+ * dlp_class_sum_rhs: E[:, j] = R[:, j] / scale[j] for j < K - 1 and E[:, K - 1] = R[:, K] / scale[K]
+ * (R: fp64 n x (K + 1), the K classes and h; E: fp32 n x K, the classes but the last, and h).
+ * dlp_class_sum_update: Z[:, j] += D[:, j] scale[j] for j < K - 1, Z[:, K] += D[:, K - 1] scale[K],
+ * then Z[:, K - 1] = 1 - sum_{j < K - 1} Z[:, j] on the rows with solved[r] != 0 (every row when
+ * solved is NULL) and 0 elsewhere (Z: fp64 n x (K + 1); D: fp32 n x K). 2 <= K <= 15. Asynchronous. */
+int dlp_class_sum_rhs(int32_t n, int32_t K, const double *R, int64_t ldr, const double *scale, float *E,
+                      int64_t lde, dlp_stream_t stream);
+int dlp_class_sum_update(int32_t n, int32_t K, const float *D, int64_t ldd, const double *scale, double *Z,
+                         int64_t ldz, const uint8_t *solved, dlp_stream_t stream);
+
 /* Labels of the rows (solvers.predict, dynlp/solvers.py:166-167): binary != 0 (the K == 2 column):
  * label = F[r,0] > 0.5; otherwise the first column of the row's maximum over C columns (numpy
  * argmax). Rows with mask[r] == 0 get -1 (mask NULL: every row). labels[0..n) holds the previous

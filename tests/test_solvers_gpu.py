@@ -87,11 +87,12 @@ def _whole_row_system(C, n=3000, seed=None):
     return S, A, diag, rhs
 
 
-@pytest.mark.parametrize("C", [9, 12])
+@pytest.mark.parametrize("C", [8, 9, 12])
 @pytest.mark.parametrize("graph", [True, False])
 @pytest.mark.parametrize("eps", [None, 1e-6])
 def test_two_kernel_iteration_follows_three_kernel_one(C, graph, eps):
-    """fp32 solves whose rows take the whole-row gather run two kernels per iteration (the SpMM also
+    """fp32 solves whose rows take the whole-row gather (8 floats in one load, 9-12 in two) run two
+    kernels per iteration (the SpMM also
     sums q = sum AP^2/diag and predicts beta; one sweep updates R, Z and the next direction, P and AP
     trading places). Against the three-kernel iteration on the same system: iteration counts within
     one, scores equal to fp32 rounding, and both meet the target on the fp64 residual."""
@@ -354,6 +355,40 @@ def test_incremental_solver_relres_on_edge_batches():
         R_true = S64.rhs_h.cpu().numpy() - (S64.diag.cpu().numpy()[:, None] * solver.Z.cpu().numpy() - A @ solver.Z.cpu().numpy())
         drift = np.abs(R_true - solver.R.cpu().numpy()).max() / S64.diag.cpu().numpy().min()
         assert drift < 1e-9, drift
+
+
+@pytest.mark.parametrize("K", [4, 8])
+def test_incremental_solver_class_sum(K):
+    """class_sum: the refinement's corrections solve K - 1 class columns and h and set the last class
+    to one minus the others (the scores of a grounded row sum to one). On an edge stream: every
+    column meets the relative-residual target on the fp64 residual, the kept residual stays the true
+    one, the scores sum to one on the solved rows and match the full solve's to 1e-5."""
+    n = 20_000
+    ds = graphs.er_graph(n, 10, K, seed=6)
+    lab = graphs.label_mask(n, 0.01, seed=6)
+    up = graphs.EdgeUpdates(ds.A, seed=6)
+    batches = [up.next(400) for _ in range(5)]
+    out = []
+    for cs in (True, False):
+        es = stream.EdgeStream(ds, lab)
+        solver = solvers.IncrementalLP(n, K, "float32", tol=1e-3, method="pcg", target_relres=1e-6, full_every=4,
+                                       class_sum=cs)
+        solver.solve(es.system)
+        for t, b in enumerate(batches):
+            S = es.apply_edges(**b)
+            st = solver.solve(S)
+            S64 = S.astype(torch.float64)
+            A = es.G.to_csr("w").to_scipy().astype(np.float64)
+            Z = solver.Z.cpu().numpy()
+            rel = O.relres(A, S64.diag.cpu().numpy(), Z[:, :K], S64.rhs.cpu().numpy())
+            assert rel <= 1e-6 and st.relres <= 1e-6, (cs, t, rel, st.relres)
+            R_true = S64.rhs_h.cpu().numpy() - (S64.diag.cpu().numpy()[:, None] * Z - A @ Z)
+            assert np.abs(R_true - solver.R.cpu().numpy()).max() / S64.diag.cpu().numpy().min() < 1e-9
+        solved = S.solved.cpu().numpy()
+        if cs:
+            np.testing.assert_allclose(Z[solved, :K].sum(axis=1), 1.0, rtol=0, atol=1e-12)
+        out.append(Z[:, :K])
+    np.testing.assert_allclose(out[0], out[1], rtol=0, atol=1e-5)
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
