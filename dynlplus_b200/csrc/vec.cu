@@ -1,5 +1,6 @@
 // Column-scaled vector updates of the refinement loop and the grounding update.
 #include "common.cuh"
+#include "gather.cuh"
 
 namespace dlp {
 
@@ -137,11 +138,30 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
   return check_launch();
 }
 
+extern "C++" {
 // Class-sum elimination: the right-hand side of a correction without its last class column, and the
 // update that adds the correction and sets the last class to one minus the others. One thread per row
 // (K + 1 <= 16 values), sums in ascending column order in fp64.
+// WHOLE (K = 8 with the rows aligned: R rows of 9 doubles at 16-byte boundaries with ld >= 10 even,
+// E / D rows of 8 floats at 32-byte boundaries): each row in whole-row vector loads and stores.
+template <bool WHOLE>
 __global__ void k_class_sum_rhs(int32_t n, int32_t K, const double *__restrict__ R, int64_t ldr,
                                 const double *__restrict__ scale, float *__restrict__ E, int64_t lde) {
+  if constexpr (WHOLE) {
+    double sc[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) sc[j] = scale[j];
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+      double raw[5][2];
+      const bool hi = load_row10d(R + r * ldr, raw);
+      float e[2][4];
+#pragma unroll
+      for (int j = 0; j < 7; ++j) e[j / 4][j % 4] = (float)(row10_col(raw, hi, j) / sc[j]);
+      e[1][3] = (float)(row10_col(raw, hi, 8) / sc[8]);
+      store_row8(E + r * lde, e);
+    }
+    return;
+  }
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
     const double *rr = R + r * ldr;
     float *er = E + r * lde;
@@ -150,9 +170,33 @@ __global__ void k_class_sum_rhs(int32_t n, int32_t K, const double *__restrict__
   }
 }
 
+template <bool WHOLE>
 __global__ void k_class_sum_update(int32_t n, int32_t K, const float *__restrict__ D, int64_t ldd,
                                    const double *__restrict__ scale, double *__restrict__ Z, int64_t ldz,
                                    const uint8_t *__restrict__ solved) {
+  if constexpr (WHOLE) {
+    double sc[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) sc[j] = scale[j];
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+      double raw[5][2];
+      const bool hi = load_row10d(Z + r * ldz, raw);
+      float d[2][4];
+      load_row8(D + r * ldd, d);
+      double z[10];
+      double sum = 0.0;
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        z[j] = row10_col(raw, hi, j) + (double)d[j / 4][j % 4] * sc[j];
+        sum += z[j];
+      }
+      z[8] = row10_col(raw, hi, 8) + (double)d[1][3] * sc[8];
+      z[7] = (!solved || solved[r]) ? 1.0 - sum : 0.0;
+      z[9] = 0.0;
+      store_row10d<false>(Z + r * ldz, z);  // exactly the 9 values: the tenth slot is padding
+    }
+    return;
+  }
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
     const float *dr = D + r * ldd;
     double *zr = Z + r * ldz;
@@ -166,6 +210,8 @@ __global__ void k_class_sum_update(int32_t n, int32_t K, const float *__restrict
     zr[K - 1] = (!solved || solved[r]) ? 1.0 - sum : 0.0;
   }
 }
+
+}  // extern "C++"
 
 size_t dlp_predict_workspace_bytes(int32_t n) {
   return ((size_t)(n > 0 ? n : 1) + 255) / 256 * 256 + compact_ws_bytes(n);
@@ -213,7 +259,10 @@ int dlp_class_sum_rhs(int32_t n, int32_t K, const double *R, int64_t ldr, const 
   if (n == 0) return DLP_OK;
   if (!R || !scale || !E) return DLP_ERR_INVALID;
   const int grid = (int)std::min<long long>(ceil_div_i((long long)n, 256LL), (long long)sm_count() * 8);
-  k_class_sum_rhs<<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, R, ldr, scale, E, lde);
+  const bool whole = K == 8 && (uintptr_t)R % 16 == 0 && ldr % 2 == 0 && ldr >= 10 && (uintptr_t)E % 32 == 0 &&
+                     lde % 8 == 0;
+  if (whole) k_class_sum_rhs<true><<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, R, ldr, scale, E, lde);
+  else k_class_sum_rhs<false><<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, R, ldr, scale, E, lde);
   return check_launch();
 }
 
@@ -223,7 +272,10 @@ int dlp_class_sum_update(int32_t n, int32_t K, const float *D, int64_t ldd, cons
   if (n == 0) return DLP_OK;
   if (!D || !scale || !Z) return DLP_ERR_INVALID;
   const int grid = (int)std::min<long long>(ceil_div_i((long long)n, 256LL), (long long)sm_count() * 8);
-  k_class_sum_update<<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, D, ldd, scale, Z, ldz, solved);
+  const bool whole = K == 8 && (uintptr_t)Z % 16 == 0 && ldz % 2 == 0 && ldz >= 10 && (uintptr_t)D % 32 == 0 &&
+                     ldd % 8 == 0;
+  if (whole) k_class_sum_update<true><<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, D, ldd, scale, Z, ldz, solved);
+  else k_class_sum_update<false><<<grid, 256, 0, (cudaStream_t)stream>>>(n, K, D, ldd, scale, Z, ldz, solved);
   return check_launch();
 }
 

@@ -243,8 +243,9 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
  * SpMM; R is written in the first sweep); bit 3 = always the three-kernel iteration; bit 4 = no
  * recheck: a proposed stop is final (status 5) without the true-residual confirmation below, for a
  * caller that confirms on its own residual (R then holds the recurrence residual). Without bit 3,
- * fp32 solves whose rows take the whole-row gather (9-12 columns, ldp == ldap >= 12, P and AP on
- * 16-byte boundaries, no bf16 mirror) run two kernels per iteration: the SpMM also sums
+ * fp32 solves whose rows take a whole-row gather (9-12 columns with ldp == ldap >= 12 and P, AP on
+ * 16-byte boundaries; or 5-8 columns with ldp == ldap a multiple of 8 and P, AP on 32-byte boundaries; no
+ * bf16 mirror) run two kernels per iteration: the SpMM also sums
  * q_c = sum AP^2/diag and predicts beta = alpha^2 q / rz - 1 (exact for A-conjugate successive
  * directions), and one sweep updates R, Z and the next direction; P and AP trade places every
  * iteration (on return either may hold the last direction), and rz of the stored residual stays

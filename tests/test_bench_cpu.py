@@ -18,7 +18,7 @@ def test_traffic_file_is_consistent():
     p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles",
                      "pcg_iteration_traffic.json")
     t = json.load(open(p))
-    assert (t["n"], t["C"]) == (1_000_000, 9)
+    assert (t["n"], t["C"]) == (1_000_000, 8)  # class-sum corrections: 7 class columns and h
     assert t["dram_bytes_per_iteration"] == sum(t["per_kernel"].values())
     assert set(t["per_kernel"]) == {"k_pcg_apply", "k_pcg_fused"}  # the two-kernel iteration
 
