@@ -255,7 +255,7 @@ int dlp_ground_update(int32_t n, const int32_t *parent, const uint8_t *vmask, ui
 
 int dlp_class_sum_rhs(int32_t n, int32_t K, const double *R, int64_t ldr, const double *scale, float *E,
                       int64_t lde, dlp_stream_t stream) {
-  if (n < 0 || K < 2 || K > 15 || ldr < K + 1 || lde < K) return DLP_ERR_INVALID;
+  if (n < 0 || K < 2 || K > 256 || ldr < K + 1 || lde < K) return DLP_ERR_INVALID;
   if (n == 0) return DLP_OK;
   if (!R || !scale || !E) return DLP_ERR_INVALID;
   const int grid = (int)std::min<long long>(ceil_div_i((long long)n, 256LL), (long long)sm_count() * 8);
@@ -268,7 +268,7 @@ int dlp_class_sum_rhs(int32_t n, int32_t K, const double *R, int64_t ldr, const 
 
 int dlp_class_sum_update(int32_t n, int32_t K, const float *D, int64_t ldd, const double *scale, double *Z,
                          int64_t ldz, const uint8_t *solved, dlp_stream_t stream) {
-  if (n < 0 || K < 2 || K > 15 || ldd < K || ldz < K + 1) return DLP_ERR_INVALID;
+  if (n < 0 || K < 2 || K > 256 || ldd < K || ldz < K + 1) return DLP_ERR_INVALID;
   if (n == 0) return DLP_OK;
   if (!D || !scale || !Z) return DLP_ERR_INVALID;
   const int grid = (int)std::min<long long>(ceil_div_i((long long)n, 256LL), (long long)sm_count() * 8);

@@ -360,7 +360,7 @@ int dlp_cols_scale(int32_t n, int32_t C, const void *X, int64_t ldx, int x_dtype
  * (R: fp64 n x (K + 1), the K classes and h; E: fp32 n x K, the classes but the last, and h).
  * dlp_class_sum_update: Z[:, j] += D[:, j] scale[j] for j < K - 1, Z[:, K] += D[:, K - 1] scale[K],
  * then Z[:, K - 1] = 1 - sum_{j < K - 1} Z[:, j] on the rows with solved[r] != 0 (every row when
- * solved is NULL) and 0 elsewhere (Z: fp64 n x (K + 1); D: fp32 n x K). 2 <= K <= 15. Asynchronous. */
+ * solved is NULL) and 0 elsewhere (Z: fp64 n x (K + 1); D: fp32 n x K). 2 <= K <= 256. Asynchronous. */
 int dlp_class_sum_rhs(int32_t n, int32_t K, const double *R, int64_t ldr, const double *scale, float *E,
                       int64_t lde, dlp_stream_t stream);
 int dlp_class_sum_update(int32_t n, int32_t K, const float *D, int64_t ldd, const double *scale, double *Z,

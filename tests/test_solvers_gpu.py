@@ -357,7 +357,7 @@ def test_incremental_solver_relres_on_edge_batches():
         assert drift < 1e-9, drift
 
 
-@pytest.mark.parametrize("K", [4, 8])
+@pytest.mark.parametrize("K", [4, 8, 17])
 def test_incremental_solver_class_sum(K):
     """class_sum: the refinement's corrections solve K - 1 class columns and h and set the last class
     to one minus the others (the scores of a grounded row sum to one). On an edge stream: every
