@@ -61,7 +61,7 @@ def parse(argv=None):
                     help="launch the PCG kernels one by one instead of as a CUDA graph (for kernel profilers)")
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
     ap.add_argument("--no-class-sum", action="store_true",
-                    help="edge-stream: corrections solve all k class columns (default: k-1 and derive the last)")
+                    help="edge-stream: corrections solve all k class columns (default for k = 4, 8, 12: k-1, the last derived)")
     ap.add_argument("--three-kernel", action="store_true",
                     help="edge-stream: the three-kernel PCG iteration instead of the two-kernel one")
     ap.add_argument("--workload", default="edge-stream",
@@ -83,7 +83,7 @@ def config(a):
             "batch_updates": a.batch, "insert_frac": 0.5, "target_relres": a.target_relres, "tol": a.tol,
             "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas",
             "pcg_iteration": "three kernels" if a.three_kernel else "two kernels (fp32 whole rows)",
-            "class_sum": not a.no_class_sum}
+            "class_sum": "off" if a.no_class_sum else "auto (on for k = 4, 8, 12)"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -404,7 +404,7 @@ def ours(a):
     lab = graphs.label_mask(a.n, a.label_frac, seed=seed)
     es = stream.EdgeStream(ds, lab, components=True)  # component ids after every batch (side stream)
     solver = solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres,
-                                   full_every=16, lowp=a.lowp, class_sum=not a.no_class_sum)
+                                   full_every=16, lowp=a.lowp, class_sum=False if a.no_class_sum else "auto")
     solver.solve(es.system)  # the static solve of the initial graph (untimed)
     A0 = ds.A.to_scipy() if (rank == 0 and not a.no_cpu_baseline) else None
     Z0 = solver.Z.cpu().numpy() if A0 is not None else None

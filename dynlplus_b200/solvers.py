@@ -785,7 +785,13 @@ class IncrementalLP(DynLPPlus):
     `full_every` batches to bound drift."""
 
     def __init__(self, n_total, K, dtype="float32", tol=1e-3, full_every=16, max_rounds=50_000, method="auto",
-                 class_sum=True, **kw):
+                 class_sum="auto", **kw):
+        # auto: where dropping a class column shortens the rows to a whole number of 16-byte vectors
+        # of at most 12 floats (K = 4, 8, 12: one load fewer per gathered row); measured on B200 at
+        # K = 8 (18.6 iterations at 0.156 ms against 17.65 at 0.216) and, at K = 32 with no whole-row
+        # layout either way, slower than solving every column
+        if class_sum == "auto":
+            class_sum = K % 4 == 0 and K <= 12
         super().__init__(n_total, K, dtype, method=method, tol=tol, class_sum=class_sum, **kw)
         self.name, self.full_every, self.max_rounds = "dynlp+inc", full_every, max_rounds
         self.Z = self.R = None
