@@ -546,11 +546,14 @@ def ours(a):
     t_dev, t_e2e, value, e2e = aggregate_replicas(times, e2e_times, a.batch, world, dev)
     roof = None
     if rank == 0:
+        c_pcg = pcg_events[0][4] if pcg_events else a.k + 1  # columns the correction solves iterate on
         roof = pcg_roofline(pcg_events, es.solver_csr().nnz, peaks,
                             os.path.join(ROOT, "profiles", "pcg_iteration_traffic.json"),
-                            steady=pcg_steady(es, pcg_events[0][4] if pcg_events else a.k + 1))
+                            steady=pcg_steady(es, c_pcg))
         if roof is not None:
-            roof["spmm_alone"] = spmm_roofline(es, a.k + 1, peaks)
+            roof["spmm_alone"] = spmm_roofline(es, c_pcg, peaks)
+            if c_pcg != a.k + 1:  # every class column and h (the static solve's width)
+                roof["spmm_alone_all_columns"] = spmm_roofline(es, a.k + 1, peaks)
     cpu = None
     if rank == 0 and not a.no_cpu_baseline and world == 1:
         v, done, tw = cpu_batches(a, A0, ds.y.cpu().numpy(), lab.cpu().numpy(), Z0, cpu_sample, a.cpu_budget_s)

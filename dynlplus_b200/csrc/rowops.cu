@@ -150,6 +150,43 @@ __global__ void __launch_bounds__(kThreads) k_spmm(SpmmArgs<T> p) {
       }
       continue;
     }
+    if constexpr (ROW == kRow8F) {
+      if (valid && es == 0 && (p.own12 || p.y12)) {  // the per-column arithmetic below, 8-float rows
+        const long long orow = p.compact ? gi : (long long)r;
+        const float av = p.a ? (float)p.alpha * (float)p.a[r] : 0.f;
+        float yv[2][4];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) yv[c / 4][c % 4] = (float)p.b * acc[c / 4][c % 4];
+        if (p.a) {
+          if (p.own12) {
+            float xo[2][4];
+            load_row8(p.Xo ? (const float *)p.Xo + (long long)r * p.ldxo : (const float *)p.X + (long long)r * p.ldx,
+                      xo);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) yv[c / 4][c % 4] = fmaa(av, xo[c / 4][c % 4], yv[c / 4][c % 4]);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+              if (c < p.C)
+                yv[c / 4][c % 4] = fmaa(av, p.Xo ? (float)p.Xo[(long long)r * p.ldxo + c]
+                                                 : (float)p.X[(long long)r * p.ldx + c], yv[c / 4][c % 4]);
+          }
+        }
+        if (p.rhs) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < p.C) yv[c / 4][c % 4] += (float)p.cr * (float)p.rhs[(long long)r * p.ldr + c];
+        }
+        if (p.y12) {
+          store_row8((float *)(p.Y + orow * p.ldy), yv);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < p.C) p.Y[orow * p.ldy + c] = yv[c / 4][c % 4];
+        }
+        continue;
+      }
+    }
     if constexpr (ROW == kRow12F || ROW == kRow16H) {
       if (valid && es == 0 && (p.own12 || p.y12)) {  // the per-column arithmetic below, whole rows
         const long long orow = p.compact ? gi : (long long)r;
@@ -229,6 +266,9 @@ static int launch_spmm_vw(const SpmmArgs<T> &a, int VPL, dlp_stream_t s) {
       // bf16 rows of 16 values held whole by one lane: one 256-bit load per gathered row
       if (kRow16 && a.LV == 1 && (uintptr_t)a.X % 32 == 0 && (a.ldx * 2) % 32 == 0) {
         k_spmm<T, VW, 2, (kRow16 ? kRow16H : kRowVec)><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
+      } else if (kRow12 && a.LV == 1 && (uintptr_t)a.X % 32 == 0 && a.ldx % 8 == 0) {
+        // fp32 rows of 8 values held whole by one lane: one 256-bit load per gathered row
+        k_spmm<T, VW, 2, (kRow12 ? kRow8F : kRowVec)><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
       } else {
         k_spmm<T, VW, 2><<<grid, kThreads, 0, (cudaStream_t)s>>>(a);
       }
@@ -276,6 +316,14 @@ static int run_spmm(const int32_t *rbeg, const int32_t *rend, const int32_t *col
                       L.VW == 4 && L.VPL == 3 && L.LV == 1 && C >= 9;
   const bool bf16_16 = std::is_same<typename T::TX, bf16>::value && std::is_same<typename T::TA, float>::value &&
                        L.VW == 8 && L.VPL == 2 && L.LV == 1 && C >= 9 && C <= 12;
+  const bool f32_8 = std::is_same<typename T::TX, float>::value && std::is_same<typename T::TA, float>::value &&
+                     std::is_same<typename T::TY, float>::value && std::is_same<typename T::TV, float>::value &&
+                     L.VW == 4 && L.VPL == 2 && L.LV == 1 && (uintptr_t)X % 32 == 0 && ldx % 8 == 0;
+  if (f32_8) {  // the kRow8F layout (launch_spmm_vw): whole-row epilogue where the rows allow it
+    auto rows8 = [](const void *q, int64_t ldq) { return q && (uintptr_t)q % 32 == 0 && ldq % 8 == 0; };
+    p.own12 = Xo ? rows8(Xo, ldxo) : 1;
+    p.y12 = C == 8 && rows8(Y, ldy);
+  }
   if (std::is_same<typename T::TY, float>::value && std::is_same<typename T::TV, float>::value && (f32_12 || bf16_16)) {
     // the kRow12F / kRow16H layouts (launch_spmm_vw): whole-row epilogue (fp32 own row and output)
     // where the rows allow it

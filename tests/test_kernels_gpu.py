@@ -355,3 +355,46 @@ def test_spmm_fp32_whole_row_epilogue(C, ld_x, ld_y):
     Yc = kernels.spmm_axpy(W, Xd, rows=T(Q), compact=True)
     np.testing.assert_allclose(Yc.cpu().numpy(), (A.astype(np.float64) @ X.astype(np.float64))[Q], rtol=1e-5,
                                atol=1e-5 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("C", [5, 7, 8])
+@pytest.mark.parametrize("ld_x,ld_y", [(8, 8), (16, 16), (8, 0), (8, 9), (9, 8)])
+def test_spmm_fp32_8float_rows(C, ld_x, ld_y):
+    """fp32 rows of 5-8 values on a 32-byte pitch gathered whole (one 256-bit load per row): the own
+    row of the diagonal term read whole and, for 8 columns on a 32-byte pitch, the output written as a
+    whole row; odd pitches take the per-column path. Against numpy: full rows, a row subset in place,
+    compact rows. Output columns beyond C keep their values; the results equal the per-column path's."""
+    rs = np.random.RandomState(C * 100 + ld_x + ld_y)
+    n = 3001
+    A = O.symmetric_from_pairs(rs.randint(0, n, 30000), rs.randint(0, n, 30000), rs.rand(30000), n, np.float32)
+    W = CSR.from_scipy(A, dtype=torch.float32)
+    X, d = rs.rand(n, C).astype(np.float32), (rs.rand(n) + 1).astype(np.float32)
+    Xd = padded(X, ld_x, torch.float32)  # NaN in the padding: never read into a result
+    want = d[:, None].astype(np.float64) * X - A.astype(np.float64) @ X.astype(np.float64)
+    tol = 1e-5 * np.abs(want).max()
+
+    def out_buf():
+        if not ld_y:
+            return torch.zeros((n, C), dtype=torch.float32, device="cuda")
+        buf = torch.full((n, ld_y), -7.0, dtype=torch.float32, device="cuda")
+        buf[:, :C] = 0.0
+        return buf[:, :C]
+
+    Y = out_buf()
+    kernels.spmm_axpy(W, Xd, a=T(d), b=-1.0, out=Y)
+    np.testing.assert_allclose(Y.cpu().numpy(), want, rtol=1e-5, atol=tol)
+    if ld_y:
+        assert (Y.as_strided((n, ld_y), (ld_y, 1))[:, C:] == -7.0).all()
+    Yu = kernels.spmm_axpy(W, padded(X, 9, torch.float32), a=T(d), b=-1.0)  # odd pitch: per-column path
+    assert np.abs(Y.cpu().numpy() - Yu.cpu().numpy()).max() <= tol
+    Q = np.sort(rs.choice(n, 400, replace=False)).astype(np.int32)
+    Y = out_buf()
+    kernels.spmm_axpy(W, Xd, a=T(d), b=-1.0, out=Y, rows=T(Q))
+    Yn = Y.cpu().numpy()
+    np.testing.assert_allclose(Yn[Q], want[Q], rtol=1e-5, atol=tol)
+    assert (Yn[np.setdiff1d(np.arange(n), Q)] == 0).all()
+    Yc = kernels.spmm_axpy(W, Xd, rows=T(Q), compact=True)
+    np.testing.assert_allclose(Yc.cpu().numpy(), (A.astype(np.float64) @ X.astype(np.float64))[Q], rtol=1e-5,
+                               atol=tol)
+    Yc2 = kernels.spmm_axpy(W, T(X), rows=T(Q), compact=True)  # unpadded rows: the per-column path
+    assert np.abs(Yc.cpu().numpy() - Yc2.cpu().numpy()).max() <= tol
