@@ -19,6 +19,7 @@ throughput is the sum over ranks with the time taken as the maximum over ranks.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -62,6 +63,9 @@ def parse(argv=None):
     ap.add_argument("--lowp", action="store_true", help="edge-stream: BF16 gathers in the PCG sweeps")
     ap.add_argument("--no-class-sum", action="store_true",
                     help="edge-stream: corrections solve all k class columns (default for k = 4, 8, 12: k-1, the last derived)")
+    ap.add_argument("--refine-share", type=float, default=0.2,
+                    help="edge-stream: share of the rel-res target a correction round aims for (the fp64 "
+                         "residual after it decides whether another round runs)")
     ap.add_argument("--three-kernel", action="store_true",
                     help="edge-stream: the three-kernel PCG iteration instead of the two-kernel one")
     ap.add_argument("--workload", default="edge-stream",
@@ -83,7 +87,9 @@ def config(a):
             "batch_updates": a.batch, "insert_frac": 0.5, "target_relres": a.target_relres, "tol": a.tol,
             "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas",
             "pcg_iteration": "three kernels" if a.three_kernel else "two kernels (fp32 whole rows)",
-            "class_sum": "off" if a.no_class_sum else "auto (on for k = 4, 8, 12)"}
+            "class_sum": "off" if a.no_class_sum else "auto (on for k = 4, 8, 12)",
+            "refine_share": a.refine_share,
+            "python_gc": "collected before the timed loops, paused during them"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -404,7 +410,8 @@ def ours(a):
     lab = graphs.label_mask(a.n, a.label_frac, seed=seed)
     es = stream.EdgeStream(ds, lab, components=True)  # component ids after every batch (side stream)
     solver = solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres,
-                                   full_every=16, lowp=a.lowp, class_sum=False if a.no_class_sum else "auto")
+                                   full_every=16, lowp=a.lowp, class_sum=False if a.no_class_sum else "auto",
+                                   refine_share=a.refine_share)
     solver.solve(es.system)  # the static solve of the initial graph (untimed)
     A0 = ds.A.to_scipy() if (rank == 0 and not a.no_cpu_baseline) else None
     Z0 = solver.Z.cpu().numpy() if A0 is not None else None
@@ -502,6 +509,10 @@ def ours(a):
         clocks.mark()
     launches0 = _lib.lib().dlp_launch_count()
     solvers.PCG_EVENTS = []  # CUDA events around the fused PCG calls of the timed steps
+    # Python's cyclic collector: run once now and paused through the timed loops (as a serving
+    # process would tune it), so a collection pass does not land inside one step
+    gc.collect()
+    gc.disable()
     torch.cuda.nvtx.range_push("timed")  # lets a profiler filter the timed steps (--nvtx-include timed/)
     times, relres, paths, iters, events, checks = [], [], [], [], {}, []
     for k, b in enumerate(dev_batches):
@@ -548,6 +559,7 @@ def ours(a):
         e2e_times.append(s.elapsed_time(e))
         relres.append(st.relres)
         relabelled.append(res[0])
+    gc.enable()
     cc_last = res[1:3] if res is not None else None
     clk = clocks.stop() if clocks else None
     t_dev, t_e2e, value, e2e = aggregate_replicas(times, e2e_times, a.batch, world, dev)
@@ -579,6 +591,7 @@ def ours(a):
                 "stream_events": {str(k): v for k, v in events.items()},
                 "pcg_iters_per_batch": float(np.mean(iters)),
                 "step_ms": [round(t, 3) for t in times],
+                "e2e_step_ms": [round(t, 3) for t in e2e_times],
                 "e2e": {"value": e2e, "unit": "edge-updates/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0,
                         "result": "relabelled rows with their new labels; component and active-unlabelled counts",

@@ -548,15 +548,16 @@ class DynLPPlus(Solver):
 
     def __init__(self, n_total, K, dtype="float32", method="auto", tol=1e-3, eps_h=0.05, group="auto",
                  push_frac=0.05, push_budget=30.0, amg_hmax=2000.0, max_iter=100_000, amg_opts=None,
-                 target_relres=None, lowp=False, class_sum=False):
+                 target_relres=None, lowp=False, class_sum=False, refine_share=0.2):
         super().__init__(n_total, K, dtype, store_dtype="float64")  # float64 master copy of F and h
         self.method, self.tol, self.eps_h, self.group = method, tol, eps_h, group
         self.push_frac, self.push_budget, self.amg_hmax = push_frac, push_budget, amg_hmax
         self.max_iter, self.amg_opts = max_iter, amg_opts or {}
         self.target_relres = target_relres
         # share of the relative-residual target a correction round aims for (the rest absorbs the
-        # working-precision rounding between the PCG's own residual and the fp64 one)
-        self.refine_share = 0.2
+        # working-precision rounding between the PCG's own residual and the fp64 one); the fp64
+        # residual after the round decides whether another one runs
+        self.refine_share = refine_share
         self.lowp = lowp  # SpMM sweeps on bf16 weights and scores (fp32 accumulation)
         # refinement corrections solve K - 1 class columns and derive the last (_correct_class_sum)
         self.class_sum = class_sum
