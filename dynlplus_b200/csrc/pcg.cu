@@ -707,16 +707,24 @@ __global__ void __launch_bounds__(kSweepThreads, (sweep_min_blocks<T>()))
     finish_sweep(0, C, B, true);
 }
 
-// Coherent 256-bit row access for the row sweep (rows it reads and then writes in the same launch).
-__device__ __forceinline__ void ld_row8(const float *xr, float (&v)[8]) {
-  asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+// Coherent 256-bit row access for the row sweep (rows it reads and then writes in the same launch),
+// with an L2 eviction policy: R, Z, AP and the current direction are streamed through (evict-first)
+// and the next direction, which the next apply gathers about ten times per row, is kept (evict-last).
+// Measured on the 8-column iteration at n = 1M, degree 10: 124.4 -> 121.5 us.
+__device__ __forceinline__ uint64_t l2_evict_first_pol() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void ld_row8(const float *xr, float (&v)[8], uint64_t pol) {
+  asm volatile("ld.global.L2::cache_hint.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
                : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
-               : "l"(xr)
+               : "l"(xr), "l"(pol)
                : "memory");
 }
-__device__ __forceinline__ void st_row8(float *yr, const float (&v)[8]) {
-  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(yr), "f"(v[0]), "f"(v[1]),
-               "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+__device__ __forceinline__ void st_row8(float *yr, const float (&v)[8], uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8}, %9;" ::"l"(yr), "f"(v[0]), "f"(v[1]),
+               "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "l"(pol)
                : "memory");
 }
 
@@ -767,12 +775,13 @@ __global__ void __launch_bounds__(kSweepThreads, kRowSweepBlocks)
 #pragma unroll
   for (int c = 0; c < 8; ++c) rz[c] = ss[c] = rmax[c] = 0.0;
   const long long stride = (long long)gridDim.x * blockDim.x;
+  const uint64_t pf = l2_evict_first_pol(), pl = l2_evict_last();
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
     float rv[8], av[8], pv[8], zv[8];
-    ld_row8(R + r * ldr, rv);
-    ld_row8(AP + r * ld, av);
-    ld_row8(P + r * ld, pv);
-    ld_row8(Z + r * ldz, zv);
+    ld_row8(R + r * ldr, rv, pf);
+    ld_row8(AP + r * ld, av, pf);
+    ld_row8(P + r * ld, pv, pf);
+    ld_row8(Z + r * ldz, zv, pf);
     const double dinv = __drcp_rn((double)diag[r]);  // correctly rounded: the value of 1.0 / d
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
@@ -791,9 +800,9 @@ __global__ void __launch_bounds__(kSweepThreads, kRowSweepBlocks)
         av[c] = 0.f;
       }
     }
-    st_row8(R + r * ldr, rv);
-    st_row8(Z + r * ldz, zv);
-    st_row8(AP + r * ld, av);
+    st_row8(R + r * ldr, rv, pf);
+    st_row8(Z + r * ldz, zv, pf);
+    st_row8(AP + r * ld, av, pl);
   }
   // fp64 rounding is monotone: max over rows of (|r| / d) times eps^-1 is the max of the products
   double vmax = 0.0;
