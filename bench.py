@@ -427,10 +427,12 @@ def ours(a):
     def to_pinned(b):
         return {k: torch.from_numpy(v).pin_memory() for k, v in b.items()}
 
-    cap = 4096  # relabelled rows read back with the counts in one round trip (more: a second one)
+    # relabelled rows read back with the counts in one round trip: up to `cap` of them (a step that
+    # relabels more reads the rest in a second one and doubles the buffers for the next steps)
+    rb = {"cap": 65536}
     h_cnt = torch.zeros(3, dtype=torch.int32).pin_memory()
-    h_rows = torch.zeros(cap, dtype=torch.int32).pin_memory()
-    h_labs = torch.zeros(cap, dtype=torch.int32).pin_memory()
+    rb["rows"] = torch.zeros(rb["cap"], dtype=torch.int32).pin_memory()
+    rb["labs"] = torch.zeros(rb["cap"], dtype=torch.int32).pin_memory()
     d2h = []
 
     def step(b, host_result=False):
@@ -443,18 +445,24 @@ def ours(a):
         es.join_components()
         if not host_result:
             return st, None
+        cap, h_rows, h_labs = rb["cap"], rb["rows"], rb["labs"]
+        m = min(cap, int(chg.numel()))
         h_cnt[0:1].copy_(nchg, non_blocking=True)
         h_cnt[1:3].copy_(es._cc_counts[0:2], non_blocking=True)
-        h_rows.copy_(chg[:cap], non_blocking=True)
-        h_labs.copy_(chg_lab[:cap], non_blocking=True)
+        h_rows[:m].copy_(chg[:m], non_blocking=True)
+        h_labs[:m].copy_(chg_lab[:m], non_blocking=True)
         torch.cuda.current_stream().synchronize()
         k = int(h_cnt[0])
-        nbytes = 12 + 8 * cap
-        rows, labs = h_rows[:min(k, cap)].numpy().copy(), h_labs[:min(k, cap)].numpy().copy()
-        if k > cap:
-            rows = np.concatenate([rows, chg[cap:k].cpu().numpy()])
-            labs = np.concatenate([labs, chg_lab[cap:k].cpu().numpy()])
-            nbytes += 8 * (k - cap)
+        nbytes = 12 + 8 * m
+        rows, labs = h_rows[:min(k, m)].numpy().copy(), h_labs[:min(k, m)].numpy().copy()
+        if k > m:
+            rows = np.concatenate([rows, chg[m:k].cpu().numpy()])
+            labs = np.concatenate([labs, chg_lab[m:k].cpu().numpy()])
+            nbytes += 8 * (k - m)
+            while rb["cap"] < k:
+                rb["cap"] *= 2
+            rb["rows"] = torch.zeros(rb["cap"], dtype=torch.int32).pin_memory()
+            rb["labs"] = torch.zeros(rb["cap"], dtype=torch.int32).pin_memory()
         d2h.append(nbytes)
         return st, (k, int(h_cnt[1]), int(h_cnt[2]), rows, labs)
 
