@@ -15,6 +15,7 @@
 // Sums over rows go through per-block partials over a fixed grid and an ordered final pass, so
 // the iterates do not depend on scheduling.
 #include <cstddef>
+#include <cstring>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -72,6 +73,46 @@ static size_t pcg_ws_bytes(int C) {
   b += align256(sizeof(double) * kMaxGroups * 2 * C);        // gpart1
   b += align256(sizeof(double) * kMaxGroups * (2 * C + 1));  // gpart2
   return b;
+}
+
+// Bytes of the workspace's head: the control block and the seven per-column vectors (carve order).
+static size_t head_bytes(int C) { return align256(sizeof(PcgCtl)) + 7 * align256(sizeof(double) * C); }
+
+// Pinned host staging, one per host thread and device: the image of the workspace's head that a
+// solve uploads in one copy, and the control block's read-backs. Before the image is rewritten the
+// thread waits for the event recorded after its last upload, so a copy still in flight never sees
+// the next solve's values. Kept for the thread's lifetime.
+struct HostStage {
+  char *img = nullptr;
+  size_t cap = 0;
+  PcgCtl *rd = nullptr;
+  cudaEvent_t up = nullptr;
+};
+static thread_local HostStage t_stage[64];
+
+static int stage_get(int dev, size_t bytes, HostStage **out) {
+  if (dev < 0 || dev >= 64) return DLP_ERR_INVALID;
+  HostStage &g = t_stage[dev];
+  if (!g.up) DLP_CUDA(cudaEventCreateWithFlags(&g.up, cudaEventDisableTiming));
+  DLP_CUDA(cudaEventSynchronize(g.up));
+  if (g.cap < bytes) {
+    if (g.img) DLP_CUDA(cudaFreeHost(g.img));
+    g.img = nullptr;
+    g.cap = 0;
+    DLP_CUDA(cudaHostAlloc((void **)&g.img, bytes, cudaHostAllocPortable));
+    g.cap = bytes;
+  }
+  if (!g.rd) DLP_CUDA(cudaHostAlloc((void **)&g.rd, sizeof(PcgCtl), cudaHostAllocPortable));
+  *out = &g;
+  return DLP_OK;
+}
+
+// The control block's head, read through the thread's pinned buffer (a blocking read).
+static int read_ctl(const PcgBufs &B, HostStage *hs, cudaStream_t s, PcgCtl *cur) {
+  DLP_CUDA(cudaMemcpyAsync(hs->rd, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
+  DLP_CUDA(cudaStreamSynchronize(s));
+  std::memcpy((void *)cur, hs->rd, kCtlHead);
+  return DLP_OK;
 }
 
 static PcgBufs carve(void *ws, int C) {
@@ -1401,28 +1442,31 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   }
   PcgBufs B = carve(ws, C);
   B.cancel = cancel_word();
-  PcgCtl h{};
-  h.mode = mode & 3;
-  h.patience = patience > 0 ? patience : 400;
-  h.max_iter = max_iter;
-  h.target = target_relres;
-  DLP_CUDA(cudaMemcpyAsync(B.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  int dev = 0;
+  DLP_CUDA(cudaGetDevice(&dev));
+  HostStage *hs = nullptr;
+  DLP_TRY(stage_get(dev, head_bytes(C), &hs));
   {
-    std::vector<double> e2((size_t)C * 2);
+    // the head in one upload: control block; alpha, beta, rz, rzprev zero; eps, its inverse and the
+    // rhs norms (zero without them)
+    char *img = hs->img;
+    std::memset(img, 0, head_bytes(C));
+    PcgCtl h{};
+    h.mode = mode & 3;
+    h.patience = patience > 0 ? patience : 400;
+    h.max_iter = max_iter;
+    h.target = target_relres;
+    std::memcpy(img, &h, sizeof(h));
+    auto vec = [&](int i) { return (double *)(img + align256(sizeof(PcgCtl)) + i * align256(sizeof(double) * C)); };
+    double *e = vec(3), *rn = vec(4), *ei = vec(5);
     for (int c = 0; c < C; ++c) {
-      e2[c] = eps ? eps[c] : 1e300;
-      e2[C + c] = 1.0 / e2[c];
+      e[c] = eps ? eps[c] : 1e300;
+      ei[c] = 1.0 / e[c];
+      rn[c] = rhs_norm ? rhs_norm[c] : 0.0;
     }
-    // pageable source: staged before the call returns, so e2 may go out of scope
-    DLP_CUDA(cudaMemcpyAsync(B.eps, e2.data(), sizeof(double) * C, cudaMemcpyHostToDevice, s));
-    DLP_CUDA(cudaMemcpyAsync(B.epsinv, e2.data() + C, sizeof(double) * C, cudaMemcpyHostToDevice, s));
+    DLP_CUDA(cudaMemcpyAsync(B.ctl, img, head_bytes(C), cudaMemcpyHostToDevice, s));
+    DLP_CUDA(cudaEventRecord(hs->up, s));
   }
-  if (rhs_norm) {
-    DLP_CUDA(cudaMemcpyAsync(B.rhsn, rhs_norm, sizeof(double) * C, cudaMemcpyHostToDevice, s));
-  } else {
-    DLP_CUDA(cudaMemsetAsync(B.rhsn, 0, sizeof(double) * C, s));
-  }
-  DLP_CUDA(cudaMemsetAsync(B.rz, 0, sizeof(double) * C, s));
   // R = rhs - A Z, best = violation, rz = R.(R/diag), P = R/diag; a zero start takes R = rhs in the
   // update sweep itself and sets Z = 0 in the direction sweep (no SpMM, no separate copy)
   if (mode & 4) {
@@ -1445,8 +1489,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   cudaGraphExec_t ex = gref ? gref->ex : nullptr;
   PcgCtl cur{};
   if (max_iter <= 0) {
-    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
-    DLP_CUDA(cudaStreamSynchronize(s));
+    DLP_TRY(read_ctl(B, hs, s, &cur));
     if (cur.done == 0) cur.done = 3;
   }
   // otherwise the first chunk goes out without a round trip: when the start already meets the
@@ -1471,13 +1514,11 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
       // a stop was proposed: recheck on the true residual (dynlp/solvers.py:85-89)
       DLP_TRY(true_residual(q, s));
       DLP_TRY(update_phase(1, q, B, s));
-      DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
-      DLP_CUDA(cudaStreamSynchronize(s));
+      DLP_TRY(read_ctl(B, hs, s, &cur));
       if (cur.done != 0) break;
       DLP_TRY(dir_phase(1, q, B, s));  // resume from the true residual
     }
-    DLP_CUDA(cudaMemcpyAsync(&cur, B.ctl, kCtlHead, cudaMemcpyDeviceToHost, s));
-    DLP_CUDA(cudaStreamSynchronize(s));
+    DLP_TRY(read_ctl(B, hs, s, &cur));
     if (looped) {
       const int passes = std::max((cur.iters - it0 + kLoopBody - 1) / kLoopBody, 1);  // loop bodies run
       note_launches(3ull * kLoopBody * (unsigned long long)passes);

@@ -13,6 +13,7 @@ max_c ||rhs_c - A F_c||_2 / ||rhs_c||_2 in fp64, which the certified loops must 
 from __future__ import annotations
 
 import ctypes as ct
+import threading
 from dataclasses import dataclass
 
 import torch
@@ -50,6 +51,24 @@ def padded_empty(n, C, dt, dev, fill=None):
 
 
 _SCRATCH: dict = {}
+_PINNED = threading.local()
+
+
+def _read_host(x):
+    """A small device array read to the host through a pinned buffer of this thread (one blocking
+    copy; a pageable read stages through a driver buffer first). Returns a list."""
+    if x.device.type != "cuda":
+        return x.tolist()
+    key = (x.dtype, x.device.index)
+    bufs = getattr(_PINNED, "bufs", None)
+    if bufs is None:
+        bufs = _PINNED.bufs = {}
+    h = bufs.get(key)
+    if h is None or h.numel() < x.numel():
+        h = bufs[key] = torch.empty(max(x.numel(), 64), dtype=x.dtype, pin_memory=True)
+    h[: x.numel()].copy_(x.reshape(-1), non_blocking=True)
+    torch.cuda.current_stream(x.device).synchronize()
+    return h[: x.numel()].tolist()
 
 
 def _scratch(tag, n, C, dt, dev, padded=False):
@@ -121,7 +140,7 @@ def residual_stats(sys: System, R, rhs=None, H=None):
         _lib.call("dlp_residual_stats", n, C, ptr(R), ld(R), ptr(rhs), ld(rhs) if rhs is not None else C,
                   ptr(sys.diag.to(dt)), ptr(H), ld(H) if H is not None else 1, code(R), ptr(out), ptr(ws), ws.numel(),
                   stream())
-    v = out.cpu().tolist()
+    v = _read_host(out)
     res = _Stats((v[:C], v[C:2 * C], v[2 * C:3 * C] if rhs is not None else None, v[3 * C] if H is not None else None))
     res.dev = out  # the device copy: the refinement scales from it without an upload
     return res

@@ -483,6 +483,7 @@ class EdgeStream:
             mv, _ = kernels.flatnonzero(self.in_t, count=st[7:8], sync=False)
             Qb, _ = kernels.flatnonzero(self.changed, count=st[6:7], sync=False)
             self._csr_launch()
+            self._queue_counts()
             flags = self._read_counts()
             if flags["overflow"] == 0:
                 break
@@ -507,7 +508,7 @@ class EdgeStream:
         moved = mv[:nmoved]
         if nmoved:
             self.counters["ground_changes"] += nmoved
-            self._counts = None
+        self._counts = [flags["active"], flags["ungrounded"]]
         nq, nnz = flags["changed"], flags["nnz"]
         self.t += 1
         self._csr_set(nnz)
@@ -547,17 +548,34 @@ class EdgeStream:
         _lib.call("dlp_graph_toggle", ptr(G.rbeg), ptr(G.rend), ptr(G.indices), ptr(G.aw), ptr(G.data), None, self.n,
                   ptr(self.in_t), ptr(self.umask), ptr(self.rowsum), ptr(self.changed), stream())
 
+    def _queue_counts(self):
+        """Queue the active and ungrounded vertex counts of the batch's final membership on the
+        device (no host read: they come back with the batch's flags in _read_counts)."""
+        um = self.umask.view(torch.bool)
+        if getattr(self, "_cnt_dev", None) is None:
+            self._cnt_dev = torch.zeros(2, dtype=torch.int64, device=self.dev)
+        self._cnt_dev[0] = self.vmask.sum() + self.labeled.sum()
+        self._cnt_dev[1] = (self.vmask.view(torch.bool) & ~um).sum()
+
     def _read_counts(self):
-        """One host read of the batch's flags and counts (and the solver CSR's entry count)."""
+        """One host read of the batch's flags and counts (the solver CSR's entry count, and the
+        active and ungrounded counts when queued)."""
         if getattr(self, "_h_stat", None) is None:
             self._h_stat = torch.zeros(9, dtype=torch.int32, pin_memory=torch.cuda.is_available())
+            self._h_cnt = torch.zeros(2, dtype=torch.int64, pin_memory=torch.cuda.is_available())
         h = self._h_stat
         h[0:8].copy_(self._stat, non_blocking=True)
         h[8:9].copy_(self._csr_ptr[self.n:self.n + 1], non_blocking=True)
+        cnt = getattr(self, "_cnt_dev", None)
+        if cnt is not None:
+            self._h_cnt.copy_(cnt, non_blocking=True)
         torch.cuda.current_stream(self.dev).synchronize()
         v = h.tolist()
-        return {"error": v[0], "overflow": v[1], "deleted": v[2], "inserted": v[3], "moved": v[7],
-                "ground_error": v[5], "changed": v[6], "nnz": v[8]}
+        out = {"error": v[0], "overflow": v[1], "deleted": v[2], "inserted": v[3], "moved": v[7],
+               "ground_error": v[5], "changed": v[6], "nnz": v[8]}
+        if cnt is not None:
+            out["active"], out["ungrounded"] = self._h_cnt.tolist()
+        return out
 
     def apply_vertices(self, ins, dele, tau=None, wmax=None) -> System:
         """One vertex-arrival batch (IncrementalStream.batches, dynlp/stream.py:300-346): the
