@@ -91,23 +91,6 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, TA (&out)[VW])
   }
 }
 
-// Same for a gathered neighbour row: a 16-byte vector read without allocating it in L1 (the row is
-// rarely read again from L1; see the row loads in gather.cuh).
-template <typename T, int VW, typename TA>
-__device__ __forceinline__ void load_vec_gather(const T *__restrict__ p, TA (&out)[VW]) {
-  if constexpr (VW * sizeof(T) == 16) {
-    uint4 raw;
-    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
-        : "=r"(raw.x), "=r"(raw.y), "=r"(raw.z), "=r"(raw.w)
-        : "l"(p));
-    const T *e = reinterpret_cast<const T *>(&raw);
-#pragma unroll
-    for (int i = 0; i < VW; ++i) out[i] = cvt<TA>(e[i]);
-  } else {
-    load_vec<T, VW, TA>(p, out);
-  }
-}
-
 // Same, through the coherent path (data written earlier in the same kernel or by atomics).
 template <typename T, int VW, typename TA>
 __device__ __forceinline__ void load_vec_coherent(const T *p, TA (&out)[VW]) {

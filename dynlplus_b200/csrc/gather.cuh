@@ -94,10 +94,12 @@ __device__ __forceinline__ uint64_t l2_evict_last() {
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
-// Row loads of the gathers bypass L1 allocation (L1::no_allocate): a neighbour's row is rarely read
-// again from L1 (random neighbours), and not allocating them left L1 to the accesses that reuse it:
-// the 8-column SpMM at n = 1M, degree 10 went from 86.7 to 80.2 us, the PCG iteration on it from 132
-// to 124 us.
+// The whole-row loads of the gathers (one lane reads a neighbour's entire row) bypass L1 allocation
+// (L1::no_allocate): such a row is rarely read again from L1 (random neighbours), and not allocating
+// them left L1 to the accesses that reuse it: the 8-column SpMM at n = 1M, degree 10 went from 86.7
+// to 80.2 us, the PCG iteration on it from 132 to 124 us. The 16-byte vector gathers of wide rows
+// (several lanes per row) keep allocating: without it the k = 32 serving stream measured slower
+// (622.6 k against 637.1 k edge-updates/s, update p50 215 against 188 ms).
 __device__ __forceinline__ bool load_row12(const float *__restrict__ xr, float (&raw)[3][4]) {
   const bool hi = ((uintptr_t)xr & 16u) != 0;
   const float *p8 = xr + (hi ? 4 : 0);
@@ -335,7 +337,7 @@ __device__ __forceinline__ void gather_row(const int32_t *__restrict__ col, cons
         for (int k = 0; k < VPL; ++k) {
           const int vi = cl + k * LV;
           if (v[u] >= 0 && vi < NV) {
-            load_vec_gather<TX, VW, TA>(xr + (long long)vi * VW, t[u][k]);
+            load_vec<TX, VW, TA>(xr + (long long)vi * VW, t[u][k]);
           } else {
 #pragma unroll
             for (int i = 0; i < VW; ++i) t[u][k][i] = TA(0);
