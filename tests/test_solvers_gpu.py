@@ -523,3 +523,47 @@ def test_coalesced_batches_then_one_solve():
         F = solver.Z[:, :K].cpu().numpy()[U]
         rel = O.relres(ref["W"], ref["diag"], F, ref["rhs"])
         assert rel <= 1e-6 and st.relres <= 1e-6, (rnd, rel, st.relres)
+
+
+@pytest.mark.parametrize("C", [5, 6, 8])
+def test_row_sweep_keeps_padding_and_follows_column_sweep(C):
+    """The two-kernel iteration's sweep takes one row per thread where R, Z, P and AP all have
+    32-byte rows of at most 8 floats (k_pcg_fused_rows8), else one (row, column) element per thread.
+    Through the C ABI with every buffer on an 8-float pitch (padding columns of R and Z holding a
+    sentinel) against the same solve with Z on a 12-float pitch (the element sweep): the sentinels
+    stay, the scores agree to fp32 rounding, the iteration counts within one, and both meet the
+    relative-residual target on the fp64 residual."""
+    from dynlplus_b200 import _lib
+    from dynlplus_b200.backend import code, ld, ptr, stream, workspace
+    import ctypes as ct
+    S, A, diag, rhs = _whole_row_system(C, seed=11)
+    n = A.shape[0]
+    W = S.W
+    d32 = S.diag.to(torch.float32).contiguous()
+    b32 = S.rhs.to(torch.float32).contiguous()
+    rn = (ct.c_double * C)(*[float(x) for x in np.linalg.norm(rhs, axis=0)])
+    out = []
+    for ldz in (8, 12):
+        Rb = torch.full((n, 8), -7.0, dtype=torch.float32, device="cuda")
+        Zb = torch.full((n, ldz), -7.0, dtype=torch.float32, device="cuda")
+        Zb[:, :C] = 0.0
+        P = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+        AP = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+        R, Z = Rb[:, :C], Zb[:, :C]
+        ws = workspace("pcg_test").get(_lib.lib().dlp_pcg_workspace_bytes(C))
+        it, viol, rel, status = ct.c_int32(0), ct.c_double(0), ct.c_double(0), ct.c_int32(0)
+        _lib.call("dlp_pcg", ptr(W.rbeg), ptr(W.rend), ptr(W.indices), ptr(W.data), code(W.data), n, C, ptr(d32),
+                  ptr(b32), ld(b32), ptr(Z), ld(Z), ptr(R), ld(R), ptr(P), ld(P), ptr(AP), ld(AP), code(Z), None, rn,
+                  1e-5, 2 | 4, 10_000, 400, 8, 1, W.nnz / n, ptr(ws), ws.numel(), ct.byref(it), ct.byref(viol),
+                  ct.byref(rel), ct.byref(status), stream(), None, None, 0)
+        torch.cuda.synchronize()
+        assert status.value == 5, status.value
+        assert (Zb[:, C:] == -7.0).all() and (Rb[:, C:] == -7.0).all()
+        out.append((Z.double().cpu().numpy(), it.value))
+    (Zr, itr), (Ze, ite) = out
+    assert abs(itr - ite) <= 1, (itr, ite)
+    Ad = ssp.diags(diag) - A
+    for Zx in (Zr, Ze):
+        relv = np.linalg.norm(rhs - Ad @ Zx, axis=0) / np.linalg.norm(rhs, axis=0)
+        assert relv.max() <= 1e-5 * 1.01, relv.max()
+    np.testing.assert_allclose(Zr, Ze, rtol=0, atol=2e-5 * np.abs(Ze).max())
