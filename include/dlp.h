@@ -267,6 +267,9 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
  * (the call returns DLP_ERR_CAP), 4 breakdown (a non-finite residual entry), 6 cancelled (returns
  * DLP_ERR_CANCELLED); the outputs are filled in every case. eps may be NULL when bit 0 is unused.
  * (dtype, w_dtype) in {(f32,f32), (f64,f64), (f64,f32)}. Workspace: dlp_pcg_workspace_bytes(C).
+ * The control block and per-column constants go up in one copy from a pinned host buffer of a few
+ * KB kept per host thread and device (allocated on the first call); the control block comes back
+ * through pinned memory.
  * Mixed precision (fp32 only): with w_lo (bf16 copy of w) and P_lo (a bf16 n x C buffer, ld_lo) the
  * SpMM gathers the bf16 mirror of P that the direction update keeps (fp32 accumulation), while the
  * diagonal term, pAp and every vector update stay fp32; NULL for both = full-precision gathers. */
