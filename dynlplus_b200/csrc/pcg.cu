@@ -1042,6 +1042,74 @@ __global__ void __launch_bounds__(kSweepThreads)
   }
 }
 
+// The same statistics for fp64 residuals of at most 10 columns whose rows are whole 16-byte aligned
+// runs of 10 doubles (ld >= 10): one thread per row, the row read in three loads (load_row10d) and
+// the diagonal's reciprocal taken once per row (|R| times the correctly rounded reciprocal is
+// within 2 ulp of the quotient); rhs per column (its whole rows cost the kernel a spill).
+// Per-thread column sums in order, then a fixed xor tree over the warp and the warps in order,
+// written in k_resid_stats's partials layout for k_resid_stats_final.
+__global__ void __launch_bounds__(kSweepThreads, 2)
+    k_resid_stats_rows10(int32_t n, int32_t C, const double *__restrict__ R, int64_t ldr,
+                         const double *__restrict__ rhs, int64_t ldrhs, const double *__restrict__ diag,
+                         const double *__restrict__ H, int64_t ldh, double *part) {
+  double mx[10], rr[10], bb[10];
+#pragma unroll
+  for (int c = 0; c < 10; ++c) mx[c] = rr[c] = bb[c] = 0.0;
+  double hm = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+    double raw[5][2];
+    const bool hi = load_row10d(R + r * ldr, raw);
+    const double dinv = __drcp_rn(diag[r]);
+#pragma unroll
+    for (int c = 0; c < 10; ++c) {
+      if (c < C) {
+        const double x = row10_col(raw, hi, c);
+        mx[c] = fmax(mx[c], fabs(x) * dinv);
+        rr[c] = fma(x, x, rr[c]);
+      }
+    }
+    if (rhs) {
+#pragma unroll
+      for (int c = 0; c < 10; ++c)
+        if (c < C) {
+          const double b = rhs[r * ldrhs + c];
+          bb[c] = fma(b, b, bb[c]);
+        }
+    }
+    if (H) hm = fmax(hm, fabs(H[r * ldh]));
+  }
+  __shared__ double s_w[kSweepThreads / 32][31];
+  const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  const int NO = 3 * C + 1;
+#pragma unroll
+  for (int c = 0; c < 10; ++c) {
+    double a = mx[c], b = rr[c], e = bb[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, off));
+      b += __shfl_xor_sync(0xffffffffu, b, off);
+      e += __shfl_xor_sync(0xffffffffu, e, off);
+    }
+    if (lane == 0 && c < C) {
+      s_w[wid][c] = a;
+      s_w[wid][C + c] = b;
+      s_w[wid][2 * C + c] = e;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) hm = fmax(hm, __shfl_xor_sync(0xffffffffu, hm, off));
+  if (lane == 0) s_w[wid][3 * C] = hm;
+  __syncthreads();
+  for (int o = tid; o < NO; o += blockDim.x) {
+    const bool is_max = o < C || o == 3 * C;
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < kSweepThreads / 32; ++w) v = is_max ? fmax(v, s_w[w][o]) : v + s_w[w][o];
+    part[(long long)blockIdx.x * NO + o] = v;
+  }
+}
+
 __global__ void k_resid_stats_final(int32_t C, int nb, const double *__restrict__ part, double *out) {
   const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int NO = 3 * C + 1;
@@ -1553,14 +1621,24 @@ int dlp_residual_stats(int32_t n, int32_t C, const void *R, int64_t ldr, const v
   static const int per64 = resident_per_sm(k_resid_stats<double>, kSweepThreads);
   const int nb = sm_count() * (dtype == DLP_F32 ? per32 : per64);  // one wave, <= upd_blocks()
   double *part = (double *)ws;
-  if (dtype == DLP_F32)
+  auto rows10 = [](const void *a, int64_t lda) { return (uintptr_t)a % 16 == 0 && lda >= 10 && lda % 2 == 0; };
+  int nbu = nb;
+  if (dtype == DLP_F64 && C <= 10 && rows10(R, ldr)) {
+    // whole fp64 rows, one per thread (the decision rests on R alone, so calls with and without rhs
+    // sum R in the same order)
+    static const int per_rows = resident_per_sm(k_resid_stats_rows10, kSweepThreads);
+    nbu = std::min(sm_count() * per_rows, nb);
+    k_resid_stats_rows10<<<nbu, kSweepThreads, 0, s>>>(n, C, (const double *)R, ldr, (const double *)rhs, ldrhs,
+                                                        (const double *)diag, (const double *)H, ldh, part);
+  } else if (dtype == DLP_F32) {
     k_resid_stats<float><<<nb, kSweepThreads, 0, s>>>(n, C, (const float *)R, ldr, (const float *)rhs, ldrhs,
                                                        (const float *)diag, (const float *)H, ldh, part);
-  else
+  } else {
     k_resid_stats<double><<<nb, kSweepThreads, 0, s>>>(n, C, (const double *)R, ldr, (const double *)rhs, ldrhs,
                                                         (const double *)diag, (const double *)H, ldh, part);
+  }
   const int NO = 3 * C + 1;
-  k_resid_stats_final<<<(NO + 7) / 8, 256, 0, s>>>(C, nb, part, out);
+  k_resid_stats_final<<<(NO + 7) / 8, 256, 0, s>>>(C, nbu, part, out);
   return check_launch(2);
 }
 
