@@ -409,9 +409,13 @@ def ours(a):
     ds = graphs.er_graph(a.n, a.deg, a.k, seed=seed)
     lab = graphs.label_mask(a.n, a.label_frac, seed=seed)
     es = stream.EdgeStream(ds, lab, components=True)  # component ids after every batch (side stream)
-    solver = solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres,
-                                   full_every=16, lowp=a.lowp, class_sum=False if a.no_class_sum else "auto",
-                                   refine_share=a.refine_share)
+
+    def make_solver():
+        return solvers.IncrementalLP(a.n, a.k, "float32", tol=a.tol, method="pcg", target_relres=a.target_relres,
+                                     full_every=16, lowp=a.lowp, class_sum=False if a.no_class_sum else "auto",
+                                     refine_share=a.refine_share)
+
+    solver = make_solver()
     solver.solve(es.system)  # the static solve of the initial graph (untimed)
     A0 = ds.A.to_scipy() if (rank == 0 and not a.no_cpu_baseline) else None
     Z0 = solver.Z.cpu().numpy() if A0 is not None else None
@@ -468,11 +472,11 @@ def ours(a):
 
     fstar = {}
 
-    def check_fp64(S):
-        """Outside the timed region: the scores against an fp64 solve of the same system (fp64 block
-        PCG to a relative residual of 1e-11, started from the previous batch's fp64 solution): the
-        score error relative to the largest score, label agreement and near-ties (rows whose two
-        best fp64 scores differ by at most twice the score error)."""
+    def check_fp64(S, solver):
+        """The solver's scores for system S against an fp64 solve of S (fp64 block PCG to a relative
+        residual of 1e-11, started from the previous batch's fp64 solution): the score error relative
+        to the largest score, label agreement and near-ties (rows whose two best fp64 scores differ
+        by at most twice the score error)."""
         S64 = S.astype(torch.float64)
         C = solver.C
         Zs = fstar.get("Z")
@@ -499,7 +503,6 @@ def ours(a):
         return {"err": err / scale, "agree": float(1.0 - bad.double().mean()), "near_ties": int(tie.sum()),
                 "mismatch_outside_ties": int((bad & ~tie).sum()), "fp64_iters": st.iters, "fp64_relres": st.relres}
 
-    check_stream = torch.cuda.Stream(device=dev)
     dev_batches = [to_dev(b) for b in batches[a.warmup: a.warmup + a.steps]]
     host_batches = [to_pinned(b) for b in batches[a.warmup + a.steps:]]
     # the clock sampler starts before the warm-up, so the timed steps follow the last warm-up step
@@ -533,16 +536,6 @@ def ours(a):
         e.record()
         e.synchronize()
         times.append(s.elapsed_time(e))
-        if rank == 0 and not a.no_fp64_check:  # between timed steps, outside the timed region
-            c_before = _lib.lib().dlp_launch_count()
-            # on a stream of its own: its PCG workspace, scratch and loop graphs stay apart from the
-            # timed solver's (a shared workspace regrown by the larger fp64 solve would make the next
-            # timed step capture its loop graphs again)
-            check_stream.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(check_stream):
-                checks.append(check_fp64(es.system))
-            torch.cuda.current_stream().wait_stream(check_stream)
-            launches0 += _lib.lib().dlp_launch_count() - c_before
         relres.append(st.relres)
         paths.append(st.path)
         iters.append(st.iters)
@@ -570,6 +563,23 @@ def ours(a):
     gc.enable()
     cc_last = res[1:3] if res is not None else None
     clk = clocks.stop() if clocks else None
+    if rank == 0 and not a.no_fp64_check:
+        # after the timed loops (nothing runs between timed steps): a second resident stream and
+        # solver replay the warm-up and timed batches, and each timed batch's scores are checked
+        # against an fp64 solve of its system, on a stream of their own
+        check_stream = torch.cuda.Stream(device=dev)
+        with torch.cuda.stream(check_stream):
+            es_r, solver_r = stream.EdgeStream(ds, lab, components=True), make_solver()
+            solver_r.solve(es_r.system)
+            for i, b in enumerate(batches[: a.warmup + a.steps]):
+                S = es_r.apply_edges(**to_dev(b))
+                solver_r.solve(S)
+                solver_r.relabel(S)
+                es_r.join_components()
+                if i >= a.warmup:
+                    checks.append(check_fp64(es_r.system, solver_r))
+        torch.cuda.synchronize()
+        del es_r, solver_r
     t_dev, t_e2e, value, e2e = aggregate_replicas(times, e2e_times, a.batch, world, dev)
     roof = None
     if rank == 0:
@@ -609,6 +619,8 @@ def ours(a):
                                     "near_ties_max": max(c["near_ties"] for c in checks),
                                     "mismatch_outside_near_ties": sum(c["mismatch_outside_ties"] for c in checks),
                                     "batches": len(checks),
+                                    "replay": "a second resident stream and solver over the warm-up and timed "
+                                              "batches, after the timed loops",
                                     "reference": "fp64 block Jacobi-PCG of the same system to rel-res 1e-11"}
                                    if checks else None),
                 "components": {"n_comp": cc_last[0], "label_free_vertices": cc_last[1] - es.system.n_solved}
