@@ -373,7 +373,10 @@ def pcg_roofline(events, nnz, peaks, traffic_file, steady=None):
         tr = json.load(open(traffic_file))
         if tr.get("n") == n and tr.get("C") == C and ("k_pcg_fused" in tr.get("per_kernel", {})) == solvers.TWO_KERNEL:
             traffic, tsrc = tr.get("dram_bytes_per_iteration"), tr.get("source")
-    ks = "k_pcg_apply + k_pcg_fused" if solvers.TWO_KERNEL else "k_pcg_apply + k_pcg_update + k_pcg_dir"
+    # the sweep is one row per thread (k_pcg_fused_rows8) for rows of at most 8 floats on a 32-byte
+    # pitch, else one element per thread (k_pcg_fused)
+    sweep = "k_pcg_fused_rows8" if C <= 8 else "k_pcg_fused"
+    ks = "k_pcg_apply + " + sweep if solvers.TWO_KERNEL else "k_pcg_apply + k_pcg_update + k_pcg_dir"
     return {"bound": "hbm", "kernel": "PCG iteration: %s (fp32, C=%d, compact CSR of W_UU, nnz=%d)" % (ks, C, nnz),
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback",
