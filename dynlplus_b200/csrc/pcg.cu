@@ -886,6 +886,87 @@ __global__ void __launch_bounds__(kSweepThreads, kRowSweepBlocks)
     finish_sweep(0, C, B, true);
 }
 
+// The zero start of the two-kernel iteration on rows of at most 8 floats on a 32-byte pitch
+// (k_pcg_update phase 3 and k_pcg_dir mode 4 in one sweep): R = rhs, Z = 0, P = R / diag, and rz,
+// ||R||^2 and the violation of R with the first stop decision (finish_sweep phase 3). One thread per
+// row, whole-row accesses; the padding columns of R and Z are written back as read (read only when
+// there are any), those of P as zeros. Same arithmetic per element as the two kernels it replaces.
+__global__ void __launch_bounds__(kSweepThreads, kRowSweepBlocks)
+    k_pcg_start_rows8(int32_t n, int32_t C, const float *__restrict__ rhs, int64_t ldrhs, float *R, int64_t ldr,
+                      float *Z, int64_t ldz, float *P, int64_t ldp, const float *__restrict__ diag, PcgBufs B) {
+  PcgCtl *ctl = B.ctl;
+  __shared__ double s_w[kSweepThreads / 32][16];
+  __shared__ double s_v[kSweepThreads / 32];
+  double rz[8], ss[8], rmax[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) rz[c] = ss[c] = rmax[c] = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const uint64_t pf = l2_evict_first_pol(), pl = l2_evict_last();
+  const bool pad = C < 8;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+    float bv[8], rv[8], zv[8], pv[8];
+    ld_row8(rhs + r * ldrhs, bv, pf);
+    if (pad) {
+      ld_row8(R + r * ldr, rv, pf);
+      ld_row8(Z + r * ldz, zv, pf);
+    }
+    const double dinv = __drcp_rn((double)diag[r]);  // correctly rounded: the value of 1.0 / d
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (c < C) {
+        rv[c] = bv[c];
+        zv[c] = 0.f;
+        const double r64 = (double)bv[c];
+        pv[c] = (float)(r64 * dinv);  // the fp32 quotient R / diag (as in k_pcg_fused)
+        const double r2 = r64 * r64;
+        rz[c] += r2 * dinv;
+        ss[c] += r2;
+        rmax[c] = fmax(rmax[c], fabs(r64) * dinv);
+      } else {
+        pv[c] = 0.f;
+      }
+    }
+    st_row8(R + r * ldr, rv, pf);
+    st_row8(Z + r * ldz, zv, pf);
+    st_row8(P + r * ldp, pv, pl);
+  }
+  double vmax = 0.0;
+  bool bad = false;
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    if (c < C) {
+      vmax = fmax(vmax, rmax[c] * B.epsinv[c]);
+      bad = bad || !isfinite(ss[c]);
+    }
+  if (bad) ctl->bad = 1;
+  const int tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  double v16[16];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    v16[c] = rz[c];
+    v16[8 + c] = ss[c];
+  }
+  const double mine = warp_scatter16(v16, lane);
+  if ((lane & 1) == 0) s_w[wid][lane >> 1] = mine;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+  if (lane == 0) s_v[wid] = vmax;
+  __syncthreads();
+  if (tid < 16) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kSweepThreads / 32; ++w) t += s_w[w][tid];
+    const int c = tid & 7;
+    if (c < C) B.part2[(long long)((tid < 8 ? 0 : C) + c) * B.nbmax + blockIdx.x] = t;
+  } else if (tid == 32) {
+    double v = 0.0;
+    for (int w = 0; w < kSweepThreads / 32; ++w) v = fmax(v, s_v[w]);
+    B.part2[(long long)(2 * C) * B.nbmax + blockIdx.x] = v;
+  }
+  if (last_block_grouped<kSweepThreads>(B.part2, B.nbmax, 2 * C + 1, 2 * C, ctl->gcnt2, &ctl->cnt2, B.gpart2))
+    finish_sweep(3, C, B, false);
+}
+
 // K3: Z += alpha P; P = R/diag + beta P
 //   mode 0: both (skipping the P update when a stop was proposed)   mode 1: P update only
 //   mode 2: P = R/diag      mode 4: P = R/diag and Z = 0 (a zero start)
@@ -1306,6 +1387,20 @@ static int dir_phase(int mode, const PcgProblem &q, const PcgBufs &B, cudaStream
   return q.dtype == DLP_F32 ? launch_dir<float>(mode, q, B, s) : launch_dir<double>(mode, q, B, s);
 }
 
+// The zero start: R = rhs with its reductions and the first decision, then Z = 0 and P = R / diag;
+// one row sweep where the rows allow it (k_pcg_start_rows8), else the two element sweeps.
+static int zero_start(const PcgProblem &q, const PcgBufs &B, cudaStream_t s) {
+  if (q.rows8 && (uintptr_t)q.rhs % 32 == 0 && q.ldrhs % 8 == 0) {
+    static const int per = resident_per_sm(k_pcg_start_rows8, kSweepThreads);
+    k_pcg_start_rows8<<<sm_count() * per, kSweepThreads, 0, s>>>(q.n, q.C, (const float *)q.rhs, q.ldrhs,
+                                                                 (float *)q.R, q.ldr, (float *)q.Z, q.ldz,
+                                                                 (float *)q.P, q.ldp, (const float *)q.diag, B);
+    return check_launch();
+  }
+  DLP_TRY(update_from_rhs(q, B, s));
+  return dir_phase(4, q, B, s);
+}
+
 // Graph cache: one instantiated chunk of `k` iterations per problem signature.
 struct GraphKey {
   std::vector<uintptr_t> v;
@@ -1541,8 +1636,7 @@ int dlp_pcg(const int32_t *rbeg, const int32_t *rend, const int32_t *col, const 
   // R = rhs - A Z, best = violation, rz = R.(R/diag), P = R/diag; a zero start takes R = rhs in the
   // update sweep itself and sets Z = 0 in the direction sweep (no SpMM, no separate copy)
   if (mode & 4) {
-    DLP_TRY(update_from_rhs(q, B, s));
-    DLP_TRY(dir_phase(4, q, B, s));
+    DLP_TRY(zero_start(q, B, s));
   } else {
     DLP_TRY(true_residual(q, s));
     DLP_TRY(update_phase(2, q, B, s));
