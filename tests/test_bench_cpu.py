@@ -12,6 +12,20 @@ import bench
 def test_pcg_iteration_bytes_at_the_headline_size():
     # n = 1M rows, 9,901,056 entries of the compact W_UU, C = 9 fp32 columns: 735.6 MB
     assert bench.pcg_iteration_bytes(1_000_000, 9_901_056, 9) == 735_646_468
+    # the class-sum corrections' 8 columns on the bench's compact W_UU (9,901,194 entries): 664.0 MB
+    assert bench.pcg_iteration_bytes(1_000_000, 9_901_194, 8) == 664_047_764
+    # the model's pieces: row pointers, per entry (index, weight, gathered row), AP, diag, own row,
+    # the six vector passes and the diagonal of the sweep
+    n, nnz, C, s = 1_000_000, 9_901_194, 8, 4
+    assert bench.pcg_iteration_bytes(n, nnz, C) == (4 * (n + 1) + nnz * (4 + s + C * s) + n * C * s + n * s
+                                                    + n * C * s + 6 * n * C * s + n * s)
+
+
+def test_refine_share_reaches_the_solver():
+    from dynlplus_b200 import solvers
+    assert solvers.IncrementalLP(10, 4, "float32", refine_share=0.35).refine_share == 0.35
+    assert solvers.IncrementalLP(10, 4, "float32").refine_share == 0.2
+    assert bench.parse([]).refine_share == 0.2
 
 
 def test_traffic_file_is_consistent():
